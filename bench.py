@@ -1,0 +1,381 @@
+"""Benchmark: the join + high-cardinality GROUP BY + top-10 workload on B200.
+
+Workload (one step = one full query): dimension 1,500,000 rows (key i64), fact
+60,000,000 rows (fk i64, d i32, v f64); WHERE d > 1200, JOIN fk = key, GROUP BY fk
+with SUM(v) and COUNT(*), ORDER BY SUM(v) DESC, fk LIMIT 10.  Seeded synthetic data.
+
+* value   rows/s of the fact table with the tables already resident in HBM
+          (join build + fused filter/probe/aggregate + top-N, per step)
+* e2e     the same query through the C ABI with pinned host buffers: the host->device
+          copy of both tables and the device->host read of the 10 result rows are inside
+          every step (morsels pushed from several host threads, one stream each)
+* roofline  the fused pipeline-aggregate kernel: algorithmic bytes (20 B per fact
+          row: fk 8 + d 4 + v 8) / its CUDA-event time, vs the measured HBM copy peak
+* cpu_baseline  the CPU oracle (a C++ restatement of MiniLake's engine) on this
+          host's cores, the full workload
+
+Multi-GPU (torchrun, N ranks): weak scaling; rank r owns a 60M-row fact shard whose
+fk values are the keys with key % N == r (a fact table partitioned on the join key),
+the dimension table is replicated, every rank aggregates its disjoint groups and
+keeps its top-10; the exchange step gathers the N top-10 candidate lists to rank 0,
+which merges them (the top-10 of disjoint groups is within the union of the local
+top-10s).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FACT_ROWS = 60_000_000
+DIM_ROWS = 1_500_000
+ROW_GROUPS = 128
+BYTES_PER_ROW = 20  # fk 8 + d 4 + v 8 (the kernel's algorithmic bytes)
+METRIC = "rows/s & HBM GB/s per op; learned vs plain sizing on B200; p50/p99 latency"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_data(rank: int, world: int):
+    """Dimension table (replicated) and this rank's fact shard, as flat arrays."""
+    rng = np.random.Generator(np.random.PCG64(43))
+    key = (rng.permutation(DIM_ROWS) + 1).astype(np.int64)
+    frng = np.random.Generator(np.random.PCG64(43 + 1000 * rank))
+    # rank r's fact rows reference the keys k in 1..DIM_ROWS with k % world == r
+    first = rank if rank > 0 else world
+    count = (DIM_ROWS - first) // world + 1
+    fk = first + frng.integers(0, count, FACT_ROWS, dtype=np.int64) * world
+    d = frng.integers(0, 2557, FACT_ROWS, dtype=np.int32)
+    v = frng.uniform(900.0, 105000.0, FACT_ROWS)
+    return key, fk, d, v
+
+
+def clocks_sampler():
+    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+           "--format=csv,noheader,nounits", "-lms", "200"]
+    try:
+        return subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return None
+
+
+def clocks_summary(proc, device_index: int):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        out, _ = proc.communicate(timeout=5)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        out, _ = proc.communicate()
+    sm, mx, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in out.strip().splitlines():
+        p = [x.strip() for x in line.split(",")]
+        if len(p) < 9 or p[0] != str(device_index):
+            continue
+        try:
+            sm.append(float(p[1]))
+            mx = max(mx, float(p[2]))
+        except ValueError:
+            continue
+        for n, flag in zip(names, p[5:9]):
+            if flag.lower() == "active":
+                reasons.add(n)
+    if not sm:
+        return None
+    return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the aggregate kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "pipeline_aggregate_join_groupby.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch_full_size")
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------------------------
+class GpuQuery:
+    def __init__(self, ctx, key, fk, d, v):
+        from minilake_b200 import abi
+        from minilake_b200.columns import fixed
+        self.ctx = ctx
+        self.abi = abi
+        self.dim_cols = [fixed(abi.INT64, key)]
+        self.fact_cols = [fixed(abi.INT64, fk), fixed(abi.INT32, d), fixed(abi.FLOAT64, v)]
+        self.dim_dev = ctx.upload(self.dim_cols)
+        self.fact_dev = ctx.upload(self.fact_cols)
+
+    def run(self, dim_source, fact_sources, threads=1, size_hint=1_500_000):
+        """One query; fact_sources: list of morsels (DeviceBatch or host column lists)."""
+        from minilake_b200 import workloads
+        from minilake_b200.engine import GpuEngine
+        eng = GpuEngine(self.ctx, threads=threads)
+        j = workloads.join_groupby_build(eng, [dim_source] if not isinstance(dim_source, list) else dim_source)
+        prologue, group, aggs = workloads.join_groupby_plan(j.handle)
+        agg = eng.hashagg(fact_sources, [self.abi.INT64, self.abi.INT32, self.abi.FLOAT64], group, aggs, prologue,
+                          size_hint=size_hint)
+        res = eng.topn(agg, workloads.JG_OUT_TYPES, workloads.join_groupby_topn_keys(), 10)
+        out = res.fetch()
+        j.close()
+        return out
+
+
+def pinned_like(a: np.ndarray):
+    import torch
+    t = torch.empty(a.shape, dtype={np.int64: torch.int64, np.int32: torch.int32,
+                                    np.float64: torch.float64}[a.dtype.type], pin_memory=True)
+    arr = t.numpy()
+    arr[...] = a
+    return arr, t
+
+
+def gpu_arm(args):
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from minilake_b200.columns import fixed
+    from minilake_b200.gpu import PROFILE, Context
+    key, fk, d, v = make_data(rank, world)
+    ctx = Context(local, flags=PROFILE)
+    q = GpuQuery(ctx, key, fk, d, v)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # ---- value: HBM-resident tables, one launch over the whole fact table -------------
+    for _ in range(args.warmup):
+        q.run(q.dim_dev, [q.fact_dev])
+    ctx.profile("pipeline_aggregate", reset=True)
+    l0 = ctx.kernel_launches()
+    clk = clocks_sampler() if rank == 0 else None
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    top = None
+    for _ in range(args.steps):
+        top = q.run(q.dim_dev, [q.fact_dev])
+    e1.record()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clocks = clocks_summary(clk, local) if rank == 0 else None
+    launches = ctx.kernel_launches() - l0
+    n_agg, agg_ms = ctx.profile("pipeline_aggregate", reset=True)
+    ms_t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+
+    # ---- e2e: pinned host tables; copies inside every step ---------------------------
+    pinned, keep = [], []
+    for a in (fk, d, v):
+        p, t = pinned_like(a)
+        pinned.append(p)
+        keep.append(t)
+    pkey, tkey = pinned_like(key)
+    keep.append(tkey)
+    from minilake_b200 import abi
+    nmorsel = 16
+    bounds = np.linspace(0, FACT_ROWS, nmorsel + 1).astype(np.int64)
+    morsels = [[fixed(abi.INT64, pinned[0][bounds[i]:bounds[i + 1]]), fixed(abi.INT32, pinned[1][bounds[i]:bounds[i + 1]]),
+                fixed(abi.FLOAT64, pinned[2][bounds[i]:bounds[i + 1]])] for i in range(nmorsel)]
+    dim_host = [fixed(abi.INT64, pkey)]
+    for _ in range(max(1, args.warmup // 2)):
+        q.run(dim_host, morsels, threads=4)
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(args.steps):
+        top_e2e = q.run(dim_host, morsels, threads=4)
+    f1.record()
+    barrier()
+    e2e_ms = f0.elapsed_time(f1)
+    et = torch.tensor([e2e_ms], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(et, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = float(et.item())
+    assert np.array_equal(top_e2e[0].values, top[0].values), "e2e and HBM-resident results differ"
+
+    # ---- exchange: gather the per-rank top-10 candidates, merge on rank 0 -------------
+    if world > 1:
+        cand = np.stack([top[0].values.astype(np.float64), top[1].values, top[2].values.astype(np.float64)], 1)
+        ct = torch.tensor(cand, device="cuda", dtype=torch.float64)
+        allc = [torch.zeros_like(ct) for _ in range(world)]
+        torch.distributed.all_gather(allc, ct)
+        if rank == 0:
+            merged = np.concatenate([c.cpu().numpy() for c in allc])
+            order = np.lexsort((merged[:, 0], -merged[:, 1]))[:10]
+            log("merged top-10 fk:", merged[order, 0].astype(np.int64).tolist())
+
+    if rank == 0:
+        rows_total = FACT_ROWS * world
+        value = rows_total / (ms_max / 1e3 / args.steps)
+        e2e = rows_total / (e2e_ms / 1e3 / args.steps)
+        peak, peak_kind = measured_peak()
+        per_launch_ms = agg_ms / max(n_agg, 1)
+        achieved = FACT_ROWS * BYTES_PER_ROW / (per_launch_ms / 1e3) / 1e9
+        cpu = cpu_baseline(key, fk, d, v) if world == 1 and not args.skip_cpu else None
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "rows/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded numpy PCG64; BASELINE shapes)",
+            "config": {"workload": "join + high-cardinality GROUP BY + top-10: dim 1.5M rows (key i64), "
+                                   "fact 60M rows per GPU (fk i64, d i32, v f64), d > 1200, GROUP BY fk, "
+                                   "SUM(v), COUNT(*), ORDER BY SUM(v) DESC, fk LIMIT 10",
+                       "fact_rows_per_gpu": FACT_ROWS, "dim_rows": DIM_ROWS,
+                       "l2": "inputs larger than L2 (1.2 GB fact table per step)",
+                       "parallelism": f"weak, fact partitioned on the join key over {world} GPU(s)"},
+            "e2e": {"value": e2e, "unit": "rows/s",
+                    "h2d_bytes_per_step": int(FACT_ROWS * BYTES_PER_ROW + DIM_ROWS * 8),
+                    "d2h_bytes_per_step": int(10 * 24),
+                    "ms_per_step": e2e_ms / args.steps},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "kernel": "k_agg (fused filter + join probe + hash aggregate)",
+                         "kernel_ms_per_launch": per_launch_ms,
+                         "algorithmic_bytes_per_launch": FACT_ROWS * BYTES_PER_ROW,
+                         "traffic": profiled_traffic()},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "top10_fk": [int(x) for x in top[0].values],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    ctx.close()
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU baseline / reference arm: the oracle (C++ restatement of MiniLake's engine)
+# ---------------------------------------------------------------------------------------------
+def oracle_tables(key, fk, d, v):
+    from minilake_b200 import abi
+    from minilake_b200.columns import Table, fixed
+    dim = Table("dim", ["key"], [[fixed(abi.INT64, c)] for c in np.array_split(key, 4)])
+    idx = np.linspace(0, len(fk), ROW_GROUPS + 1).astype(np.int64)
+    fact = Table("fact", ["fk", "d", "v"],
+                 [[fixed(abi.INT64, fk[idx[i]:idx[i + 1]]), fixed(abi.INT32, d[idx[i]:idx[i + 1]]),
+                   fixed(abi.FLOAT64, v[idx[i]:idx[i + 1]])] for i in range(ROW_GROUPS)])
+    return dim, fact
+
+
+def oracle_step(eng, dim, fact):
+    from minilake_b200 import workloads
+    return workloads.run_join_groupby(eng, dim, fact)
+
+
+def cpu_baseline(key, fk, d, v, runs=3):
+    from oracle import orc
+    threads = os.cpu_count() or 1
+    dim, fact = oracle_tables(key, fk, d, v)
+    eng = orc.OracleEngine(threads=threads)
+    oracle_step(eng, dim, fact)
+    times = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        oracle_step(eng, dim, fact)
+        times.append(time.perf_counter() - t0)
+    med = float(np.median(times))
+    return {"value": len(fk) / med, "unit": "rows/s", "cores": threads, "kind": "port",
+            "sample": f"the full workload ({len(fk):,} fact rows), median of {runs} runs after 1 warm-up, "
+                      f"pre-decoded in-memory columns, {threads} threads"}
+
+
+def reference_arm(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import orc
+    key, fk, d, v = make_data(0, 1)
+    dim, fact = oracle_tables(key, fk, d, v)
+    threads = os.cpu_count() or 1
+    eng = orc.OracleEngine(threads=threads)
+    for _ in range(args.warmup):
+        oracle_step(eng, dim, fact)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle_step(eng, dim, fact)
+    dt = time.perf_counter() - t0
+    value = FACT_ROWS / (dt / args.steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded numpy PCG64; BASELINE shapes)",
+        "config": {"workload": "join + high-cardinality GROUP BY + top-10: dim 1.5M rows (key i64), "
+                               "fact 60M rows (fk i64, d i32, v f64), d > 1200, GROUP BY fk, SUM(v), COUNT(*), "
+                               "ORDER BY SUM(v) DESC, fk LIMIT 10",
+                   "engine": "C++ restatement of MiniLake's CPU engine (the Rust reference cannot be built here)"},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
+                         "sample": f"the full workload per step ({FACT_ROWS:,} fact rows), {threads} threads"},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,305 @@
+/*
+ * minilake_gpu.h — C ABI of the B200 (sm_100a) execution core for MiniLake's
+ * data-parallel hot path: filter/projection expressions over selection vectors
+ * and dictionary codes, hash aggregation, hash-join build/probe and top-N.
+ *
+ * The entry points mirror MiniLake's pipeline contract
+ * (crates/minilake-exec/src/pipeline.rs:32-79):
+ *   Operator  { execute(&self, Batch) }            -> ml_gpu_filter / ml_gpu_project /
+ *                                                    ml_gpu_join_probe
+ *   Sink      { create_local, finalize }           -> ml_gpu_{hashagg,join_build,topn}_create /
+ *                                                    *_finalize
+ *   LocalSink { sink(&mut self, Batch), combine }  -> ml_gpu_*_local_create / *_sink /
+ *                                                    *_combine
+ * A sink may be given a "prologue": the streaming operators (Filter,
+ * Projection, HashJoinProbe) that sit between the pipeline's source and the
+ * sink. The sink's kernel then runs the whole pipeline for one morsel in one
+ * pass over HBM, without materializing selection vectors or join pairs.
+ *
+ * Conventions
+ *  - Every function returns an int status (ML_OK == 0). On failure the message
+ *    is available from ml_gpu_last_error() (thread-local). Nothing aborts and
+ *    no kernel traps: device-side failures (hash-table overflow, bounded waits
+ *    that ran out) are reported through a device error word that the host reads.
+ *  - Column buffers are BORROWED for the duration of the call
+ *    (crates/minilake-exec/src/pipeline.rs:109-161 hands each batch to the
+ *    operator by value; the FFI takes (ptr, len) views).  A column may live in
+ *    host memory (it is staged through pinned memory and copied with
+ *    cudaMemcpyAsync) or in device memory (used in place).
+ *  - Handles are owned by the caller and released with the matching *_destroy.
+ *  - All calls are thread-safe.  Each local-sink handle owns a CUDA stream, so
+ *    morsels pushed from different threads run concurrently on the device.
+ */
+#ifndef MINILAKE_GPU_H
+#define MINILAKE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes: crates/minilake-core/src/error.rs:8-48 ------------------ */
+enum {
+    ML_OK = 0,
+    ML_ERR_INVALID = 1,     /* MiniLakeError::Internal / Execution (bad arguments, type errors) */
+    ML_ERR_BUDGET = 2,      /* MiniLakeError::ResourcesExhausted (memory.rs:326-339) */
+    ML_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+    ML_ERR_TIMEOUT = 4,     /* a bounded device-side wait ran out */
+    ML_ERR_UNSUPPORTED = 5, /* MiniLakeError::Unsupported */
+    ML_ERR_INTERNAL = 6
+};
+
+/* ---- data types: crates/minilake-core/src/types.rs:15-28 -------------------- */
+enum {
+    ML_TYPE_BOOL = 0,    /* one byte per value (Vec<bool>) */
+    ML_TYPE_INT32 = 1,
+    ML_TYPE_INT64 = 2,
+    ML_TYPE_FLOAT64 = 3,
+    ML_TYPE_DATE = 4,    /* i32 days since 1970-01-01 */
+    ML_TYPE_UTF8 = 5,
+    ML_TYPE_NULL = 6     /* untyped NULL literal only */
+};
+
+/* ---- string encodings: crates/minilake-core/src/column.rs:126-150 ----------- */
+enum {
+    ML_ENC_PLAIN = 0, /* values (or offsets+bytes for UTF8) */
+    ML_ENC_DICT = 1   /* u32 codes + dictionary (offsets+bytes), ColumnData::Dict */
+};
+
+enum { ML_LOC_HOST = 0, ML_LOC_DEVICE = 1 };
+
+/*
+ * A borrowed column view.  Layout follows minilake-core:
+ *  - fixed width: `data` holds `len` values (bool: u8 0/1, i32, i64, f64, date i32)
+ *  - UTF8 plain: `offsets` has len+1 u32 entries into `data` (bytes), column.rs:14-22
+ *  - UTF8 dict:  `data` holds len u32 codes; the dictionary is `dict_offsets`
+ *    (dict_len+1 u32) + `dict_data` (bytes), column.rs:126-131.  Dictionaries are
+ *    always host memory (they are small: <= 65,536 entries, parquet_reader.rs:173).
+ *  - validity: optional u64 words, bit i = row i is valid, LSB first (bitmap.rs:1-12)
+ */
+typedef struct ml_column {
+    int32_t dtype;
+    int32_t encoding;
+    int32_t location;
+    int32_t _pad;
+    int64_t len;
+    const void* data;
+    const uint32_t* offsets;
+    const uint64_t* validity;
+    int64_t dict_len;
+    const uint32_t* dict_offsets;
+    const uint8_t* dict_data;
+} ml_column;
+
+/* ---- expressions: crates/minilake-exec/src/expr/mod.rs:18-173 --------------- */
+enum { /* BinaryOp, expr/mod.rs:20-47 */
+    ML_BIN_ADD = 0, ML_BIN_SUB, ML_BIN_MUL, ML_BIN_DIV, ML_BIN_MOD,
+    ML_BIN_EQ, ML_BIN_NOTEQ, ML_BIN_LT, ML_BIN_LTEQ, ML_BIN_GT, ML_BIN_GTEQ,
+    ML_BIN_AND, ML_BIN_OR
+};
+
+enum { /* PhysicalExpr variants, expr/mod.rs:109-173 */
+    ML_EXPR_COLUMN = 0,  /* i64 = column index in the input batch */
+    ML_EXPR_LITERAL = 1, /* dtype + i64 / f64 / str */
+    ML_EXPR_BINARY = 2,  /* op = ML_BIN_*, 2 children */
+    ML_EXPR_NOT = 3,     /* 1 child */
+    ML_EXPR_NEGATE = 4,  /* 1 child */
+    ML_EXPR_IS_NULL = 5, /* flag = negated (IS NOT NULL), 1 child */
+    ML_EXPR_LIKE = 6,    /* flag = negated, str = pattern, 1 child */
+    ML_EXPR_IN_LIST = 7, /* flag = negated, child 0 = operand, children 1.. = literals */
+    ML_EXPR_CASE = 8,    /* flag = has ELSE; children: cond0, val0, cond1, val1, ..., [else];
+                            dtype = result type */
+    ML_EXPR_CAST = 9     /* dtype = target type, 1 child */
+};
+
+/*
+ * One node of an expression tree, serialized in prefix order: a node is
+ * followed by its `nchild` subtrees.
+ */
+typedef struct ml_expr_node {
+    int32_t kind;
+    int32_t op;     /* BINARY: ML_BIN_* */
+    int32_t dtype;  /* LITERAL: value type; CAST: target; CASE: result type */
+    int32_t nchild;
+    int32_t flag;   /* negated / has_else */
+    int32_t _pad;
+    int64_t i64;    /* COLUMN: index; LITERAL int/bool/date value */
+    double f64;     /* LITERAL float value */
+    const char* str;/* LITERAL utf8 value / LIKE pattern (not NUL-terminated) */
+    int64_t str_len;
+} ml_expr_node;
+
+/* One expression = pointer to its first node + node count. */
+typedef struct ml_expr {
+    const ml_expr_node* nodes;
+    int32_t nnodes;
+    int32_t dtype; /* the planner's output type for this expression (evaluate_to_column's dt) */
+} ml_expr;
+
+/* ---- aggregates: operators/aggregate/accumulator.rs:25-38 ------------------- */
+enum { ML_AGG_COUNT_STAR = 0, ML_AGG_COUNT, ML_AGG_SUM, ML_AGG_AVG, ML_AGG_MIN, ML_AGG_MAX };
+
+typedef struct ml_agg_spec {  /* AggregateExpr, operators/aggregate/mod.rs:22-31 */
+    int32_t func;
+    int32_t arg_type;   /* type of the argument expression; ignored for COUNT(*) */
+    ml_expr arg;        /* nnodes == 0 for COUNT(*) */
+} ml_agg_spec;
+
+typedef struct ml_sort_key {  /* SortKey, operators/sort.rs:25-32 */
+    ml_expr expr;
+    int32_t asc;
+    int32_t nulls_first;
+} ml_sort_key;
+
+/* ---- streaming operators (the prologue of a fused sink) --------------------- */
+enum { ML_PIPE_FILTER = 0, ML_PIPE_PROJECT = 1, ML_PIPE_PROBE = 2 };
+
+typedef struct ml_join_table ml_join_table; /* finalized JoinBuildSink (JoinTableRef, join.rs:58) */
+
+typedef struct ml_pipe_op {
+    int32_t kind;
+    int32_t nexprs;
+    const ml_expr* exprs;  /* FILTER: 1 predicate; PROJECT: output exprs; PROBE: probe key exprs */
+    ml_join_table* join;   /* PROBE only */
+    int32_t build_is_left; /* PROBE only: output = build columns ++ probe columns (join.rs:252-253) */
+    int32_t _pad;
+} ml_pipe_op;
+
+/* ---- opaque handles ---------------------------------------------------------- */
+typedef struct ml_ctx ml_ctx;
+typedef struct ml_batch ml_batch;          /* device-resident columns (an HBM table or a sink's output) */
+typedef struct ml_hashagg ml_hashagg;      /* HashAggregateSink */
+typedef struct ml_hashagg_local ml_hashagg_local; /* HashAggLocal */
+typedef struct ml_join_build ml_join_build;
+typedef struct ml_join_build_local ml_join_build_local;
+typedef struct ml_topn ml_topn;
+typedef struct ml_topn_local ml_topn_local;
+
+/* ---- context, memory pool, errors -------------------------------------------- */
+/* flags: ML_CTX_PROFILE times the library's main kernels with CUDA events recorded on the
+ * stream each kernel is launched on (read back with ml_gpu_profile_read). */
+enum { ML_CTX_DETERMINISTIC = 1, ML_CTX_PROFILE = 2 };
+
+/* ExecConfig (context.rs:14-34) for one device: hbm_budget_bytes is the query-wide
+ * MemoryPool limit (memory.rs:22-26) applied to device bytes; 0 = unlimited. */
+int ml_gpu_ctx_create(int device, uint64_t hbm_budget_bytes, uint32_t flags, ml_ctx** out);
+int ml_gpu_ctx_destroy(ml_ctx* ctx);
+/* MemoryPool::used / peak / limit (memory.rs:250-263). */
+int ml_gpu_pool_stats(ml_ctx* ctx, uint64_t* used, uint64_t* peak, uint64_t* limit);
+/* Details of the last ML_ERR_BUDGET on this thread: ResourcesExhausted{operator, requested,
+ * used, limit} (error.rs).  `op` receives a NUL-terminated operator name. */
+int ml_gpu_last_budget_error(char* op, size_t op_cap, uint64_t* requested, uint64_t* used,
+                             uint64_t* limit);
+const char* ml_gpu_last_error(void);
+/* Wait for all work issued on the context (every stream). */
+int ml_gpu_ctx_synchronize(ml_ctx* ctx);
+
+/* ---- device-resident batches ------------------------------------------------- */
+/* Copy columns into HBM (pinned staging + cudaMemcpyAsync); the batch is reserved
+ * against the pool like a join build side (join.rs:122-157). */
+int ml_gpu_batch_upload(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64_t nrows,
+                        ml_batch** out);
+int ml_gpu_batch_num_rows(const ml_batch* b, int64_t* nrows);
+int ml_gpu_batch_num_columns(const ml_batch* b, int32_t* ncols);
+/* Device views of the columns (location = ML_LOC_DEVICE), for feeding another operator. */
+int ml_gpu_batch_columns(const ml_batch* b, ml_column* out, int32_t ncols);
+/* dtype and, for UTF8 columns, the number of string bytes (to size fetch buffers). */
+int ml_gpu_batch_column_info(const ml_batch* b, int32_t col, int32_t* dtype, int64_t* str_bytes,
+                             int32_t* has_validity);
+/* Copy one column to caller-allocated host buffers.  `values`: len values (UTF8: str_bytes
+ * bytes); `offsets`: len+1 (UTF8 only); `validity`: ceil(len/64) words or NULL. */
+int ml_gpu_batch_fetch(const ml_batch* b, int32_t col, void* values, uint32_t* offsets,
+                       uint64_t* validity);
+int ml_gpu_batch_destroy(ml_batch* b);
+
+/* ---- Operator: FilterOperator (operators/filter.rs:19-25, expr/eval.rs:167-196) --- */
+/* Rows of the selection (or of 0..n when sel_in is NULL) where `pred` is TRUE, in increasing
+ * order.  sel_out must have room for n (or nsel_in) entries; sel_in/sel_out are host or
+ * device memory as `location` says. */
+int ml_gpu_filter(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32_t ncols,
+                  int64_t nrows, const uint32_t* sel_in, int64_t nsel_in, int32_t location,
+                  uint32_t* sel_out, int64_t* nsel_out);
+
+/* ---- Operator: ProjectionOperator (operators/projection.rs:21-32) -------------- */
+/* Evaluate `expr` over ALL physical rows into a new device column (batch of 1 column). */
+int ml_gpu_project(ml_ctx* ctx, const ml_expr* expr, const ml_column* cols, int32_t ncols,
+                   int64_t nrows, ml_batch** out);
+
+/* ---- kernels/hash.rs:16-23: one hash per active row over the key columns -------- */
+int ml_gpu_hash_columns(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64_t nrows,
+                        const uint32_t* sel, int64_t nsel, int32_t location, uint64_t* out);
+
+/* ---- Sink: HashAggregateSink (operators/aggregate/hash.rs:434-634) ------------- */
+/* `input_types` describes the pipeline source's columns (the prologue's first input).
+ * `size_hint` presizes the device table (expected number of groups; 0 = start small and
+ * grow on overflow, swiss.rs:287-301). */
+int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue,
+                          const int32_t* input_types, int32_t ninput, const ml_expr* group_exprs,
+                          int32_t ngroup, const ml_agg_spec* aggs, int32_t nagg,
+                          int64_t size_hint, ml_hashagg** out);
+int ml_gpu_hashagg_local_create(ml_hashagg* sink, ml_hashagg_local** out);
+/* LocalSink::sink: run the prologue and the aggregation over one morsel.  `sel` (optional)
+ * is the batch's selection vector (batch.rs:8-14). */
+int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t ncols,
+                        int64_t nrows, const uint32_t* sel, int64_t nsel);
+/* LocalSink::combine: merge into the global state (device-side partial-state merge). */
+int ml_gpu_hashagg_combine(ml_hashagg_local* local);
+/* Sink::finalize: final values (AVG = sum/count, seen-flags -> NULL), one row per group:
+ * key columns then one column per aggregate (hash.rs:307-314). */
+int ml_gpu_hashagg_finalize(ml_hashagg* sink, ml_batch** out);
+/* Number of groups, table capacity and number of resize-on-overflow events so far. */
+int ml_gpu_hashagg_stats(ml_hashagg* sink, int64_t* groups, int64_t* capacity, int64_t* resizes);
+int ml_gpu_hashagg_destroy(ml_hashagg* sink);
+
+/* ---- Sink: JoinBuildSink (operators/join.rs:72-242) --------------------------- */
+/* `build_input_types`: columns of the batches pushed into the build side (after the
+ * prologue, these become the build batch whose columns HashJoinProbe gathers). */
+int ml_gpu_join_build_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue,
+                             const int32_t* input_types, int32_t ninput, const ml_expr* key_exprs,
+                             int32_t nkeys, ml_join_build** out);
+int ml_gpu_join_build_local_create(ml_join_build* sink, ml_join_build_local** out);
+int ml_gpu_join_build_sink(ml_join_build_local* local, const ml_column* cols, int32_t ncols,
+                           int64_t nrows, const uint32_t* sel, int64_t nsel);
+int ml_gpu_join_build_combine(ml_join_build_local* local);
+/* Sink::finalize -> build_table (join.rs:160-203).  The table stays owned by the sink. */
+int ml_gpu_join_build_finalize(ml_join_build* sink, ml_join_table** table);
+int ml_gpu_join_table_stats(const ml_join_table* t, int64_t* build_rows, int64_t* distinct_keys,
+                            int64_t* capacity);
+int ml_gpu_join_build_destroy(ml_join_build* sink);
+
+/* ---- Operator: HashJoinProbe (operators/join.rs:244-337) ----------------------- */
+/* All (probe_row, build_row) pairs of the active rows.  Pairs are ordered by probe row.
+ * out arrays need `cap` entries; *npairs receives the count (if it exceeds cap, nothing is
+ * written and ML_ERR_INVALID is returned with *npairs set, so the caller can retry). */
+int ml_gpu_join_probe(ml_ctx* ctx, ml_join_table* table, const ml_expr* key_exprs, int32_t nkeys,
+                      const ml_column* cols, int32_t ncols, int64_t nrows, const uint32_t* sel,
+                      int64_t nsel, int32_t location, uint32_t* probe_idx, uint32_t* build_idx,
+                      int64_t cap, int64_t* npairs);
+
+/* ---- Sink: SortSink with a limit (top-N; operators/sort.rs:85-132, 186-267) ---- */
+/* Output = the input columns (after the prologue) of the best `limit` rows, sorted.
+ * limit <= 4096. */
+int ml_gpu_topn_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue,
+                       const int32_t* input_types, int32_t ninput, const ml_sort_key* keys,
+                       int32_t nkeys, int64_t limit, ml_topn** out);
+int ml_gpu_topn_local_create(ml_topn* sink, ml_topn_local** out);
+int ml_gpu_topn_sink(ml_topn_local* local, const ml_column* cols, int32_t ncols, int64_t nrows,
+                     const uint32_t* sel, int64_t nsel);
+int ml_gpu_topn_combine(ml_topn_local* local);
+int ml_gpu_topn_finalize(ml_topn* sink, ml_batch** out);
+int ml_gpu_topn_destroy(ml_topn* sink);
+
+/* ---- profiling ------------------------------------------------------------------ */
+/* Number of kernels this library has launched since the context was created. */
+int ml_gpu_kernel_launches(ml_ctx* ctx, uint64_t* count);
+/* With ML_CTX_PROFILE: launches and summed device time (ms, CUDA events) of one kernel
+ * family: "pipeline_aggregate" (fused filter/probe/aggregate), "join_insert", "topn",
+ * "select" (filter compaction).  `reset` clears the counters after reading. */
+int ml_gpu_profile_read(ml_ctx* ctx, const char* kernel, uint64_t* launches, double* total_ms, int32_t reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MINILAKE_GPU_H */

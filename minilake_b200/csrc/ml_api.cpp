@@ -1,0 +1,1616 @@
+// C ABI of the MiniLake B200 execution core (include/minilake_gpu.h).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <shared_mutex>
+
+#include "ml_pipeline.hpp"
+
+using namespace mlg;
+
+struct ml_ctx : Ctx {
+    using Ctx::Ctx;
+    std::mutex op_mu;  // serializes the standalone operators on the context stream
+};
+
+#define API_BEGIN try {
+#define API_END                                       \
+    }                                                 \
+    catch (const MlError& e) {                        \
+        set_last_error(e.what());                     \
+        return e.code;                                \
+    }                                                 \
+    catch (const std::bad_alloc&) {                   \
+        set_last_error("host allocation failed");    \
+        return ML_ERR_INTERNAL;                       \
+    }                                                 \
+    catch (const std::exception& e) {                 \
+        set_last_error(e.what());                     \
+        return ML_ERR_INTERNAL;                       \
+    }                                                 \
+    return ML_OK;
+
+#define REQUIRE(c, msg) \
+    if (!(c)) raise(ML_ERR_INVALID, msg)
+
+namespace {
+
+uint64_t pow2_at_least(uint64_t x) {
+    uint64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+bool is_device_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Selection vector on the device (copied when it is host memory).
+const uint32_t* device_sel(Ctx* ctx, const uint32_t* sel, int64_t nsel, DevBuf& hold, cudaStream_t s) {
+    if (!sel) return nullptr;
+    if (nsel < 0) raise(ML_ERR_INVALID, "negative selection length");
+    if (is_device_ptr(sel)) return sel;
+    hold = DevBuf(ctx, std::max<size_t>((size_t)nsel * 4, 4), nullptr);
+    if (nsel) CK(cudaMemcpyAsync(hold.get(), sel, (size_t)nsel * 4, cudaMemcpyHostToDevice, s));
+    return hold.get<uint32_t>();
+}
+
+void check_sel_bounds(const uint32_t* sel, int64_t nsel, int64_t nrows) {
+    if (!sel || is_device_ptr(sel)) return;  // device selections are trusted like device columns
+    for (int64_t i = 0; i < nsel; i++)
+        if (sel[i] >= (uint64_t)nrows) raise(ML_ERR_INVALID, "selection index out of range");
+}
+
+// Deep copy of expressions (the caller's nodes are borrowed only for the call).
+struct OwnedExprs {
+    std::vector<std::vector<ml_expr_node>> nodes;
+    std::vector<std::string> strs;
+    std::vector<ml_expr> exprs;
+    void add(const ml_expr& e) {
+        if (!e.nodes || e.nnodes <= 0) raise(ML_ERR_INVALID, "empty expression");
+        nodes.emplace_back(e.nodes, e.nodes + e.nnodes);
+        exprs.push_back(e);
+    }
+    void finish() {
+        strs.reserve(4096);
+        for (size_t i = 0; i < nodes.size(); i++) {
+            for (auto& n : nodes[i])
+                if (n.str) {
+                    strs.emplace_back(n.str, (size_t)n.str_len);
+                    n.str = strs.back().data();
+                }
+            exprs[i].nodes = nodes[i].data();
+        }
+    }
+};
+
+std::unique_ptr<DevColumn> copy_column(Ctx* ctx, const DevColumn& s, cudaStream_t st, Reservation* res) {
+    auto d = std::make_unique<DevColumn>();
+    d->dtype = s.dtype;
+    d->kind = s.kind;
+    d->n = s.n;
+    d->dict = s.dict;
+    if (s.kind == CK_UTF8) {
+        uint32_t first = 0, last = 0;
+        if (s.n) {
+            CK(cudaMemcpyAsync(&first, s.optr(), 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&last, s.optr() + s.n, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        d->offsets = DevBuf(ctx, (size_t)(s.n + 1) * 4, res);
+        launch_offsets_rebase(s.optr(), s.n, 0, d->offsets.get<uint32_t>(), st);
+        ctx->count_launch();
+        d->data = DevBuf(ctx, std::max<size_t>(last - first, 1), res);
+        if (last > first)
+            CK(cudaMemcpyAsync(d->data.get(), (const uint8_t*)s.dptr() + first, last - first, cudaMemcpyDeviceToDevice, st));
+    } else {
+        size_t w = s.kind == CK_DICT ? 4 : (size_t)width_of(s.dtype);
+        d->data = DevBuf(ctx, std::max<size_t>(s.n * w, 1), res);
+        if (s.n) CK(cudaMemcpyAsync(d->data.get(), s.dptr(), s.n * w, cudaMemcpyDeviceToDevice, st));
+    }
+    if (s.vptr()) {
+        size_t vb = (size_t)(s.n + 63) / 64 * 8;
+        d->validity = DevBuf(ctx, std::max<size_t>(vb, 8), res);
+        if (vb) CK(cudaMemcpyAsync(d->validity.get(), s.vptr(), vb, cudaMemcpyDeviceToDevice, st));
+    }
+    return d;
+}
+
+// Rows `idx` (device, k entries; nullptr = all rows) of a column into a new owned column.
+// Dictionary strings are decoded into plain UTF8.
+std::unique_ptr<DevColumn> gather_column(Ctx* ctx, const DevColumn& s, const uint32_t* idx, int64_t k, cudaStream_t st,
+                                         Reservation* res) {
+    if (!idx && s.kind != CK_DICT) return copy_column(ctx, s, st, res);
+    auto d = std::make_unique<DevColumn>();
+    d->dtype = s.dtype;
+    d->n = k;
+    if (s.kind == CK_FIXED) {
+        d->kind = CK_FIXED;
+        int w = width_of(s.dtype);
+        d->data = DevBuf(ctx, std::max<size_t>((size_t)k * w, 1), res);
+        launch_gather_fixed(s.dptr(), w, idx, k, d->data.get(), st);
+        ctx->count_launch();
+    } else if (s.kind == CK_UTF8) {
+        gather_utf8(ctx, s.optr(), (const uint8_t*)s.dptr(), idx, k, *d, st, res);
+    } else {  // dictionary: codes -> dictionary strings
+        DevBuf codes;
+        const uint32_t* cidx = (const uint32_t*)s.dptr();
+        if (idx) {
+            codes = DevBuf(ctx, std::max<size_t>((size_t)k * 4, 4), nullptr);
+            launch_gather_fixed(s.dptr(), 4, idx, k, codes.get(), st);
+            ctx->count_launch();
+            cidx = codes.get<uint32_t>();
+        }
+        const HostDict& hd = *s.dict;
+        DevBuf doff(ctx, hd.off.size() * 4, nullptr), dbytes(ctx, std::max<size_t>(hd.bytes.size(), 1), nullptr);
+        CK(cudaMemcpyAsync(doff.get(), hd.off.data(), hd.off.size() * 4, cudaMemcpyHostToDevice, st));
+        if (!hd.bytes.empty()) CK(cudaMemcpyAsync(dbytes.get(), hd.bytes.data(), hd.bytes.size(), cudaMemcpyHostToDevice, st));
+        gather_utf8(ctx, doff.get<uint32_t>(), dbytes.get<uint8_t>(), cidx, k, *d, st, res);
+        CK(cudaStreamSynchronize(st));
+    }
+    if (s.vptr()) {
+        size_t words = (size_t)(k + 63) / 64;
+        d->validity = DevBuf(ctx, std::max<size_t>(words * 8, 8), res);
+        CK(cudaMemsetAsync(d->validity.get(), 0, std::max<size_t>(words * 8, 8), st));
+        if (idx) {
+            launch_gather_valid(s.vptr(), idx, k, d->validity.get<uint32_t>(), st);
+        } else {
+            launch_copy_bits(s.vptr(), k, d->validity.get<uint64_t>(), 0, st);
+        }
+        ctx->count_launch();
+    }
+    return d;
+}
+
+// Evaluate program `p` for the rows of launch `P` into a new fixed-width column.
+std::unique_ptr<DevColumn> project_column(Ctx* ctx, const PipeArgs& P, Prog p, int type, cudaStream_t st, Reservation* res) {
+    auto d = std::make_unique<DevColumn>();
+    d->dtype = type;
+    d->kind = CK_FIXED;
+    d->n = P.n;
+    d->data = DevBuf(ctx, std::max<size_t>((size_t)P.n * width_of(type), 1), res);
+    size_t words = (size_t)(P.n + 63) / 64;
+    d->validity = DevBuf(ctx, std::max<size_t>(words * 8, 8), res);
+    CK(cudaMemsetAsync(d->validity.get(), 0, std::max<size_t>(words * 8, 8), st));
+    launch_project(P, p, type, d->data.get(), d->validity.get<uint32_t>(), st);
+    ctx->count_launch();
+    return d;
+}
+
+void check_device_error(Ctx* ctx, uint32_t err) {
+    (void)ctx;
+    if (err & DE_TIMEOUT) raise(ML_ERR_TIMEOUT, "a bounded device-side wait ran out");
+    if (err & DE_OVERFLOW_LOST) raise(ML_ERR_INTERNAL, "hash-table overflow buffer exhausted");
+    if (err) raise(ML_ERR_INTERNAL, "device error word " + std::to_string(err));
+}
+
+struct ErrWord {  // a device error word plus a pinned readback slot
+    DevBuf d;
+    uint32_t* h = nullptr;
+    Ctx* ctx;
+    explicit ErrWord(Ctx* c) : d(c, 64, nullptr), ctx(c) { h = (uint32_t*)c->halloc(64); }
+    ~ErrWord() { ctx->hfree(h); }
+};
+
+// The prologue's output for one batch, materialized as owned device columns.
+std::unique_ptr<ml_batch> materialize(Ctx* ctx, Pipeline& pipe, const std::vector<Prog>& out_progs, Pipeline::Launch& L,
+                                      cudaStream_t st, Reservation* res, ErrWord& ew) {
+    DevBuf idx;
+    const uint32_t* rows = L.P.sel;
+    int64_t k = L.P.n;
+    if (pipe.nstages > 0) {
+        CK(cudaMemsetAsync(ew.d.get(), 0, 4, st));
+        L.P.err = ew.d.get<uint32_t>();
+        k = run_select(ctx, L.P, idx, st);
+        rows = idx.get<uint32_t>();
+    }
+    auto b = std::make_unique<ml_batch>();
+    b->ctx = ctx;
+    b->nrows = k;
+    PipeArgs Q = L.P;
+    Q.sel = rows;
+    Q.n = k;
+    Q.nstages = 0;
+    for (size_t c = 0; c < pipe.out.size(); c++) {
+        const ColRef& r = pipe.out[c];
+        if (r.kind == 0) {
+            b->cols.push_back(gather_column(ctx, *L.src[r.index], rows, k, st, res));
+        } else if (r.kind == 2) {
+            if (r.dtype == ML_TYPE_UTF8) raise(ML_ERR_UNSUPPORTED, "computed string column on the GPU");
+            b->cols.push_back(project_column(ctx, Q, out_progs[c], r.dtype, st, res));
+        } else {
+            raise(ML_ERR_UNSUPPORTED, "a probe in front of this sink");
+        }
+    }
+    CK(cudaStreamSynchronize(st));
+    return b;
+}
+
+std::vector<Prog> compile_outputs(Pipeline& pipe) {
+    std::vector<Prog> progs(pipe.out.size());
+    for (size_t c = 0; c < pipe.out.size(); c++) {
+        const ColRef& r = pipe.out[c];
+        if (r.kind == 2 && r.dtype != ML_TYPE_UTF8) progs[c] = pipe.C.compile_value(*r.expr, *r.env, r.dtype);
+    }
+    return progs;
+}
+
+std::vector<ml_column> device_views(const ml_batch& b) {
+    std::vector<ml_column> v;
+    for (auto& c : b.cols) {
+        ml_column m{};
+        m.dtype = c->dtype;
+        m.encoding = c->kind == CK_DICT ? ML_ENC_DICT : ML_ENC_PLAIN;
+        m.location = ML_LOC_DEVICE;
+        m.len = c->n;
+        m.data = c->dptr();
+        m.offsets = c->optr();
+        m.validity = c->vptr();
+        if (c->dict) {
+            m.dict_len = (int64_t)c->dict->len();
+            m.dict_offsets = c->dict->off.data();
+            m.dict_data = c->dict->bytes.data();
+        }
+        v.push_back(m);
+    }
+    return v;
+}
+
+// Concatenate batches column by column into one owned batch.
+std::unique_ptr<ml_batch> concat_batches(Ctx* ctx, std::vector<std::unique_ptr<ml_batch>>& parts, const std::vector<int>& types,
+                                         cudaStream_t st, Reservation* res) {
+    auto out = std::make_unique<ml_batch>();
+    out->ctx = ctx;
+    int64_t n = 0;
+    for (auto& p : parts) n += p->nrows;
+    out->nrows = n;
+    if (parts.size() == 1) {
+        out->cols = std::move(parts[0]->cols);
+        return out;
+    }
+    for (size_t c = 0; c < types.size(); c++) {
+        auto d = std::make_unique<DevColumn>();
+        d->dtype = types[c];
+        d->n = n;
+        bool utf8 = types[c] == ML_TYPE_UTF8;
+        d->kind = utf8 ? CK_UTF8 : CK_FIXED;
+        bool any_valid = false;
+        for (auto& p : parts) any_valid |= p->cols[c]->vptr() != nullptr;
+        if (utf8) {
+            std::vector<uint32_t> sizes;
+            uint64_t total = 0;
+            for (auto& p : parts) {
+                uint32_t first = 0, last = 0;
+                const DevColumn& s = *p->cols[c];
+                if (s.n) {
+                    CK(cudaMemcpy(&first, s.optr(), 4, cudaMemcpyDeviceToHost));
+                    CK(cudaMemcpy(&last, s.optr() + s.n, 4, cudaMemcpyDeviceToHost));
+                }
+                sizes.push_back(last - first);
+                total += last - first;
+            }
+            if (total > 0xFFFFFFFFull) raise(ML_ERR_UNSUPPORTED, "string column larger than 4 GiB");
+            d->offsets = DevBuf(ctx, (size_t)(n + 1) * 4, res);
+            d->data = DevBuf(ctx, std::max<size_t>(total, 1), res);
+            uint64_t row = 0, byte = 0;
+            for (size_t i = 0; i < parts.size(); i++) {
+                const DevColumn& s = *parts[i]->cols[c];
+                launch_offsets_rebase(s.optr(), s.n, (uint32_t)byte, d->offsets.get<uint32_t>() + row, st);
+                uint32_t first = 0;
+                if (s.n) CK(cudaMemcpy(&first, s.optr(), 4, cudaMemcpyDeviceToHost));
+                if (sizes[i])
+                    CK(cudaMemcpyAsync(d->data.get<uint8_t>() + byte, (const uint8_t*)s.dptr() + first, sizes[i],
+                                       cudaMemcpyDeviceToDevice, st));
+                row += s.n;
+                byte += sizes[i];
+                ctx->count_launch();
+            }
+        } else {
+            int w = width_of(types[c]);
+            d->data = DevBuf(ctx, std::max<size_t>((size_t)n * w, 1), res);
+            uint64_t row = 0;
+            for (auto& p : parts) {
+                const DevColumn& s = *p->cols[c];
+                if (s.n) CK(cudaMemcpyAsync(d->data.get<uint8_t>() + row * w, s.dptr(), (size_t)s.n * w, cudaMemcpyDeviceToDevice, st));
+                row += s.n;
+            }
+        }
+        if (any_valid) {
+            size_t vb = std::max<size_t>((size_t)(n + 63) / 64 * 8, 8);
+            d->validity = DevBuf(ctx, vb, res);
+            CK(cudaMemsetAsync(d->validity.get(), 0, vb, st));
+            uint64_t row = 0;
+            for (auto& p : parts) {
+                const DevColumn& s = *p->cols[c];
+                launch_copy_bits(s.vptr(), s.n, d->validity.get<uint64_t>(), (int64_t)row, st);
+                ctx->count_launch();
+                row += s.n;
+            }
+        }
+        out->cols.push_back(std::move(d));
+    }
+    CK(cudaStreamSynchronize(st));
+    return out;
+}
+
+// ---- top-N over a device batch (sort.rs:85-132) ------------------------------------------
+struct SortKeySpec {
+    ExprNode expr;
+    int type;
+    bool asc, nulls_first;
+};
+
+std::unique_ptr<ml_batch> topn_batch(Ctx* ctx, ml_batch& b, const std::vector<SortKeySpec>& keys, int64_t limit,
+                                     cudaStream_t st, Reservation* res) {
+    int64_t n = b.nrows;
+    int64_t k = std::min<int64_t>(limit, n);
+    auto out = std::make_unique<ml_batch>();
+    out->ctx = ctx;
+    out->nrows = k;
+    std::vector<int> types;
+    for (auto& c : b.cols) types.push_back(c->dtype);
+    if (k <= 0) {
+        for (auto& c : b.cols) {
+            auto d = std::make_unique<DevColumn>();
+            d->dtype = c->dtype;
+            d->kind = c->dtype == ML_TYPE_UTF8 ? CK_UTF8 : CK_FIXED;
+            d->n = 0;
+            if (d->kind == CK_UTF8) {
+                d->offsets = DevBuf(ctx, 4, res);
+                CK(cudaMemsetAsync(d->offsets.get(), 0, 4, st));
+                d->data = DevBuf(ctx, 1, res);
+            } else {
+                d->data = DevBuf(ctx, 8, res);
+            }
+            out->cols.push_back(std::move(d));
+        }
+        out->nrows = 0;
+        return out;
+    }
+    // key columns: plain column references read the batch; other expressions are evaluated
+    Pipeline kp(ctx);
+    kp.build(nullptr, 0, types.data(), (int)types.size());
+    std::vector<std::unique_ptr<DevColumn>> temps;
+    SortDev S{};
+    S.nkeys = (int)keys.size();
+    std::vector<Prog> progs;
+    std::vector<int> direct;
+    for (auto& key : keys) {
+        if (key.expr.kind == ML_EXPR_COLUMN && key.expr.index >= 0 && (size_t)key.expr.index < types.size() &&
+            types[key.expr.index] == key.type) {
+            direct.push_back((int)key.expr.index);
+            progs.push_back(Prog{});
+        } else {
+            direct.push_back(-1);
+            progs.push_back(kp.C.compile_value(key.expr, kp.out, key.type));
+        }
+    }
+    kp.upload();
+    Staging stg(ctx);
+    Pipeline::Launch L;
+    auto views = device_views(b);
+    kp.prepare(L, views.data(), (int)views.size(), n, nullptr, 0, st, stg, nullptr);
+    for (size_t i = 0; i < keys.size(); i++) {
+        const DevColumn* c;
+        if (direct[i] >= 0) {
+            c = b.cols[direct[i]].get();
+        } else {
+            temps.push_back(project_column(ctx, L.P, progs[i], keys[i].type, st, nullptr));
+            c = temps.back().get();
+        }
+        if (c->kind == CK_DICT) raise(ML_ERR_UNSUPPORTED, "sorting a dictionary column on the GPU");
+        DCol& d = S.cols[i];
+        d.dt = c->dtype;
+        d.kind = c->kind;
+        d.data = c->dptr();
+        d.off = c->optr();
+        d.valid = c->vptr();
+        d.n = c->n;
+        S.asc[i] = keys[i].asc;
+        S.nulls_first[i] = keys[i].nulls_first;
+    }
+    // rounds of chunk sorts until one chunk remains
+    DevBuf a, bb;
+    const uint32_t* in = nullptr;
+    int64_t m = n;
+    for (;;) {
+        int64_t nb = (m + kTopNChunk - 1) / kTopNChunk;
+        DevBuf& dst = (in == a.get<uint32_t>() && in) ? bb : a;
+        dst = DevBuf(ctx, (size_t)nb * k * 4, nullptr);
+        {
+            KernelTimer kt(ctx, st, "topn");
+            launch_topn_chunk(S, in, m, (int)k, dst.get<uint32_t>(), st);
+            kt.stop();
+        }
+        ctx->count_launch();
+        in = dst.get<uint32_t>();
+        if (nb == 1) break;
+        m = nb * k;
+    }
+    CK(cudaStreamSynchronize(st));
+    for (auto& c : b.cols) out->cols.push_back(gather_column(ctx, *c, in, k, st, res));
+    CK(cudaStreamSynchronize(st));
+    return out;
+}
+
+}  // namespace
+
+// =====================================================================================================
+// context
+// =====================================================================================================
+extern "C" {
+
+const char* ml_gpu_last_error(void) { return last_error(); }
+
+int ml_gpu_last_budget_error(char* op, size_t op_cap, uint64_t* requested, uint64_t* used, uint64_t* limit) {
+    const BudgetInfo& b = last_budget();
+    if (op && op_cap) {
+        strncpy(op, b.op.c_str(), op_cap - 1);
+        op[op_cap - 1] = 0;
+    }
+    if (requested) *requested = b.requested;
+    if (used) *used = b.used;
+    if (limit) *limit = b.limit;
+    return ML_OK;
+}
+
+int ml_gpu_ctx_create(int device, uint64_t hbm_budget_bytes, uint32_t flags, ml_ctx** out) {
+    API_BEGIN
+    REQUIRE(out, "null output");
+    *out = new ml_ctx(device, hbm_budget_bytes, flags);
+    API_END
+}
+
+int ml_gpu_ctx_destroy(ml_ctx* ctx) {
+    API_BEGIN
+    delete ctx;
+    API_END
+}
+
+int ml_gpu_pool_stats(ml_ctx* ctx, uint64_t* used, uint64_t* peak, uint64_t* limit) {
+    API_BEGIN
+    REQUIRE(ctx, "null context");
+    if (used) *used = ctx->pool.used.load();
+    if (peak) *peak = ctx->pool.peak.load();
+    if (limit) *limit = ctx->pool.limit;
+    API_END
+}
+
+int ml_gpu_ctx_synchronize(ml_ctx* ctx) {
+    API_BEGIN
+    REQUIRE(ctx, "null context");
+    ctx->sync_all();
+    API_END
+}
+
+int ml_gpu_kernel_launches(ml_ctx* ctx, uint64_t* count) {
+    API_BEGIN
+    REQUIRE(ctx && count, "null argument");
+    *count = ctx->launches.load();
+    API_END
+}
+
+int ml_gpu_profile_read(ml_ctx* ctx, const char* kernel, uint64_t* launches, double* total_ms, int32_t reset) {
+    API_BEGIN
+    REQUIRE(ctx && kernel, "null argument");
+    ctx->read_profile(kernel, launches, total_ms, reset != 0);
+    API_END
+}
+
+// =====================================================================================================
+// batches
+// =====================================================================================================
+int ml_gpu_batch_upload(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64_t nrows, ml_batch** out) {
+    API_BEGIN
+    REQUIRE(ctx && out && (cols || ncols == 0) && ncols >= 0 && nrows >= 0, "bad arguments");
+    ctx->set_current();
+    std::lock_guard<std::mutex> g(ctx->op_mu);
+    auto b = std::make_unique<ml_batch>();
+    b->ctx = ctx;
+    b->nrows = nrows;
+    b->res = std::make_unique<Reservation>(ctx, "Batch");
+    Staging st(ctx);
+    for (int c = 0; c < ncols; c++) {
+        auto col = stage_column(ctx, cols[c], nrows, ctx->stream, st, b->res.get());
+        if (cols[c].location == ML_LOC_DEVICE) col = copy_column(ctx, *col, ctx->stream, b->res.get());
+        b->cols.push_back(std::move(col));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    *out = b.release();
+    API_END
+}
+
+int ml_gpu_batch_num_rows(const ml_batch* b, int64_t* nrows) {
+    API_BEGIN
+    REQUIRE(b && nrows, "null argument");
+    *nrows = b->nrows;
+    API_END
+}
+
+int ml_gpu_batch_num_columns(const ml_batch* b, int32_t* ncols) {
+    API_BEGIN
+    REQUIRE(b && ncols, "null argument");
+    *ncols = (int32_t)b->cols.size();
+    API_END
+}
+
+int ml_gpu_batch_columns(const ml_batch* b, ml_column* out, int32_t ncols) {
+    API_BEGIN
+    REQUIRE(b && out, "null argument");
+    REQUIRE(ncols == (int32_t)b->cols.size(), "column count mismatch");
+    auto v = device_views(*b);
+    for (int i = 0; i < ncols; i++) out[i] = v[i];
+    API_END
+}
+
+int ml_gpu_batch_column_info(const ml_batch* b, int32_t col, int32_t* dtype, int64_t* str_bytes, int32_t* has_validity) {
+    API_BEGIN
+    REQUIRE(b, "null batch");
+    REQUIRE(col >= 0 && col < (int32_t)b->cols.size(), "column out of range");
+    b->ctx->set_current();
+    const DevColumn& c = *b->cols[col];
+    if (dtype) *dtype = c.dtype;
+    if (has_validity) *has_validity = c.vptr() != nullptr;
+    if (str_bytes) {
+        if (c.kind == CK_UTF8) *str_bytes = c.str_bytes_host();
+        else if (c.kind == CK_DICT) {
+            std::vector<uint32_t> codes(c.n);
+            if (c.n) CK(cudaMemcpy(codes.data(), c.dptr(), c.n * 4, cudaMemcpyDeviceToHost));
+            int64_t s = 0;
+            for (uint32_t k : codes) s += c.dict->off[k + 1] - c.dict->off[k];
+            *str_bytes = s;
+        } else *str_bytes = 0;
+    }
+    API_END
+}
+
+int ml_gpu_batch_fetch(const ml_batch* b, int32_t col, void* values, uint32_t* offsets, uint64_t* validity) {
+    API_BEGIN
+    REQUIRE(b, "null batch");
+    REQUIRE(col >= 0 && col < (int32_t)b->cols.size(), "column out of range");
+    b->ctx->set_current();
+    const DevColumn& c = *b->cols[col];
+    int64_t n = c.n;
+    if (c.kind == CK_UTF8) {
+        REQUIRE(offsets, "UTF8 fetch needs an offsets buffer");
+        std::vector<uint32_t> off(n + 1);
+        CK(cudaMemcpy(off.data(), c.optr(), (n + 1) * 4, cudaMemcpyDeviceToHost));
+        uint32_t first = off[0];
+        for (auto& o : off) o -= first;
+        memcpy(offsets, off.data(), (n + 1) * 4);
+        if (off[n]) {
+            REQUIRE(values, "null values buffer");
+            CK(cudaMemcpy(values, (const uint8_t*)c.dptr() + first, off[n], cudaMemcpyDeviceToHost));
+        }
+    } else if (c.kind == CK_DICT) {
+        REQUIRE(offsets, "UTF8 fetch needs an offsets buffer");
+        std::vector<uint32_t> codes(n);
+        if (n) CK(cudaMemcpy(codes.data(), c.dptr(), n * 4, cudaMemcpyDeviceToHost));
+        uint32_t pos = 0;
+        for (int64_t i = 0; i < n; i++) {
+            offsets[i] = pos;
+            uint32_t a = c.dict->off[codes[i]], e = c.dict->off[codes[i] + 1];
+            memcpy((uint8_t*)values + pos, c.dict->bytes.data() + a, e - a);
+            pos += e - a;
+        }
+        offsets[n] = pos;
+    } else if (n) {
+        REQUIRE(values, "null values buffer");
+        CK(cudaMemcpy(values, c.dptr(), (size_t)n * width_of(c.dtype), cudaMemcpyDeviceToHost));
+    }
+    if (validity) {
+        size_t words = (size_t)(n + 63) / 64;
+        if (c.vptr()) {
+            if (words) CK(cudaMemcpy(validity, c.vptr(), words * 8, cudaMemcpyDeviceToHost));
+            if (n % 64) validity[words - 1] &= (1ull << (n % 64)) - 1;
+        } else {
+            for (size_t w = 0; w < words; w++) validity[w] = ~0ull;
+            if (n % 64) validity[words - 1] = (1ull << (n % 64)) - 1;
+        }
+    }
+    API_END
+}
+
+int ml_gpu_batch_destroy(ml_batch* b) {
+    API_BEGIN
+    if (b) {
+        b->ctx->set_current();
+        b->cols.clear();
+        delete b;
+    }
+    API_END
+}
+
+// =====================================================================================================
+// operators
+// =====================================================================================================
+int ml_gpu_filter(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32_t ncols, int64_t nrows,
+                  const uint32_t* sel_in, int64_t nsel_in, int32_t location, uint32_t* sel_out, int64_t* nsel_out) {
+    API_BEGIN
+    REQUIRE(ctx && pred && sel_out && nsel_out, "null argument");
+    ctx->set_current();
+    std::lock_guard<std::mutex> g(ctx->op_mu);
+    cudaStream_t s = ctx->stream;
+    if (location == ML_LOC_HOST) check_sel_bounds(sel_in, nsel_in, nrows);
+    std::vector<int32_t> types;
+    for (int c = 0; c < ncols; c++) types.push_back(cols[c].dtype);
+    Pipeline p(ctx);
+    ml_pipe_op op{};
+    op.kind = ML_PIPE_FILTER;
+    op.nexprs = 1;
+    op.exprs = pred;
+    p.build(&op, 1, types.data(), ncols);
+    p.upload();
+    Staging st(ctx);
+    DevBuf sel_hold;
+    const uint32_t* dsel = device_sel(ctx, sel_in, nsel_in, sel_hold, s);
+    Pipeline::Launch L;
+    p.prepare(L, cols, ncols, nrows, dsel, nsel_in, s, st, nullptr);
+    ErrWord ew(ctx);
+    CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
+    L.P.err = ew.d.get<uint32_t>();
+    DevBuf out;
+    int64_t k = run_select(ctx, L.P, out, s);
+    CK(cudaMemcpyAsync(ew.h, ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
+    if (k) CK(cudaMemcpyAsync(sel_out, out.get(), (size_t)k * 4,
+                              location == ML_LOC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    check_device_error(ctx, *ew.h);
+    *nsel_out = k;
+    API_END
+}
+
+int ml_gpu_project(ml_ctx* ctx, const ml_expr* expr, const ml_column* cols, int32_t ncols, int64_t nrows, ml_batch** out) {
+    API_BEGIN
+    REQUIRE(ctx && expr && out, "null argument");
+    ctx->set_current();
+    std::lock_guard<std::mutex> g(ctx->op_mu);
+    cudaStream_t s = ctx->stream;
+    std::vector<int32_t> types;
+    for (int c = 0; c < ncols; c++) types.push_back(cols[c].dtype);
+    Pipeline p(ctx);
+    p.build(nullptr, 0, types.data(), ncols);
+    ExprNode e = parse_expr(*expr);
+    Staging st(ctx);
+    auto b = std::make_unique<ml_batch>();
+    b->ctx = ctx;
+    b->nrows = nrows;
+    b->res = std::make_unique<Reservation>(ctx, "Projection");
+    auto origin = p.C.column_origin(e, p.out);
+    if (origin && types[origin->index] == expr->dtype) {  // pass-through column (an Arc clone in the reference)
+        Pipeline::Launch L;
+        p.upload();
+        p.prepare(L, cols, ncols, nrows, nullptr, 0, s, st, nullptr);
+        b->cols.push_back(gather_column(ctx, *L.src[origin->index], nullptr, nrows, s, b->res.get()));
+    } else {
+        Prog pr = p.C.compile_value(e, p.out, expr->dtype);
+        p.upload();
+        Pipeline::Launch L;
+        p.prepare(L, cols, ncols, nrows, nullptr, 0, s, st, nullptr);
+        b->cols.push_back(project_column(ctx, L.P, pr, expr->dtype, s, b->res.get()));
+    }
+    CK(cudaStreamSynchronize(s));
+    *out = b.release();
+    API_END
+}
+
+int ml_gpu_hash_columns(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64_t nrows, const uint32_t* sel, int64_t nsel,
+                        int32_t location, uint64_t* out) {
+    API_BEGIN
+    REQUIRE(ctx && out && (cols || ncols == 0), "null argument");
+    REQUIRE(ncols <= kMaxCols, "too many columns");
+    ctx->set_current();
+    std::lock_guard<std::mutex> g(ctx->op_mu);
+    cudaStream_t s = ctx->stream;
+    if (location == ML_LOC_HOST) check_sel_bounds(sel, nsel, nrows);
+    Staging st(ctx);
+    std::vector<std::unique_ptr<DevColumn>> staged;
+    PipeArgs P{};
+    DevBuf sel_hold;
+    P.sel = device_sel(ctx, sel, nsel, sel_hold, s);
+    P.n = sel ? nsel : nrows;
+    std::vector<DevBuf> dh;
+    std::vector<const uint64_t*> dh_ptr(ncols, nullptr);
+    for (int c = 0; c < ncols; c++) {
+        staged.push_back(stage_column(ctx, cols[c], nrows, s, st, nullptr));
+        const DevColumn& col = *staged.back();
+        DCol& d = P.cols[c];
+        d.dt = col.dtype;
+        d.kind = col.kind;
+        d.data = col.dptr();
+        d.off = col.optr();
+        d.valid = col.vptr();
+        d.n = col.n;
+        if (col.kind == CK_DICT) d.dict_len = (uint32_t)col.dict->len();
+        if (col.kind == CK_DICT) {  // kernels/hash.rs:66-77: hash each dictionary entry once
+            std::vector<uint64_t> h(col.dict->len() + 1);
+            for (size_t e = 0; e < col.dict->len(); e++) {
+                uint64_t x = 0x243F6A8885A308D3ull ^ ((uint64_t)(col.dict->off[e + 1] - col.dict->off[e]) * 0x9E3779B97F4A7C15ull);
+                const uint8_t* b = col.dict->bytes.data() + col.dict->off[e];
+                size_t nb = col.dict->off[e + 1] - col.dict->off[e];
+                auto fm = [](uint64_t a, uint64_t m) {
+                    unsigned __int128 r = (unsigned __int128)a * m;
+                    return (uint64_t)r ^ (uint64_t)(r >> 64);
+                };
+                size_t full = nb / 8;
+                for (size_t q = 0; q < full; q++) {
+                    uint64_t w;
+                    memcpy(&w, b + q * 8, 8);
+                    x = fm(x ^ w, 0x9E3779B97F4A7C15ull);
+                }
+                if (nb % 8) {
+                    uint64_t w = 0;
+                    memcpy(&w, b + full * 8, nb % 8);
+                    x = fm(x ^ w, 0xBF58476D1CE4E5B9ull);
+                }
+                h[e] = x;
+            }
+            dh.emplace_back(ctx, h.size() * 8, nullptr);
+            CK(cudaMemcpyAsync(dh.back().get(), h.data(), h.size() * 8, cudaMemcpyHostToDevice, s));
+            dh_ptr[c] = dh.back().get<uint64_t>();
+        }
+    }
+    DevBuf ptrs(ctx, std::max<size_t>(ncols * 8, 8), nullptr);
+    if (ncols) CK(cudaMemcpyAsync(ptrs.get(), dh_ptr.data(), ncols * 8, cudaMemcpyHostToDevice, s));
+    DevBuf o(ctx, std::max<size_t>((size_t)P.n * 8, 8), nullptr);
+    launch_hash_columns(P, ncols, ptrs.get<const uint64_t*>(), o.get<uint64_t>(), s);
+    ctx->count_launch();
+    if (P.n) CK(cudaMemcpyAsync(out, o.get(), (size_t)P.n * 8,
+                                location == ML_LOC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    API_END
+}
+
+}  // extern "C"
+
+// =====================================================================================================
+// JoinBuildSink (join.rs:72-242)
+// =====================================================================================================
+struct ml_join_build {
+    Ctx* ctx;
+    Pipeline pipe;
+    std::vector<Prog> out_progs;
+    OwnedExprs keys;
+    std::vector<int> out_types;
+    std::mutex mu;
+    std::vector<std::unique_ptr<ml_batch>> parts;
+    std::unique_ptr<Reservation> res;
+    std::unique_ptr<ml_join_table> table;
+    ml_join_build(Ctx* c) : ctx(c), pipe(c) {}
+};
+struct ml_join_build_local {
+    ml_join_build* sink;
+    cudaStream_t s;
+    Staging st;
+    std::unique_ptr<ErrWord> ew;
+    ml_join_build_local(ml_join_build* k) : sink(k), s(k->ctx->new_stream()), st(k->ctx), ew(new ErrWord(k->ctx)) {}
+    ~ml_join_build_local() { sink->ctx->free_stream(s); }
+};
+
+extern "C" {
+
+int ml_gpu_join_build_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue, const int32_t* input_types,
+                             int32_t ninput, const ml_expr* key_exprs, int32_t nkeys, ml_join_build** out) {
+    API_BEGIN
+    REQUIRE(ctx && out && key_exprs && nkeys > 0, "bad arguments");
+    REQUIRE(nkeys <= kMaxKeys, "too many join keys");
+    ctx->set_current();
+    auto j = std::make_unique<ml_join_build>(ctx);
+    j->pipe.build(prologue, nprologue, input_types, ninput);
+    for (auto& r : j->pipe.out) j->out_types.push_back(r.dtype);
+    j->out_progs = compile_outputs(j->pipe);
+    j->pipe.upload();
+    for (int k = 0; k < nkeys; k++) {
+        if (key_exprs[k].dtype == ML_TYPE_UTF8) raise(ML_ERR_UNSUPPORTED, "string join keys on the GPU");
+        j->keys.add(key_exprs[k]);
+    }
+    j->keys.finish();
+    j->res = std::make_unique<Reservation>(ctx, "HashJoinBuild");
+    *out = j.release();
+    API_END
+}
+
+int ml_gpu_join_build_local_create(ml_join_build* sink, ml_join_build_local** out) {
+    API_BEGIN
+    REQUIRE(sink && out, "null argument");
+    sink->ctx->set_current();
+    *out = new ml_join_build_local(sink);
+    API_END
+}
+
+// BuildLocal::sink: compact the batch and keep it (join.rs:217-222)
+int ml_gpu_join_build_sink(ml_join_build_local* local, const ml_column* cols, int32_t ncols, int64_t nrows, const uint32_t* sel,
+                           int64_t nsel) {
+    API_BEGIN
+    REQUIRE(local, "null local sink");
+    ml_join_build* j = local->sink;
+    REQUIRE(!j->table, "join build sink already finalized");
+    Ctx* ctx = j->ctx;
+    ctx->set_current();
+    check_sel_bounds(sel, nsel, nrows);
+    DevBuf sel_hold;
+    const uint32_t* dsel = device_sel(ctx, sel, nsel, sel_hold, local->s);
+    Pipeline::Launch L;
+    j->pipe.prepare(L, cols, ncols, nrows, dsel, nsel, local->s, local->st, nullptr);
+    auto part = materialize(ctx, j->pipe, j->out_progs, L, local->s, j->res.get(), *local->ew);
+    CK(cudaMemcpyAsync(local->ew->h, local->ew->d.get(), 4, cudaMemcpyDeviceToHost, local->s));
+    CK(cudaStreamSynchronize(local->s));
+    check_device_error(ctx, j->pipe.nstages > 0 ? *local->ew->h : 0);
+    std::lock_guard<std::mutex> g(j->mu);
+    j->parts.push_back(std::move(part));
+    API_END
+}
+
+int ml_gpu_join_build_combine(ml_join_build_local* local) {
+    API_BEGIN
+    if (local) {
+        local->sink->ctx->set_current();
+        CK(cudaStreamSynchronize(local->s));
+        delete local;
+    }
+    API_END
+}
+
+// build_table (join.rs:160-203)
+int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
+    API_BEGIN
+    REQUIRE(j && table, "null argument");
+    Ctx* ctx = j->ctx;
+    ctx->set_current();
+    if (j->table) {
+        *table = j->table.get();
+        return ML_OK;
+    }
+    ctx->sync_all();
+    cudaStream_t s = ctx->stream;
+    auto jt = std::make_unique<ml_join_table>();
+    jt->ctx = ctx;
+    jt->res = std::make_unique<Reservation>(ctx, "HashJoinBuild(table)");
+    std::vector<std::unique_ptr<ml_batch>> parts;
+    {
+        std::lock_guard<std::mutex> g(j->mu);
+        parts = std::move(j->parts);
+    }
+    if (parts.empty()) {
+        auto e = std::make_unique<ml_batch>();
+        e->ctx = ctx;
+        for (int t : j->out_types) {
+            auto d = std::make_unique<DevColumn>();
+            d->dtype = t;
+            d->kind = t == ML_TYPE_UTF8 ? CK_UTF8 : CK_FIXED;
+            if (d->kind == CK_UTF8) {
+                d->offsets = DevBuf(ctx, 4, j->res.get());
+                CK(cudaMemsetAsync(d->offsets.get(), 0, 4, s));
+            }
+            d->data = DevBuf(ctx, 8, j->res.get());
+            e->cols.push_back(std::move(d));
+        }
+        parts.push_back(std::move(e));
+    }
+    auto merged = concat_batches(ctx, parts, j->out_types, s, j->res.get());
+    jt->batch.ctx = ctx;
+    jt->batch.nrows = merged->nrows;
+    jt->batch.cols = std::move(merged->cols);
+    int64_t n = jt->batch.nrows;
+    REQUIRE(n < 0xFFFFFFFFll, "build side larger than 2^32 rows");
+    for (int k = 0; k < (int)j->keys.exprs.size(); k++) jt->key_types.push_back(j->keys.exprs[k].dtype);
+    // key programs over the build batch
+    Pipeline kp(ctx);
+    kp.build(nullptr, 0, j->out_types.data(), (int)j->out_types.size());
+    KeyLayout L = kp.key_layout(j->keys.exprs.data(), (int)j->keys.exprs.size(), kp.out, false, nullptr);
+    kp.upload();
+    jt->nwords = L.nwords;
+    jt->cap = pow2_at_least(std::max<uint64_t>(16, (uint64_t)n * 2));
+    jt->state = DevBuf(ctx, jt->cap * 4, jt->res.get());
+    jt->keys = DevBuf(ctx, jt->cap * 8 * L.nwords, jt->res.get());
+    jt->payload = DevBuf(ctx, jt->cap * 4, jt->res.get());
+    jt->next = DevBuf(ctx, std::max<size_t>((size_t)n * 4, 4), jt->res.get());
+    jt->dup = DevBuf(ctx, 8, nullptr);
+    CK(cudaMemsetAsync(jt->state.get(), 0, jt->cap * 4, s));
+    CK(cudaMemsetAsync(jt->next.get(), 0xFF, std::max<size_t>((size_t)n * 4, 4), s));
+    CK(cudaMemsetAsync(jt->dup.get(), 0, 8, s));
+    Staging st(ctx);
+    Pipeline::Launch LA;
+    auto views = device_views(jt->batch);
+    kp.prepare(LA, views.data(), (int)views.size(), n, nullptr, 0, s, st, nullptr);
+    ErrWord ew(ctx);
+    CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
+    LA.P.err = ew.d.get<uint32_t>();
+    {
+        KernelTimer kt(ctx, s, "join_insert");
+        launch_join_insert(LA.P, L, jt->view(), jt->next.get<uint32_t>(), jt->dup.get<uint32_t>(), n, s);
+        kt.stop();
+    }
+    ctx->count_launch();
+    // canonical ids of the build side's strings (GROUP BY on a build-side string column)
+    for (auto& c : jt->batch.cols) {
+        if (c->kind != CK_UTF8 || n == 0) continue;
+        uint64_t cap = pow2_at_least(std::max<uint64_t>(16, (uint64_t)n * 2));
+        DevBuf tstate(ctx, cap * 4, nullptr), tkeys(ctx, cap * 8, nullptr), tpay(ctx, cap * 4, nullptr);
+        CK(cudaMemsetAsync(tstate.get(), 0, cap * 4, s));
+        TableView tv{tstate.get<uint32_t>(), tkeys.get<uint64_t>(), tpay.get<uint32_t>(), cap - 1, 1, 0};
+        c->strid = DevBuf(ctx, (size_t)n * 4, jt->res.get());
+        launch_strid(c->optr(), (const uint8_t*)c->dptr(), c->vptr(), n, tv, c->strid.get<uint32_t>(), ew.d.get<uint32_t>(), s);
+        ctx->count_launch();
+        CK(cudaStreamSynchronize(s));
+    }
+    uint32_t dup = 0;
+    CK(cudaMemcpyAsync(&dup, jt->dup.get(), 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(ew.h, ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    check_device_error(ctx, *ew.h);
+    jt->has_dups = dup != 0;
+    jt->distinct = -1;
+    j->table = std::move(jt);
+    *table = j->table.get();
+    API_END
+}
+
+int ml_gpu_join_table_stats(const ml_join_table* t, int64_t* build_rows, int64_t* distinct_keys, int64_t* capacity) {
+    API_BEGIN
+    REQUIRE(t, "null table");
+    t->ctx->set_current();
+    if (build_rows) *build_rows = t->batch.nrows;
+    if (capacity) *capacity = (int64_t)t->cap;
+    if (distinct_keys) {
+        std::vector<uint32_t> st(t->cap);
+        CK(cudaMemcpy(st.data(), t->state.get(), t->cap * 4, cudaMemcpyDeviceToHost));
+        int64_t d = 0;
+        for (uint32_t x : st) d += x != 0;
+        *distinct_keys = d;
+    }
+    API_END
+}
+
+int ml_gpu_join_build_destroy(ml_join_build* j) {
+    API_BEGIN
+    if (j) {
+        j->ctx->set_current();
+        j->ctx->sync_all();
+        delete j;
+    }
+    API_END
+}
+
+// HashJoinProbe::execute (join.rs:263-315): all (probe_row, build_row) pairs, by probe row.
+int ml_gpu_join_probe(ml_ctx* ctx, ml_join_table* table, const ml_expr* key_exprs, int32_t nkeys, const ml_column* cols,
+                      int32_t ncols, int64_t nrows, const uint32_t* sel, int64_t nsel, int32_t location, uint32_t* probe_idx,
+                      uint32_t* build_idx, int64_t cap, int64_t* npairs) {
+    API_BEGIN
+    REQUIRE(ctx && table && key_exprs && npairs, "null argument");
+    ctx->set_current();
+    std::lock_guard<std::mutex> g(ctx->op_mu);
+    cudaStream_t s = ctx->stream;
+    if (location == ML_LOC_HOST) check_sel_bounds(sel, nsel, nrows);
+    std::vector<int32_t> types;
+    for (int c = 0; c < ncols; c++) types.push_back(cols[c].dtype);
+    Pipeline p(ctx);
+    ml_pipe_op op{};
+    op.kind = ML_PIPE_PROBE;
+    op.nexprs = nkeys;
+    op.exprs = key_exprs;
+    op.join = table;
+    p.build(&op, 1, types.data(), ncols);
+    p.upload();
+    Staging st(ctx);
+    DevBuf sel_hold;
+    const uint32_t* dsel = device_sel(ctx, sel, nsel, sel_hold, s);
+    Pipeline::Launch L;
+    p.prepare(L, cols, ncols, nrows, dsel, nsel, s, st, nullptr);
+    ErrWord ew(ctx);
+    CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
+    L.P.err = ew.d.get<uint32_t>();
+    DevBuf counts(ctx, std::max<size_t>((size_t)L.P.n * 4, 4), nullptr);
+    launch_probe_count(L.P, counts.get<uint32_t>(), s);
+    ctx->count_launch();
+    DevBuf offs;
+    uint64_t total = scan_counts(ctx, counts.get<uint32_t>(), L.P.n, offs, s);
+    *npairs = (int64_t)total;
+    if ((int64_t)total > cap) raise(ML_ERR_INVALID, "pair buffer too small: " + std::to_string(total) + " pairs");
+    DevBuf pi(ctx, std::max<size_t>(total * 4, 4), nullptr), bi(ctx, std::max<size_t>(total * 4, 4), nullptr);
+    launch_probe_write(L.P, offs.get<uint64_t>(), pi.get<uint32_t>(), bi.get<uint32_t>(), s);
+    ctx->count_launch();
+    auto kind = location == ML_LOC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (total) {
+        REQUIRE(probe_idx && build_idx, "null pair buffers");
+        CK(cudaMemcpyAsync(probe_idx, pi.get(), total * 4, kind, s));
+        CK(cudaMemcpyAsync(build_idx, bi.get(), total * 4, kind, s));
+    }
+    CK(cudaMemcpyAsync(ew.h, ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    check_device_error(ctx, *ew.h);
+    API_END
+}
+
+}  // extern "C"
+
+// =====================================================================================================
+// HashAggregateSink (aggregate/hash.rs:434-634)
+// =====================================================================================================
+namespace {
+struct AggState {
+    int func, kind, arg_type, in_type, out_type;
+    bool has_arg;
+    Prog arg{};
+    bool vcnt_on = false;  // valid-input counts maintained (AVG always)
+    DevBuf v0, vcnt;
+};
+}  // namespace
+
+struct ml_hashagg {
+    Ctx* ctx;
+    Pipeline pipe;
+    KeyLayout keys{};
+    std::vector<KeyDecode> dec;
+    std::vector<AggState> aggs;
+    bool ungrouped = false;
+    double max_load = 0.5;
+    std::unique_ptr<Reservation> res;
+    std::shared_mutex rw;  // shared: a launch in flight; exclusive: table growth
+    uint64_t cap = 0;
+    uint32_t gid_cap = 0;
+    DevBuf state, tkeys, payload, gkeys, gnull, rows, ngroups;
+    int64_t resizes = 0;
+    int smem_groups = 256;
+    ml_hashagg(Ctx* c) : ctx(c), pipe(c) {}
+
+    AggArgs args(const Pipeline::Launch& L, unsigned long long* ovf_count, uint32_t* ovf, uint64_t ovf_cap) {
+        AggArgs A{};
+        A.keys = keys;
+        A.t = TableView{state.get<uint32_t>(), tkeys.get<uint64_t>(), payload.get<uint32_t>(), cap ? cap - 1 : 0, keys.nwords, 0};
+        A.gkeys = gkeys.get<uint64_t>();
+        A.gnull = gnull.get<uint32_t>();
+        A.ngroups = ngroups.get<uint32_t>();
+        A.gid_cap = gid_cap;
+        A.nagg = (int)aggs.size();
+        A.ungrouped = ungrouped;
+        A.smem_groups = std::min<int>(smem_groups, (int)gid_cap);
+        A.rows = rows.get<uint64_t>();
+        A.ovf = ovf;
+        A.ovf_count = ovf_count;
+        A.ovf_cap = ovf_cap;
+        for (size_t k = 0; k < aggs.size(); k++) {
+            AggDev& d = A.aggs[k];
+            const AggState& a = aggs[k];
+            d.kind = a.kind;
+            d.func = a.func;
+            d.has_arg = a.has_arg;
+            d.count_valid = a.vcnt_on;
+            d.arg = a.arg;
+            d.v0 = a.v0.get();
+            d.vcnt = a.vcnt.get<uint64_t>();
+        }
+        (void)L;
+        return A;
+    }
+
+    // Allocate (or grow to) `want` group ids; existing groups are rehashed into the new
+    // table (the doubling of SwissTable::reserve, swiss.rs:287-301).
+    void grow(uint32_t want, cudaStream_t s, ErrWord& ew) {
+        uint32_t old_cap = gid_cap;
+        uint64_t ncap = ungrouped ? 1 : pow2_at_least((uint64_t)std::ceil(std::max<uint32_t>(want, 8) / max_load));
+        uint32_t ngid = ungrouped ? 1 : (uint32_t)std::min<uint64_t>((uint64_t)(ncap * max_load), 0xFFFFFFF0ull);
+        uint32_t ng = 0;
+        if (old_cap) {
+            CK(cudaMemcpyAsync(ew.h, ngroups.get(), 4, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            ng = std::min(*ew.h, old_cap);
+        }
+        int nw = keys.nwords ? keys.nwords : 1;
+        DevBuf nstate, ntkeys, npay;
+        if (!ungrouped) {
+            nstate = DevBuf(ctx, ncap * 4, res.get());
+            ntkeys = DevBuf(ctx, ncap * 8 * nw, res.get());
+            npay = DevBuf(ctx, ncap * 4, res.get());
+            CK(cudaMemsetAsync(nstate.get(), 0, ncap * 4, s));
+        }
+        DevBuf ngk(ctx, (size_t)ngid * 8 * nw, res.get()), ngn(ctx, (size_t)ngid * 4, res.get());
+        DevBuf nrows(ctx, (size_t)ngid * 8, res.get());
+        std::vector<DevBuf> nv0(aggs.size()), nvc(aggs.size());
+        for (size_t k = 0; k < aggs.size(); k++) {
+            if (aggs[k].func != ML_AGG_COUNT_STAR) nv0[k] = DevBuf(ctx, (size_t)ngid * 8, res.get());
+            if (aggs[k].vcnt_on) nvc[k] = DevBuf(ctx, (size_t)ngid * 8, res.get());
+        }
+        if (old_cap) {  // keep the existing groups
+            for (int w = 0; w < nw; w++)
+                if (ng) CK(cudaMemcpyAsync(ngk.get<uint64_t>() + (size_t)w * ngid, gkeys.get<uint64_t>() + (size_t)w * old_cap,
+                                           (size_t)ng * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(ngn.get(), gnull.get(), (size_t)old_cap * 4, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(nrows.get(), rows.get(), (size_t)old_cap * 8, cudaMemcpyDeviceToDevice, s));
+            for (size_t k = 0; k < aggs.size(); k++) {
+                if (nv0[k]) CK(cudaMemcpyAsync(nv0[k].get(), aggs[k].v0.get(), (size_t)old_cap * 8, cudaMemcpyDeviceToDevice, s));
+                if (nvc[k]) CK(cudaMemcpyAsync(nvc[k].get(), aggs[k].vcnt.get(), (size_t)old_cap * 8, cudaMemcpyDeviceToDevice, s));
+            }
+        }
+        state = std::move(nstate);
+        tkeys = std::move(ntkeys);
+        payload = std::move(npay);
+        gkeys = std::move(ngk);
+        gnull = std::move(ngn);
+        rows = std::move(nrows);
+        for (size_t k = 0; k < aggs.size(); k++) {
+            aggs[k].v0 = std::move(nv0[k]);
+            aggs[k].vcnt = std::move(nvc[k]);
+        }
+        cap = ungrouped ? 0 : ncap;
+        gid_cap = ngid;
+        Pipeline::Launch none;
+        AggArgs A = args(none, nullptr, nullptr, 0);
+        launch_agg_init(A, old_cap, ngid, s);
+        ctx->count_launch();
+        if (!ungrouped && ng) {
+            CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
+            launch_agg_rehash(A.t, gkeys.get<uint64_t>(), gnull.get<uint32_t>(), gid_cap, ng, nw, ew.d.get<uint32_t>(), s);
+            ctx->count_launch();
+            CK(cudaMemcpyAsync(ew.h, ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
+        }
+        CK(cudaMemcpyAsync(ngroups.get(), &ng, 4, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+        if (!ungrouped && ng) check_device_error(ctx, *ew.h);
+    }
+};
+
+struct ml_hashagg_local {
+    ml_hashagg* sink;
+    cudaStream_t s;
+    Staging st;
+    ErrWord ew;
+    DevBuf ovf_count;  // u64
+    uint64_t* h_count;
+    ml_hashagg_local(ml_hashagg* k)
+        : sink(k), s(k->ctx->new_stream()), st(k->ctx), ew(k->ctx), ovf_count(k->ctx, 16, nullptr) {
+        h_count = (uint64_t*)k->ctx->halloc(16);
+    }
+    ~ml_hashagg_local() {
+        sink->ctx->hfree(h_count);
+        sink->ctx->free_stream(s);
+    }
+};
+
+extern "C" {
+
+int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue, const int32_t* input_types, int32_t ninput,
+                          const ml_expr* group_exprs, int32_t ngroup, const ml_agg_spec* aggs, int32_t nagg, int64_t size_hint,
+                          ml_hashagg** out) {
+    API_BEGIN
+    REQUIRE(ctx && out, "null argument");
+    REQUIRE(ngroup >= 0 && nagg >= 0 && (ngroup == 0 || group_exprs) && (nagg == 0 || aggs), "bad arguments");
+    REQUIRE(nagg <= kMaxAggs, "too many aggregates");
+    ctx->set_current();
+    auto h = std::make_unique<ml_hashagg>(ctx);
+    h->pipe.build(prologue, nprologue, input_types, ninput);
+    h->ungrouped = ngroup == 0;
+    if (!h->ungrouped) h->keys = h->pipe.key_layout(group_exprs, ngroup, h->pipe.out, true, &h->dec);
+    for (int k = 0; k < nagg; k++) {  // Accumulator::new (accumulator.rs:110-169)
+        AggState a{};
+        a.func = aggs[k].func;
+        a.arg_type = aggs[k].arg_type;
+        int t = a.arg_type;
+        auto bad = [&]() { raise(ML_ERR_UNSUPPORTED, "aggregate function " + std::to_string(a.func) + " over type " + std::to_string(t)); };
+        switch (a.func) {
+            case ML_AGG_COUNT_STAR: a.kind = A_COUNT; a.in_type = -1; a.out_type = ML_TYPE_INT64; break;
+            case ML_AGG_COUNT: a.kind = A_COUNT; a.in_type = t; a.out_type = ML_TYPE_INT64; break;
+            case ML_AGG_SUM:
+                if (t == ML_TYPE_INT32 || t == ML_TYPE_INT64 || t == ML_TYPE_BOOL) { a.kind = A_SUM_I64; a.in_type = ML_TYPE_INT64; a.out_type = ML_TYPE_INT64; }
+                else if (t == ML_TYPE_FLOAT64) { a.kind = A_SUM_F64; a.in_type = t; a.out_type = t; }
+                else bad();
+                break;
+            case ML_AGG_AVG:
+                if (t == ML_TYPE_INT32 || t == ML_TYPE_INT64 || t == ML_TYPE_FLOAT64) { a.kind = A_AVG; a.in_type = ML_TYPE_FLOAT64; a.out_type = ML_TYPE_FLOAT64; a.vcnt_on = true; }
+                else bad();
+                break;
+            case ML_AGG_MIN:
+            case ML_AGG_MAX: {
+                bool mn = a.func == ML_AGG_MIN;
+                if (t == ML_TYPE_INT32 || t == ML_TYPE_INT64 || t == ML_TYPE_DATE) { a.kind = mn ? A_MIN_I64 : A_MAX_I64; a.in_type = ML_TYPE_INT64; a.out_type = t; }
+                else if (t == ML_TYPE_FLOAT64) { a.kind = mn ? A_MIN_F64 : A_MAX_F64; a.in_type = t; a.out_type = t; }
+                else bad();
+                break;
+            }
+            default: bad();
+        }
+        a.has_arg = a.func != ML_AGG_COUNT_STAR;
+        if (a.has_arg) {
+            REQUIRE(aggs[k].arg.nnodes > 0, "aggregate without an argument");
+            ExprNode e = parse_expr(aggs[k].arg);
+            if (t == ML_TYPE_UTF8) {  // COUNT(string): only validity matters
+                int slot;
+                a.arg = h->pipe.C.compile_string_key(e, h->pipe.out, &slot);
+            } else {
+                a.arg = h->pipe.C.compile_value(e, h->pipe.out, t);
+                if (a.in_type >= 0 && a.in_type != t) {  // Accumulator::prepare_input cast
+                    Instr c{};
+                    c.op = I_CAST;
+                    c.sub = (uint8_t)a.in_type;
+                    c.t = (uint8_t)t;
+                    h->pipe.C.code.push_back(c);
+                    a.arg.len++;
+                    a.arg.type = a.in_type;
+                }
+            }
+        }
+        h->aggs.push_back(std::move(a));
+    }
+    h->pipe.upload();
+    h->res = std::make_unique<Reservation>(ctx, "HashAggregate");
+    h->ngroups = DevBuf(ctx, 16, nullptr);
+    CK(cudaMemset(h->ngroups.get(), 0, 16));
+    ErrWord ew(ctx);
+    uint32_t want = h->ungrouped ? 1 : (uint32_t)std::min<int64_t>(std::max<int64_t>(size_hint > 0 ? size_hint : 1024, 16), 0x7FFFFFFF);
+    h->grow(want, ctx->stream, ew);
+    *out = h.release();
+    API_END
+}
+
+int ml_gpu_hashagg_local_create(ml_hashagg* sink, ml_hashagg_local** out) {
+    API_BEGIN
+    REQUIRE(sink && out, "null argument");
+    sink->ctx->set_current();
+    *out = new ml_hashagg_local(sink);
+    API_END
+}
+
+int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t ncols, int64_t nrows, const uint32_t* sel,
+                        int64_t nsel) {
+    API_BEGIN
+    REQUIRE(local, "null local sink");
+    ml_hashagg* h = local->sink;
+    Ctx* ctx = h->ctx;
+    ctx->set_current();
+    cudaStream_t s = local->s;
+    check_sel_bounds(sel, nsel, nrows);
+    DevBuf sel_hold;
+    const uint32_t* dsel = device_sel(ctx, sel, nsel, sel_hold, s);
+    Pipeline::Launch L;
+    h->pipe.prepare(L, cols, ncols, nrows, dsel, nsel, s, local->st, nullptr);
+    for (const KeyDecode& d : h->dec)
+        if (d.str_kind == 1 && L.P.cols[d.slot].kind != CK_DICT)
+            raise(ML_ERR_UNSUPPORTED, "GROUP BY on a plain (not dictionary-encoded) string column of the source");
+    // seen-tracking: once an argument can be NULL, count valid inputs per group
+    for (auto& a : h->aggs) {
+        if (!a.has_arg || a.vcnt_on || a.kind == A_COUNT) continue;
+        if (a.arg.maybe_null || h->pipe.reads_nullable(a.arg, L)) {
+            std::unique_lock<std::shared_mutex> lk(h->rw);
+            if (!a.vcnt_on) {
+                ctx->sync_all();
+                a.vcnt = DevBuf(ctx, (size_t)h->gid_cap * 8, h->res.get());
+                CK(cudaMemcpyAsync(a.vcnt.get(), h->rows.get(), (size_t)h->gid_cap * 8, cudaMemcpyDeviceToDevice, s));
+                CK(cudaStreamSynchronize(s));
+                a.vcnt_on = true;
+            }
+        }
+    }
+    int w = 1 + (int)h->pipe.probes.size();
+    uint64_t ovf_cap = std::max<uint64_t>((uint64_t)L.P.n, 1024);
+    DevBuf ovf(ctx, ovf_cap * w * 4, nullptr);
+    uint64_t count;
+    {
+        std::shared_lock<std::shared_mutex> lk(h->rw);
+        CK(cudaMemsetAsync(local->ovf_count.get(), 0, 8, s));
+        CK(cudaMemsetAsync(local->ew.d.get(), 0, 4, s));
+        L.P.err = local->ew.d.get<uint32_t>();
+        AggArgs A = h->args(L, local->ovf_count.get<unsigned long long>(), ovf.get<uint32_t>(), ovf_cap);
+        KernelTimer kt(ctx, s, "pipeline_aggregate");
+        launch_agg(L.P, A, agg_smem_bytes(A), s);
+        kt.stop();
+        ctx->count_launch();
+        CK(cudaMemcpyAsync(local->h_count, local->ovf_count.get(), 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(local->ew.h, local->ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        check_device_error(ctx, *local->ew.h);
+        count = *local->h_count;
+    }
+    // resize-on-overflow: grow the table, then aggregate the rows that did not fit
+    while (count) {
+        std::unique_lock<std::shared_mutex> lk(h->rw);
+        ctx->sync_all();
+        CK(cudaMemcpyAsync(local->ew.h, h->ngroups.get(), 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        uint32_t ng = std::min(*local->ew.h, h->gid_cap);
+        uint64_t want = std::max<uint64_t>((uint64_t)h->gid_cap * 2, (uint64_t)ng + std::min<uint64_t>(count, 1ull << 30));
+        h->grow((uint32_t)std::min<uint64_t>(want, 0x7FFFFFFFull), s, local->ew);
+        h->resizes++;
+        DevBuf ovf2(ctx, count * w * 4, nullptr);
+        CK(cudaMemsetAsync(local->ovf_count.get(), 0, 8, s));
+        CK(cudaMemsetAsync(local->ew.d.get(), 0, 4, s));
+        L.P.err = local->ew.d.get<uint32_t>();
+        AggArgs A = h->args(L, local->ovf_count.get<unsigned long long>(), ovf2.get<uint32_t>(), count);
+        launch_agg_resume(L.P, A, ovf.get<uint32_t>(), count, w, agg_smem_bytes(A), s);
+        ctx->count_launch();
+        CK(cudaMemcpyAsync(local->h_count, local->ovf_count.get(), 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(local->ew.h, local->ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        check_device_error(ctx, *local->ew.h);
+        count = *local->h_count;
+        ovf = std::move(ovf2);
+    }
+    API_END
+}
+
+int ml_gpu_hashagg_combine(ml_hashagg_local* local) {
+    API_BEGIN
+    if (local) {  // every local sink updates the one device table: combine only waits
+        local->sink->ctx->set_current();
+        CK(cudaStreamSynchronize(local->s));
+        delete local;
+    }
+    API_END
+}
+
+// Sink::finalize -> final_batches (aggregate/hash.rs:307-314)
+int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
+    API_BEGIN
+    REQUIRE(h && out, "null argument");
+    Ctx* ctx = h->ctx;
+    ctx->set_current();
+    std::unique_lock<std::shared_mutex> lk(h->rw);
+    ctx->sync_all();
+    cudaStream_t s = ctx->stream;
+    uint32_t ng = 1;
+    if (!h->ungrouped) {
+        CK(cudaMemcpy(&ng, h->ngroups.get(), 4, cudaMemcpyDeviceToHost));
+        ng = std::min(ng, h->gid_cap);
+    }
+    auto b = std::make_unique<ml_batch>();
+    b->ctx = ctx;
+    b->nrows = ng;
+    b->res = std::make_unique<Reservation>(ctx, "HashAggregate(output)");
+    FinalArgs F{};
+    F.ngroups = ng;
+    F.gid_cap = h->gid_cap;
+    F.nkeys = h->ungrouped ? 0 : h->keys.nkeys;
+    F.nagg = (int)h->aggs.size();
+    F.ungrouped = h->ungrouped;
+    F.gkeys = h->gkeys.get<uint64_t>();
+    F.gnull = h->gnull.get<uint32_t>();
+    F.rows = h->rows.get<uint64_t>();
+    size_t vbytes = std::max<size_t>((size_t)(ng + 63) / 64 * 8, 8);
+    std::vector<std::unique_ptr<DevColumn>> keycols, aggcols;
+    std::vector<DevBuf> id_bufs(F.nkeys);
+    for (int k = 0; k < F.nkeys; k++) {
+        F.f[k] = h->keys.f[k];
+        auto d = std::make_unique<DevColumn>();
+        d->dtype = h->dec[k].type;
+        d->kind = CK_FIXED;
+        d->n = ng;
+        d->validity = DevBuf(ctx, vbytes, b->res.get());
+        CK(cudaMemsetAsync(d->validity.get(), 0, vbytes, s));
+        if (h->dec[k].str_kind) {
+            id_bufs[k] = DevBuf(ctx, std::max<size_t>((size_t)ng * 4, 4), nullptr);
+            F.key_out[k] = id_bufs[k].get();
+        } else {
+            d->data = DevBuf(ctx, std::max<size_t>((size_t)ng * width_of(d->dtype), 8), b->res.get());
+            F.key_out[k] = d->data.get();
+        }
+        F.key_valid[k] = d->validity.get<uint32_t>();
+        keycols.push_back(std::move(d));
+    }
+    for (int k = 0; k < F.nagg; k++) {
+        const AggState& a = h->aggs[k];
+        AggDev& ad = F.aggs[k];
+        ad.kind = a.kind;
+        ad.func = a.func;
+        ad.v0 = a.v0.get();
+        ad.vcnt = a.vcnt_on ? a.vcnt.get<uint64_t>() : nullptr;
+        F.out_type[k] = a.out_type;
+        auto d = std::make_unique<DevColumn>();
+        d->dtype = a.out_type;
+        d->kind = CK_FIXED;
+        d->n = ng;
+        d->data = DevBuf(ctx, std::max<size_t>((size_t)ng * width_of(a.out_type), 8), b->res.get());
+        d->validity = DevBuf(ctx, vbytes, b->res.get());
+        CK(cudaMemsetAsync(d->validity.get(), 0, vbytes, s));
+        F.agg_out[k] = d->data.get();
+        F.agg_valid[k] = d->validity.get<uint32_t>();
+        aggcols.push_back(std::move(d));
+    }
+    launch_agg_final(F, s);
+    ctx->count_launch();
+    CK(cudaStreamSynchronize(s));
+    // string keys: dictionary ids decode on the host, build-side ids gather on the device
+    for (int k = 0; k < F.nkeys; k++) {
+        const KeyDecode& d = h->dec[k];
+        if (!d.str_kind) continue;
+        auto& kc = keycols[k];
+        kc->kind = CK_UTF8;
+        if (d.str_kind == 1) {
+            std::vector<uint32_t> ids(ng);
+            if (ng) CK(cudaMemcpy(ids.data(), id_bufs[k].get(), (size_t)ng * 4, cudaMemcpyDeviceToHost));
+            std::vector<uint64_t> valid((ng + 63) / 64 + 1, 0);
+            if (ng) CK(cudaMemcpy(valid.data(), kc->validity.get(), (size_t)(ng + 63) / 64 * 8, cudaMemcpyDeviceToHost));
+            std::vector<uint32_t> off(ng + 1, 0);
+            std::string bytes;
+            {
+                std::lock_guard<std::mutex> g(h->pipe.intern.mu);
+                for (uint32_t g2 = 0; g2 < ng; g2++) {
+                    bool v = (valid[g2 / 64] >> (g2 % 64)) & 1;
+                    if (v) bytes += h->pipe.intern.strs.at(ids[g2]);
+                    off[g2 + 1] = (uint32_t)bytes.size();
+                }
+            }
+            kc->offsets = DevBuf(ctx, (size_t)(ng + 1) * 4, b->res.get());
+            kc->data = DevBuf(ctx, std::max<size_t>(bytes.size(), 1), b->res.get());
+            CK(cudaMemcpy(kc->offsets.get(), off.data(), (size_t)(ng + 1) * 4, cudaMemcpyHostToDevice));
+            if (!bytes.empty()) CK(cudaMemcpy(kc->data.get(), bytes.data(), bytes.size(), cudaMemcpyHostToDevice));
+        } else {
+            const DevColumn& src = *h->pipe.probes[d.build].jt->batch.cols[d.build_col];
+            DevColumn tmp;
+            gather_utf8(ctx, src.optr(), (const uint8_t*)src.dptr(), id_bufs[k].get<uint32_t>(), ng, tmp, s, b->res.get());
+            kc->offsets = std::move(tmp.offsets);
+            kc->data = std::move(tmp.data);
+            CK(cudaStreamSynchronize(s));
+        }
+    }
+    for (auto& c : keycols) b->cols.push_back(std::move(c));
+    for (auto& c : aggcols) b->cols.push_back(std::move(c));
+    *out = b.release();
+    API_END
+}
+
+int ml_gpu_hashagg_stats(ml_hashagg* h, int64_t* groups, int64_t* capacity, int64_t* resizes) {
+    API_BEGIN
+    REQUIRE(h, "null sink");
+    h->ctx->set_current();
+    if (groups) {
+        uint32_t ng = 1;
+        if (!h->ungrouped) {
+            CK(cudaMemcpy(&ng, h->ngroups.get(), 4, cudaMemcpyDeviceToHost));
+            ng = std::min(ng, h->gid_cap);
+        }
+        *groups = ng;
+    }
+    if (capacity) *capacity = (int64_t)h->cap;
+    if (resizes) *resizes = h->resizes;
+    API_END
+}
+
+int ml_gpu_hashagg_destroy(ml_hashagg* h) {
+    API_BEGIN
+    if (h) {
+        h->ctx->set_current();
+        h->ctx->sync_all();
+        delete h;
+    }
+    API_END
+}
+
+}  // extern "C"
+
+// =====================================================================================================
+// SortSink with a limit (sort.rs:145-267)
+// =====================================================================================================
+struct ml_topn {
+    Ctx* ctx;
+    Pipeline pipe;
+    std::vector<Prog> out_progs;
+    std::vector<SortKeySpec> keys;
+    std::vector<int> out_types;
+    int64_t limit;
+    std::mutex mu;
+    std::vector<std::unique_ptr<ml_batch>> cands;
+    std::unique_ptr<Reservation> res;
+    ml_topn(Ctx* c) : ctx(c), pipe(c) {}
+};
+struct ml_topn_local {
+    ml_topn* sink;
+    cudaStream_t s;
+    Staging st;
+    std::unique_ptr<ErrWord> ew;
+    ml_topn_local(ml_topn* k) : sink(k), s(k->ctx->new_stream()), st(k->ctx), ew(new ErrWord(k->ctx)) {}
+    ~ml_topn_local() { sink->ctx->free_stream(s); }
+};
+
+extern "C" {
+
+int ml_gpu_topn_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue, const int32_t* input_types, int32_t ninput,
+                       const ml_sort_key* keys, int32_t nkeys, int64_t limit, ml_topn** out) {
+    API_BEGIN
+    REQUIRE(ctx && out && keys && nkeys > 0, "bad arguments");
+    REQUIRE(nkeys <= kMaxKeys, "too many sort keys");
+    REQUIRE(limit >= 0 && limit <= kMaxTopN, "limit out of range (0..2048)");
+    ctx->set_current();
+    auto t = std::make_unique<ml_topn>(ctx);
+    t->pipe.build(prologue, nprologue, input_types, ninput);
+    for (auto& r : t->pipe.out) t->out_types.push_back(r.dtype);
+    t->out_progs = compile_outputs(t->pipe);
+    t->pipe.upload();
+    for (int k = 0; k < nkeys; k++)
+        t->keys.push_back(SortKeySpec{parse_expr(keys[k].expr), keys[k].expr.dtype, keys[k].asc != 0, keys[k].nulls_first != 0});
+    t->limit = limit;
+    t->res = std::make_unique<Reservation>(ctx, "Sort");
+    *out = t.release();
+    API_END
+}
+
+int ml_gpu_topn_local_create(ml_topn* sink, ml_topn_local** out) {
+    API_BEGIN
+    REQUIRE(sink && out, "null argument");
+    sink->ctx->set_current();
+    *out = new ml_topn_local(sink);
+    API_END
+}
+
+// SortLocal::sink + truncate: keep only this batch's best `limit` rows
+int ml_gpu_topn_sink(ml_topn_local* local, const ml_column* cols, int32_t ncols, int64_t nrows, const uint32_t* sel, int64_t nsel) {
+    API_BEGIN
+    REQUIRE(local, "null local sink");
+    ml_topn* t = local->sink;
+    Ctx* ctx = t->ctx;
+    ctx->set_current();
+    check_sel_bounds(sel, nsel, nrows);
+    DevBuf sel_hold;
+    const uint32_t* dsel = device_sel(ctx, sel, nsel, sel_hold, local->s);
+    Pipeline::Launch L;
+    t->pipe.prepare(L, cols, ncols, nrows, dsel, nsel, local->s, local->st, nullptr);
+    auto part = materialize(ctx, t->pipe, t->out_progs, L, local->s, nullptr, *local->ew);
+    auto best = topn_batch(ctx, *part, t->keys, t->limit, local->s, t->res.get());
+    std::lock_guard<std::mutex> g(t->mu);
+    t->cands.push_back(std::move(best));
+    API_END
+}
+
+int ml_gpu_topn_combine(ml_topn_local* local) {
+    API_BEGIN
+    if (local) {
+        local->sink->ctx->set_current();
+        CK(cudaStreamSynchronize(local->s));
+        delete local;
+    }
+    API_END
+}
+
+int ml_gpu_topn_finalize(ml_topn* t, ml_batch** out) {
+    API_BEGIN
+    REQUIRE(t && out, "null argument");
+    Ctx* ctx = t->ctx;
+    ctx->set_current();
+    ctx->sync_all();
+    std::vector<std::unique_ptr<ml_batch>> cands;
+    {
+        std::lock_guard<std::mutex> g(t->mu);
+        cands = std::move(t->cands);
+    }
+    cudaStream_t s = ctx->stream;
+    std::unique_ptr<ml_batch> all;
+    if (cands.empty()) {
+        all = std::make_unique<ml_batch>();
+        all->ctx = ctx;
+        for (int ty : t->out_types) {
+            auto d = std::make_unique<DevColumn>();
+            d->dtype = ty;
+            d->kind = ty == ML_TYPE_UTF8 ? CK_UTF8 : CK_FIXED;
+            d->n = 0;
+            if (d->kind == CK_UTF8) {
+                d->offsets = DevBuf(ctx, 4, nullptr);
+                CK(cudaMemsetAsync(d->offsets.get(), 0, 4, s));
+            }
+            d->data = DevBuf(ctx, 8, nullptr);
+            all->cols.push_back(std::move(d));
+        }
+    } else {
+        all = concat_batches(ctx, cands, t->out_types, s, nullptr);
+    }
+    auto res = std::make_unique<Reservation>(ctx, "Sort(output)");
+    auto best = topn_batch(ctx, *all, t->keys, t->limit, s, res.get());
+    best->res = std::move(res);
+    *out = best.release();
+    API_END
+}
+
+int ml_gpu_topn_destroy(ml_topn* t) {
+    API_BEGIN
+    if (t) {
+        t->ctx->set_current();
+        t->ctx->sync_all();
+        delete t;
+    }
+    API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,921 @@
+// sm_100a kernels of the MiniLake execution core.
+//
+// All of MiniLake's hot-path operators are HBM-bandwidth or L2-latency bound
+// integer/byte/FP64 work: nothing here is a dense contraction, so there is no
+// tensor-core code.  The design rules are the ones that matter for HBM-bound
+// kernels on B200: one pass over each column with coalesced loads, grids sized
+// as a multiple of the 148 SMs, state that fits in L2 (126 MB) kept there, and
+// shared-memory privatization wherever many rows hit few addresses.
+#include <cuda/atomic>
+
+#include "ml_device.cuh"
+#include "ml_kernels.cuh"
+
+namespace mlg {
+
+namespace {
+constexpr int kThreads = 256;
+int g_sms = 0;
+int num_sms() {
+    if (!g_sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (g_sms <= 0) g_sms = 148;
+    }
+    return g_sms;
+}
+int grid_for(int64_t n, int per_sm = 8) {
+    int64_t want = (n + kThreads - 1) / kThreads;
+    int64_t cap = (int64_t)num_sms() * per_sm;
+    if (want < 1) want = 1;
+    return (int)(want < cap ? want : cap);
+}
+
+__device__ __forceinline__ EvalEnv env_of(const PipeArgs& P) {
+    return EvalEnv{P.cols, P.prog, P.arena, P.luts};
+}
+
+__device__ __forceinline__ uint32_t get_cur(const uint32_t (&c)[4], int p) {
+    switch (p) {
+        case 0: return c[0];
+        case 1: return c[1];
+        case 2: return c[2];
+        default: return c[3];
+    }
+}
+__device__ __forceinline__ void set_cur(uint32_t (&c)[4], int p, uint32_t v) {
+    switch (p) {
+        case 0: c[0] = v; break;
+        case 1: c[1] = v; break;
+        case 2: c[2] = v; break;
+        default: c[3] = v; break;
+    }
+}
+
+// Run the streaming stages for one source row; call sink(ctx) for every surviving
+// (row, build matches...) combination.  Duplicate build keys are walked through their
+// chains with backtracking, like HashJoinProbe's chain walk (join.rs:297-309).
+template <class Sink>
+__device__ __forceinline__ void run_stages(const PipeArgs& P, const EvalEnv& env, RowCtx& x, Sink&& sink) {
+    uint32_t cur[4] = {kNone, kNone, kNone, kNone};
+    int s = 0;
+    for (;;) {
+        bool advance = false;
+        if (s == P.nstages) {
+            sink(x);
+        } else {
+            const Stage st = P.stages[s];
+            if (st.kind == 0) {
+                uint64_t v;
+                bool ok;
+                eval_prog(env, P.filters[st.idx], x, v, ok);
+                advance = ok && (v & 1);
+            } else {
+                const ProbeDev& pd = P.probes[st.idx];
+                uint64_t w[2];
+                uint32_t nm;
+                if (make_key(env, pd.keys, x, w, &nm, true)) {
+                    uint32_t b = table_find(pd.t, w, key_hash(w, pd.t.nwords));
+                    if (b != kNone) {
+                        x.set_build(st.idx, b);
+                        set_cur(cur, st.idx, pd.next ? __ldg(pd.next + b) : kNone);
+                        advance = true;
+                    }
+                }
+            }
+        }
+        if (advance) {
+            s++;
+            continue;
+        }
+        int q = s - 1;
+        for (; q >= 0; q--) {
+            const Stage st = P.stages[q];
+            if (st.kind != 1) continue;
+            uint32_t c = get_cur(cur, st.idx);
+            if (c != kNone) {
+                x.set_build(st.idx, c);
+                set_cur(cur, st.idx, __ldg(P.probes[st.idx].next + c));
+                break;
+            }
+        }
+        if (q < 0) return;
+        s = q + 1;
+    }
+}
+
+// ---- hash aggregation ---------------------------------------------------------------------
+struct SmemAgg {
+    uint32_t* rows;        // [SG]
+    uint64_t* v[kMaxAggs]; // [SG] value words
+    uint32_t* c[kMaxAggs]; // [SG] valid counts
+};
+
+__device__ __forceinline__ uint64_t agg_identity(int kind) {
+    switch (kind) {
+        case A_MIN_I64: return 0x7FFFFFFFFFFFFFFFull;
+        case A_MAX_I64: return 0x8000000000000000ull;
+        case A_MIN_F64: return ~0ull;
+        case A_MAX_F64: return 0ull;
+        default: return 0ull;
+    }
+}
+
+__device__ __forceinline__ void acc_global(const AggDev& a, uint32_t g, uint64_t v) {
+    switch (a.kind) {
+        case A_SUM_I64: atomicAdd((unsigned long long*)a.v0 + g, (unsigned long long)v); break;
+        case A_SUM_F64:
+        case A_AVG: atomicAdd((double*)a.v0 + g, as_f64(v)); break;
+        case A_MIN_I64: atomicMin((long long*)a.v0 + g, (long long)v); break;
+        case A_MAX_I64: atomicMax((long long*)a.v0 + g, (long long)v); break;
+        case A_MIN_F64: atomicMin((unsigned long long*)a.v0 + g, (unsigned long long)f64_order(as_f64(v))); break;
+        case A_MAX_F64: atomicMax((unsigned long long*)a.v0 + g, (unsigned long long)f64_order(as_f64(v))); break;
+        default: atomicAdd((unsigned long long*)a.v0 + g, 1ull); break;  // COUNT(x)
+    }
+}
+__device__ __forceinline__ void acc_shared(int kind, uint64_t* slot, uint64_t v) {
+    switch (kind) {
+        case A_SUM_I64: atomicAdd((unsigned long long*)slot, (unsigned long long)v); break;
+        case A_SUM_F64:
+        case A_AVG: atomicAdd((double*)slot, as_f64(v)); break;
+        case A_MIN_I64: atomicMin((long long*)slot, (long long)v); break;
+        case A_MAX_I64: atomicMax((long long*)slot, (long long)v); break;
+        case A_MIN_F64: atomicMin((unsigned long long*)slot, (unsigned long long)f64_order(as_f64(v))); break;
+        case A_MAX_F64: atomicMax((unsigned long long*)slot, (unsigned long long)f64_order(as_f64(v))); break;
+        default: atomicAdd((unsigned long long*)slot, 1ull); break;
+    }
+}
+
+__device__ void record_overflow(const PipeArgs& P, const AggArgs& A, const RowCtx& x) {
+    unsigned long long k = atomicAdd(A.ovf_count, 1ull);
+    if (k >= A.ovf_cap) {
+        atomicOr(P.err, (uint32_t)DE_OVERFLOW_LOST);
+        return;
+    }
+    int w = 1 + P.nprobes;
+    uint32_t* o = A.ovf + k * (uint64_t)w;
+    o[0] = x.r;
+    if (w > 1) o[1] = x.b0;
+    if (w > 2) o[2] = x.b1;
+    if (w > 3) o[3] = x.b2;
+    if (w > 4) o[4] = x.b3;
+}
+
+__device__ __forceinline__ void agg_update(const PipeArgs& P, const AggArgs& A, const EvalEnv& env, const RowCtx& x,
+                                           const SmemAgg& S) {
+    uint32_t g = 0;
+    if (!A.ungrouped) {
+        uint64_t w[2];
+        uint32_t nm;
+        make_key(env, A.keys, x, w, &nm, false);
+        uint64_t h = key_hash(w, A.keys.nwords, nm);
+        bool inserted;
+        uint64_t slot;
+        g = table_upsert(
+            A.t, w, nm, h, P.err,
+            [&]() -> uint32_t {
+                uint32_t id = atomicAdd(A.ngroups, 1u);
+                return id < A.gid_cap ? id : kNone;
+            },
+            &inserted, &slot);
+        if (g == kNone) {
+            record_overflow(P, A, x);
+            return;
+        }
+        if (inserted) {
+            A.gkeys[g] = w[0];
+            if (A.keys.nwords > 1) A.gkeys[(uint64_t)A.gid_cap + g] = w[1];
+            A.gnull[g] = nm;
+        }
+    }
+    bool local = (int)g < A.smem_groups;
+    if (local) atomicAdd(S.rows + g, 1u);
+    else atomicAdd((unsigned long long*)A.rows + g, 1ull);
+    for (int k = 0; k < A.nagg; k++) {
+        const AggDev& a = A.aggs[k];
+        if (a.func == ML_AGG_COUNT_STAR) continue;  // COUNT(*) is the row counter
+        uint64_t v = 0;
+        bool ok = true;
+        if (a.has_arg) eval_prog(env, a.arg, x, v, ok);
+        if (!ok) continue;
+        if (local) {
+            acc_shared(a.kind, S.v[k] + g, v);
+            if (a.count_valid) atomicAdd(S.c[k] + g, 1u);
+        } else {
+            acc_global(a, g, v);
+            if (a.count_valid) atomicAdd((unsigned long long*)a.vcnt + g, 1ull);
+        }
+    }
+}
+
+__device__ void smem_setup(const AggArgs& A, SmemAgg& S, uint8_t* base) {
+    int SG = A.smem_groups;
+    S.rows = (uint32_t*)base;
+    uint8_t* p = base + (((size_t)SG * 4 + 15) & ~(size_t)15);
+    for (int k = 0; k < A.nagg; k++) {
+        S.v[k] = (uint64_t*)p;
+        p += (size_t)SG * 8;
+        S.c[k] = (uint32_t*)p;
+        p += (((size_t)SG * 4 + 15) & ~(size_t)15);
+    }
+    for (int g = threadIdx.x; g < SG; g += blockDim.x) {
+        S.rows[g] = 0;
+        for (int k = 0; k < A.nagg; k++) {
+            S.v[k][g] = agg_identity(A.aggs[k].kind);
+            S.c[k][g] = 0;
+        }
+    }
+}
+
+__device__ void smem_flush(const AggArgs& A, const SmemAgg& S) {
+    int SG = A.smem_groups;
+    for (int g = threadIdx.x; g < SG; g += blockDim.x) {
+        uint32_t r = S.rows[g];
+        if (!r) continue;
+        atomicAdd((unsigned long long*)A.rows + g, (unsigned long long)r);
+        for (int k = 0; k < A.nagg; k++) {
+            const AggDev& a = A.aggs[k];
+            if (a.func == ML_AGG_COUNT_STAR) continue;
+            if (a.count_valid && S.c[k][g]) atomicAdd((unsigned long long*)a.vcnt + g, (unsigned long long)S.c[k][g]);
+            uint64_t v = S.v[k][g];
+            switch (a.kind) {
+                case A_COUNT: if (v) atomicAdd((unsigned long long*)a.v0 + g, (unsigned long long)v); break;
+                case A_SUM_I64: atomicAdd((unsigned long long*)a.v0 + g, (unsigned long long)v); break;
+                case A_SUM_F64:
+                case A_AVG: atomicAdd((double*)a.v0 + g, as_f64(v)); break;
+                case A_MIN_I64: atomicMin((long long*)a.v0 + g, (long long)v); break;
+                case A_MAX_I64: atomicMax((long long*)a.v0 + g, (long long)v); break;
+                case A_MIN_F64: atomicMin((unsigned long long*)a.v0 + g, (unsigned long long)v); break;
+                case A_MAX_F64: atomicMax((unsigned long long*)a.v0 + g, (unsigned long long)v); break;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_agg(const __grid_constant__ PipeArgs P, const __grid_constant__ AggArgs A) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    SmemAgg S;
+    smem_setup(A, S, smem);
+    __syncthreads();
+    const EvalEnv env = env_of(P);
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {
+        RowCtx x;
+        x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        x.b0 = x.b1 = x.b2 = x.b3 = 0;
+        run_stages(P, env, x, [&](const RowCtx& c) { agg_update(P, A, env, c, S); });
+    }
+    __syncthreads();
+    smem_flush(A, S);
+}
+
+__global__ void __launch_bounds__(kThreads) k_agg_resume(const __grid_constant__ PipeArgs P, const __grid_constant__ AggArgs A,
+                                                         const uint32_t* ctx, uint64_t count, int w) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    SmemAgg S;
+    smem_setup(A, S, smem);
+    __syncthreads();
+    const EvalEnv env = env_of(P);
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const uint32_t* c = ctx + i * (uint64_t)w;
+        RowCtx x;
+        x.r = c[0];
+        x.b0 = w > 1 ? c[1] : 0;
+        x.b1 = w > 2 ? c[2] : 0;
+        x.b2 = w > 3 ? c[3] : 0;
+        x.b3 = w > 4 ? c[4] : 0;
+        agg_update(P, A, env, x, S);
+    }
+    __syncthreads();
+    smem_flush(A, S);
+}
+
+__global__ void k_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
+                             int nwords, uint32_t* err) {
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroups) return;
+    uint64_t w[2] = {gkeys[g], nwords > 1 ? gkeys[(uint64_t)gid_cap + g] : 0ull};
+    uint32_t nm = gnull[g];
+    bool inserted;
+    uint64_t slot;
+    table_upsert(t, w, nm, key_hash(w, nwords, nm), err, [&]() { return g; }, &inserted, &slot);
+}
+
+__global__ void k_agg_init(AggArgs A, uint32_t from, uint32_t to) {
+    uint32_t g = from + blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= to) return;
+    A.rows[g] = 0;
+    for (int k = 0; k < A.nagg; k++) {
+        const AggDev& a = A.aggs[k];
+        if (a.func != ML_AGG_COUNT_STAR) ((uint64_t*)a.v0)[g] = agg_identity(a.kind);
+        if (a.vcnt) a.vcnt[g] = 0;
+    }
+}
+
+// Final values (accumulator.rs:500-526): AVG = sum / count, empty -> NULL.
+__global__ void k_agg_final(const __grid_constant__ FinalArgs F) {
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    bool in = g < F.ngroups;
+    uint32_t lane = threadIdx.x & 31;
+    for (int k = 0; k < F.nkeys; k++) {
+        const KeyField f = F.f[k];
+        bool valid = true;
+        if (in) {
+            uint64_t w = F.gkeys[(uint64_t)f.word * F.gid_cap + g];
+            valid = !((F.gnull[g] >> k) & 1u);
+            uint64_t m = f.width >= 64 ? ~0ull : ((1ull << f.width) - 1);
+            uint64_t v = (w >> f.shift) & m;
+            if (f.strid) ((uint32_t*)F.key_out[k])[g] = (uint32_t)v;
+            else if (f.type == ML_TYPE_BOOL) ((uint8_t*)F.key_out[k])[g] = (uint8_t)v;
+            else if (f.type == ML_TYPE_INT32 || f.type == ML_TYPE_DATE) ((int32_t*)F.key_out[k])[g] = (int32_t)(uint32_t)v;
+            else ((uint64_t*)F.key_out[k])[g] = v;
+        }
+        uint32_t bits = __ballot_sync(0xFFFFFFFFu, in && valid);
+        if (lane == 0 && (g >> 5) < (F.ngroups + 31) / 32) F.key_valid[k][g >> 5] = bits;
+    }
+    for (int k = 0; k < F.nagg; k++) {
+        const AggDev& a = F.aggs[k];
+        bool valid = false;
+        if (in) {
+            uint64_t rows = F.rows[g];
+            uint64_t vc = a.vcnt ? a.vcnt[g] : rows;
+            if (a.func == ML_AGG_COUNT_STAR) {
+                ((int64_t*)F.agg_out[k])[g] = (int64_t)rows;
+                valid = true;
+            } else if (a.func == ML_AGG_COUNT) {
+                ((int64_t*)F.agg_out[k])[g] = (int64_t)((uint64_t*)a.v0)[g];
+                valid = true;
+            } else {
+                uint64_t v = ((uint64_t*)a.v0)[g];
+                valid = vc > 0;
+                switch (a.kind) {
+                    case A_AVG: {
+                        double s = as_f64(v);
+                        double r = vc == 0 ? 0.0 : __ddiv_rn(s, __ll2double_rn((long long)vc));
+                        ((double*)F.agg_out[k])[g] = r;
+                        break;
+                    }
+                    case A_MIN_F64:
+                    case A_MAX_F64: ((double*)F.agg_out[k])[g] = valid ? f64_unorder(v) : 0.0; break;
+                    case A_MIN_I64:
+                    case A_MAX_I64:
+                        if (F.out_type[k] == ML_TYPE_INT32 || F.out_type[k] == ML_TYPE_DATE)
+                            ((int32_t*)F.agg_out[k])[g] = valid ? (int32_t)(int64_t)v : 0;
+                        else
+                            ((int64_t*)F.agg_out[k])[g] = valid ? (int64_t)v : 0;
+                        break;
+                    default: ((uint64_t*)F.agg_out[k])[g] = v; break;
+                }
+            }
+        }
+        uint32_t bits = __ballot_sync(0xFFFFFFFFu, in && valid);
+        if (lane == 0 && (g >> 5) < (F.ngroups + 31) / 32) F.agg_valid[k][g >> 5] = bits;
+    }
+}
+
+// ---- filter: pass bits + per-block counts, then ordered compaction ---------------------------
+constexpr int kSelRowsPerBlock = kThreads * 8;
+
+__global__ void __launch_bounds__(kThreads) k_select_flags(const __grid_constant__ PipeArgs P, uint32_t* bits,
+                                                           uint32_t* block_counts) {
+    const EvalEnv env = env_of(P);
+    int64_t base = (int64_t)blockIdx.x * kSelRowsPerBlock;
+    uint32_t cnt = 0;
+    for (int it = 0; it < 8; it++) {
+        int64_t i = base + it * kThreads + threadIdx.x;
+        bool pass = false;
+        if (i < P.n) {
+            RowCtx x;
+            x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+            x.b0 = x.b1 = x.b2 = x.b3 = 0;
+            run_stages(P, env, x, [&](const RowCtx&) { pass = true; });
+        }
+        uint32_t b = __ballot_sync(0xFFFFFFFFu, pass);
+        if ((threadIdx.x & 31) == 0 && base + it * kThreads + (threadIdx.x & ~31) < P.n)
+            bits[(base + it * kThreads + threadIdx.x) >> 5] = b;
+        cnt += pass;
+    }
+    // block reduce
+    __shared__ uint32_t red[kThreads / 32];
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kThreads / 32; w++) t += red[w];
+        block_counts[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_select_write(const __grid_constant__ PipeArgs P, const uint32_t* bits,
+                                                           const uint64_t* block_offsets, uint32_t* out) {
+    __shared__ uint32_t warp_tot[kThreads / 32 * 8];
+    int64_t base = (int64_t)blockIdx.x * kSelRowsPerBlock;
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // each warp handles 8 words: word index (base/32) + it*8 + warp
+    uint32_t w[8];
+    for (int it = 0; it < 8; it++) {
+        int64_t wi = (base >> 5) + it * (kThreads / 32) + warp;
+        int64_t row0 = wi * 32;
+        w[it] = row0 < P.n ? bits[wi] : 0u;
+        if (lane == 0) warp_tot[it * (kThreads / 32) + warp] = __popc(w[it]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // exclusive scan over the 64 words in row order
+        uint32_t s = 0;
+        for (int k = 0; k < 8 * (kThreads / 32); k++) {
+            uint32_t t = warp_tot[k];
+            warp_tot[k] = s;
+            s += t;
+        }
+    }
+    __syncthreads();
+    uint64_t off = block_offsets[blockIdx.x];
+    for (int it = 0; it < 8; it++) {
+        int64_t wi = (base >> 5) + it * (kThreads / 32) + warp;
+        uint32_t m = w[it];
+        if ((m >> lane) & 1u) {
+            uint32_t pos = warp_tot[it * (kThreads / 32) + warp] + __popc(m & ((1u << lane) - 1u));
+            int64_t i = wi * 32 + lane;
+            out[off + pos] = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        }
+    }
+}
+
+// ---- scan (exclusive, u32 -> u64) ------------------------------------------------------------
+constexpr int kScanItems = 4;
+constexpr int kScanBlock = 1024 * kScanItems;
+
+__device__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* tmp, uint64_t* total) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) tmp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int nw = blockDim.x >> 5;
+        uint64_t t = lane < nw ? tmp[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t y = __shfl_up_sync(0xFFFFFFFFu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < nw) tmp[lane] = t;
+    }
+    __syncthreads();
+    uint64_t before = warp ? tmp[warp - 1] : 0;
+    if (total) *total = tmp[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void k_scan_reduce(const uint32_t* in, int64_t n, uint64_t* sums) {
+    __shared__ uint64_t tmp[32];
+    int64_t base = (int64_t)blockIdx.x * kScanBlock;
+    uint64_t s = 0;
+    for (int k = 0; k < kScanItems; k++) {
+        int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
+        if (i < n) s += in[i];
+    }
+    uint64_t total;
+    block_exclusive_scan(s, tmp, &total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+__global__ void k_scan_sums(uint64_t* sums, int64_t nb) {  // single block, in place, exclusive
+    __shared__ uint64_t tmp[32];
+    __shared__ uint64_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int64_t base = 0; base < nb; base += blockDim.x) {
+        int64_t i = base + threadIdx.x;
+        uint64_t v = i < nb ? sums[i] : 0;
+        uint64_t total;
+        uint64_t ex = block_exclusive_scan(v, tmp, &total);
+        if (i < nb) sums[i] = carry + ex;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[nb] = carry;
+}
+__global__ void k_scan_apply(const uint32_t* in, int64_t n, const uint64_t* sums, uint64_t* out) {
+    __shared__ uint64_t tmp[32];
+    int64_t base = (int64_t)blockIdx.x * kScanBlock;
+    uint64_t vals[kScanItems];
+    uint64_t s = 0;
+    for (int k = 0; k < kScanItems; k++) {
+        int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
+        vals[k] = i < n ? in[i] : 0;
+        s += vals[k];
+    }
+    uint64_t ex = block_exclusive_scan(s, tmp, nullptr) + sums[blockIdx.x];
+    for (int k = 0; k < kScanItems; k++) {
+        int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
+        if (i < n) out[i] = ex;
+        ex += vals[k];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) out[n] = ex;
+}
+
+// ---- projection / hashing ---------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_project(const __grid_constant__ PipeArgs P, Prog prog, int out_type,
+                                                      void* out, uint32_t* valid) {
+    const EvalEnv env = env_of(P);
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    // the loop trip count is uniform per warp (stride is a multiple of 32)
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < P.n; i0 += stride) {
+        int64_t i = i0 + threadIdx.x;
+        bool in = i < P.n, ok = false;
+        if (in) {
+            RowCtx x;
+            x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+            x.b0 = x.b1 = x.b2 = x.b3 = 0;
+            uint64_t v;
+            eval_prog(env, prog, x, v, ok);
+            switch (out_type) {
+                case ML_TYPE_BOOL: ((uint8_t*)out)[i] = (uint8_t)(v & 1); break;
+                case ML_TYPE_INT32:
+                case ML_TYPE_DATE: ((int32_t*)out)[i] = (int32_t)(uint32_t)v; break;
+                case ML_TYPE_UTF8: ((uint32_t*)out)[i] = (uint32_t)v; break;
+                default: ((uint64_t*)out)[i] = v; break;
+            }
+        }
+        uint32_t b = __ballot_sync(0xFFFFFFFFu, in && ok);
+        if ((threadIdx.x & 31) == 0 && i < P.n) valid[i >> 5] = b;
+    }
+}
+
+// kernels/hash.rs:16-79: h = SEED; for col: h = combine(h, valid ? hash(col[r]) : NULL_HASH)
+__global__ void k_hash_columns(const __grid_constant__ PipeArgs P, int ncols, const uint64_t* const* dict_hash,
+                               uint64_t* out) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {
+        uint32_t r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        uint64_t h = kSeed;
+        for (int c = 0; c < ncols; c++) {
+            const DCol& col = P.cols[c];
+            uint64_t x = kNullHash;
+            if (valid_bit(col.valid, r)) {
+                if (col.kind == CK_DICT) {
+                    x = dict_hash[c][dict_code(col, r)];
+                } else if (col.kind == CK_UTF8) {
+                    Str s = col_str(col, r);
+                    x = hash_bytes(s.p, s.n);
+                } else {
+                    uint64_t v = load_value(col, r);
+                    if (col.dt == ML_TYPE_FLOAT64 && as_f64(v) == 0.0) v = 0;
+                    x = hash_u64(v);
+                }
+            }
+            h = hash_combine(h, x);
+        }
+        out[i] = h;
+    }
+}
+
+// ---- join build / probe --------------------------------------------------------------------------
+// build_table (join.rs:160-203): one table entry per distinct key; rows with the same
+// key are chained through `next`.  NULL keys are not inserted.
+__global__ void k_join_insert(const __grid_constant__ PipeArgs P, const __grid_constant__ KeyLayout L, TableView t,
+                              uint32_t* next, uint32_t* dup_flag, int64_t n) {
+    const EvalEnv env = env_of(P);
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        RowCtx x;
+        x.r = (uint32_t)i;
+        x.b0 = x.b1 = x.b2 = x.b3 = 0;
+        uint64_t w[2];
+        uint32_t nm;
+        if (!make_key(env, L, x, w, &nm, true)) continue;
+        bool inserted;
+        uint64_t slot;
+        uint32_t r = (uint32_t)i;
+        uint32_t p = table_upsert(t, w, 0u, key_hash(w, t.nwords), P.err, [&]() { return r; }, &inserted, &slot);
+        if (p == kNone) continue;  // error already flagged (timeout) or table full (never: presized)
+        if (!inserted) {
+            uint32_t old = atomicExch(t.payload + slot, r);
+            next[r] = old;
+            if (*dup_flag == 0) atomicExch(dup_flag, 1u);
+        }
+    }
+}
+
+__global__ void k_probe_count(const __grid_constant__ PipeArgs P, uint32_t* counts) {
+    const EvalEnv env = env_of(P);
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {
+        RowCtx x;
+        x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        x.b0 = x.b1 = x.b2 = x.b3 = 0;
+        uint32_t c = 0;
+        run_stages(P, env, x, [&](const RowCtx&) { c++; });
+        counts[i] = c;
+    }
+}
+__global__ void k_probe_write(const __grid_constant__ PipeArgs P, const uint64_t* offsets, uint32_t* pi, uint32_t* bi) {
+    const EvalEnv env = env_of(P);
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {
+        RowCtx x;
+        x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        x.b0 = x.b1 = x.b2 = x.b3 = 0;
+        uint64_t o = offsets[i];
+        run_stages(P, env, x, [&](const RowCtx& c) {
+            pi[o] = c.r;
+            bi[o] = c.b0;
+            o++;
+        });
+    }
+}
+
+// ---- canonical string ids (equal strings -> the smallest-claimed row) ---------------------------
+__global__ void k_strid(const uint32_t* off, const uint8_t* bytes, const uint64_t* valid, int64_t n, TableView t,
+                        uint32_t* canon, uint32_t* err) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        uint32_t r = (uint32_t)i;
+        if (!valid_bit(valid, r)) {
+            canon[r] = r;
+            continue;
+        }
+        uint32_t a = off[r], b = off[r + 1];
+        uint64_t h = hash_bytes(bytes + a, b - a);
+        uint64_t s = h & t.mask;
+        uint32_t result = kNone;
+        for (uint64_t k = 0; k <= t.mask && result == kNone;) {
+            uint32_t st = load_state(t.state + s);
+            if (st == 0) {
+                uint32_t old = atomicCAS(t.state + s, 0u, 1u);
+                if (old == 0) {
+                    t.keys[s] = h;
+                    t.payload[s] = r;
+                    publish_state(t.state + s, 2);
+                    result = r;
+                    break;
+                }
+                st = old;
+            }
+            if (st == 1) {
+                uint32_t spins = 0;
+                do {
+                    __nanosleep(20);
+                    st = load_state(t.state + s);
+                } while (st == 1 && ++spins < kSpinLimit);
+                if (st == 1) {
+                    atomicOr(err, (uint32_t)DE_TIMEOUT);
+                    result = r;
+                    break;
+                }
+            }
+            if (t.keys[s] == h) {
+                uint32_t c = t.payload[s];
+                uint32_t ca = off[c], cb = off[c + 1];
+                if (cb - ca == b - a && bytes_eq(bytes + a, bytes + ca, b - a)) {
+                    result = c;
+                    break;
+                }
+            }
+            s = (s + 1) & t.mask;
+            k++;
+        }
+        canon[r] = result == kNone ? r : result;
+    }
+}
+
+// ---- gathers ------------------------------------------------------------------------------------
+__global__ void k_gather_fixed(const uint8_t* src, int width, const uint32_t* idx, int64_t k, uint8_t* dst) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += stride) {
+        uint64_t r = idx[i];
+        switch (width) {
+            case 1: dst[i] = src[r]; break;
+            case 4: ((uint32_t*)dst)[i] = ((const uint32_t*)src)[r]; break;
+            default: ((uint64_t*)dst)[i] = ((const uint64_t*)src)[r]; break;
+        }
+    }
+}
+__global__ void k_gather_valid(const uint64_t* src, const uint32_t* idx, int64_t k, uint32_t* dst) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < k; i0 += stride) {
+        int64_t i = i0 + threadIdx.x;
+        bool v = false;
+        if (i < k) v = valid_bit(src, idx[i]);
+        uint32_t b = __ballot_sync(0xFFFFFFFFu, v);
+        if ((threadIdx.x & 31) == 0 && i < k) dst[i >> 5] = b;
+    }
+}
+__global__ void k_utf8_lengths(const uint32_t* off, const uint32_t* idx, int64_t k, uint32_t* len) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += stride) {
+        uint32_t r = idx ? idx[i] : (uint32_t)i;
+        len[i] = off[r + 1] - off[r];
+    }
+}
+__global__ void k_utf8_copy(const uint32_t* off, const uint8_t* bytes, const uint32_t* idx, int64_t k,
+                            const uint64_t* dst_off, uint8_t* dst) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += stride) {
+        uint32_t r = idx ? idx[i] : (uint32_t)i;
+        uint32_t a = off[r], b = off[r + 1];
+        uint8_t* d = dst + dst_off[i];
+        for (uint32_t j = a; j < b; j++) d[j - a] = bytes[j];
+    }
+}
+__global__ void k_u64_to_u32(const uint64_t* in, uint32_t* out, int64_t n) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (uint32_t)in[i];
+}
+__global__ void k_fill_u32(uint32_t* p, uint32_t v, int64_t n) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
+}
+
+__global__ void k_offsets_rebase(const uint32_t* src, int64_t n, uint32_t base, uint32_t* dst) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    uint32_t first = src[0];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += stride) dst[i] = src[i] - first + base;
+}
+__global__ void k_copy_bits(const uint64_t* src, int64_t n, uint64_t* dst, int64_t dst_off) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        bool v = src == nullptr || ((src[i >> 6] >> (i & 63)) & 1ull);
+        if (v) {
+            int64_t o = dst_off + i;
+            atomicOr((unsigned long long*)dst + (o >> 6), 1ull << (o & 63));
+        }
+    }
+}
+
+// ---- top-N -------------------------------------------------------------------------------------------
+// compare_rows (sort.rs:43-82): per key, NULLs first/last, f64 by total order, asc/desc.
+__device__ __forceinline__ int64_t total_key(double d) {
+    int64_t x = __double_as_longlong(d);
+    return x ^ (int64_t)(((uint64_t)(x >> 63)) >> 1);
+}
+__device__ int cmp_rows(const SortDev& S, uint32_t a, uint32_t b) {
+    if (a == kNone || b == kNone) return (a == kNone) - (b == kNone);  // padding sorts last
+    for (int k = 0; k < S.nkeys; k++) {
+        const DCol& c = S.cols[k];
+        bool va = valid_bit(c.valid, a), vb = valid_bit(c.valid, b);
+        int o = 0;
+        if (!va && !vb) o = 0;
+        else if (!va) return S.nulls_first[k] ? -1 : 1;
+        else if (!vb) return S.nulls_first[k] ? 1 : -1;
+        else {
+            if (c.kind == CK_UTF8) {
+                o = str_cmp(col_str(c, a), col_str(c, b));
+            } else {
+                uint64_t x = load_value(c, a), y = load_value(c, b);
+                switch (c.dt) {
+                    case ML_TYPE_FLOAT64: {
+                        int64_t p = total_key(as_f64(x)), q = total_key(as_f64(y));
+                        o = p < q ? -1 : (p > q);
+                        break;
+                    }
+                    case ML_TYPE_BOOL: o = (x < y) ? -1 : (x > y); break;
+                    default: o = ((int64_t)x < (int64_t)y) ? -1 : ((int64_t)x > (int64_t)y); break;
+                }
+            }
+            if (!S.asc[k]) o = -o;
+        }
+        if (o) return o;
+    }
+    return 0;
+}
+
+__global__ void __launch_bounds__(1024) k_topn_chunk(const __grid_constant__ SortDev S, const uint32_t* in, int64_t n,
+                                                    int k, uint32_t* out) {
+    __shared__ uint32_t idx[kTopNChunk];
+    int64_t base = (int64_t)blockIdx.x * kTopNChunk;
+    for (int j = threadIdx.x; j < kTopNChunk; j += blockDim.x) {
+        int64_t i = base + j;
+        idx[j] = i < n ? (in ? in[i] : (uint32_t)i) : kNone;
+    }
+    __syncthreads();
+    // bitonic sort, ascending by cmp_rows
+    for (int size = 2; size <= kTopNChunk; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = threadIdx.x; t < kTopNChunk / 2; t += blockDim.x) {
+                int lo = 2 * t - (t & (stride - 1));
+                int hi = lo + stride;
+                bool up = (lo & size) == 0;
+                uint32_t a = idx[lo], b = idx[hi];
+                int c = cmp_rows(S, a, b);
+                if ((c > 0) == up && c != 0) {
+                    idx[lo] = b;
+                    idx[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int j = threadIdx.x; j < k; j += blockDim.x) out[(int64_t)blockIdx.x * k + j] = idx[j];
+}
+
+}  // namespace
+
+// ---- launch wrappers -------------------------------------------------------------------------------
+int agg_smem_bytes(const AggArgs& A) {
+    size_t SG = (size_t)A.smem_groups;
+    size_t b = ((SG * 4 + 15) & ~(size_t)15);
+    b += (size_t)A.nagg * (SG * 8 + ((SG * 4 + 15) & ~(size_t)15));
+    return (int)b;
+}
+void launch_agg(const PipeArgs& P, const AggArgs& A, int smem_bytes, cudaStream_t s) {
+    k_agg<<<grid_for(P.n, 8), kThreads, smem_bytes, s>>>(P, A);
+}
+void launch_agg_resume(const PipeArgs& P, const AggArgs& A, const uint32_t* ctx, uint64_t count, int w, int smem_bytes,
+                       cudaStream_t s) {
+    k_agg_resume<<<grid_for((int64_t)count, 8), kThreads, smem_bytes, s>>>(P, A, ctx, count, w);
+}
+void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
+                       int nwords, uint32_t* err, cudaStream_t s) {
+    if (!ngroups) return;
+    k_agg_rehash<<<(ngroups + kThreads - 1) / kThreads, kThreads, 0, s>>>(t, gkeys, gnull, gid_cap, ngroups, nwords, err);
+}
+void launch_agg_init(const AggArgs& A, uint32_t from, uint32_t to, cudaStream_t s) {
+    if (to <= from) return;
+    k_agg_init<<<(to - from + kThreads - 1) / kThreads, kThreads, 0, s>>>(A, from, to);
+}
+void launch_agg_final(const FinalArgs& F, cudaStream_t s) {
+    if (!F.ngroups) return;
+    k_agg_final<<<(F.ngroups + kThreads - 1) / kThreads, kThreads, 0, s>>>(F);
+}
+
+int select_blocks(int64_t n) { return (int)((n + kSelRowsPerBlock - 1) / kSelRowsPerBlock); }
+void launch_select_flags(const PipeArgs& P, uint32_t* bits, uint32_t* block_counts, cudaStream_t s) {
+    int nb = select_blocks(P.n);
+    if (nb) k_select_flags<<<nb, kThreads, 0, s>>>(P, bits, block_counts);
+}
+void launch_select_write(const PipeArgs& P, const uint32_t* bits, const uint64_t* block_offsets, uint32_t* out,
+                         cudaStream_t s) {
+    int nb = select_blocks(P.n);
+    if (nb) k_select_write<<<nb, kThreads, 0, s>>>(P, bits, block_offsets, out);
+}
+size_t scan_scratch_words(int64_t n) { return (size_t)((n + kScanBlock - 1) / kScanBlock) + 2; }
+void launch_scan_u32(const uint32_t* in, uint64_t* out, int64_t n, uint64_t* scratch, cudaStream_t s) {
+    int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+    if (nb == 0) {
+        cudaMemsetAsync(out, 0, sizeof(uint64_t), s);
+        return;
+    }
+    k_scan_reduce<<<(unsigned)nb, 1024, 0, s>>>(in, n, scratch);
+    k_scan_sums<<<1, 1024, 0, s>>>(scratch, nb);
+    k_scan_apply<<<(unsigned)nb, 1024, 0, s>>>(in, n, scratch, out);
+}
+
+void launch_project(const PipeArgs& P, Prog prog, int out_type, void* out, uint32_t* valid, cudaStream_t s) {
+    if (P.n) k_project<<<grid_for(P.n, 8), kThreads, 0, s>>>(P, prog, out_type, out, valid);
+}
+void launch_hash_columns(const PipeArgs& P, int ncols, const uint64_t* const* dict_hash, uint64_t* out, cudaStream_t s) {
+    if (P.n) k_hash_columns<<<grid_for(P.n, 8), kThreads, 0, s>>>(P, ncols, dict_hash, out);
+}
+void launch_join_insert(const PipeArgs& P, const KeyLayout& L, TableView t, uint32_t* next, uint32_t* dup_flag,
+                        int64_t n, cudaStream_t s) {
+    if (n) k_join_insert<<<grid_for(n, 8), kThreads, 0, s>>>(P, L, t, next, dup_flag, n);
+}
+void launch_probe_count(const PipeArgs& P, uint32_t* counts, cudaStream_t s) {
+    if (P.n) k_probe_count<<<grid_for(P.n, 8), kThreads, 0, s>>>(P, counts);
+}
+void launch_probe_write(const PipeArgs& P, const uint64_t* offsets, uint32_t* pi, uint32_t* bi, cudaStream_t s) {
+    if (P.n) k_probe_write<<<grid_for(P.n, 8), kThreads, 0, s>>>(P, offsets, pi, bi);
+}
+void launch_strid(const uint32_t* off, const uint8_t* bytes, const uint64_t* valid, int64_t n, TableView t,
+                  uint32_t* canon, uint32_t* err, cudaStream_t s) {
+    if (n) k_strid<<<grid_for(n, 8), kThreads, 0, s>>>(off, bytes, valid, n, t, canon, err);
+}
+void launch_gather_fixed(const void* src, int width, const uint32_t* idx, int64_t k, void* dst, cudaStream_t s) {
+    if (k) k_gather_fixed<<<grid_for(k, 8), kThreads, 0, s>>>((const uint8_t*)src, width, idx, k, (uint8_t*)dst);
+}
+void launch_gather_valid(const uint64_t* src, const uint32_t* idx, int64_t k, uint32_t* dst, cudaStream_t s) {
+    if (k) k_gather_valid<<<grid_for(k, 8), kThreads, 0, s>>>(src, idx, k, dst);
+}
+void launch_utf8_lengths(const uint32_t* off, const uint32_t* idx, int64_t k, uint32_t* len, cudaStream_t s) {
+    if (k) k_utf8_lengths<<<grid_for(k, 8), kThreads, 0, s>>>(off, idx, k, len);
+}
+void launch_utf8_copy(const uint32_t* off, const uint8_t* bytes, const uint32_t* idx, int64_t k, const uint64_t* dst_off,
+                      uint8_t* dst, cudaStream_t s) {
+    if (k) k_utf8_copy<<<grid_for(k, 8), kThreads, 0, s>>>(off, bytes, idx, k, dst_off, dst);
+}
+void launch_u64_to_u32(const uint64_t* in, uint32_t* out, int64_t n, cudaStream_t s) {
+    if (n) k_u64_to_u32<<<grid_for(n, 8), kThreads, 0, s>>>(in, out, n);
+}
+void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, uint32_t* out, cudaStream_t s) {
+    int64_t nb = (n + kTopNChunk - 1) / kTopNChunk;
+    if (nb) k_topn_chunk<<<(unsigned)nb, 1024, 0, s>>>(S, in, n, k, out);
+}
+void launch_offsets_rebase(const uint32_t* src, int64_t n, uint32_t base, uint32_t* dst, cudaStream_t s) {
+    k_offsets_rebase<<<grid_for(n + 1, 8), kThreads, 0, s>>>(src, n, base, dst);
+}
+void launch_copy_bits(const uint64_t* src, int64_t n, uint64_t* dst, int64_t dst_off, cudaStream_t s) {
+    if (n) k_copy_bits<<<grid_for(n, 8), kThreads, 0, s>>>(src, n, dst, dst_off);
+}
+void launch_fill_u32(uint32_t* p, uint32_t v, int64_t n, cudaStream_t s) {
+    if (n) k_fill_u32<<<grid_for(n, 8), kThreads, 0, s>>>(p, v, n);
+}
+
+}  // namespace mlg

@@ -1,0 +1,129 @@
+// Kernel argument blocks and launch wrappers shared by ml_kernels.cu and the host runtime.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ml_internal.hpp"
+
+namespace mlg {
+
+struct Stage {
+    int8_t kind;  // 0 = filter, 1 = probe
+    int8_t idx;
+};
+
+struct ProbeDev {
+    TableView t;
+    const uint32_t* next;  // chain links, nullptr when every build key is distinct
+    KeyLayout keys;
+};
+
+// The streaming part of a pipeline (Filter / Projection folded into expressions /
+// HashJoinProbe) for one launch.
+struct PipeArgs {
+    int64_t n;               // rows to visit (selection length when `sel` is set)
+    const uint32_t* sel;     // optional input selection vector
+    const Instr* prog;
+    const uint8_t* arena;
+    uint32_t* err;
+    int32_t nstages, nprobes;
+    Stage stages[kMaxFilters + kMaxProbes];
+    Prog filters[kMaxFilters];
+    ProbeDev probes[kMaxProbes];
+    const uint8_t* luts[kMaxLuts];
+    DCol cols[kMaxCols];
+};
+
+struct AggArgs {
+    KeyLayout keys;
+    TableView t;
+    uint64_t* gkeys;          // normalized key words by group id (nwords x gid_cap)
+    uint32_t* gnull;          // null mask by group id
+    uint32_t* ngroups;
+    uint32_t gid_cap;
+    int32_t nagg;
+    int32_t ungrouped;        // no GROUP BY: every row goes to group 0
+    int32_t smem_groups;      // group ids below this are pre-aggregated in shared memory
+    uint64_t* rows;           // rows per group (COUNT(*) and seen-tracking)
+    uint32_t* ovf;            // overflow row contexts
+    unsigned long long* ovf_count;
+    uint64_t ovf_cap;
+    AggDev aggs[kMaxAggs];
+};
+
+struct SortDev {
+    int32_t nkeys, pad;
+    DCol cols[kMaxKeys];
+    int32_t asc[kMaxKeys], nulls_first[kMaxKeys];
+};
+
+// ---- launch wrappers (defined in ml_kernels.cu) -----------------------------------------
+void launch_agg(const PipeArgs& P, const AggArgs& A, int smem_bytes, cudaStream_t s);
+void launch_agg_resume(const PipeArgs& P, const AggArgs& A, const uint32_t* ctx, uint64_t count, int ctx_words,
+                       int smem_bytes, cudaStream_t s);
+int agg_smem_bytes(const AggArgs& A);
+void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
+                       int nwords, uint32_t* err, cudaStream_t s);
+// Final values: keys decoded into `key_out` (fixed-width or u32 string ids), aggregates into
+// `agg_out`; validity as u32 words (LSB first) in *_valid.
+struct FinalArgs {
+    uint32_t ngroups, gid_cap;
+    int32_t nkeys, nagg, ungrouped, pad;
+    KeyField f[kMaxKeys];
+    const uint64_t* gkeys;
+    const uint32_t* gnull;
+    const uint64_t* rows;
+    void* key_out[kMaxKeys];
+    uint32_t* key_valid[kMaxKeys];
+    AggDev aggs[kMaxAggs];
+    int32_t out_type[kMaxAggs];
+    void* agg_out[kMaxAggs];
+    uint32_t* agg_valid[kMaxAggs];
+};
+void launch_agg_final(const FinalArgs& F, cudaStream_t s);
+void launch_agg_init(const AggArgs& A, uint32_t from, uint32_t to, cudaStream_t s);
+
+// Filter: pass bits (u32 words) + per-block counts, then ordered compaction.
+int select_blocks(int64_t n);
+void launch_select_flags(const PipeArgs& P, uint32_t* bits, uint32_t* block_counts, cudaStream_t s);
+void launch_select_write(const PipeArgs& P, const uint32_t* bits, const uint64_t* block_offsets, uint32_t* out,
+                         cudaStream_t s);
+// Exclusive scan of u32 counts into u64 offsets (offsets[n] = total).
+void launch_scan_u32(const uint32_t* in, uint64_t* out, int64_t n, uint64_t* scratch, cudaStream_t s);
+size_t scan_scratch_words(int64_t n);
+
+// Projection: evaluate program `prog` for output row i = row idx[i] (or i) of the source.
+void launch_project(const PipeArgs& P, Prog prog, int out_type, void* out, uint32_t* valid, cudaStream_t s);
+void launch_hash_columns(const PipeArgs& P, int ncols, const uint64_t* const* dict_hash, uint64_t* out,
+                         cudaStream_t s);
+
+// Join build: insert rows 0..n of the build batch.
+void launch_join_insert(const PipeArgs& P, const KeyLayout& L, TableView t, uint32_t* next, uint32_t* dup_flag,
+                        int64_t n, cudaStream_t s);
+// Standalone probe: per-row match counts, then pair output.
+void launch_probe_count(const PipeArgs& P, uint32_t* counts, cudaStream_t s);
+void launch_probe_write(const PipeArgs& P, const uint64_t* offsets, uint32_t* pi, uint32_t* bi, cudaStream_t s);
+
+// Canonical ids of a plain UTF8 column (equal strings -> the same row id).
+void launch_strid(const uint32_t* off, const uint8_t* bytes, const uint64_t* valid, int64_t n, TableView t,
+                  uint32_t* canon, uint32_t* err, cudaStream_t s);
+
+// Gathers.
+void launch_gather_fixed(const void* src, int width, const uint32_t* idx, int64_t k, void* dst, cudaStream_t s);
+void launch_gather_valid(const uint64_t* src, const uint32_t* idx, int64_t k, uint32_t* dst, cudaStream_t s);
+void launch_utf8_lengths(const uint32_t* off, const uint32_t* idx, int64_t k, uint32_t* len, cudaStream_t s);
+void launch_utf8_copy(const uint32_t* off, const uint8_t* bytes, const uint32_t* idx, int64_t k,
+                      const uint64_t* dst_off, uint8_t* dst, cudaStream_t s);
+void launch_u64_to_u32(const uint64_t* in, uint32_t* out, int64_t n, cudaStream_t s);
+
+// Top-N: each CTA sorts a chunk of candidate rows and keeps the best k.
+void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, uint32_t* out, cudaStream_t s);
+
+// Fill / concatenation helpers
+void launch_fill_u32(uint32_t* p, uint32_t v, int64_t n, cudaStream_t s);
+// dst[i] = src[i] - src[0] + base for i in 0..=n
+void launch_offsets_rebase(const uint32_t* src, int64_t n, uint32_t base, uint32_t* dst, cudaStream_t s);
+// OR the first n validity bits of src (nullptr = all valid) into dst at bit dst_off
+void launch_copy_bits(const uint64_t* src, int64_t n, uint64_t* dst, int64_t dst_off, cudaStream_t s);
+
+}  // namespace mlg

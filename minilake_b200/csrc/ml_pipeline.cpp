@@ -1,0 +1,373 @@
+// Pipeline construction and per-launch preparation.
+#include "ml_pipeline.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+namespace mlg {
+
+uint32_t StringIntern::id(const std::string& s) {
+    auto it = ids.find(s);
+    if (it != ids.end()) return it->second;
+    uint32_t v = (uint32_t)strs.size();
+    ids.emplace(s, v);
+    strs.push_back(s);
+    return v;
+}
+
+static int key_width(int t) {
+    switch (t) {
+        case ML_TYPE_BOOL: return 8;
+        case ML_TYPE_INT32:
+        case ML_TYPE_DATE:
+        case ML_TYPE_UTF8: return 32;
+        default: return 64;
+    }
+}
+
+// Field placement depends only on the key types, so a join's build and probe sides
+// (whose key types are equal) always produce identical normalized keys.
+static void place_fields(KeyLayout& L, const std::vector<int>& types) {
+    int word = 0, used = 0;
+    for (size_t k = 0; k < types.size(); k++) {
+        int w = key_width(types[k]);
+        if (used + w > 64) {
+            word++;
+            used = 0;
+        }
+        if (word >= kKeyWords) raise(ML_ERR_UNSUPPORTED, "key tuple wider than 128 bits on the GPU");
+        L.f[k].word = (int8_t)word;
+        L.f[k].shift = (int8_t)used;
+        L.f[k].width = (int8_t)w;
+        L.f[k].type = (int8_t)types[k];
+        L.f[k].strid = types[k] == ML_TYPE_UTF8;
+        used += w;
+    }
+    L.nkeys = (int)types.size();
+    L.nwords = word + 1;
+}
+
+KeyLayout Pipeline::key_layout(const ml_expr* exprs, int n, const Schema& schema, bool group, std::vector<KeyDecode>* dec) {
+    if (n > kMaxKeys) raise(ML_ERR_UNSUPPORTED, "more than 4 key expressions on the GPU");
+    KeyLayout L{};
+    std::vector<int> types;
+    for (int k = 0; k < n; k++) types.push_back(exprs[k].dtype);
+    place_fields(L, types);
+    for (int k = 0; k < n; k++) {
+        ExprNode e = parse_expr(exprs[k]);
+        KeyDecode d;
+        d.type = types[k];
+        if (types[k] == ML_TYPE_UTF8) {
+            if (!group) raise(ML_ERR_UNSUPPORTED, "string join keys on the GPU");
+            int slot;
+            L.prog[k] = C.compile_string_key(e, schema, &slot);
+            d.slot = slot;
+            const SlotInfo& si = C.slots[slot];
+            if (si.src == 0) {
+                d.str_kind = 1;
+            } else {
+                d.str_kind = 2;
+                d.build = si.src - 1;
+                d.build_col = si.index;
+            }
+        } else {
+            L.prog[k] = C.compile_value(e, schema, types[k]);
+        }
+        if (dec) dec->push_back(d);
+    }
+    return L;
+}
+
+void Pipeline::build(const ml_pipe_op* ops, int nops, const int32_t* types, int ntypes) {
+    if (ntypes < 0 || (ntypes > 0 && !types)) raise(ML_ERR_INVALID, "bad input types");
+    input_types.assign(types, types + ntypes);
+    out.clear();
+    for (int i = 0; i < ntypes; i++) {
+        if (types[i] < 0 || types[i] > ML_TYPE_UTF8) raise(ML_ERR_INVALID, "bad input type");
+        ColRef r;
+        r.kind = 0;
+        r.src = 0;
+        r.index = i;
+        r.dtype = types[i];
+        out.push_back(r);
+    }
+    if (nops < 0 || (nops > 0 && !ops)) raise(ML_ERR_INVALID, "bad prologue");
+    for (int o = 0; o < nops; o++) {
+        const ml_pipe_op& op = ops[o];
+        if (op.nexprs < 0 || (op.nexprs > 0 && !op.exprs)) raise(ML_ERR_INVALID, "operator without expressions");
+        switch (op.kind) {
+            case ML_PIPE_FILTER: {  // filter.rs:19-25
+                if (op.nexprs != 1) raise(ML_ERR_INVALID, "filter takes one predicate");
+                if ((int)filters.size() >= kMaxFilters || nstages >= kMaxFilters + kMaxProbes)
+                    raise(ML_ERR_UNSUPPORTED, "too many filters in one pipeline");
+                filters.push_back(C.compile_value(parse_expr(op.exprs[0]), out, ML_TYPE_BOOL));
+                stages[nstages++] = Stage{0, (int8_t)(filters.size() - 1)};
+                break;
+            }
+            case ML_PIPE_PROJECT: {  // projection.rs:21-32: expressions over the input
+                auto env = std::make_shared<Schema>(out);
+                Schema next;
+                for (int k = 0; k < op.nexprs; k++) {
+                    auto e = std::make_shared<ExprNode>(parse_expr(op.exprs[k]));
+                    if (e->kind == ML_EXPR_COLUMN) {
+                        if (e->index < 0 || (size_t)e->index >= env->size()) raise(ML_ERR_INVALID, "projection column missing");
+                        ColRef r = (*env)[e->index];
+                        if (r.dtype != op.exprs[k].dtype && r.kind != 2) {
+                            ColRef c;
+                            c.kind = 2;
+                            c.dtype = op.exprs[k].dtype;
+                            c.expr = std::make_shared<ExprNode>();
+                            c.expr->kind = ML_EXPR_CAST;
+                            c.expr->dtype = op.exprs[k].dtype;
+                            c.expr->kids.push_back(*e);
+                            c.env = env;
+                            next.push_back(c);
+                        } else {
+                            next.push_back(r);
+                        }
+                        continue;
+                    }
+                    ColRef c;
+                    c.kind = 2;
+                    c.dtype = op.exprs[k].dtype;
+                    if (op.exprs[k].dtype != ML_TYPE_UTF8) {  // evaluate_to_column's cast to the output type
+                        c.expr = std::make_shared<ExprNode>();
+                        c.expr->kind = ML_EXPR_CAST;
+                        c.expr->dtype = op.exprs[k].dtype;
+                        c.expr->kids.push_back(*e);
+                    } else {
+                        c.expr = e;
+                    }
+                    c.env = env;
+                    next.push_back(c);
+                }
+                out = next;
+                break;
+            }
+            case ML_PIPE_PROBE: {  // join.rs:263-337
+                if ((int)probes.size() >= kMaxProbes) raise(ML_ERR_UNSUPPORTED, "more than 4 probes in one pipeline");
+                if (!op.join) raise(ML_ERR_INVALID, "probe without a join table");
+                ml_join_table* jt = op.join;
+                if ((int)jt->key_types.size() != op.nexprs) raise(ML_ERR_INVALID, "probe key count differs from the build");
+                for (int k = 0; k < op.nexprs; k++)
+                    if (op.exprs[k].dtype != jt->key_types[k]) raise(ML_ERR_INVALID, "probe key type differs from the build");
+                ProbeInfo pi;
+                pi.jt = jt;
+                pi.keys = key_layout(op.exprs, op.nexprs, out, false, nullptr);
+                probes.push_back(pi);
+                int p = (int)probes.size() - 1;
+                stages[nstages++] = Stage{1, (int8_t)p};
+                Schema bcols;
+                for (size_t j = 0; j < jt->batch.cols.size(); j++) {
+                    ColRef r;
+                    r.kind = 1;
+                    r.src = p + 1;
+                    r.index = (int)j;
+                    r.dtype = jt->batch.cols[j]->dtype;
+                    bcols.push_back(r);
+                }
+                Schema next;
+                if (op.build_is_left) {
+                    next = bcols;
+                    next.insert(next.end(), out.begin(), out.end());
+                } else {
+                    next = out;
+                    next.insert(next.end(), bcols.begin(), bcols.end());
+                }
+                out = next;
+                break;
+            }
+            default: raise(ML_ERR_INVALID, "bad pipeline operator");
+        }
+    }
+}
+
+void Pipeline::upload() {
+    size_t pb = std::max<size_t>(C.code.size() * sizeof(Instr), 32);
+    size_t ab = std::max<size_t>(C.arena.size(), 16);
+    d_prog = DevBuf(ctx, pb, nullptr);
+    d_arena = DevBuf(ctx, ab, nullptr);
+    if (!C.code.empty()) CK(cudaMemcpy(d_prog.get(), C.code.data(), C.code.size() * sizeof(Instr), cudaMemcpyHostToDevice));
+    if (!C.arena.empty()) CK(cudaMemcpy(d_arena.get(), C.arena.data(), C.arena.size(), cudaMemcpyHostToDevice));
+}
+
+static bool dict_pred(const LutSpec& L, const std::string& s) {  // per-entry predicate
+    bool r;
+    if (L.what == SW_CMP) {
+        int c = s.compare(L.lit);
+        c = c < 0 ? -1 : (c > 0);
+        switch (L.op) {
+            case ML_BIN_EQ: r = c == 0; break;
+            case ML_BIN_NOTEQ: r = c != 0; break;
+            case ML_BIN_LT: r = c < 0; break;
+            case ML_BIN_LTEQ: r = c <= 0; break;
+            case ML_BIN_GT: r = c > 0; break;
+            default: r = c >= 0; break;
+        }
+    } else if (L.what == SW_LIKE) {
+        r = like_match_host(s, L.lit, L.shape);
+    } else {
+        r = std::find(L.list.begin(), L.list.end(), s) != L.list.end();
+    }
+    return r != L.negated;
+}
+
+void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrows, const uint32_t* sel, int64_t nsel,
+                       cudaStream_t s, Staging& st, Reservation* res) {
+    if (ncols != (int)input_types.size())
+        raise(ML_ERR_INVALID, "batch has " + std::to_string(ncols) + " columns, the pipeline expects " +
+                                  std::to_string(input_types.size()));
+    if (nrows < 0 || nrows > 0xFFFFFFFFll) raise(ML_ERR_INVALID, "batch row count out of range");
+    if (ncols > 0 && !cols) raise(ML_ERR_INVALID, "null column array");
+    L.src.clear();
+    for (int c = 0; c < ncols; c++) {
+        if (cols[c].dtype != input_types[c])
+            raise(ML_ERR_INVALID, "column " + std::to_string(c) + " has type " + std::to_string(cols[c].dtype) +
+                                      ", the pipeline expects " + std::to_string(input_types[c]));
+        L.src.push_back(stage_column(ctx, cols[c], nrows, s, st, res));
+    }
+    PipeArgs& P = L.P;
+    P = PipeArgs{};
+    P.n = sel ? nsel : nrows;
+    P.sel = sel;
+    P.prog = d_prog.get<Instr>();
+    P.arena = d_arena.get<uint8_t>();
+    P.nstages = nstages;
+    P.nprobes = (int)probes.size();
+    for (int i = 0; i < nstages; i++) P.stages[i] = stages[i];
+    for (size_t i = 0; i < filters.size(); i++) P.filters[i] = filters[i];
+    for (size_t p = 0; p < probes.size(); p++) {
+        ml_join_table* jt = probes[p].jt;
+        P.probes[p].t = jt->view();
+        P.probes[p].next = jt->has_dups ? jt->next.get<uint32_t>() : nullptr;
+        P.probes[p].keys = probes[p].keys;
+    }
+    // scratch: dictionary id maps and predicate tables for this batch
+    std::vector<uint8_t> scratch;
+    std::vector<std::pair<int, size_t>> gid_at;   // slot -> offset
+    std::vector<std::pair<int, size_t>> lut_at;   // lut -> offset
+    std::vector<std::pair<int, size_t>> dict_at, dbytes_at;  // slot -> dictionary offsets / bytes
+    auto put = [&](const void* p, size_t n) {
+        size_t o = (scratch.size() + 15) & ~(size_t)15;
+        scratch.resize(o + n);
+        if (n) memcpy(scratch.data() + o, p, n);
+        return o;
+    };
+    L.col_valid.assign(C.slots.size(), 0);
+    for (size_t i = 0; i < C.slots.size(); i++) {
+        const SlotInfo& si = C.slots[i];
+        DCol& d = P.cols[i];
+        const DevColumn* col;
+        if (si.src == 0) {
+            if (si.index < 0 || si.index >= (int)L.src.size()) raise(ML_ERR_INVALID, "column slot out of range");
+            col = L.src[si.index].get();
+        } else {
+            ml_join_table* jt = probes[si.src - 1].jt;
+            col = jt->batch.cols[si.index].get();
+            d.gid = col->strid ? col->strid.get<uint32_t>() : nullptr;
+        }
+        d.dt = col->dtype;
+        d.kind = col->kind;
+        d.src = si.src;
+        d.data = col->dptr();
+        d.off = col->optr();
+        d.valid = col->vptr();
+        d.n = col->n;
+        L.col_valid[i] = d.valid != nullptr;
+        if (col->kind == CK_DICT) {
+            const HostDict& hd = *col->dict;
+            std::vector<uint32_t> g(hd.len() + 1, 0);
+            {
+                std::lock_guard<std::mutex> lk(intern.mu);
+                for (size_t e = 0; e < hd.len(); e++) g[e] = intern.id(hd.get(e));
+                g[hd.len()] = intern.id(std::string());  // spare entry for clamped codes
+            }
+            d.dict_len = (uint32_t)hd.len();
+            gid_at.push_back({(int)i, put(g.data(), g.size() * 4)});
+            std::vector<uint32_t> doff(hd.off);
+            doff.push_back(hd.off.back());  // the spare entry is the empty string
+            dict_at.push_back({(int)i, put(doff.data(), doff.size() * 4)});
+            dbytes_at.push_back({(int)i, put(hd.bytes.data(), std::max<size_t>(hd.bytes.size(), 1))});
+        }
+    }
+    for (size_t l = 0; l < C.luts.size(); l++) {
+        const LutSpec& spec = C.luts[l];
+        const DevColumn* col = spec.slot < (int)C.slots.size() && C.slots[spec.slot].src == 0
+                                   ? L.src[C.slots[spec.slot].index].get()
+                                   : nullptr;
+        if (!col || col->kind != CK_DICT) continue;
+        std::vector<uint8_t> t(col->dict->len() + 1, 0);
+        for (size_t e = 0; e < col->dict->len(); e++) t[e] = dict_pred(spec, col->dict->get(e));
+        lut_at.push_back({(int)l, put(t.data(), t.size())});
+    }
+    if (!scratch.empty()) {
+        L.scratch = DevBuf(ctx, scratch.size(), nullptr);
+        void* h = st.get(scratch.size());
+        CK(cudaStreamSynchronize(s));  // the staging buffer may still feed an earlier copy
+        memcpy(h, scratch.data(), scratch.size());
+        CK(cudaMemcpyAsync(L.scratch.get(), h, scratch.size(), cudaMemcpyHostToDevice, s));
+        uint8_t* base = L.scratch.get<uint8_t>();
+        for (auto& g : gid_at) P.cols[g.first].gid = (const uint32_t*)(base + g.second);
+        for (auto& g : dict_at) P.cols[g.first].off = (const uint32_t*)(base + g.second);
+        for (auto& g : dbytes_at) P.cols[g.first].dbytes = base + g.second;
+        for (auto& t : lut_at) P.luts[t.first] = base + t.second;
+    }
+}
+
+bool Pipeline::reads_nullable(const Prog& p, const Launch& L) const {
+    for (int i = 0; i < p.len; i++) {
+        const Instr& in = C.code[p.start + i];
+        if ((in.op == I_COL || in.op == I_STRPRED) && L.col_valid[in.a]) return true;
+        if (in.op == I_STRCMP_COL && (L.col_valid[in.a] || L.col_valid[in.b])) return true;
+    }
+    return false;
+}
+
+uint64_t scan_counts(Ctx* ctx, const uint32_t* counts, int64_t n, DevBuf& offsets, cudaStream_t s) {
+    offsets = DevBuf(ctx, (size_t)(n + 1) * 8, nullptr);
+    DevBuf scratch(ctx, scan_scratch_words(n) * 8, nullptr);
+    launch_scan_u32(counts, offsets.get<uint64_t>(), n, scratch.get<uint64_t>(), s);
+    ctx->count_launch(3);
+    uint64_t total = 0;
+    CK(cudaMemcpyAsync(&total, offsets.get<uint64_t>() + n, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return total;
+}
+
+int64_t run_select(Ctx* ctx, const PipeArgs& P, DevBuf& out, cudaStream_t s) {
+    int nb = select_blocks(P.n);
+    DevBuf bits(ctx, std::max<size_t>((size_t)(P.n + 31) / 32 * 4, 4), nullptr);
+    DevBuf counts(ctx, std::max<size_t>((size_t)nb * 4, 4), nullptr);
+    {
+        KernelTimer kt(ctx, s, "select");
+        launch_select_flags(P, bits.get<uint32_t>(), counts.get<uint32_t>(), s);
+        kt.stop();
+    }
+    ctx->count_launch();
+    DevBuf offs;
+    uint64_t total = scan_counts(ctx, counts.get<uint32_t>(), nb, offs, s);
+    out = DevBuf(ctx, std::max<size_t>(total * 4, 4), nullptr);
+    launch_select_write(P, bits.get<uint32_t>(), offs.get<uint64_t>(), out.get<uint32_t>(), s);
+    ctx->count_launch();
+    CK(cudaStreamSynchronize(s));
+    return (int64_t)total;
+}
+
+void gather_utf8(Ctx* ctx, const uint32_t* off, const uint8_t* bytes, const uint32_t* idx, int64_t k, DevColumn& out,
+                 cudaStream_t s, Reservation* res) {
+    DevBuf lens(ctx, std::max<size_t>((size_t)k * 4, 4), nullptr);
+    launch_utf8_lengths(off, idx, k, lens.get<uint32_t>(), s);
+    DevBuf offs64;
+    uint64_t total = scan_counts(ctx, lens.get<uint32_t>(), k, offs64, s);
+    if (total > 0xFFFFFFFFull) raise(ML_ERR_UNSUPPORTED, "string column larger than 4 GiB");
+    out.kind = CK_UTF8;
+    out.dtype = ML_TYPE_UTF8;
+    out.n = k;
+    out.offsets = DevBuf(ctx, (size_t)(k + 1) * 4, res);
+    launch_u64_to_u32(offs64.get<uint64_t>(), out.offsets.get<uint32_t>(), k + 1, s);
+    out.data = DevBuf(ctx, std::max<size_t>(total, 1), res);
+    launch_utf8_copy(off, bytes, idx, k, offs64.get<uint64_t>(), out.data.get<uint8_t>(), s);
+    ctx->count_launch(3);
+}
+
+}  // namespace mlg

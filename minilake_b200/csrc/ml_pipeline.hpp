@@ -1,0 +1,97 @@
+// Pipelines: the streaming operators fused in front of a sink, compiled once and
+// launched per pushed batch (morsel).
+#pragma once
+
+#include "ml_runtime.hpp"
+
+struct ml_join_table;
+
+namespace mlg {
+
+// How a key field is decoded back into a column.
+struct KeyDecode {
+    int type = 0;
+    int str_kind = 0;  // 0 = not a string, 1 = dictionary global id, 2 = build-side canonical row
+    int build = -1;    // str_kind 2: probe index whose build batch holds the strings
+    int build_col = -1;
+    int slot = -1;     // column slot the key reads
+};
+
+// Global string ids for dictionary-encoded source columns (the dictionaries differ per
+// row group; the ids are the pipeline's interning of their entries).
+struct StringIntern {
+    std::mutex mu;
+    std::unordered_map<std::string, uint32_t> ids;
+    std::vector<std::string> strs;
+    uint32_t id(const std::string& s);
+};
+
+struct ProbeInfo {
+    ml_join_table* jt = nullptr;
+    KeyLayout keys{};
+};
+
+class Pipeline {
+   public:
+    Pipeline(Ctx* ctx) : ctx(ctx) {}
+    Ctx* ctx;
+    Compiler C;
+    std::vector<int> input_types;
+    Schema out;  // schema after the prologue (what the sink reads)
+    int nstages = 0;
+    Stage stages[kMaxFilters + kMaxProbes]{};
+    std::vector<Prog> filters;
+    std::vector<ProbeInfo> probes;
+    StringIntern intern;
+    DevBuf d_prog, d_arena;
+
+    void build(const ml_pipe_op* ops, int nops, const int32_t* types, int ntypes);
+    KeyLayout key_layout(const ml_expr* exprs, int n, const Schema& schema, bool group, std::vector<KeyDecode>* dec);
+    void upload();
+
+    // Per-launch state: staged source columns, gid maps and predicate tables.
+    struct Launch {
+        std::vector<std::unique_ptr<DevColumn>> src;
+        DevBuf scratch;
+        PipeArgs P{};
+        std::vector<int> col_valid;  // slot has a validity bitmap in this launch
+    };
+    void prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrows, const uint32_t* sel, int64_t nsel,
+                 cudaStream_t s, Staging& st, Reservation* res);
+    // Slot mask check: does program `p` read a column with a validity bitmap?
+    bool reads_nullable(const Prog& p, const Launch& L) const;
+};
+
+// Ordered selection of the rows where all of the pipeline's stages pass (no probes).
+// Returns the number of selected rows; `out` holds them (device).
+int64_t run_select(Ctx* ctx, const PipeArgs& P, DevBuf& out, cudaStream_t s);
+
+// Exclusive scan helper (device u32 counts -> u64 offsets incl. total); returns the total.
+uint64_t scan_counts(Ctx* ctx, const uint32_t* counts, int64_t n, DevBuf& offsets, cudaStream_t s);
+
+// Gather a plain UTF8 column: strings at `idx` (or all rows) into a new column.
+void gather_utf8(Ctx* ctx, const uint32_t* off, const uint8_t* bytes, const uint32_t* idx, int64_t k, DevColumn& out,
+                 cudaStream_t s, Reservation* res);
+
+}  // namespace mlg
+
+struct ml_join_table {
+    mlg::Ctx* ctx = nullptr;
+    ml_batch batch;  // the concatenated build side
+    std::vector<int> key_types;
+    int nwords = 1;
+    mlg::DevBuf state, keys, payload, next, dup;
+    uint64_t cap = 0;
+    int64_t distinct = 0;
+    bool has_dups = false;
+    std::unique_ptr<mlg::Reservation> res;
+    mlg::TableView view() const {
+        mlg::TableView t{};
+        t.state = state.get<uint32_t>();
+        t.keys = keys.get<uint64_t>();
+        t.payload = payload.get<uint32_t>();
+        t.mask = cap - 1;
+        t.nwords = nwords;
+        return t;
+    }
+};

@@ -1,0 +1,476 @@
+"""Python face of the B200 execution core: a thin ctypes layer over
+``libminilake_gpu.so`` (the C ABI in ``include/minilake_gpu.h``).
+
+The classes mirror MiniLake's pipeline contract (crates/minilake-exec/src/pipeline.rs):
+``FilterOperator`` / ``ProjectionOperator`` / ``HashJoinProbe`` are streaming
+operators; ``HashAggregateSink`` / ``JoinBuildSink`` / ``SortSink`` are sinks with
+``create_local()`` -> ``LocalSink.sink(batch)`` -> ``LocalSink.combine()`` ->
+``finalize()``.  A sink may be given the streaming operators that precede it
+(the "prologue"); its kernel then runs the whole pipeline per morsel.
+
+There is no CPU fallback: importing this module fails loudly when the CUDA
+library has not been built, and every call runs on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .columns import HostColumn, Table
+
+_LIB_PATH = os.path.join(os.path.dirname(__file__), "_lib", "libminilake_gpu.so")
+
+
+class MiniLakeError(RuntimeError):
+    """MiniLakeError (crates/minilake-core/src/error.rs); `code` is the C status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+class ResourcesExhausted(MiniLakeError):
+    """ResourcesExhausted{operator, requested, used, limit} (memory.rs:326-339)."""
+
+    def __init__(self, code, msg, operator, requested, used, limit):
+        super().__init__(code, msg)
+        self.operator, self.requested, self.used, self.limit = operator, requested, used, limit
+
+
+def _load():
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"{_LIB_PATH} is missing: build the CUDA library first "
+                          "(python -c 'import __graft_entry__ as g; g.build()')")
+    lib = C.CDLL(_LIB_PATH)
+    P, I32, I64, U64, VP = C.POINTER, C.c_int32, C.c_int64, C.c_uint64, C.c_void_p
+    sigs = {
+        "ml_gpu_last_error": ([], C.c_char_p),
+        "ml_gpu_last_budget_error": ([C.c_char_p, C.c_size_t, P(U64), P(U64), P(U64)], C.c_int),
+        "ml_gpu_ctx_create": ([C.c_int, U64, C.c_uint32, P(VP)], C.c_int),
+        "ml_gpu_ctx_destroy": ([VP], C.c_int),
+        "ml_gpu_pool_stats": ([VP, P(U64), P(U64), P(U64)], C.c_int),
+        "ml_gpu_ctx_synchronize": ([VP], C.c_int),
+        "ml_gpu_kernel_launches": ([VP, P(U64)], C.c_int),
+        "ml_gpu_profile_read": ([VP, C.c_char_p, P(U64), P(C.c_double), I32], C.c_int),
+        "ml_gpu_batch_upload": ([VP, P(abi.MlColumn), I32, I64, P(VP)], C.c_int),
+        "ml_gpu_batch_num_rows": ([VP, P(I64)], C.c_int),
+        "ml_gpu_batch_num_columns": ([VP, P(I32)], C.c_int),
+        "ml_gpu_batch_columns": ([VP, P(abi.MlColumn), I32], C.c_int),
+        "ml_gpu_batch_column_info": ([VP, I32, P(I32), P(I64), P(I32)], C.c_int),
+        "ml_gpu_batch_fetch": ([VP, I32, VP, VP, VP], C.c_int),
+        "ml_gpu_batch_destroy": ([VP], C.c_int),
+        "ml_gpu_filter": ([VP, P(abi.MlExpr), P(abi.MlColumn), I32, I64, VP, I64, I32, VP, P(I64)], C.c_int),
+        "ml_gpu_project": ([VP, P(abi.MlExpr), P(abi.MlColumn), I32, I64, P(VP)], C.c_int),
+        "ml_gpu_hash_columns": ([VP, P(abi.MlColumn), I32, I64, VP, I64, I32, VP], C.c_int),
+        "ml_gpu_hashagg_create": ([VP, P(abi.MlPipeOp), I32, VP, I32, P(abi.MlExpr), I32, P(abi.MlAggSpec), I32,
+                                   I64, P(VP)], C.c_int),
+        "ml_gpu_hashagg_local_create": ([VP, P(VP)], C.c_int),
+        "ml_gpu_hashagg_sink": ([VP, P(abi.MlColumn), I32, I64, VP, I64], C.c_int),
+        "ml_gpu_hashagg_combine": ([VP], C.c_int),
+        "ml_gpu_hashagg_finalize": ([VP, P(VP)], C.c_int),
+        "ml_gpu_hashagg_stats": ([VP, P(I64), P(I64), P(I64)], C.c_int),
+        "ml_gpu_hashagg_destroy": ([VP], C.c_int),
+        "ml_gpu_join_build_create": ([VP, P(abi.MlPipeOp), I32, VP, I32, P(abi.MlExpr), I32, P(VP)], C.c_int),
+        "ml_gpu_join_build_local_create": ([VP, P(VP)], C.c_int),
+        "ml_gpu_join_build_sink": ([VP, P(abi.MlColumn), I32, I64, VP, I64], C.c_int),
+        "ml_gpu_join_build_combine": ([VP], C.c_int),
+        "ml_gpu_join_build_finalize": ([VP, P(VP)], C.c_int),
+        "ml_gpu_join_table_stats": ([VP, P(I64), P(I64), P(I64)], C.c_int),
+        "ml_gpu_join_build_destroy": ([VP], C.c_int),
+        "ml_gpu_join_probe": ([VP, VP, P(abi.MlExpr), I32, P(abi.MlColumn), I32, I64, VP, I64, I32, VP, VP, I64,
+                               P(I64)], C.c_int),
+        "ml_gpu_topn_create": ([VP, P(abi.MlPipeOp), I32, VP, I32, P(abi.MlSortKey), I32, I64, P(VP)], C.c_int),
+        "ml_gpu_topn_local_create": ([VP, P(VP)], C.c_int),
+        "ml_gpu_topn_sink": ([VP, P(abi.MlColumn), I32, I64, VP, I64], C.c_int),
+        "ml_gpu_topn_combine": ([VP], C.c_int),
+        "ml_gpu_topn_finalize": ([VP, P(VP)], C.c_int),
+        "ml_gpu_topn_destroy": ([VP], C.c_int),
+    }
+    for name, (args, res) in sigs.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    return lib
+
+
+LIB = _load()
+
+
+def _check(status: int):
+    if status == abi.OK:
+        return
+    msg = LIB.ml_gpu_last_error().decode(errors="replace")
+    if status == abi.ERR_BUDGET:
+        op = C.create_string_buffer(128)
+        r, u, l = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        LIB.ml_gpu_last_budget_error(op, 128, C.byref(r), C.byref(u), C.byref(l))
+        raise ResourcesExhausted(status, msg, op.value.decode(), r.value, u.value, l.value)
+    raise MiniLakeError(status, msg)
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data
+
+
+PROFILE = 2  # ML_CTX_PROFILE
+
+
+class Context:
+    """One device + the query-wide HBM budget (ExecConfig / MemoryPool)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, flags: int = 0):
+        h = C.c_void_p()
+        _check(LIB.ml_gpu_ctx_create(device, hbm_budget, flags, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            LIB.ml_gpu_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def pool_stats(self):
+        u, p, l = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(LIB.ml_gpu_pool_stats(self.h, C.byref(u), C.byref(p), C.byref(l)))
+        return u.value, p.value, l.value
+
+    def synchronize(self):
+        _check(LIB.ml_gpu_ctx_synchronize(self.h))
+
+    def kernel_launches(self) -> int:
+        c = C.c_uint64()
+        _check(LIB.ml_gpu_kernel_launches(self.h, C.byref(c)))
+        return c.value
+
+    def profile(self, kernel: str, reset: bool = False):
+        """(launches, total device ms) of a kernel family; needs flags=PROFILE."""
+        n, ms = C.c_uint64(), C.c_double()
+        _check(LIB.ml_gpu_profile_read(self.h, kernel.encode(), C.byref(n), C.byref(ms), int(reset)))
+        return n.value, ms.value
+
+    def upload(self, cols: Sequence[HostColumn]) -> "DeviceBatch":
+        keep = abi.Keep()
+        arr = (abi.MlColumn * max(len(cols), 1))()
+        for i, c in enumerate(cols):
+            arr[i] = c.to_ml()
+        n = len(cols[0]) if cols else 0
+        h = C.c_void_p()
+        _check(LIB.ml_gpu_batch_upload(self.h, arr, len(cols), n, C.byref(h)))
+        del keep
+        return DeviceBatch(self, h)
+
+    def upload_table(self, table: Table) -> List["DeviceBatch"]:
+        return [self.upload(rg) for rg in table.row_groups]
+
+
+class DeviceBatch:
+    """Columns resident in HBM (an uploaded table or a sink's output)."""
+
+    def __init__(self, ctx: Context, h):
+        self.ctx, self.h = ctx, h
+
+    def close(self):
+        if self.h:
+            LIB.ml_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_rows(self) -> int:
+        n = C.c_int64()
+        _check(LIB.ml_gpu_batch_num_rows(self.h, C.byref(n)))
+        return n.value
+
+    @property
+    def num_columns(self) -> int:
+        n = C.c_int32()
+        _check(LIB.ml_gpu_batch_num_columns(self.h, C.byref(n)))
+        return n.value
+
+    def ml_columns(self):
+        n = self.num_columns
+        arr = (abi.MlColumn * max(n, 1))()
+        _check(LIB.ml_gpu_batch_columns(self.h, arr, n))
+        return arr, n
+
+    @property
+    def types(self) -> List[int]:
+        out = []
+        for i in range(self.num_columns):
+            t = C.c_int32()
+            _check(LIB.ml_gpu_batch_column_info(self.h, i, C.byref(t), None, None))
+            out.append(t.value)
+        return out
+
+    def fetch(self) -> List[HostColumn]:
+        n = self.num_rows
+        cols = []
+        words = (n + 63) // 64
+        for i in range(self.num_columns):
+            t, sb, hv = C.c_int32(), C.c_int64(), C.c_int32()
+            _check(LIB.ml_gpu_batch_column_info(self.h, i, C.byref(t), C.byref(sb), C.byref(hv)))
+            valid = np.zeros(max(words, 1), dtype=np.uint64)
+            if t.value == abi.UTF8:
+                data = np.zeros(max(sb.value, 1), dtype=np.uint8)
+                off = np.zeros(n + 1, dtype=np.uint32)
+                _check(LIB.ml_gpu_batch_fetch(self.h, i, _ptr(data), _ptr(off), _ptr(valid)))
+                col = HostColumn(abi.UTF8, data[:sb.value], offsets=off)
+            else:
+                data = np.zeros(max(n, 1), dtype=abi.NP_DTYPE[t.value])
+                _check(LIB.ml_gpu_batch_fetch(self.h, i, _ptr(data), None, _ptr(valid)))
+                col = HostColumn(t.value, data[:n])
+            if hv.value:
+                col.validity = valid[:words]
+            cols.append(col)
+        return cols
+
+
+def _cols_arg(cols, location=None):
+    """HostColumn list / DeviceBatch / (MlColumn array, n) -> (MlColumn*, ncols, nrows, keep)."""
+    if isinstance(cols, DeviceBatch):
+        arr, n = cols.ml_columns()
+        return arr, n, cols.num_rows, cols
+    if isinstance(cols, tuple):
+        arr, n, nrows = cols
+        return arr, n, nrows, None
+    arr = (abi.MlColumn * max(len(cols), 1))()
+    for i, c in enumerate(cols):
+        arr[i] = c.to_ml()
+    return arr, len(cols), (len(cols[0]) if cols else 0), cols
+
+
+def _sel_arg(sel):
+    if sel is None:
+        return None, 0, None
+    s = np.ascontiguousarray(sel, dtype=np.uint32)
+    return s.ctypes.data, len(s), s
+
+
+# ---- streaming operators ---------------------------------------------------------------
+class FilterOperator:
+    """WHERE: refines the selection vector (operators/filter.rs:19-25)."""
+
+    def __init__(self, ctx: Context, predicate: abi.Expr):
+        self.ctx, self.pred = ctx, predicate
+
+    def execute(self, cols, sel=None) -> np.ndarray:
+        keep = abi.Keep()
+        e = abi.encode_expr(self.pred, abi.BOOL, keep)
+        arr, nc, n, _hold = _cols_arg(cols)
+        sp, ns, _s = _sel_arg(sel)
+        out = np.zeros(max(ns if sel is not None else n, 1), dtype=np.uint32)
+        k = C.c_int64()
+        _check(LIB.ml_gpu_filter(self.ctx.h, C.byref(e), arr, nc, n, sp, ns, abi.LOC_HOST, _ptr(out), C.byref(k)))
+        return out[:k.value]
+
+
+class ProjectionOperator:
+    """SELECT expr: one output column over all physical rows (projection.rs:21-32)."""
+
+    def __init__(self, ctx: Context, expr: abi.Expr, out_type: int):
+        self.ctx, self.expr, self.out_type = ctx, expr, out_type
+
+    def execute(self, cols) -> DeviceBatch:
+        keep = abi.Keep()
+        e = abi.encode_expr(self.expr, self.out_type, keep)
+        arr, nc, n, _hold = _cols_arg(cols)
+        h = C.c_void_p()
+        _check(LIB.ml_gpu_project(self.ctx.h, C.byref(e), arr, nc, n, C.byref(h)))
+        return DeviceBatch(self.ctx, h)
+
+
+def hash_columns(ctx: Context, cols, sel=None) -> np.ndarray:
+    """kernels/hash.rs:16-23 on the device."""
+    arr, nc, n, _hold = _cols_arg(cols)
+    sp, ns, _s = _sel_arg(sel)
+    out = np.zeros(max(ns if sel is not None else n, 1), dtype=np.uint64)
+    _check(LIB.ml_gpu_hash_columns(ctx.h, arr, nc, n, sp, ns, abi.LOC_HOST, _ptr(out)))
+    return out[:(ns if sel is not None else n)]
+
+
+class LocalSink:
+    """The per-thread half of a sink (pipeline.rs:69-79); owns a CUDA stream."""
+
+    def __init__(self, owner, h, fn_sink, fn_combine):
+        self.owner, self.h, self._sink, self._combine = owner, h, fn_sink, fn_combine
+
+    def sink(self, cols, sel=None):
+        """LocalSink::sink: push one batch (HostColumns, a DeviceBatch, or an
+        (MlColumn array, ncols, nrows) tuple) with an optional selection vector."""
+        arr, nc, n, _hold = _cols_arg(cols)
+        sp, ns, _s = _sel_arg(sel)
+        _check(self._sink(self.h, arr, nc, n, sp, ns))
+
+    def combine(self):
+        """LocalSink::combine: merge into the global state (ends this handle)."""
+        if self.h:
+            _check(self._combine(self.h))
+            self.h = None
+
+
+def _local(sink, create, fn_sink, fn_combine) -> LocalSink:
+    h = C.c_void_p()
+    _check(create(sink.h, C.byref(h)))
+    return LocalSink(sink, h, fn_sink, fn_combine)
+
+
+# ---- sinks ------------------------------------------------------------------------------------
+class HashAggregateSink:
+    """GROUP BY (operators/aggregate/hash.rs:434-634); no GROUP BY = ungrouped (ungrouped.rs)."""
+
+    def __init__(self, ctx: Context, input_types: Sequence[int], group_exprs: Sequence[tuple],
+                 aggs: Sequence[abi.AggSpec], prologue: Sequence[abi.PipeOp] = (), size_hint: int = 0):
+        self.ctx = ctx
+        keep = abi.Keep()
+        ops, nops = abi.encode_ops(prologue, keep)
+        g, ng = abi.encode_exprs(group_exprs, keep)
+        a, na = abi.encode_aggs(aggs, keep)
+        types = np.asarray(input_types, dtype=np.int32)
+        h = C.c_void_p()
+        _check(LIB.ml_gpu_hashagg_create(ctx.h, ops, nops, _ptr(types), len(types), g, ng, a, na, size_hint,
+                                          C.byref(h)))
+        self.h = h
+
+    def create_local(self):
+        return _local(self, LIB.ml_gpu_hashagg_local_create, LIB.ml_gpu_hashagg_sink, LIB.ml_gpu_hashagg_combine)
+
+    def finalize(self) -> DeviceBatch:
+        h = C.c_void_p()
+        _check(LIB.ml_gpu_hashagg_finalize(self.h, C.byref(h)))
+        return DeviceBatch(self.ctx, h)
+
+    def stats(self):
+        g, c, r = C.c_int64(), C.c_int64(), C.c_int64()
+        _check(LIB.ml_gpu_hashagg_stats(self.h, C.byref(g), C.byref(c), C.byref(r)))
+        return {"groups": g.value, "capacity": c.value, "resizes": r.value}
+
+    def close(self):
+        if self.h:
+            LIB.ml_gpu_hashagg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class JoinBuildSink:
+    """Build side of the hash join (operators/join.rs:72-242)."""
+
+    def __init__(self, ctx: Context, input_types: Sequence[int], key_exprs: Sequence[tuple],
+                 prologue: Sequence[abi.PipeOp] = ()):
+        self.ctx = ctx
+        keep = abi.Keep()
+        ops, nops = abi.encode_ops(prologue, keep)
+        k, nk = abi.encode_exprs(key_exprs, keep)
+        types = np.asarray(input_types, dtype=np.int32)
+        h = C.c_void_p()
+        _check(LIB.ml_gpu_join_build_create(ctx.h, ops, nops, _ptr(types), len(types), k, nk, C.byref(h)))
+        self.h = h
+        self.table = None
+
+    def create_local(self):
+        return _local(self, LIB.ml_gpu_join_build_local_create, LIB.ml_gpu_join_build_sink,
+                      LIB.ml_gpu_join_build_combine)
+
+    def finalize(self):
+        t = C.c_void_p()
+        _check(LIB.ml_gpu_join_build_finalize(self.h, C.byref(t)))
+        self.table = t.value
+        return self.table
+
+    @property
+    def handle(self):
+        """The finalized table (JoinTableRef) for a HashJoinProbe / Probe operator."""
+        return self.table
+
+    def stats(self):
+        r, d, c = C.c_int64(), C.c_int64(), C.c_int64()
+        _check(LIB.ml_gpu_join_table_stats(self.table, C.byref(r), C.byref(d), C.byref(c)))
+        return {"build_rows": r.value, "distinct_keys": d.value, "capacity": c.value}
+
+    def close(self):
+        if self.h:
+            LIB.ml_gpu_join_build_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HashJoinProbe:
+    """Probe side of the hash join (operators/join.rs:244-337): (probe_row, build_row) pairs."""
+
+    def __init__(self, ctx: Context, table, key_exprs: Sequence[tuple]):
+        self.ctx, self.table, self.keys = ctx, table, key_exprs
+
+    def execute(self, cols, sel=None, cap: Optional[int] = None):
+        keep = abi.Keep()
+        k, nk = abi.encode_exprs(self.keys, keep)
+        arr, nc, n, _hold = _cols_arg(cols)
+        sp, ns, _s = _sel_arg(sel)
+        cap = cap if cap is not None else max(n, 16)
+        while True:
+            pi = np.zeros(max(cap, 1), dtype=np.uint32)
+            bi = np.zeros(max(cap, 1), dtype=np.uint32)
+            npairs = C.c_int64()
+            st = LIB.ml_gpu_join_probe(self.ctx.h, self.table, k, nk, arr, nc, n, sp, ns, abi.LOC_HOST, _ptr(pi),
+                                       _ptr(bi), cap, C.byref(npairs))
+            if st == abi.ERR_INVALID and npairs.value > cap:
+                cap = npairs.value
+                continue
+            _check(st)
+            return pi[:npairs.value], bi[:npairs.value]
+
+
+class SortSink:
+    """ORDER BY ... LIMIT n (top-N; operators/sort.rs:85-267); limit <= 2048."""
+
+    def __init__(self, ctx: Context, input_types: Sequence[int], keys: Sequence[abi.SortKey], limit: int,
+                 prologue: Sequence[abi.PipeOp] = ()):
+        self.ctx = ctx
+        keep = abi.Keep()
+        ops, nops = abi.encode_ops(prologue, keep)
+        k, nk = abi.encode_sort_keys(keys, keep)
+        types = np.asarray(input_types, dtype=np.int32)
+        h = C.c_void_p()
+        _check(LIB.ml_gpu_topn_create(ctx.h, ops, nops, _ptr(types), len(types), k, nk, limit, C.byref(h)))
+        self.h = h
+
+    def create_local(self):
+        return _local(self, LIB.ml_gpu_topn_local_create, LIB.ml_gpu_topn_sink, LIB.ml_gpu_topn_combine)
+
+    def finalize(self) -> DeviceBatch:
+        h = C.c_void_p()
+        _check(LIB.ml_gpu_topn_finalize(self.h, C.byref(h)))
+        return DeviceBatch(self.ctx, h)
+
+    def close(self):
+        if self.h:
+            LIB.ml_gpu_topn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
