@@ -173,8 +173,10 @@ def gpu_arm(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     from minilake_b200.columns import fixed
     from minilake_b200.gpu import PROFILE, Context
+    log(f"[rank {rank}] generating data")
     key, fk, d, v = make_data(rank, world)
     ctx = Context(local, flags=PROFILE)
+    log(f"[rank {rank}] uploading tables")
     q = GpuQuery(ctx, key, fk, d, v)
 
     def barrier():
@@ -183,6 +185,7 @@ def gpu_arm(args):
         torch.cuda.synchronize()
 
     # ---- value: HBM-resident tables, one launch over the whole fact table -------------
+    log(f"[rank {rank}] warm-up")
     for _ in range(args.warmup):
         q.run(q.dim_dev, [q.fact_dev])
     ctx.profile("pipeline_aggregate", reset=True)
@@ -206,6 +209,7 @@ def gpu_arm(args):
     ms_max = float(ms_t.item())
 
     # ---- e2e: pinned host tables; copies inside every step ---------------------------
+    log(f"[rank {rank}] device-resident: {ms_max / args.steps:.3f} ms/step; end-to-end next")
     pinned, keep = [], []
     for a in (fk, d, v):
         p, t = pinned_like(a)
@@ -253,6 +257,7 @@ def gpu_arm(args):
         peak, peak_kind = measured_peak()
         per_launch_ms = agg_ms / max(n_agg, 1)
         achieved = FACT_ROWS * BYTES_PER_ROW / (per_launch_ms / 1e3) / 1e9
+        log("CPU baseline")
         cpu = cpu_baseline(key, fk, d, v) if world == 1 and not args.skip_cpu else None
         line = {
             "metric": METRIC,

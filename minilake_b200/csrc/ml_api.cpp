@@ -596,7 +596,7 @@ int ml_gpu_batch_fetch(const ml_batch* b, int32_t col, void* values, uint32_t* o
         for (int64_t i = 0; i < n; i++) {
             offsets[i] = pos;
             uint32_t a = c.dict->off[codes[i]], e = c.dict->off[codes[i] + 1];
-            memcpy((uint8_t*)values + pos, c.dict->bytes.data() + a, e - a);
+            if (e > a) memcpy((uint8_t*)values + pos, c.dict->bytes.data() + a, e - a);
             pos += e - a;
         }
         offsets[n] = pos;
@@ -774,13 +774,13 @@ int ml_gpu_hash_columns(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64
 // =====================================================================================================
 struct ml_join_build {
     Ctx* ctx;
+    std::unique_ptr<Reservation> res;  // declared before everything charged to it
     Pipeline pipe;
     std::vector<Prog> out_progs;
     OwnedExprs keys;
     std::vector<int> out_types;
     std::mutex mu;
     std::vector<std::unique_ptr<ml_batch>> parts;
-    std::unique_ptr<Reservation> res;
     std::unique_ptr<ml_join_table> table;
     ml_join_build(Ctx* c) : ctx(c), pipe(c) {}
 };
@@ -1045,13 +1045,13 @@ struct AggState {
 
 struct ml_hashagg {
     Ctx* ctx;
+    std::unique_ptr<Reservation> res;  // declared before everything charged to it
     Pipeline pipe;
     KeyLayout keys{};
     std::vector<KeyDecode> dec;
     std::vector<AggState> aggs;
     bool ungrouped = false;
     double max_load = 0.5;
-    std::unique_ptr<Reservation> res;
     std::shared_mutex rw;  // shared: a launch in flight; exclusive: table growth
     uint64_t cap = 0;
     uint32_t gid_cap = 0;
@@ -1487,6 +1487,7 @@ int ml_gpu_hashagg_destroy(ml_hashagg* h) {
 // =====================================================================================================
 struct ml_topn {
     Ctx* ctx;
+    std::unique_ptr<Reservation> res;  // declared before everything charged to it
     Pipeline pipe;
     std::vector<Prog> out_progs;
     std::vector<SortKeySpec> keys;
@@ -1494,7 +1495,6 @@ struct ml_topn {
     int64_t limit;
     std::mutex mu;
     std::vector<std::unique_ptr<ml_batch>> cands;
-    std::unique_ptr<Reservation> res;
     ml_topn(Ctx* c) : ctx(c), pipe(c) {}
 };
 struct ml_topn_local {

@@ -247,10 +247,10 @@ void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrow
     std::vector<std::pair<int, size_t>> gid_at;   // slot -> offset
     std::vector<std::pair<int, size_t>> lut_at;   // lut -> offset
     std::vector<std::pair<int, size_t>> dict_at, dbytes_at;  // slot -> dictionary offsets / bytes
-    auto put = [&](const void* p, size_t n) {
+    auto put = [&](const void* p, size_t n) {  // n bytes (at least one, zeroed) at a 16-byte offset
         size_t o = (scratch.size() + 15) & ~(size_t)15;
-        scratch.resize(o + n);
-        if (n) memcpy(scratch.data() + o, p, n);
+        scratch.resize(o + std::max<size_t>(n, 1), 0);
+        if (n && p) memcpy(scratch.data() + o, p, n);
         return o;
     };
     L.col_valid.assign(C.slots.size(), 0);
@@ -287,7 +287,7 @@ void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrow
             std::vector<uint32_t> doff(hd.off);
             doff.push_back(hd.off.back());  // the spare entry is the empty string
             dict_at.push_back({(int)i, put(doff.data(), doff.size() * 4)});
-            dbytes_at.push_back({(int)i, put(hd.bytes.data(), std::max<size_t>(hd.bytes.size(), 1))});
+            dbytes_at.push_back({(int)i, put(hd.bytes.data(), hd.bytes.size())});
         }
     }
     for (size_t l = 0; l < C.luts.size(); l++) {

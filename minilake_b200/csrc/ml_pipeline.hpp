@@ -77,6 +77,7 @@ void gather_utf8(Ctx* ctx, const uint32_t* off, const uint8_t* bytes, const uint
 
 struct ml_join_table {
     mlg::Ctx* ctx = nullptr;
+    std::unique_ptr<mlg::Reservation> res;  // declared first: released last
     ml_batch batch;  // the concatenated build side
     std::vector<int> key_types;
     int nwords = 1;
@@ -84,7 +85,6 @@ struct ml_join_table {
     uint64_t cap = 0;
     int64_t distinct = 0;
     bool has_dups = false;
-    std::unique_ptr<mlg::Reservation> res;
     mlg::TableView view() const {
         mlg::TableView t{};
         t.state = state.get<uint32_t>();

@@ -786,7 +786,7 @@ Compiler::CV Compiler::compile(const ExprNode& e, const Schema& schema) {
             v.kind = 1;
             v.type = r.dtype;
             v.depth = 1;
-            v.maybe_null = true;
+            v.maybe_null = false;  // a column's validity is checked per launch (Pipeline::reads_nullable)
             v.code.push_back(mk(I_COL, 0, (uint8_t)r.dtype, 0, slot));
             return v;
         }

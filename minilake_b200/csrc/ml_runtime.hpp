@@ -181,11 +181,13 @@ struct DevColumn {
 
 }  // namespace mlg
 
+// Members are destroyed in reverse order: every reservation is declared before the
+// device buffers charged to it, so the buffers are released while it is alive.
 struct ml_batch {
     mlg::Ctx* ctx = nullptr;
+    std::unique_ptr<mlg::Reservation> res;
     int64_t nrows = 0;
     std::vector<std::unique_ptr<mlg::DevColumn>> cols;
-    std::unique_ptr<mlg::Reservation> res;
 };
 
 namespace mlg {

@@ -70,23 +70,31 @@ class GpuEngine:
 
     def join_build(self, source, input_types, key_exprs, prologue=()):
         sink = JoinBuildSink(self.ctx, input_types, key_exprs, prologue)
-        self.drive(sink, source)
-        sink.finalize()
+        try:
+            self.drive(sink, source)
+            sink.finalize()
+        except BaseException:
+            sink.close()  # a failed operator releases everything it reserved
+            raise
         return sink
 
     def hashagg(self, source, input_types, group_exprs, aggs, prologue=(), size_hint=0):
         sink = HashAggregateSink(self.ctx, input_types, group_exprs, aggs, prologue, size_hint)
-        self.drive(sink, source)
-        out = sink.finalize()
-        out.sink_stats = sink.stats()
-        sink.close()
+        try:
+            self.drive(sink, source)
+            out = sink.finalize()
+            out.sink_stats = sink.stats()
+        finally:
+            sink.close()
         return out
 
     def topn(self, source, input_types, keys, limit, prologue=()):
         sink = SortSink(self.ctx, input_types, keys, limit, prologue)
-        self.drive(sink, source)
-        out = sink.finalize()
-        sink.close()
+        try:
+            self.drive(sink, source)
+            out = sink.finalize()
+        finally:
+            sink.close()
         return out
 
     @staticmethod

@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -123,12 +124,20 @@ class Context:
     """One device + the query-wide HBM budget (ExecConfig / MemoryPool)."""
 
     def __init__(self, device: int = 0, hbm_budget: int = 0, flags: int = 0):
+        self.h = None
+        self._children = weakref.WeakSet()  # batches and sinks that must go before the context
         h = C.c_void_p()
         _check(LIB.ml_gpu_ctx_create(device, hbm_budget, flags, C.byref(h)))
         self.h = h
 
+    def _own(self, obj):
+        self._children.add(obj)
+        return obj
+
     def close(self):
         if self.h:
+            for child in list(self._children):
+                child.close()
             LIB.ml_gpu_ctx_destroy(self.h)
             self.h = None
 
@@ -177,6 +186,7 @@ class DeviceBatch:
 
     def __init__(self, ctx: Context, h):
         self.ctx, self.h = ctx, h
+        ctx._own(self)
 
     def close(self):
         if self.h:
@@ -344,6 +354,7 @@ class HashAggregateSink:
         _check(LIB.ml_gpu_hashagg_create(ctx.h, ops, nops, _ptr(types), len(types), g, ng, a, na, size_hint,
                                           C.byref(h)))
         self.h = h
+        ctx._own(self)
 
     def create_local(self):
         return _local(self, LIB.ml_gpu_hashagg_local_create, LIB.ml_gpu_hashagg_sink, LIB.ml_gpu_hashagg_combine)
@@ -384,6 +395,7 @@ class JoinBuildSink:
         _check(LIB.ml_gpu_join_build_create(ctx.h, ops, nops, _ptr(types), len(types), k, nk, C.byref(h)))
         self.h = h
         self.table = None
+        ctx._own(self)
 
     def create_local(self):
         return _local(self, LIB.ml_gpu_join_build_local_create, LIB.ml_gpu_join_build_sink,
@@ -455,6 +467,7 @@ class SortSink:
         h = C.c_void_p()
         _check(LIB.ml_gpu_topn_create(ctx.h, ops, nops, _ptr(types), len(types), k, nk, limit, C.byref(h)))
         self.h = h
+        ctx._own(self)
 
     def create_local(self):
         return _local(self, LIB.ml_gpu_topn_local_create, LIB.ml_gpu_topn_sink, LIB.ml_gpu_topn_combine)
