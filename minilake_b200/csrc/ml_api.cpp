@@ -194,8 +194,8 @@ struct ErrWord {  // a device error word plus a pinned readback slot
     DevBuf d;
     uint32_t* h = nullptr;
     Ctx* ctx;
-    explicit ErrWord(Ctx* c) : d(c, 64, nullptr), ctx(c) { h = (uint32_t*)c->halloc(64); }
-    ~ErrWord() { ctx->hfree(h); }
+    explicit ErrWord(Ctx* c) : d(c, 64, nullptr), ctx(c) { h = (uint32_t*)c->pinned_slot(); }
+    ~ErrWord() { ctx->release_slot(h); }
 };
 
 // The prologue's output for one batch, materialized as owned device columns.
@@ -906,13 +906,17 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
     KeyLayout L = kp.key_layout(j->keys.exprs.data(), (int)j->keys.exprs.size(), kp.out, false, nullptr);
     kp.upload();
     jt->nwords = L.nwords;
-    jt->cap = pow2_at_least(std::max<uint64_t>(16, (uint64_t)n * 2));
-    jt->state = DevBuf(ctx, jt->cap * 4, jt->res.get());
-    jt->keys = DevBuf(ctx, jt->cap * 8 * L.nwords, jt->res.get());
-    jt->payload = DevBuf(ctx, jt->cap * 4, jt->res.get());
+    jt->cap = pow2_at_least(std::max<uint64_t>(16, ((uint64_t)n * 4 + 2) / 3));  // load factor <= 3/4
+    size_t slot_bytes = jt->cap * 8 * (L.nwords == 1 ? 2 : 4);
+    jt->slots = DevBuf(ctx, slot_bytes, jt->res.get());
     jt->next = DevBuf(ctx, std::max<size_t>((size_t)n * 4, 4), jt->res.get());
     jt->dup = DevBuf(ctx, 8, nullptr);
-    CK(cudaMemsetAsync(jt->state.get(), 0, jt->cap * 4, s));
+    CK(cudaMemsetAsync(jt->slots.get(), 0, slot_bytes, s));
+    for (auto& k : j->keys.exprs) {  // which build column each key reads (for GROUP BY the join key)
+        ExprNode e = parse_expr(k);
+        auto o = kp.C.column_origin(e, kp.out);
+        jt->key_cols.push_back(o && e.kind == ML_EXPR_COLUMN ? o->index : -1);
+    }
     CK(cudaMemsetAsync(jt->next.get(), 0xFF, std::max<size_t>((size_t)n * 4, 4), s));
     CK(cudaMemsetAsync(jt->dup.get(), 0, 8, s));
     Staging st(ctx);
@@ -932,9 +936,9 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
     for (auto& c : jt->batch.cols) {
         if (c->kind != CK_UTF8 || n == 0) continue;
         uint64_t cap = pow2_at_least(std::max<uint64_t>(16, (uint64_t)n * 2));
-        DevBuf tstate(ctx, cap * 4, nullptr), tkeys(ctx, cap * 8, nullptr), tpay(ctx, cap * 4, nullptr);
-        CK(cudaMemsetAsync(tstate.get(), 0, cap * 4, s));
-        TableView tv{tstate.get<uint32_t>(), tkeys.get<uint64_t>(), tpay.get<uint32_t>(), cap - 1, 1, 0};
+        DevBuf tslots(ctx, cap * 16, nullptr);
+        CK(cudaMemsetAsync(tslots.get(), 0, cap * 16, s));
+        TableView tv{tslots.get<uint64_t>(), cap - 1, 1, 2};
         c->strid = DevBuf(ctx, (size_t)n * 4, jt->res.get());
         launch_strid(c->optr(), (const uint8_t*)c->dptr(), c->vptr(), n, tv, c->strid.get<uint32_t>(), ew.d.get<uint32_t>(), s);
         ctx->count_launch();
@@ -946,7 +950,6 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
     CK(cudaStreamSynchronize(s));
     check_device_error(ctx, *ew.h);
     jt->has_dups = dup != 0;
-    jt->distinct = -1;
     j->table = std::move(jt);
     *table = j->table.get();
     API_END
@@ -959,11 +962,14 @@ int ml_gpu_join_table_stats(const ml_join_table* t, int64_t* build_rows, int64_t
     if (build_rows) *build_rows = t->batch.nrows;
     if (capacity) *capacity = (int64_t)t->cap;
     if (distinct_keys) {
-        std::vector<uint32_t> st(t->cap);
-        CK(cudaMemcpy(st.data(), t->state.get(), t->cap * 4, cudaMemcpyDeviceToHost));
-        int64_t d = 0;
-        for (uint32_t x : st) d += x != 0;
-        *distinct_keys = d;
+        DevBuf c(t->ctx, 8, nullptr);
+        CK(cudaMemset(c.get(), 0, 8));
+        launch_count_slots(t->view(), c.get<unsigned long long>(), t->ctx->stream);
+        t->ctx->count_launch();
+        unsigned long long d = 0;
+        CK(cudaMemcpyAsync(&d, c.get(), 8, cudaMemcpyDeviceToHost, t->ctx->stream));
+        CK(cudaStreamSynchronize(t->ctx->stream));
+        *distinct_keys = (int64_t)d;
     }
     API_END
 }
@@ -1037,9 +1043,10 @@ namespace {
 struct AggState {
     int func, kind, arg_type, in_type, out_type;
     bool has_arg;
+    int off = 0;           // word offset in the group block
     Prog arg{};
-    bool vcnt_on = false;  // valid-input counts maintained (AVG always)
-    DevBuf v0, vcnt;
+    bool vcnt_on = false;  // valid-input counts maintained
+    DevBuf vcnt;
 };
 }  // namespace
 
@@ -1051,27 +1058,37 @@ struct ml_hashagg {
     std::vector<KeyDecode> dec;
     std::vector<AggState> aggs;
     bool ungrouped = false;
+    int group_probe = -1;  // GROUP BY the join key of this probe: group id = matched build row
+    std::vector<int> group_build_cols;
     double max_load = 0.5;
+    int stride = 1;        // u64 words per group block
     std::shared_mutex rw;  // shared: a launch in flight; exclusive: table growth
     uint64_t cap = 0;
     uint32_t gid_cap = 0;
-    DevBuf state, tkeys, payload, gkeys, gnull, rows, ngroups;
+    DevBuf slots, gkeys, gnull, acc, ngroups;
     int64_t resizes = 0;
+    int64_t final_groups = -1;  // set by finalize
     int smem_groups = 256;
     ml_hashagg(Ctx* c) : ctx(c), pipe(c) {}
 
-    AggArgs args(const Pipeline::Launch& L, unsigned long long* ovf_count, uint32_t* ovf, uint64_t ovf_cap) {
+    TableView table() const {
+        return TableView{slots.get<uint64_t>(), cap ? cap - 1 : 0, keys.nwords, keys.nwords == 1 ? 2 : 4};
+    }
+
+    AggArgs args(unsigned long long* ovf_count, uint32_t* ovf, uint64_t ovf_cap) {
         AggArgs A{};
         A.keys = keys;
-        A.t = TableView{state.get<uint32_t>(), tkeys.get<uint64_t>(), payload.get<uint32_t>(), cap ? cap - 1 : 0, keys.nwords, 0};
+        A.t = table();
         A.gkeys = gkeys.get<uint64_t>();
         A.gnull = gnull.get<uint32_t>();
         A.ngroups = ngroups.get<uint32_t>();
         A.gid_cap = gid_cap;
         A.nagg = (int)aggs.size();
         A.ungrouped = ungrouped;
+        A.group_probe = group_probe;
+        A.stride = stride;
+        A.acc = acc.get<uint64_t>();
         A.smem_groups = std::min<int>(smem_groups, (int)gid_cap);
-        A.rows = rows.get<uint64_t>();
         A.ovf = ovf;
         A.ovf_count = ovf_count;
         A.ovf_cap = ovf_cap;
@@ -1081,70 +1098,64 @@ struct ml_hashagg {
             d.kind = a.kind;
             d.func = a.func;
             d.has_arg = a.has_arg;
-            d.count_valid = a.vcnt_on;
+            d.off = a.off;
+            d.count_valid = a.vcnt_on && a.kind != A_AVG;
             d.arg = a.arg;
-            d.v0 = a.v0.get();
-            d.vcnt = a.vcnt.get<uint64_t>();
+            d.vcnt = a.vcnt_on && a.kind != A_AVG ? a.vcnt.get<uint64_t>() : nullptr;
         }
-        (void)L;
         return A;
     }
 
     // Allocate (or grow to) `want` group ids; existing groups are rehashed into the new
     // table (the doubling of SwissTable::reserve, swiss.rs:287-301).
-    void grow(uint32_t want, cudaStream_t s, ErrWord& ew) {
+    void grow(uint64_t want, cudaStream_t s, ErrWord& ew) {
         uint32_t old_cap = gid_cap;
-        uint64_t ncap = ungrouped ? 1 : pow2_at_least((uint64_t)std::ceil(std::max<uint32_t>(want, 8) / max_load));
-        uint32_t ngid = ungrouped ? 1 : (uint32_t)std::min<uint64_t>((uint64_t)(ncap * max_load), 0xFFFFFFF0ull);
+        bool hashed = !ungrouped && group_probe < 0;
+        uint64_t ncap = hashed ? pow2_at_least((uint64_t)std::ceil(std::max<uint64_t>(want, 8) / max_load)) : 0;
+        uint32_t ngid = hashed ? (uint32_t)std::min<uint64_t>((uint64_t)(ncap * max_load), 0xFFFFFFF0ull)
+                               : (uint32_t)std::max<uint64_t>(want, 1);
         uint32_t ng = 0;
-        if (old_cap) {
+        if (old_cap && hashed) {
             CK(cudaMemcpyAsync(ew.h, ngroups.get(), 4, cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
             ng = std::min(*ew.h, old_cap);
         }
         int nw = keys.nwords ? keys.nwords : 1;
-        DevBuf nstate, ntkeys, npay;
-        if (!ungrouped) {
-            nstate = DevBuf(ctx, ncap * 4, res.get());
-            ntkeys = DevBuf(ctx, ncap * 8 * nw, res.get());
-            npay = DevBuf(ctx, ncap * 4, res.get());
-            CK(cudaMemsetAsync(nstate.get(), 0, ncap * 4, s));
+        int sw = nw == 1 ? 2 : 4;
+        DevBuf nslots, ngk, ngn;
+        if (hashed) {
+            nslots = DevBuf(ctx, ncap * 8 * sw, res.get());
+            CK(cudaMemsetAsync(nslots.get(), 0, ncap * 8 * sw, s));
+            ngk = DevBuf(ctx, (size_t)ngid * 8 * nw, res.get());
+            ngn = DevBuf(ctx, (size_t)ngid * 4, res.get());
         }
-        DevBuf ngk(ctx, (size_t)ngid * 8 * nw, res.get()), ngn(ctx, (size_t)ngid * 4, res.get());
-        DevBuf nrows(ctx, (size_t)ngid * 8, res.get());
-        std::vector<DevBuf> nv0(aggs.size()), nvc(aggs.size());
-        for (size_t k = 0; k < aggs.size(); k++) {
-            if (aggs[k].func != ML_AGG_COUNT_STAR) nv0[k] = DevBuf(ctx, (size_t)ngid * 8, res.get());
-            if (aggs[k].vcnt_on) nvc[k] = DevBuf(ctx, (size_t)ngid * 8, res.get());
-        }
+        DevBuf nacc(ctx, (size_t)ngid * 8 * stride, res.get());
+        std::vector<DevBuf> nvc(aggs.size());
+        for (size_t k = 0; k < aggs.size(); k++)
+            if (aggs[k].vcnt_on && aggs[k].kind != A_AVG) nvc[k] = DevBuf(ctx, (size_t)ngid * 8, res.get());
         if (old_cap) {  // keep the existing groups
-            for (int w = 0; w < nw; w++)
-                if (ng) CK(cudaMemcpyAsync(ngk.get<uint64_t>() + (size_t)w * ngid, gkeys.get<uint64_t>() + (size_t)w * old_cap,
-                                           (size_t)ng * 8, cudaMemcpyDeviceToDevice, s));
-            CK(cudaMemcpyAsync(ngn.get(), gnull.get(), (size_t)old_cap * 4, cudaMemcpyDeviceToDevice, s));
-            CK(cudaMemcpyAsync(nrows.get(), rows.get(), (size_t)old_cap * 8, cudaMemcpyDeviceToDevice, s));
-            for (size_t k = 0; k < aggs.size(); k++) {
-                if (nv0[k]) CK(cudaMemcpyAsync(nv0[k].get(), aggs[k].v0.get(), (size_t)old_cap * 8, cudaMemcpyDeviceToDevice, s));
-                if (nvc[k]) CK(cudaMemcpyAsync(nvc[k].get(), aggs[k].vcnt.get(), (size_t)old_cap * 8, cudaMemcpyDeviceToDevice, s));
+            if (hashed) {
+                for (int w = 0; w < nw; w++)
+                    if (ng) CK(cudaMemcpyAsync(ngk.get<uint64_t>() + (size_t)w * ngid, gkeys.get<uint64_t>() + (size_t)w * old_cap,
+                                               (size_t)ng * 8, cudaMemcpyDeviceToDevice, s));
+                if (ng) CK(cudaMemcpyAsync(ngn.get(), gnull.get(), (size_t)ng * 4, cudaMemcpyDeviceToDevice, s));
             }
+            CK(cudaMemcpyAsync(nacc.get(), acc.get(), (size_t)old_cap * 8 * stride, cudaMemcpyDeviceToDevice, s));
+            for (size_t k = 0; k < aggs.size(); k++)
+                if (nvc[k]) CK(cudaMemcpyAsync(nvc[k].get(), aggs[k].vcnt.get(), (size_t)old_cap * 8, cudaMemcpyDeviceToDevice, s));
         }
-        state = std::move(nstate);
-        tkeys = std::move(ntkeys);
-        payload = std::move(npay);
+        slots = std::move(nslots);
         gkeys = std::move(ngk);
         gnull = std::move(ngn);
-        rows = std::move(nrows);
-        for (size_t k = 0; k < aggs.size(); k++) {
-            aggs[k].v0 = std::move(nv0[k]);
-            aggs[k].vcnt = std::move(nvc[k]);
-        }
-        cap = ungrouped ? 0 : ncap;
+        acc = std::move(nacc);
+        for (size_t k = 0; k < aggs.size(); k++) aggs[k].vcnt = std::move(nvc[k]);
+        cap = ncap;
         gid_cap = ngid;
-        Pipeline::Launch none;
-        AggArgs A = args(none, nullptr, nullptr, 0);
-        launch_agg_init(A, old_cap, ngid, s);
+        AggArgs A = args(nullptr, nullptr, 0);
+        for (size_t k = 0; k < aggs.size(); k++) A.aggs[k].vcnt = aggs[k].vcnt.get<uint64_t>();
+        launch_acc_init(A, old_cap, ngid, s);
         ctx->count_launch();
-        if (!ungrouped && ng) {
+        if (hashed && ng) {
             CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
             launch_agg_rehash(A.t, gkeys.get<uint64_t>(), gnull.get<uint32_t>(), gid_cap, ng, nw, ew.d.get<uint32_t>(), s);
             ctx->count_launch();
@@ -1152,7 +1163,40 @@ struct ml_hashagg {
         }
         CK(cudaMemcpyAsync(ngroups.get(), &ng, 4, cudaMemcpyHostToDevice, s));
         CK(cudaStreamSynchronize(s));
-        if (!ungrouped && ng) check_device_error(ctx, *ew.h);
+        if (hashed && ng) check_device_error(ctx, *ew.h);
+    }
+
+    // The join key of probe p is the GROUP BY key when every group key reads the same
+    // column as the probe key (or the build key it matched) with the same type: then the
+    // matched build row identifies the group and no aggregate hash table is needed.
+    void detect_group_probe(const ml_expr* group, int ngroup) {
+        for (int p = (int)pipe.probes.size() - 1; p >= 0 && ngroup > 0; p--) {
+            ml_join_table* jt = pipe.probes[p].jt;
+            if ((int)jt->key_types.size() != ngroup) continue;
+            const KeyLayout& pk = pipe.probes[p].keys;
+            bool ok = true;
+            std::vector<int> cols;
+            for (int k = 0; k < ngroup && ok; k++) {
+                ExprNode ge = parse_expr(group[k]);
+                auto go = pipe.C.column_origin(ge, pipe.out);
+                int bc = jt->key_cols[k];
+                ok = go && group[k].dtype == jt->key_types[k] && group[k].dtype != ML_TYPE_UTF8 && bc >= 0;
+                if (!ok) break;
+                // the probe key program is a single column load (a column reference)
+                const Prog& pr = pk.prog[k];
+                bool probe_col = pr.len == 1 && pipe.C.code[pr.start].op == I_COL;
+                const SlotInfo* ps = probe_col ? &pipe.C.slots[pipe.C.code[pr.start].a] : nullptr;
+                bool same_probe = ps && ps->src == go->src && ps->index == go->index;
+                bool same_build = go->src == p + 1 && go->index == bc;
+                ok = same_probe || same_build;
+                cols.push_back(bc);
+            }
+            if (ok) {
+                group_probe = p;
+                group_build_cols = cols;
+                return;
+            }
+        }
     }
 };
 
@@ -1165,10 +1209,10 @@ struct ml_hashagg_local {
     uint64_t* h_count;
     ml_hashagg_local(ml_hashagg* k)
         : sink(k), s(k->ctx->new_stream()), st(k->ctx), ew(k->ctx), ovf_count(k->ctx, 16, nullptr) {
-        h_count = (uint64_t*)k->ctx->halloc(16);
+        h_count = (uint64_t*)k->ctx->pinned_slot();
     }
     ~ml_hashagg_local() {
-        sink->ctx->hfree(h_count);
+        sink->ctx->release_slot(h_count);
         sink->ctx->free_stream(s);
     }
 };
@@ -1186,7 +1230,11 @@ int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprol
     auto h = std::make_unique<ml_hashagg>(ctx);
     h->pipe.build(prologue, nprologue, input_types, ninput);
     h->ungrouped = ngroup == 0;
-    if (!h->ungrouped) h->keys = h->pipe.key_layout(group_exprs, ngroup, h->pipe.out, true, &h->dec);
+    if (!h->ungrouped) {
+        h->detect_group_probe(group_exprs, ngroup);
+        if (h->group_probe < 0) h->keys = h->pipe.key_layout(group_exprs, ngroup, h->pipe.out, true, &h->dec);
+    }
+    int words = 1;  // word 0: rows of the group
     for (int k = 0; k < nagg; k++) {  // Accumulator::new (accumulator.rs:110-169)
         AggState a{};
         a.func = aggs[k].func;
@@ -1215,6 +1263,10 @@ int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprol
             }
             default: bad();
         }
+        if (a.func != ML_AGG_COUNT_STAR) {
+            a.off = words;
+            words += a.kind == A_AVG ? 2 : 1;
+        }
         a.has_arg = a.func != ML_AGG_COUNT_STAR;
         if (a.has_arg) {
             REQUIRE(aggs[k].arg.nnodes > 0, "aggregate without an argument");
@@ -1232,17 +1284,22 @@ int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprol
                     h->pipe.C.code.push_back(c);
                     a.arg.len++;
                     a.arg.type = a.in_type;
+                    classify(a.arg, h->pipe.C.code);
                 }
             }
         }
         h->aggs.push_back(std::move(a));
     }
+    h->stride = words;
     h->pipe.upload();
     h->res = std::make_unique<Reservation>(ctx, "HashAggregate");
     h->ngroups = DevBuf(ctx, 16, nullptr);
     CK(cudaMemset(h->ngroups.get(), 0, 16));
     ErrWord ew(ctx);
-    uint32_t want = h->ungrouped ? 1 : (uint32_t)std::min<int64_t>(std::max<int64_t>(size_hint > 0 ? size_hint : 1024, 16), 0x7FFFFFFF);
+    uint64_t want;
+    if (h->ungrouped) want = 1;
+    else if (h->group_probe >= 0) want = (uint64_t)std::max<int64_t>(h->pipe.probes[h->group_probe].jt->batch.nrows, 1);
+    else want = (uint64_t)std::min<int64_t>(std::max<int64_t>(size_hint > 0 ? size_hint : 1024, 16), 0x7FFFFFFF);
     h->grow(want, ctx->stream, ew);
     *out = h.release();
     API_END
@@ -1280,22 +1337,26 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
             if (!a.vcnt_on) {
                 ctx->sync_all();
                 a.vcnt = DevBuf(ctx, (size_t)h->gid_cap * 8, h->res.get());
-                CK(cudaMemcpyAsync(a.vcnt.get(), h->rows.get(), (size_t)h->gid_cap * 8, cudaMemcpyDeviceToDevice, s));
+                // every contribution so far was valid: start from the groups' row counts
+                CK(cudaMemcpy2DAsync(a.vcnt.get(), 8, h->acc.get(), (size_t)h->stride * 8, 8, h->gid_cap,
+                                     cudaMemcpyDeviceToDevice, s));
                 CK(cudaStreamSynchronize(s));
                 a.vcnt_on = true;
             }
         }
     }
     int w = 1 + (int)h->pipe.probes.size();
-    uint64_t ovf_cap = std::max<uint64_t>((uint64_t)L.P.n, 1024);
-    DevBuf ovf(ctx, ovf_cap * w * 4, nullptr);
+    bool can_overflow = !h->ungrouped && h->group_probe < 0;
+    uint64_t ovf_cap = can_overflow ? std::max<uint64_t>((uint64_t)L.P.n, 1024) : 0;
+    DevBuf ovf(ctx, std::max<uint64_t>(ovf_cap * w * 4, 16), nullptr);
     uint64_t count;
     {
         std::shared_lock<std::shared_mutex> lk(h->rw);
         CK(cudaMemsetAsync(local->ovf_count.get(), 0, 8, s));
         CK(cudaMemsetAsync(local->ew.d.get(), 0, 4, s));
         L.P.err = local->ew.d.get<uint32_t>();
-        AggArgs A = h->args(L, local->ovf_count.get<unsigned long long>(), ovf.get<uint32_t>(), ovf_cap);
+        L.P.head_probe = h->group_probe;
+        AggArgs A = h->args(local->ovf_count.get<unsigned long long>(), ovf.get<uint32_t>(), ovf_cap);
         KernelTimer kt(ctx, s, "pipeline_aggregate");
         launch_agg(L.P, A, agg_smem_bytes(A), s);
         kt.stop();
@@ -1314,13 +1375,13 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
         CK(cudaStreamSynchronize(s));
         uint32_t ng = std::min(*local->ew.h, h->gid_cap);
         uint64_t want = std::max<uint64_t>((uint64_t)h->gid_cap * 2, (uint64_t)ng + std::min<uint64_t>(count, 1ull << 30));
-        h->grow((uint32_t)std::min<uint64_t>(want, 0x7FFFFFFFull), s, local->ew);
+        h->grow(std::min<uint64_t>(want, 0x7FFFFFFFull), s, local->ew);
         h->resizes++;
         DevBuf ovf2(ctx, count * w * 4, nullptr);
         CK(cudaMemsetAsync(local->ovf_count.get(), 0, 8, s));
         CK(cudaMemsetAsync(local->ew.d.get(), 0, 4, s));
         L.P.err = local->ew.d.get<uint32_t>();
-        AggArgs A = h->args(L, local->ovf_count.get<unsigned long long>(), ovf2.get<uint32_t>(), count);
+        AggArgs A = h->args(local->ovf_count.get<unsigned long long>(), ovf2.get<uint32_t>(), count);
         launch_agg_resume(L.P, A, ovf.get<uint32_t>(), count, w, agg_smem_bytes(A), s);
         ctx->count_launch();
         CK(cudaMemcpyAsync(local->h_count, local->ovf_count.get(), 8, cudaMemcpyDeviceToHost, s));
@@ -1335,7 +1396,7 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
 
 int ml_gpu_hashagg_combine(ml_hashagg_local* local) {
     API_BEGIN
-    if (local) {  // every local sink updates the one device table: combine only waits
+    if (local) {  // every local sink updates the one device state: combine only waits
         local->sink->ctx->set_current();
         CK(cudaStreamSynchronize(local->s));
         delete local;
@@ -1353,10 +1414,24 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
     ctx->sync_all();
     cudaStream_t s = ctx->stream;
     uint32_t ng = 1;
-    if (!h->ungrouped) {
+    DevBuf gids;  // output row -> group id (GROUP BY the join key: the non-empty build rows)
+    if (h->group_probe >= 0) {
+        int64_t n = h->gid_cap;
+        int nb = select_blocks(n);
+        DevBuf bits(ctx, std::max<size_t>((size_t)(n + 31) / 32 * 4, 4), nullptr);
+        DevBuf counts(ctx, std::max<size_t>((size_t)nb * 4, 4), nullptr);
+        launch_group_flags(h->acc.get<uint64_t>(), h->stride, n, bits.get<uint32_t>(), counts.get<uint32_t>(), s);
+        DevBuf offs;
+        uint64_t total = scan_counts(ctx, counts.get<uint32_t>(), nb, offs, s);
+        gids = DevBuf(ctx, std::max<size_t>(total * 4, 4), nullptr);
+        launch_index_write(n, bits.get<uint32_t>(), offs.get<uint64_t>(), gids.get<uint32_t>(), s);
+        ctx->count_launch(2);
+        ng = (uint32_t)total;
+    } else if (!h->ungrouped) {
         CK(cudaMemcpy(&ng, h->ngroups.get(), 4, cudaMemcpyDeviceToHost));
         ng = std::min(ng, h->gid_cap);
     }
+    h->final_groups = ng;
     auto b = std::make_unique<ml_batch>();
     b->ctx = ctx;
     b->nrows = ng;
@@ -1364,15 +1439,17 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
     FinalArgs F{};
     F.ngroups = ng;
     F.gid_cap = h->gid_cap;
-    F.nkeys = h->ungrouped ? 0 : h->keys.nkeys;
+    F.nkeys = h->ungrouped || h->group_probe >= 0 ? 0 : h->keys.nkeys;
     F.nagg = (int)h->aggs.size();
     F.ungrouped = h->ungrouped;
+    F.stride = h->stride;
     F.gkeys = h->gkeys.get<uint64_t>();
     F.gnull = h->gnull.get<uint32_t>();
-    F.rows = h->rows.get<uint64_t>();
+    F.acc = h->acc.get<uint64_t>();
+    F.gids = gids.get<uint32_t>();
     size_t vbytes = std::max<size_t>((size_t)(ng + 63) / 64 * 8, 8);
     std::vector<std::unique_ptr<DevColumn>> keycols, aggcols;
-    std::vector<DevBuf> id_bufs(F.nkeys);
+    std::vector<DevBuf> id_bufs(std::max(F.nkeys, 0));
     for (int k = 0; k < F.nkeys; k++) {
         F.f[k] = h->keys.f[k];
         auto d = std::make_unique<DevColumn>();
@@ -1391,13 +1468,17 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
         F.key_valid[k] = d->validity.get<uint32_t>();
         keycols.push_back(std::move(d));
     }
+    if (h->group_probe >= 0) {  // the keys are the build keys of the matched rows
+        const ml_batch& bb = h->pipe.probes[h->group_probe].jt->batch;
+        for (int c : h->group_build_cols) keycols.push_back(gather_column(ctx, *bb.cols[c], gids.get<uint32_t>(), ng, s, b->res.get()));
+    }
     for (int k = 0; k < F.nagg; k++) {
         const AggState& a = h->aggs[k];
         AggDev& ad = F.aggs[k];
         ad.kind = a.kind;
         ad.func = a.func;
-        ad.v0 = a.v0.get();
-        ad.vcnt = a.vcnt_on ? a.vcnt.get<uint64_t>() : nullptr;
+        ad.off = a.off;
+        ad.vcnt = a.vcnt_on && a.kind != A_AVG ? a.vcnt.get<uint64_t>() : nullptr;
         F.out_type[k] = a.out_type;
         auto d = std::make_unique<DevColumn>();
         d->dtype = a.out_type;
@@ -1449,6 +1530,7 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
     }
     for (auto& c : keycols) b->cols.push_back(std::move(c));
     for (auto& c : aggcols) b->cols.push_back(std::move(c));
+    CK(cudaStreamSynchronize(s));
     *out = b.release();
     API_END
 }
@@ -1459,7 +1541,10 @@ int ml_gpu_hashagg_stats(ml_hashagg* h, int64_t* groups, int64_t* capacity, int6
     h->ctx->set_current();
     if (groups) {
         uint32_t ng = 1;
-        if (!h->ungrouped) {
+        if (h->group_probe >= 0) {
+            REQUIRE(h->final_groups >= 0, "the number of groups is known after finalize");
+            ng = (uint32_t)h->final_groups;
+        } else if (!h->ungrouped) {
             CK(cudaMemcpy(&ng, h->ngroups.get(), 4, cudaMemcpyDeviceToHost));
             ng = std::min(ng, h->gid_cap);
         }

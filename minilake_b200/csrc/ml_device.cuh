@@ -43,6 +43,7 @@ __device__ inline uint64_t hash_bytes(const uint8_t* b, uint32_t n) {
 struct RowCtx {
     uint32_t r;
     uint32_t b0, b1, b2, b3;
+    uint32_t head;  // first match (chain head) of the probe whose join key is the GROUP BY key
     __device__ __forceinline__ uint32_t row_of(int src) const {
         switch (src) {
             case 0: return r;
@@ -73,10 +74,47 @@ __device__ __forceinline__ uint32_t dict_code(const DCol& c, uint32_t row) {
     return code < c.dict_len ? code : c.dict_len;
 }
 
+// Streaming column reads are read once: load them with an L2 evict-first policy so they
+// do not push the hash tables and accumulators (re-read at random) out of L2.
+__device__ __forceinline__ uint64_t l2_evict_first() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint32_t ld_stream_u32(const void* a) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(l2_evict_first()));
+    return v;
+}
+__device__ __forceinline__ uint64_t ld_stream_u64(const void* a) {
+    uint64_t v;
+    asm volatile("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
+    return v;
+}
+__device__ __forceinline__ uint32_t ld_stream_u8(const void* a) {
+    uint16_t v;
+    asm volatile("ld.global.nc.L2::cache_hint.u8 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(l2_evict_first()));
+    return v;
+}
+
 // Typed load: BOOL 0/1, I32/DATE sign-extended, I64/F64 raw bits, strings as ids.
+// Source columns (src 0) stream; build-side columns are read at random and stay in L2.
 __device__ __forceinline__ uint64_t load_value(const DCol& c, uint32_t row) {
     if (c.kind == CK_DICT) return (uint64_t)__ldg(c.gid + dict_code(c, row));
     if (c.kind == CK_UTF8 || c.kind == CK_STRID) return c.gid ? (uint64_t)__ldg(c.gid + row) : (uint64_t)row;
+    if (c.src == 0) {
+        switch (c.dt) {
+            case ML_TYPE_BOOL: return (uint64_t)ld_stream_u8((const uint8_t*)c.data + row);
+            case ML_TYPE_INT32:
+            case ML_TYPE_DATE: return (uint64_t)(int64_t)(int32_t)ld_stream_u32((const int32_t*)c.data + row);
+            default: return ld_stream_u64((const unsigned long long*)c.data + row);
+        }
+    }
     switch (c.dt) {
         case ML_TYPE_BOOL: return (uint64_t)__ldg((const uint8_t*)c.data + row);
         case ML_TYPE_INT32:
@@ -296,7 +334,42 @@ struct EvalEnv {
     const uint8_t* const* luts;
 };
 
+__device__ __forceinline__ void load_col(const EvalEnv& env, int a, const RowCtx& x, uint64_t& v, bool& ok) {
+    const DCol& c = env.cols[a];
+    uint32_t row = x.row_of(c.src);
+    v = load_value(c, row);
+    ok = valid_bit(c.valid, row);
+}
+
 __device__ inline void eval_prog(const EvalEnv& env, Prog p, const RowCtx& x, uint64_t& out, bool& out_ok) {
+    switch (p.fast) {  // the shape is the same for every thread: a uniform branch
+        case FP_COL: {
+            load_col(env, env.prog[p.start].a, x, out, out_ok);
+            return;
+        }
+        case FP_COL_LIT_BIN: {
+            const Instr& lit = env.prog[p.start + 1];
+            const Instr& bin = env.prog[p.start + 2];
+            uint64_t a;
+            bool av;
+            load_col(env, env.prog[p.start].a, x, a, av);
+            out = binop(bin.sub, bin.t, a, lit.bits, out_ok, av, lit.lit_valid != 0);
+            return;
+        }
+        case FP_COL_LCB_BIN: {
+            const Instr& lit = env.prog[p.start + 1];
+            const Instr& b1 = env.prog[p.start + 3];
+            const Instr& b2 = env.prog[p.start + 4];
+            uint64_t a, b;
+            bool av, bv, tv;
+            load_col(env, env.prog[p.start].a, x, a, av);
+            load_col(env, env.prog[p.start + 2].a, x, b, bv);
+            uint64_t t = binop(b1.sub, b1.t, lit.bits, b, tv, lit.lit_valid != 0, bv);
+            out = binop(b2.sub, b2.t, a, t, out_ok, av, tv);
+            return;
+        }
+        default: break;
+    }
     Stack s;
     s.ok = 0;
     s.v0 = s.v1 = s.v2 = s.v3 = s.v4 = s.v5 = 0;
@@ -382,6 +455,7 @@ __device__ inline void eval_prog(const EvalEnv& env, Prog p, const RowCtx& x, ui
 // Returns false when a key is NULL and `null_kills` (join keys: NULL never matches).
 __device__ inline bool make_key(const EvalEnv& env, const KeyLayout& L, const RowCtx& x, uint64_t* w, uint32_t* nm,
                                 bool null_kills) {
+    uint64_t w0 = 0, w1 = 0;
     w[0] = 0;
     w[1] = 0;
     *nm = 0;
@@ -397,8 +471,12 @@ __device__ inline bool make_key(const EvalEnv& env, const KeyLayout& L, const Ro
         }
         if (f.type == ML_TYPE_FLOAT64 && as_f64(v) == 0.0) v = 0;  // +0.0 == -0.0 (kernels/hash.rs:52-53)
         uint64_t m = f.width >= 64 ? ~0ull : ((1ull << f.width) - 1);
-        w[f.word] |= (v & m) << f.shift;
+        uint64_t bits = (v & m) << f.shift;
+        if (f.word == 0) w0 |= bits;  // named registers: no dynamic indexing of w[]
+        else w1 |= bits;
     }
+    w[0] = w0;
+    w[1] = w1;
     return true;
 }
 __device__ __forceinline__ uint64_t key_hash(const uint64_t* w, int nwords, uint32_t nm = 0) {
@@ -418,21 +496,19 @@ __device__ __forceinline__ void publish_state(uint32_t* p, uint32_t v) {
     cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(*p);
     a.store(v, cuda::memory_order_release);
 }
-__device__ __forceinline__ bool keys_equal(const TableView& t, uint64_t slot, const uint64_t* w) {
-    if (t.keys[slot] != w[0]) return false;
-    if (t.nwords > 1 && t.keys[(t.mask + 1) + slot] != w[1]) return false;
-    return true;
-}
+__device__ __forceinline__ uint64_t* slot_at(const TableView& t, uint64_t i) { return t.slots + i * t.stride; }
 
-// Read-only lookup in a finished table (join probe).
+// Read-only lookup in a finished table (join probe): one 128-bit load per slot.
 __device__ inline uint32_t table_find(const TableView& t, const uint64_t* w, uint64_t h) {
     uint64_t i = h & t.mask;
     for (uint64_t n = 0; n <= t.mask; n++, i = (i + 1) & t.mask) {
-        uint32_t st = __ldg(t.state + i);
-        if (st == 0) return kNone;
-        if (__ldg((const unsigned long long*)t.keys + i) == w[0] &&
-            (t.nwords == 1 || __ldg((const unsigned long long*)t.keys + (t.mask + 1) + i) == w[1]))
-            return __ldg(t.payload + i);
+        ulonglong2 v;
+        asm volatile("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
+                     : "=l"(v.x), "=l"(v.y)
+                     : "l"(slot_at(t, i)), "l"(l2_evict_last()));
+        if ((uint32_t)v.x == 0) return kNone;
+        if (v.y == w[0] && (t.nwords == 1 || __ldg((const unsigned long long*)slot_at(t, i) + 2) == w[1]))
+            return (uint32_t)(v.x >> 32);
     }
     return kNone;
 }
@@ -447,19 +523,21 @@ __device__ inline uint32_t table_upsert(const TableView& t, const uint64_t* w, u
     const uint32_t full = 2u | (nm << 8);
     *inserted = false;
     for (uint64_t n = 0; n <= t.mask;) {
-        uint32_t st = load_state(t.state + i);
+        uint64_t* s = slot_at(t, i);
+        uint32_t* st_p = (uint32_t*)s;
+        uint32_t st = load_state(st_p);
         if (st == 0) {
-            uint32_t old = atomicCAS(t.state + i, 0u, 1u);
+            uint32_t old = atomicCAS(st_p, 0u, 1u);
             if (old == 0) {
                 uint32_t p = assign();
                 if (p == kNone) {
-                    publish_state(t.state + i, 0);
+                    publish_state(st_p, 0);
                     return kNone;
                 }
-                t.keys[i] = w[0];
-                if (t.nwords > 1) t.keys[(t.mask + 1) + i] = w[1];
-                t.payload[i] = p;
-                publish_state(t.state + i, full);
+                s[1] = w[0];
+                if (t.nwords > 1) s[2] = w[1];
+                st_p[1] = p;
+                publish_state(st_p, full);
                 *inserted = true;
                 *slot_out = i;
                 return p;
@@ -470,7 +548,7 @@ __device__ inline uint32_t table_upsert(const TableView& t, const uint64_t* w, u
             uint32_t spins = 0;
             do {
                 __nanosleep(20);
-                st = load_state(t.state + i);
+                st = load_state(st_p);
             } while (st == 1 && ++spins < kSpinLimit);
             if (st == 1) {
                 atomicOr(err, (uint32_t)DE_TIMEOUT);
@@ -478,9 +556,9 @@ __device__ inline uint32_t table_upsert(const TableView& t, const uint64_t* w, u
             }
             if (st == 0) continue;  // the claimer released the slot: retry it
         }
-        if (st == full && keys_equal(t, i, w)) {
+        if (st == full && s[1] == w[0] && (t.nwords == 1 || s[2] == w[1])) {
             *slot_out = i;
-            return t.payload[i];
+            return st_p[1];
         }
         i = (i + 1) & t.mask;
         n++;

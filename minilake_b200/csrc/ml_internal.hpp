@@ -78,10 +78,19 @@ struct Instr {
 };
 static_assert(sizeof(Instr) == 32, "Instr layout");
 
+// Common program shapes get a direct evaluation path (no interpreter loop).
+enum FastPath : int32_t {
+    FP_NONE = 0,
+    FP_COL = 1,           // [COL a]
+    FP_COL_LIT_BIN = 2,   // [COL a, LIT, BIN]              a <op> lit
+    FP_COL_LCB_BIN = 3,   // [COL a, LIT, COL b, BIN, BIN]   a <op2> (lit <op1> b)
+};
+
 struct Prog {
     int32_t start, len;  // range in the pipeline's instruction array
     int32_t type;        // result type
     int32_t maybe_null;  // host analysis: result can be NULL
+    int32_t fast;        // FastPath
 };
 
 // ---- normalized keys -----------------------------------------------------------------
@@ -99,25 +108,29 @@ struct KeyLayout {
 };
 
 // ---- hash tables ---------------------------------------------------------------------
-// Open addressing, power-of-two capacity, linear probing.  Slot state: 0 empty,
-// 1 claimed (being written), 2 | nullmask << 8 full.  Insertion claims a slot
-// with a CAS on the state word, writes the key and payload, then publishes the
-// full state; a thread that meets a claimed slot waits for it with a bounded spin.
+// Open addressing, power-of-two capacity, linear probing, array-of-structs slots:
+//   u64 word 0 = state (low 32 bits) | payload (high 32 bits), words 1.. = key words
+// (16-byte slots for one key word, 32-byte slots for two), so one probe reads one
+// 32-byte sector.  State: 0 empty, 1 claimed (being written), 2 | nullmask << 8 full.
+// Insertion claims a slot with a CAS on the state, writes key and payload, then
+// publishes the full state; a thread that meets a claimed slot waits for it with a
+// bounded spin.
 struct TableView {
-    uint32_t* state;
-    uint64_t* keys;      // nwords x capacity (word-major)
-    uint32_t* payload;   // group id (aggregate) / chain head (join)
+    uint64_t* slots;
     uint64_t mask;       // capacity - 1
-    int32_t nwords;
-    int32_t pad;
+    int32_t nwords;      // key words (1 or 2)
+    int32_t stride;      // u64 words per slot (2 or 4)
 };
 
 // ---- device error word bits -------------------------------------------------------------
 enum DevErr : uint32_t { DE_TIMEOUT = 1u, DE_OVERFLOW_LOST = 2u, DE_BAD_INDEX = 4u };
 
 // ---- aggregate accumulators ---------------------------------------------------------------
+// Every group owns a block of `stride` u64 words: word 0 counts its rows (COUNT(*) and
+// the seen-flags), each aggregate has its value word at `off` (AVG: sum at off, count
+// at off+1).  A group's accumulators thus share one or two 32-byte sectors.
 enum AccKind : int32_t {
-    A_COUNT = 0,   // u64 counts (COUNT(*) / COUNT(x))
+    A_COUNT = 0,   // u64 count of valid inputs (COUNT(x)); COUNT(*) reads word 0
     A_SUM_I64,     // i64 wrapping sum
     A_SUM_F64,
     A_AVG,         // f64 sum + u64 count of valid inputs
@@ -129,10 +142,11 @@ struct AggDev {
     int32_t kind;
     int32_t func;         // ML_AGG_*
     int32_t has_arg;
+    int32_t off;          // word offset inside the group block
     int32_t count_valid;  // maintain vcnt (valid-input counter) in this launch
+    int32_t pad;
     Prog arg;
-    void* v0;             // sum / min / max / count array
-    uint64_t* vcnt;       // valid-input counts (AVG count; seen-tracking for SUM/MIN/MAX)
+    uint64_t* vcnt;       // valid-input counts by group (seen-tracking for SUM/MIN/MAX)
 };
 
 }  // namespace mlg

@@ -36,29 +36,55 @@ __device__ __forceinline__ EvalEnv env_of(const PipeArgs& P) {
     return EvalEnv{P.cols, P.prog, P.arena, P.luts};
 }
 
-__device__ __forceinline__ uint32_t get_cur(const uint32_t (&c)[4], int p) {
-    switch (p) {
-        case 0: return c[0];
-        case 1: return c[1];
-        case 2: return c[2];
-        default: return c[3];
+// Chain cursors of up to four probes, in named registers (no local-memory array).
+struct Cursors {
+    uint32_t c0 = kNone, c1 = kNone, c2 = kNone, c3 = kNone;
+    __device__ __forceinline__ uint32_t get(int p) const {
+        switch (p) {
+            case 0: return c0;
+            case 1: return c1;
+            case 2: return c2;
+            default: return c3;
+        }
     }
-}
-__device__ __forceinline__ void set_cur(uint32_t (&c)[4], int p, uint32_t v) {
-    switch (p) {
-        case 0: c[0] = v; break;
-        case 1: c[1] = v; break;
-        case 2: c[2] = v; break;
-        default: c[3] = v; break;
+    __device__ __forceinline__ void set(int p, uint32_t v) {
+        switch (p) {
+            case 0: c0 = v; break;
+            case 1: c1 = v; break;
+            case 2: c2 = v; break;
+            default: c3 = v; break;
+        }
     }
-}
+};
 
 // Run the streaming stages for one source row; call sink(ctx) for every surviving
 // (row, build matches...) combination.  Duplicate build keys are walked through their
 // chains with backtracking, like HashJoinProbe's chain walk (join.rs:297-309).
 template <class Sink>
 __device__ __forceinline__ void run_stages(const PipeArgs& P, const EvalEnv& env, RowCtx& x, Sink&& sink) {
-    uint32_t cur[4] = {kNone, kNone, kNone, kNone};
+    if (!P.has_chains) {  // every build key is distinct: at most one match per probe, no backtracking
+        for (int s = 0; s < P.nstages; s++) {
+            const Stage st = P.stages[s];
+            if (st.kind == 0) {
+                uint64_t v;
+                bool ok;
+                eval_prog(env, P.filters[st.idx], x, v, ok);
+                if (!(ok && (v & 1))) return;
+            } else {
+                const ProbeDev& pd = P.probes[st.idx];
+                uint64_t w[2];
+                uint32_t nm;
+                if (!make_key(env, pd.keys, x, w, &nm, true)) return;
+                uint32_t b = table_find(pd.t, w, key_hash(w, pd.t.nwords));
+                if (b == kNone) return;
+                x.set_build(st.idx, b);
+                if (st.idx == P.head_probe) x.head = b;
+            }
+        }
+        sink(x);
+        return;
+    }
+    Cursors cur;
     int s = 0;
     for (;;) {
         bool advance = false;
@@ -79,7 +105,8 @@ __device__ __forceinline__ void run_stages(const PipeArgs& P, const EvalEnv& env
                     uint32_t b = table_find(pd.t, w, key_hash(w, pd.t.nwords));
                     if (b != kNone) {
                         x.set_build(st.idx, b);
-                        set_cur(cur, st.idx, pd.next ? __ldg(pd.next + b) : kNone);
+                        if (st.idx == P.head_probe) x.head = b;
+                        cur.set(st.idx, pd.next ? __ldg(pd.next + b) : kNone);
                         advance = true;
                     }
                 }
@@ -93,10 +120,10 @@ __device__ __forceinline__ void run_stages(const PipeArgs& P, const EvalEnv& env
         for (; q >= 0; q--) {
             const Stage st = P.stages[q];
             if (st.kind != 1) continue;
-            uint32_t c = get_cur(cur, st.idx);
+            uint32_t c = cur.get(st.idx);
             if (c != kNone) {
                 x.set_build(st.idx, c);
-                set_cur(cur, st.idx, __ldg(P.probes[st.idx].next + c));
+                cur.set(st.idx, __ldg(P.probes[st.idx].next + c));
                 break;
             }
         }
@@ -106,12 +133,6 @@ __device__ __forceinline__ void run_stages(const PipeArgs& P, const EvalEnv& env
 }
 
 // ---- hash aggregation ---------------------------------------------------------------------
-struct SmemAgg {
-    uint32_t* rows;        // [SG]
-    uint64_t* v[kMaxAggs]; // [SG] value words
-    uint32_t* c[kMaxAggs]; // [SG] valid counts
-};
-
 __device__ __forceinline__ uint64_t agg_identity(int kind) {
     switch (kind) {
         case A_MIN_I64: return 0x7FFFFFFFFFFFFFFFull;
@@ -122,28 +143,37 @@ __device__ __forceinline__ uint64_t agg_identity(int kind) {
     }
 }
 
-__device__ __forceinline__ void acc_global(const AggDev& a, uint32_t g, uint64_t v) {
-    switch (a.kind) {
-        case A_SUM_I64: atomicAdd((unsigned long long*)a.v0 + g, (unsigned long long)v); break;
-        case A_SUM_F64:
-        case A_AVG: atomicAdd((double*)a.v0 + g, as_f64(v)); break;
-        case A_MIN_I64: atomicMin((long long*)a.v0 + g, (long long)v); break;
-        case A_MAX_I64: atomicMax((long long*)a.v0 + g, (long long)v); break;
-        case A_MIN_F64: atomicMin((unsigned long long*)a.v0 + g, (unsigned long long)f64_order(as_f64(v))); break;
-        case A_MAX_F64: atomicMax((unsigned long long*)a.v0 + g, (unsigned long long)f64_order(as_f64(v))); break;
-        default: atomicAdd((unsigned long long*)a.v0 + g, 1ull); break;  // COUNT(x)
+// Fold value v into the accumulator word(s) at `w` (shared or global memory).
+__device__ __forceinline__ void acc_apply(int kind, uint64_t* w, uint64_t v) {
+    switch (kind) {
+        case A_SUM_I64: atomicAdd((unsigned long long*)w, (unsigned long long)v); break;
+        case A_SUM_F64: atomicAdd((double*)w, as_f64(v)); break;
+        case A_AVG:
+            atomicAdd((double*)w, as_f64(v));
+            atomicAdd((unsigned long long*)w + 1, 1ull);
+            break;
+        case A_MIN_I64: atomicMin((long long*)w, (long long)v); break;
+        case A_MAX_I64: atomicMax((long long*)w, (long long)v); break;
+        case A_MIN_F64: atomicMin((unsigned long long*)w, (unsigned long long)f64_order(as_f64(v))); break;
+        case A_MAX_F64: atomicMax((unsigned long long*)w, (unsigned long long)f64_order(as_f64(v))); break;
+        default: atomicAdd((unsigned long long*)w, 1ull); break;  // COUNT(x)
     }
 }
-__device__ __forceinline__ void acc_shared(int kind, uint64_t* slot, uint64_t v) {
+// Merge a shared-memory partial (word(s) at src) into the global block word(s) at dst.
+__device__ __forceinline__ void acc_merge(int kind, uint64_t* dst, const uint64_t* src) {
+    uint64_t v = src[0];
     switch (kind) {
-        case A_SUM_I64: atomicAdd((unsigned long long*)slot, (unsigned long long)v); break;
-        case A_SUM_F64:
-        case A_AVG: atomicAdd((double*)slot, as_f64(v)); break;
-        case A_MIN_I64: atomicMin((long long*)slot, (long long)v); break;
-        case A_MAX_I64: atomicMax((long long*)slot, (long long)v); break;
-        case A_MIN_F64: atomicMin((unsigned long long*)slot, (unsigned long long)f64_order(as_f64(v))); break;
-        case A_MAX_F64: atomicMax((unsigned long long*)slot, (unsigned long long)f64_order(as_f64(v))); break;
-        default: atomicAdd((unsigned long long*)slot, 1ull); break;
+        case A_SUM_I64:
+        case A_COUNT: if (v) atomicAdd((unsigned long long*)dst, (unsigned long long)v); break;
+        case A_SUM_F64: atomicAdd((double*)dst, as_f64(v)); break;
+        case A_AVG:
+            atomicAdd((double*)dst, as_f64(v));
+            if (src[1]) atomicAdd((unsigned long long*)dst + 1, (unsigned long long)src[1]);
+            break;
+        case A_MIN_I64: atomicMin((long long*)dst, (long long)v); break;
+        case A_MAX_I64: atomicMax((long long*)dst, (long long)v); break;
+        case A_MIN_F64: atomicMin((unsigned long long*)dst, (unsigned long long)v); break;
+        case A_MAX_F64: atomicMax((unsigned long long*)dst, (unsigned long long)v); break;
     }
 }
 
@@ -162,10 +192,29 @@ __device__ void record_overflow(const PipeArgs& P, const AggArgs& A, const RowCt
     if (w > 4) o[4] = x.b3;
 }
 
+__device__ __forceinline__ void agg_fold(const PipeArgs& P, const AggArgs& A, const EvalEnv& env, const RowCtx& x,
+                                         uint64_t* blk, uint32_t g) {
+    atomicAdd((unsigned long long*)blk, 1ull);
+    for (int k = 0; k < A.nagg; k++) {
+        const AggDev& a = A.aggs[k];
+        if (a.func == ML_AGG_COUNT_STAR) continue;  // COUNT(*) is the row counter (word 0)
+        uint64_t v = 0;
+        bool ok = true;
+        if (a.has_arg) eval_prog(env, a.arg, x, v, ok);
+        if (!ok) continue;
+        acc_apply(a.kind, blk + a.off, v);
+        if (a.count_valid) atomicAdd((unsigned long long*)a.vcnt + g, 1ull);
+    }
+}
+
 __device__ __forceinline__ void agg_update(const PipeArgs& P, const AggArgs& A, const EvalEnv& env, const RowCtx& x,
-                                           const SmemAgg& S) {
-    uint32_t g = 0;
-    if (!A.ungrouped) {
+                                           uint64_t* smem) {
+    uint32_t g;
+    if (A.group_probe >= 0) {
+        g = x.head;  // every row of a key's chain aggregates into the chain head's group
+    } else if (A.ungrouped) {
+        g = 0;
+    } else {
         uint64_t w[2];
         uint32_t nm;
         make_key(env, A.keys, x, w, &nm, false);
@@ -189,74 +238,36 @@ __device__ __forceinline__ void agg_update(const PipeArgs& P, const AggArgs& A, 
             A.gnull[g] = nm;
         }
     }
-    bool local = (int)g < A.smem_groups;
-    if (local) atomicAdd(S.rows + g, 1u);
-    else atomicAdd((unsigned long long*)A.rows + g, 1ull);
-    for (int k = 0; k < A.nagg; k++) {
-        const AggDev& a = A.aggs[k];
-        if (a.func == ML_AGG_COUNT_STAR) continue;  // COUNT(*) is the row counter
-        uint64_t v = 0;
-        bool ok = true;
-        if (a.has_arg) eval_prog(env, a.arg, x, v, ok);
-        if (!ok) continue;
-        if (local) {
-            acc_shared(a.kind, S.v[k] + g, v);
-            if (a.count_valid) atomicAdd(S.c[k] + g, 1u);
-        } else {
-            acc_global(a, g, v);
-            if (a.count_valid) atomicAdd((unsigned long long*)a.vcnt + g, 1ull);
-        }
+    if ((int)g < A.smem_groups) agg_fold(P, A, env, x, smem + (uint64_t)g * A.stride, g);
+    else agg_fold(P, A, env, x, A.acc + (uint64_t)g * A.stride, g);
+}
+
+__device__ void smem_setup(const AggArgs& A, uint64_t* smem) {
+    for (int g = threadIdx.x; g < A.smem_groups; g += blockDim.x) {
+        uint64_t* b = smem + (uint64_t)g * A.stride;
+        for (int w = 0; w < A.stride; w++) b[w] = 0;
+        for (int k = 0; k < A.nagg; k++)
+            if (A.aggs[k].func != ML_AGG_COUNT_STAR) b[A.aggs[k].off] = agg_identity(A.aggs[k].kind);
     }
 }
 
-__device__ void smem_setup(const AggArgs& A, SmemAgg& S, uint8_t* base) {
-    int SG = A.smem_groups;
-    S.rows = (uint32_t*)base;
-    uint8_t* p = base + (((size_t)SG * 4 + 15) & ~(size_t)15);
-    for (int k = 0; k < A.nagg; k++) {
-        S.v[k] = (uint64_t*)p;
-        p += (size_t)SG * 8;
-        S.c[k] = (uint32_t*)p;
-        p += (((size_t)SG * 4 + 15) & ~(size_t)15);
-    }
-    for (int g = threadIdx.x; g < SG; g += blockDim.x) {
-        S.rows[g] = 0;
-        for (int k = 0; k < A.nagg; k++) {
-            S.v[k][g] = agg_identity(A.aggs[k].kind);
-            S.c[k][g] = 0;
-        }
-    }
-}
-
-__device__ void smem_flush(const AggArgs& A, const SmemAgg& S) {
-    int SG = A.smem_groups;
-    for (int g = threadIdx.x; g < SG; g += blockDim.x) {
-        uint32_t r = S.rows[g];
-        if (!r) continue;
-        atomicAdd((unsigned long long*)A.rows + g, (unsigned long long)r);
+__device__ void smem_flush(const AggArgs& A, const uint64_t* smem) {
+    for (int g = threadIdx.x; g < A.smem_groups; g += blockDim.x) {
+        const uint64_t* b = smem + (uint64_t)g * A.stride;
+        if (!b[0]) continue;
+        uint64_t* d = A.acc + (uint64_t)g * A.stride;
+        atomicAdd((unsigned long long*)d, (unsigned long long)b[0]);
         for (int k = 0; k < A.nagg; k++) {
             const AggDev& a = A.aggs[k];
             if (a.func == ML_AGG_COUNT_STAR) continue;
-            if (a.count_valid && S.c[k][g]) atomicAdd((unsigned long long*)a.vcnt + g, (unsigned long long)S.c[k][g]);
-            uint64_t v = S.v[k][g];
-            switch (a.kind) {
-                case A_COUNT: if (v) atomicAdd((unsigned long long*)a.v0 + g, (unsigned long long)v); break;
-                case A_SUM_I64: atomicAdd((unsigned long long*)a.v0 + g, (unsigned long long)v); break;
-                case A_SUM_F64:
-                case A_AVG: atomicAdd((double*)a.v0 + g, as_f64(v)); break;
-                case A_MIN_I64: atomicMin((long long*)a.v0 + g, (long long)v); break;
-                case A_MAX_I64: atomicMax((long long*)a.v0 + g, (long long)v); break;
-                case A_MIN_F64: atomicMin((unsigned long long*)a.v0 + g, (unsigned long long)v); break;
-                case A_MAX_F64: atomicMax((unsigned long long*)a.v0 + g, (unsigned long long)v); break;
-            }
+            acc_merge(a.kind, d + a.off, b + a.off);
         }
     }
 }
 
 __global__ void __launch_bounds__(kThreads) k_agg(const __grid_constant__ PipeArgs P, const __grid_constant__ AggArgs A) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    SmemAgg S;
-    smem_setup(A, S, smem);
+    extern __shared__ __align__(16) uint64_t smem[];
+    smem_setup(A, smem);
     __syncthreads();
     const EvalEnv env = env_of(P);
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -264,17 +275,17 @@ __global__ void __launch_bounds__(kThreads) k_agg(const __grid_constant__ PipeAr
         RowCtx x;
         x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
         x.b0 = x.b1 = x.b2 = x.b3 = 0;
-        run_stages(P, env, x, [&](const RowCtx& c) { agg_update(P, A, env, c, S); });
+        x.head = 0;
+        run_stages(P, env, x, [&](const RowCtx& c) { agg_update(P, A, env, c, smem); });
     }
     __syncthreads();
-    smem_flush(A, S);
+    smem_flush(A, smem);
 }
 
 __global__ void __launch_bounds__(kThreads) k_agg_resume(const __grid_constant__ PipeArgs P, const __grid_constant__ AggArgs A,
                                                          const uint32_t* ctx, uint64_t count, int w) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    SmemAgg S;
-    smem_setup(A, S, smem);
+    extern __shared__ __align__(16) uint64_t smem[];
+    smem_setup(A, smem);
     __syncthreads();
     const EvalEnv env = env_of(P);
     uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -286,10 +297,11 @@ __global__ void __launch_bounds__(kThreads) k_agg_resume(const __grid_constant__
         x.b1 = w > 2 ? c[2] : 0;
         x.b2 = w > 3 ? c[3] : 0;
         x.b3 = w > 4 ? c[4] : 0;
-        agg_update(P, A, env, x, S);
+        x.head = 0;
+        agg_update(P, A, env, x, smem);
     }
     __syncthreads();
-    smem_flush(A, S);
+    smem_flush(A, smem);
 }
 
 __global__ void k_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
@@ -303,21 +315,23 @@ __global__ void k_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t*
     table_upsert(t, w, nm, key_hash(w, nwords, nm), err, [&]() { return g; }, &inserted, &slot);
 }
 
-__global__ void k_agg_init(AggArgs A, uint32_t from, uint32_t to) {
+__global__ void k_acc_init(AggArgs A, uint32_t from, uint32_t to) {
     uint32_t g = from + blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= to) return;
-    A.rows[g] = 0;
+    uint64_t* b = A.acc + (uint64_t)g * A.stride;
+    for (int w = 0; w < A.stride; w++) b[w] = 0;
     for (int k = 0; k < A.nagg; k++) {
         const AggDev& a = A.aggs[k];
-        if (a.func != ML_AGG_COUNT_STAR) ((uint64_t*)a.v0)[g] = agg_identity(a.kind);
+        if (a.func != ML_AGG_COUNT_STAR) b[a.off] = agg_identity(a.kind);
         if (a.vcnt) a.vcnt[g] = 0;
     }
 }
 
 // Final values (accumulator.rs:500-526): AVG = sum / count, empty -> NULL.
 __global__ void k_agg_final(const __grid_constant__ FinalArgs F) {
-    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    bool in = g < F.ngroups;
+    uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    bool in = o < F.ngroups;
+    uint32_t g = in ? (F.gids ? F.gids[o] : o) : 0;
     uint32_t lane = threadIdx.x & 31;
     for (int k = 0; k < F.nkeys; k++) {
         const KeyField f = F.f[k];
@@ -327,51 +341,53 @@ __global__ void k_agg_final(const __grid_constant__ FinalArgs F) {
             valid = !((F.gnull[g] >> k) & 1u);
             uint64_t m = f.width >= 64 ? ~0ull : ((1ull << f.width) - 1);
             uint64_t v = (w >> f.shift) & m;
-            if (f.strid) ((uint32_t*)F.key_out[k])[g] = (uint32_t)v;
-            else if (f.type == ML_TYPE_BOOL) ((uint8_t*)F.key_out[k])[g] = (uint8_t)v;
-            else if (f.type == ML_TYPE_INT32 || f.type == ML_TYPE_DATE) ((int32_t*)F.key_out[k])[g] = (int32_t)(uint32_t)v;
-            else ((uint64_t*)F.key_out[k])[g] = v;
+            if (f.strid) ((uint32_t*)F.key_out[k])[o] = (uint32_t)v;
+            else if (f.type == ML_TYPE_BOOL) ((uint8_t*)F.key_out[k])[o] = (uint8_t)v;
+            else if (f.type == ML_TYPE_INT32 || f.type == ML_TYPE_DATE) ((int32_t*)F.key_out[k])[o] = (int32_t)(uint32_t)v;
+            else ((uint64_t*)F.key_out[k])[o] = v;
         }
         uint32_t bits = __ballot_sync(0xFFFFFFFFu, in && valid);
-        if (lane == 0 && (g >> 5) < (F.ngroups + 31) / 32) F.key_valid[k][g >> 5] = bits;
+        if (lane == 0 && (o >> 5) < (F.ngroups + 31) / 32) F.key_valid[k][o >> 5] = bits;
     }
+    const uint64_t* blk = F.acc + (uint64_t)g * F.stride;
     for (int k = 0; k < F.nagg; k++) {
         const AggDev& a = F.aggs[k];
         bool valid = false;
         if (in) {
-            uint64_t rows = F.rows[g];
+            uint64_t rows = blk[0];
             uint64_t vc = a.vcnt ? a.vcnt[g] : rows;
             if (a.func == ML_AGG_COUNT_STAR) {
-                ((int64_t*)F.agg_out[k])[g] = (int64_t)rows;
+                ((int64_t*)F.agg_out[k])[o] = (int64_t)rows;
                 valid = true;
             } else if (a.func == ML_AGG_COUNT) {
-                ((int64_t*)F.agg_out[k])[g] = (int64_t)((uint64_t*)a.v0)[g];
+                ((int64_t*)F.agg_out[k])[o] = (int64_t)blk[a.off];
                 valid = true;
             } else {
-                uint64_t v = ((uint64_t*)a.v0)[g];
+                uint64_t v = blk[a.off];
                 valid = vc > 0;
                 switch (a.kind) {
                     case A_AVG: {
-                        double s = as_f64(v);
-                        double r = vc == 0 ? 0.0 : __ddiv_rn(s, __ll2double_rn((long long)vc));
-                        ((double*)F.agg_out[k])[g] = r;
+                        uint64_t c = blk[a.off + 1];
+                        valid = c > 0;
+                        double r = c == 0 ? 0.0 : __ddiv_rn(as_f64(v), __ll2double_rn((long long)c));
+                        ((double*)F.agg_out[k])[o] = r;
                         break;
                     }
                     case A_MIN_F64:
-                    case A_MAX_F64: ((double*)F.agg_out[k])[g] = valid ? f64_unorder(v) : 0.0; break;
+                    case A_MAX_F64: ((double*)F.agg_out[k])[o] = valid ? f64_unorder(v) : 0.0; break;
                     case A_MIN_I64:
                     case A_MAX_I64:
                         if (F.out_type[k] == ML_TYPE_INT32 || F.out_type[k] == ML_TYPE_DATE)
-                            ((int32_t*)F.agg_out[k])[g] = valid ? (int32_t)(int64_t)v : 0;
+                            ((int32_t*)F.agg_out[k])[o] = valid ? (int32_t)(int64_t)v : 0;
                         else
-                            ((int64_t*)F.agg_out[k])[g] = valid ? (int64_t)v : 0;
+                            ((int64_t*)F.agg_out[k])[o] = valid ? (int64_t)v : 0;
                         break;
-                    default: ((uint64_t*)F.agg_out[k])[g] = v; break;
+                    default: ((uint64_t*)F.agg_out[k])[o] = v; break;
                 }
             }
         }
         uint32_t bits = __ballot_sync(0xFFFFFFFFu, in && valid);
-        if (lane == 0 && (g >> 5) < (F.ngroups + 31) / 32) F.agg_valid[k][g >> 5] = bits;
+        if (lane == 0 && (o >> 5) < (F.ngroups + 31) / 32) F.agg_valid[k][o >> 5] = bits;
     }
 }
 
@@ -390,6 +406,7 @@ __global__ void __launch_bounds__(kThreads) k_select_flags(const __grid_constant
             RowCtx x;
             x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
             x.b0 = x.b1 = x.b2 = x.b3 = 0;
+        x.head = 0;
             run_stages(P, env, x, [&](const RowCtx&) { pass = true; });
         }
         uint32_t b = __ballot_sync(0xFFFFFFFFu, pass);
@@ -409,17 +426,16 @@ __global__ void __launch_bounds__(kThreads) k_select_flags(const __grid_constant
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_select_write(const __grid_constant__ PipeArgs P, const uint32_t* bits,
-                                                           const uint64_t* block_offsets, uint32_t* out) {
+// Bits of a pass mask (u32 words) -> the ordered positions (sel[i] when a selection is given).
+__global__ void __launch_bounds__(kThreads) k_index_write(int64_t n, const uint32_t* sel, const uint32_t* bits,
+                                                          const uint64_t* block_offsets, uint32_t* out) {
     __shared__ uint32_t warp_tot[kThreads / 32 * 8];
     int64_t base = (int64_t)blockIdx.x * kSelRowsPerBlock;
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // each warp handles 8 words: word index (base/32) + it*8 + warp
     uint32_t w[8];
     for (int it = 0; it < 8; it++) {
         int64_t wi = (base >> 5) + it * (kThreads / 32) + warp;
-        int64_t row0 = wi * 32;
-        w[it] = row0 < P.n ? bits[wi] : 0u;
+        w[it] = wi * 32 < n ? bits[wi] : 0u;
         if (lane == 0) warp_tot[it * (kThreads / 32) + warp] = __popc(w[it]);
     }
     __syncthreads();
@@ -439,8 +455,30 @@ __global__ void __launch_bounds__(kThreads) k_select_write(const __grid_constant
         if ((m >> lane) & 1u) {
             uint32_t pos = warp_tot[it * (kThreads / 32) + warp] + __popc(m & ((1u << lane) - 1u));
             int64_t i = wi * 32 + lane;
-            out[off + pos] = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+            out[off + pos] = sel ? __ldg(sel + i) : (uint32_t)i;
         }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_group_flags(const uint64_t* acc, int stride, int64_t n, uint32_t* bits,
+                                                          uint32_t* block_counts) {
+    int64_t base = (int64_t)blockIdx.x * kSelRowsPerBlock;
+    uint32_t cnt = 0;
+    for (int it = 0; it < 8; it++) {
+        int64_t i = base + it * kThreads + threadIdx.x;
+        bool pass = i < n && acc[i * stride] != 0;
+        uint32_t b = __ballot_sync(0xFFFFFFFFu, pass);
+        if ((threadIdx.x & 31) == 0 && base + it * kThreads + (threadIdx.x & ~31) < n) bits[(base + it * kThreads + threadIdx.x) >> 5] = b;
+        cnt += pass;
+    }
+    __shared__ uint32_t red[kThreads / 32];
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kThreads / 32; w++) t += red[w];
+        block_counts[blockIdx.x] = t;
     }
 }
 
@@ -534,6 +572,7 @@ __global__ void __launch_bounds__(kThreads) k_project(const __grid_constant__ Pi
             RowCtx x;
             x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
             x.b0 = x.b1 = x.b2 = x.b3 = 0;
+        x.head = 0;
             uint64_t v;
             eval_prog(env, prog, x, v, ok);
             switch (out_type) {
@@ -588,6 +627,7 @@ __global__ void k_join_insert(const __grid_constant__ PipeArgs P, const __grid_c
         RowCtx x;
         x.r = (uint32_t)i;
         x.b0 = x.b1 = x.b2 = x.b3 = 0;
+        x.head = 0;
         uint64_t w[2];
         uint32_t nm;
         if (!make_key(env, L, x, w, &nm, true)) continue;
@@ -597,7 +637,7 @@ __global__ void k_join_insert(const __grid_constant__ PipeArgs P, const __grid_c
         uint32_t p = table_upsert(t, w, 0u, key_hash(w, t.nwords), P.err, [&]() { return r; }, &inserted, &slot);
         if (p == kNone) continue;  // error already flagged (timeout) or table full (never: presized)
         if (!inserted) {
-            uint32_t old = atomicExch(t.payload + slot, r);
+            uint32_t old = atomicExch((uint32_t*)slot_at(t, slot) + 1, r);
             next[r] = old;
             if (*dup_flag == 0) atomicExch(dup_flag, 1u);
         }
@@ -611,6 +651,7 @@ __global__ void k_probe_count(const __grid_constant__ PipeArgs P, uint32_t* coun
         RowCtx x;
         x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
         x.b0 = x.b1 = x.b2 = x.b3 = 0;
+        x.head = 0;
         uint32_t c = 0;
         run_stages(P, env, x, [&](const RowCtx&) { c++; });
         counts[i] = c;
@@ -623,6 +664,7 @@ __global__ void k_probe_write(const __grid_constant__ PipeArgs P, const uint64_t
         RowCtx x;
         x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
         x.b0 = x.b1 = x.b2 = x.b3 = 0;
+        x.head = 0;
         uint64_t o = offsets[i];
         run_stages(P, env, x, [&](const RowCtx& c) {
             pi[o] = c.r;
@@ -630,6 +672,15 @@ __global__ void k_probe_write(const __grid_constant__ PipeArgs P, const uint64_t
             o++;
         });
     }
+}
+
+__global__ void k_count_slots(TableView t, unsigned long long* out) {
+    uint64_t n = t.mask + 1;
+    unsigned long long c = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        c += (uint32_t)slot_at(t, i)[0] != 0;
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
 
 // ---- canonical string ids (equal strings -> the smallest-claimed row) ---------------------------
@@ -647,13 +698,15 @@ __global__ void k_strid(const uint32_t* off, const uint8_t* bytes, const uint64_
         uint64_t s = h & t.mask;
         uint32_t result = kNone;
         for (uint64_t k = 0; k <= t.mask && result == kNone;) {
-            uint32_t st = load_state(t.state + s);
+            uint64_t* sl = slot_at(t, s);
+            uint32_t* st_p = (uint32_t*)sl;
+            uint32_t st = load_state(st_p);
             if (st == 0) {
-                uint32_t old = atomicCAS(t.state + s, 0u, 1u);
+                uint32_t old = atomicCAS(st_p, 0u, 1u);
                 if (old == 0) {
-                    t.keys[s] = h;
-                    t.payload[s] = r;
-                    publish_state(t.state + s, 2);
+                    sl[1] = h;
+                    st_p[1] = r;
+                    publish_state(st_p, 2);
                     result = r;
                     break;
                 }
@@ -663,7 +716,7 @@ __global__ void k_strid(const uint32_t* off, const uint8_t* bytes, const uint64_
                 uint32_t spins = 0;
                 do {
                     __nanosleep(20);
-                    st = load_state(t.state + s);
+                    st = load_state(st_p);
                 } while (st == 1 && ++spins < kSpinLimit);
                 if (st == 1) {
                     atomicOr(err, (uint32_t)DE_TIMEOUT);
@@ -671,8 +724,8 @@ __global__ void k_strid(const uint32_t* off, const uint8_t* bytes, const uint64_
                     break;
                 }
             }
-            if (t.keys[s] == h) {
-                uint32_t c = t.payload[s];
+            if (sl[1] == h) {
+                uint32_t c = st_p[1];
                 uint32_t ca = off[c], cb = off[c + 1];
                 if (cb - ca == b - a && bytes_eq(bytes + a, bytes + ca, b - a)) {
                     result = c;
@@ -819,12 +872,7 @@ __global__ void __launch_bounds__(1024) k_topn_chunk(const __grid_constant__ Sor
 }  // namespace
 
 // ---- launch wrappers -------------------------------------------------------------------------------
-int agg_smem_bytes(const AggArgs& A) {
-    size_t SG = (size_t)A.smem_groups;
-    size_t b = ((SG * 4 + 15) & ~(size_t)15);
-    b += (size_t)A.nagg * (SG * 8 + ((SG * 4 + 15) & ~(size_t)15));
-    return (int)b;
-}
+int agg_smem_bytes(const AggArgs& A) { return (int)((size_t)A.smem_groups * A.stride * 8); }
 void launch_agg(const PipeArgs& P, const AggArgs& A, int smem_bytes, cudaStream_t s) {
     k_agg<<<grid_for(P.n, 8), kThreads, smem_bytes, s>>>(P, A);
 }
@@ -837,9 +885,9 @@ void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull
     if (!ngroups) return;
     k_agg_rehash<<<(ngroups + kThreads - 1) / kThreads, kThreads, 0, s>>>(t, gkeys, gnull, gid_cap, ngroups, nwords, err);
 }
-void launch_agg_init(const AggArgs& A, uint32_t from, uint32_t to, cudaStream_t s) {
+void launch_acc_init(const AggArgs& A, uint32_t from, uint32_t to, cudaStream_t s) {
     if (to <= from) return;
-    k_agg_init<<<(to - from + kThreads - 1) / kThreads, kThreads, 0, s>>>(A, from, to);
+    k_acc_init<<<(to - from + kThreads - 1) / kThreads, kThreads, 0, s>>>(A, from, to);
 }
 void launch_agg_final(const FinalArgs& F, cudaStream_t s) {
     if (!F.ngroups) return;
@@ -854,7 +902,19 @@ void launch_select_flags(const PipeArgs& P, uint32_t* bits, uint32_t* block_coun
 void launch_select_write(const PipeArgs& P, const uint32_t* bits, const uint64_t* block_offsets, uint32_t* out,
                          cudaStream_t s) {
     int nb = select_blocks(P.n);
-    if (nb) k_select_write<<<nb, kThreads, 0, s>>>(P, bits, block_offsets, out);
+    if (nb) k_index_write<<<nb, kThreads, 0, s>>>(P.n, P.sel, bits, block_offsets, out);
+}
+void launch_index_write(int64_t n, const uint32_t* bits, const uint64_t* block_offsets, uint32_t* out, cudaStream_t s) {
+    int nb = select_blocks(n);
+    if (nb) k_index_write<<<nb, kThreads, 0, s>>>(n, nullptr, bits, block_offsets, out);
+}
+void launch_group_flags(const uint64_t* acc, int stride, int64_t n, uint32_t* bits, uint32_t* block_counts,
+                        cudaStream_t s) {
+    int nb = select_blocks(n);
+    if (nb) k_group_flags<<<nb, kThreads, 0, s>>>(acc, stride, n, bits, block_counts);
+}
+void launch_count_slots(TableView t, unsigned long long* out, cudaStream_t s) {
+    k_count_slots<<<grid_for((int64_t)t.mask + 1, 8), kThreads, 0, s>>>(t, out);
 }
 size_t scan_scratch_words(int64_t n) { return (size_t)((n + kScanBlock - 1) / kScanBlock) + 2; }
 void launch_scan_u32(const uint32_t* in, uint64_t* out, int64_t n, uint64_t* scratch, cudaStream_t s) {

@@ -27,6 +27,8 @@ struct PipeArgs {
     const uint8_t* arena;
     uint32_t* err;
     int32_t nstages, nprobes;
+    int32_t head_probe;      // record the chain head of this probe in RowCtx::head (-1: none)
+    int32_t has_chains;      // some probed build side has duplicate keys
     Stage stages[kMaxFilters + kMaxProbes];
     Prog filters[kMaxFilters];
     ProbeDev probes[kMaxProbes];
@@ -43,8 +45,10 @@ struct AggArgs {
     uint32_t gid_cap;
     int32_t nagg;
     int32_t ungrouped;        // no GROUP BY: every row goes to group 0
+    int32_t group_probe;      // >= 0: GROUP BY the join key of this probe; group id = matched build row
     int32_t smem_groups;      // group ids below this are pre-aggregated in shared memory
-    uint64_t* rows;           // rows per group (COUNT(*) and seen-tracking)
+    int32_t stride;           // u64 words per group block
+    uint64_t* acc;            // group blocks (gid_cap x stride)
     uint32_t* ovf;            // overflow row contexts
     unsigned long long* ovf_count;
     uint64_t ovf_cap;
@@ -64,15 +68,18 @@ void launch_agg_resume(const PipeArgs& P, const AggArgs& A, const uint32_t* ctx,
 int agg_smem_bytes(const AggArgs& A);
 void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                        int nwords, uint32_t* err, cudaStream_t s);
+// Initialize group blocks [from, to) to the identities of the aggregates.
+void launch_acc_init(const AggArgs& A, uint32_t from, uint32_t to, cudaStream_t s);
 // Final values: keys decoded into `key_out` (fixed-width or u32 string ids), aggregates into
 // `agg_out`; validity as u32 words (LSB first) in *_valid.
 struct FinalArgs {
     uint32_t ngroups, gid_cap;
-    int32_t nkeys, nagg, ungrouped, pad;
+    int32_t nkeys, nagg, ungrouped, stride;
     KeyField f[kMaxKeys];
     const uint64_t* gkeys;
     const uint32_t* gnull;
-    const uint64_t* rows;
+    const uint64_t* acc;
+    const uint32_t* gids;  // output row -> group id (nullptr: identity)
     void* key_out[kMaxKeys];
     uint32_t* key_valid[kMaxKeys];
     AggDev aggs[kMaxAggs];
@@ -81,13 +88,17 @@ struct FinalArgs {
     uint32_t* agg_valid[kMaxAggs];
 };
 void launch_agg_final(const FinalArgs& F, cudaStream_t s);
-void launch_agg_init(const AggArgs& A, uint32_t from, uint32_t to, cudaStream_t s);
 
 // Filter: pass bits (u32 words) + per-block counts, then ordered compaction.
 int select_blocks(int64_t n);
 void launch_select_flags(const PipeArgs& P, uint32_t* bits, uint32_t* block_counts, cudaStream_t s);
 void launch_select_write(const PipeArgs& P, const uint32_t* bits, const uint64_t* block_offsets, uint32_t* out,
                          cudaStream_t s);
+// Groups with at least one row (group blocks' word 0 > 0): pass bits + per-block counts;
+// then launch_index_write turns bits into the ordered list of group ids.
+void launch_group_flags(const uint64_t* acc, int stride, int64_t n, uint32_t* bits, uint32_t* block_counts,
+                        cudaStream_t s);
+void launch_index_write(int64_t n, const uint32_t* bits, const uint64_t* block_offsets, uint32_t* out, cudaStream_t s);
 // Exclusive scan of u32 counts into u64 offsets (offsets[n] = total).
 void launch_scan_u32(const uint32_t* in, uint64_t* out, int64_t n, uint64_t* scratch, cudaStream_t s);
 size_t scan_scratch_words(int64_t n);
@@ -100,6 +111,8 @@ void launch_hash_columns(const PipeArgs& P, int ncols, const uint64_t* const* di
 // Join build: insert rows 0..n of the build batch.
 void launch_join_insert(const PipeArgs& P, const KeyLayout& L, TableView t, uint32_t* next, uint32_t* dup_flag,
                         int64_t n, cudaStream_t s);
+// Occupied slots of a table (distinct keys).
+void launch_count_slots(TableView t, unsigned long long* out, cudaStream_t s);
 // Standalone probe: per-row match counts, then pair output.
 void launch_probe_count(const PipeArgs& P, uint32_t* counts, cudaStream_t s);
 void launch_probe_write(const PipeArgs& P, const uint64_t* offsets, uint32_t* pi, uint32_t* bi, cudaStream_t s);

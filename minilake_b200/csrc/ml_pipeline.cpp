@@ -234,13 +234,16 @@ void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrow
     P.arena = d_arena.get<uint8_t>();
     P.nstages = nstages;
     P.nprobes = (int)probes.size();
+    P.head_probe = -1;
     for (int i = 0; i < nstages; i++) P.stages[i] = stages[i];
     for (size_t i = 0; i < filters.size(); i++) P.filters[i] = filters[i];
+    P.has_chains = 0;
     for (size_t p = 0; p < probes.size(); p++) {
         ml_join_table* jt = probes[p].jt;
         P.probes[p].t = jt->view();
         P.probes[p].next = jt->has_dups ? jt->next.get<uint32_t>() : nullptr;
         P.probes[p].keys = probes[p].keys;
+        P.has_chains |= jt->has_dups ? 1 : 0;
     }
     // scratch: dictionary id maps and predicate tables for this batch
     std::vector<uint8_t> scratch;

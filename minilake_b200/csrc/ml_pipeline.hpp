@@ -80,18 +80,17 @@ struct ml_join_table {
     std::unique_ptr<mlg::Reservation> res;  // declared first: released last
     ml_batch batch;  // the concatenated build side
     std::vector<int> key_types;
+    std::vector<int> key_cols;  // build key k is build column key_cols[k] (-1: a computed key)
     int nwords = 1;
-    mlg::DevBuf state, keys, payload, next, dup;
+    mlg::DevBuf slots, next, dup;
     uint64_t cap = 0;
-    int64_t distinct = 0;
     bool has_dups = false;
     mlg::TableView view() const {
         mlg::TableView t{};
-        t.state = state.get<uint32_t>();
-        t.keys = keys.get<uint64_t>();
-        t.payload = payload.get<uint32_t>();
+        t.slots = slots.get<uint64_t>();
         t.mask = cap - 1;
         t.nwords = nwords;
+        t.stride = nwords == 1 ? 2 : 4;
         return t;
     }
 };

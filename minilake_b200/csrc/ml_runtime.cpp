@@ -102,8 +102,27 @@ Ctx::~Ctx() {
     cudaSetDevice(device);
     cudaDeviceSynchronize();
     for (auto s : streams_) cudaStreamDestroy(s);
+    for (auto s : idle_streams_) cudaStreamDestroy(s);
     if (stream) cudaStreamDestroy(stream);
     for (auto& kv : free_) cudaFree(kv.second);
+    for (void* p : slabs_) cudaFreeHost(p);
+}
+void* Ctx::pinned_slot() {
+    std::lock_guard<std::mutex> g(mu_);
+    if (free_slots_.empty()) {
+        const size_t slab = 64 * 1024;
+        void* p = nullptr;
+        CK(cudaHostAlloc(&p, slab, cudaHostAllocDefault));
+        slabs_.push_back(p);
+        for (size_t o = 0; o < slab; o += 64) free_slots_.push_back((uint8_t*)p + o);
+    }
+    void* p = free_slots_.back();
+    free_slots_.pop_back();
+    return p;
+}
+void Ctx::release_slot(void* p) {
+    std::lock_guard<std::mutex> g(mu_);
+    free_slots_.push_back(p);
 }
 void Ctx::set_current() const { CK(cudaSetDevice(device)); }
 
@@ -157,7 +176,16 @@ void* Ctx::halloc(size_t bytes) {
     return p;
 }
 void Ctx::hfree(void* p) { cudaFreeHost(p); }
-cudaStream_t Ctx::new_stream() {
+cudaStream_t Ctx::new_stream() {  // streams are pooled: local sinks come and go per pipeline
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        if (!idle_streams_.empty()) {
+            cudaStream_t s = idle_streams_.back();
+            idle_streams_.pop_back();
+            streams_.push_back(s);
+            return s;
+        }
+    }
     cudaStream_t s;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     std::lock_guard<std::mutex> g(mu_);
@@ -165,12 +193,12 @@ cudaStream_t Ctx::new_stream() {
     return s;
 }
 void Ctx::free_stream(cudaStream_t s) {
+    cudaStreamSynchronize(s);
     std::lock_guard<std::mutex> g(mu_);
     auto it = std::find(streams_.begin(), streams_.end(), s);
     if (it != streams_.end()) {
-        cudaStreamSynchronize(s);
-        cudaStreamDestroy(s);
         streams_.erase(it);
+        idle_streams_.push_back(s);
     }
 }
 void Ctx::sync_all() {
@@ -966,6 +994,33 @@ Compiler::CV Compiler::compile(const ExprNode& e, const Schema& schema) {
     raise(ML_ERR_INVALID, "bad expression");
 }
 
+// Peephole: [COL(i32) CAST(->i64) LIT(v) BIN(cmp)] compares in 32 bits when v fits (the
+// planner's Int64 literals against Int32/Date columns, e.g. d <= 2467).
+static void fold_casts(std::vector<Instr>& c) {
+    for (size_t i = 0; i + 3 < c.size(); i++) {
+        Instr &col = c[i], &cast = c[i + 1], &lit = c[i + 2], &bin = c[i + 3];
+        bool narrow = col.t == ML_TYPE_INT32 || col.t == ML_TYPE_DATE;
+        if (col.op == I_COL && narrow && cast.op == I_CAST && cast.t == col.t && cast.sub == ML_TYPE_INT64 &&
+            lit.op == I_LIT && bin.op == I_BIN && bin.sub >= ML_BIN_EQ && bin.sub <= ML_BIN_GTEQ && bin.t == ML_TYPE_INT64) {
+            int64_t v = (int64_t)lit.bits;
+            if (lit.lit_valid && v >= INT32_MIN && v <= INT32_MAX) {
+                lit.t = ML_TYPE_INT32;
+                bin.t = ML_TYPE_INT32;
+                c.erase(c.begin() + (long)i + 1);
+            }
+        }
+    }
+}
+
+void classify(Prog& p, const std::vector<Instr>& code) {
+    auto op = [&](int k) { return code[p.start + k].op; };
+    p.fast = FP_NONE;
+    if (p.len == 1 && op(0) == I_COL) p.fast = FP_COL;
+    else if (p.len == 3 && op(0) == I_COL && op(1) == I_LIT && op(2) == I_BIN) p.fast = FP_COL_LIT_BIN;
+    else if (p.len == 5 && op(0) == I_COL && op(1) == I_LIT && op(2) == I_COL && op(3) == I_BIN && op(4) == I_BIN)
+        p.fast = FP_COL_LCB_BIN;
+}
+
 Prog Compiler::compile_value(const ExprNode& e, const Schema& schema, int out_type) {
     CV c = compile(e, schema);
     if (c.kind == 2) {
@@ -993,12 +1048,14 @@ Prog Compiler::compile_value(const ExprNode& e, const Schema& schema, int out_ty
         v = c;
     }
     if (v.depth > kStack) raise(ML_ERR_UNSUPPORTED, "expression needs a deeper evaluation stack than the GPU kernels keep");
-    Prog p;
+    fold_casts(v.code);
+    Prog p{};
     p.start = (int)code.size();
     p.len = (int)v.code.size();
     p.type = out_type;
     p.maybe_null = v.maybe_null;
     code.insert(code.end(), v.code.begin(), v.code.end());
+    classify(p, code);
     return p;
 }
 
@@ -1006,12 +1063,13 @@ Prog Compiler::compile_string_key(const ExprNode& e, const Schema& schema, int* 
     CV c = compile(e, schema);
     if (c.kind != 2) raise(ML_ERR_UNSUPPORTED, "string key must be a column reference on the GPU");
     *slot_out = c.slot;
-    Prog p;
+    Prog p{};
     p.start = (int)code.size();
     p.len = 1;
     p.type = ML_TYPE_UTF8;
     p.maybe_null = 1;
     code.push_back(mk(I_COL, 0, ML_TYPE_UTF8, 0, c.slot));
+    classify(p, code);
     return p;
 }
 

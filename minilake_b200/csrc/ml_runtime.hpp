@@ -108,6 +108,10 @@ class Ctx {
     void dfree(void* p, size_t cap);
     void* halloc(size_t bytes);  // pinned
     void hfree(void* p);
+    // 64-byte pinned slots for small device->host readbacks (error words, counters),
+    // carved from slabs that live as long as the context.
+    void* pinned_slot();
+    void release_slot(void* p);
     void set_current() const;
     cudaStream_t new_stream();
     void free_stream(cudaStream_t s);
@@ -121,7 +125,8 @@ class Ctx {
     std::mutex mu_, prof_mu_;
     std::map<std::string, std::pair<uint64_t, double>> prof_;
     std::multimap<size_t, void*> free_;  // cached device blocks by capacity
-    std::vector<cudaStream_t> streams_;
+    std::vector<cudaStream_t> streams_, idle_streams_;
+    std::vector<void*> slabs_, free_slots_;
     size_t cached_bytes_ = 0;
 };
 
@@ -278,6 +283,7 @@ class Compiler {
 };
 
 int like_shape(const std::string& pattern, std::string* inner);
+void classify(Prog& p, const std::vector<Instr>& code);  // sets Prog::fast
 bool like_match_host(const std::string& s, const std::string& p, int shape);
 
 }  // namespace mlg

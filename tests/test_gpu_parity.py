@@ -330,3 +330,27 @@ def test_multithreaded_local_sinks_share_one_table(ctx):
     assert got[0].strings() == want[0].strings() and got[1].strings() == want[1].strings()
     assert np.array_equal(got[5].values, want[5].values) and np.array_equal(got[2].values, want[2].values)
     assert rel_err(got[3].values, want[3].values).max() <= F64_TOL
+
+
+@pytest.mark.parametrize("by_build_column", [False, True])
+def test_group_by_join_key_with_duplicate_and_null_build_keys(gpu_engine, by_build_column):
+    rng = np.random.default_rng(11)
+    nd = 3000
+    dk = rng.integers(0, 500, nd).astype(np.int64)  # duplicate keys: chains
+    dim = Table("d", ["k", "x"], [[fixed(INT64, dk, rng.random(nd) > 0.02), fixed(INT32, rng.integers(0, 9, nd))]])
+    fact = Table("f", ["fk", "d", "v"], [[fixed(INT64, rng.integers(-5, 520, 40_000)),
+                                          fixed(INT32, rng.integers(0, 100, 40_000)),
+                                          fixed(FLOAT64, rng.random(40_000), rng.random(40_000) > 0.03)]
+                                         for _ in range(2)])
+    # the build (dim) is on the right: [fk, d, v, k, x]
+    key = Col(3) if by_build_column else Col(0)
+    aggs = [AggSpec(SUM, Col(2), FLOAT64), AggSpec(COUNT_STAR), AggSpec(MIN, Col(1), INT32), AggSpec(COUNT, Col(2), FLOAT64)]
+    res = {}
+    for name, eng in (("gpu", gpu_engine), ("oracle", orc.OracleEngine(threads=2))):
+        j = eng.join_build(dim, [INT64, INT32], [(Col(0), INT64)])
+        out = eng.hashagg(fact, [INT64, INT32, FLOAT64], [(key, INT64)], aggs,
+                          prologue=[Filter(Col(1) < Lit(90)), Probe(j.handle, [(Col(0), INT64)])])
+        if name == "gpu":
+            assert out.sink_stats["capacity"] == 0, "expected the join-key group mode (no aggregate table)"
+        res[name] = eng.fetch(out)
+    assert_same_rows(res["gpu"], res["oracle"], 1, {1})
