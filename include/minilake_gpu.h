@@ -179,8 +179,11 @@ typedef struct ml_topn_local ml_topn_local;
 
 /* ---- context, memory pool, errors -------------------------------------------- */
 /* flags: ML_CTX_PROFILE times the library's main kernels with CUDA events recorded on the
- * stream each kernel is launched on (read back with ml_gpu_profile_read). */
-enum { ML_CTX_DETERMINISTIC = 1, ML_CTX_PROFILE = 2 };
+ * stream each kernel is launched on (read back with ml_gpu_profile_read).
+ * ML_CTX_INTERPRET runs every fused pipeline through the ahead-of-time interpreter kernels;
+ * by default the aggregate and join-build pipelines are specialized at run time (NVRTC,
+ * compiled once per pipeline shape and cached for the process).  Both give the same results. */
+enum { ML_CTX_DETERMINISTIC = 1, ML_CTX_PROFILE = 2, ML_CTX_INTERPRET = 4 };
 
 /* ExecConfig (context.rs:14-34) for one device: hbm_budget_bytes is the query-wide
  * MemoryPool limit (memory.rs:22-26) applied to device bytes; 0 = unlimited. */
@@ -296,7 +299,9 @@ int ml_gpu_topn_destroy(ml_topn* sink);
 int ml_gpu_kernel_launches(ml_ctx* ctx, uint64_t* count);
 /* With ML_CTX_PROFILE: launches and summed device time (ms, CUDA events) of one kernel
  * family: "pipeline_aggregate" (fused filter/probe/aggregate), "join_insert", "topn",
- * "select" (filter compaction).  `reset` clears the counters after reading. */
+ * "select" (filter compaction).  Always recorded: "jit_compile" (runtime compilations and
+ * their host time) and "jit_launch" (launches of runtime-specialized kernels; time 0).
+ * `reset` clears the counters after reading. */
 int ml_gpu_profile_read(ml_ctx* ctx, const char* kernel, uint64_t* launches, double* total_ms, int32_t reset);
 
 #ifdef __cplusplus

@@ -1,0 +1,93 @@
+// Accumulator updates of the hash aggregate (accumulator.rs:110-594), shared by the
+// ahead-of-time kernels and the runtime-specialized pipeline kernels.
+#pragma once
+
+#include "ml_args.hpp"
+#include "ml_device.cuh"
+
+namespace mlg {
+
+// ---- hash aggregation ---------------------------------------------------------------------
+__device__ __forceinline__ uint64_t agg_identity(int kind) {
+    switch (kind) {
+        case A_MIN_I64: return 0x7FFFFFFFFFFFFFFFull;
+        case A_MAX_I64: return 0x8000000000000000ull;
+        case A_MIN_F64: return ~0ull;
+        case A_MAX_F64: return 0ull;
+        default: return 0ull;
+    }
+}
+
+// Fold value v into the accumulator word(s) at `w` (shared or global memory).
+__device__ __forceinline__ void acc_apply(int kind, uint64_t* w, uint64_t v) {
+    switch (kind) {
+        case A_SUM_I64: atomicAdd((unsigned long long*)w, (unsigned long long)v); break;
+        case A_SUM_F64: atomicAdd((double*)w, as_f64(v)); break;
+        case A_AVG:
+            atomicAdd((double*)w, as_f64(v));
+            atomicAdd((unsigned long long*)w + 1, 1ull);
+            break;
+        case A_MIN_I64: atomicMin((long long*)w, (long long)v); break;
+        case A_MAX_I64: atomicMax((long long*)w, (long long)v); break;
+        case A_MIN_F64: atomicMin((unsigned long long*)w, (unsigned long long)f64_order(as_f64(v))); break;
+        case A_MAX_F64: atomicMax((unsigned long long*)w, (unsigned long long)f64_order(as_f64(v))); break;
+        default: atomicAdd((unsigned long long*)w, 1ull); break;  // COUNT(x)
+    }
+}
+// Merge a shared-memory partial (word(s) at src) into the global block word(s) at dst.
+__device__ __forceinline__ void acc_merge(int kind, uint64_t* dst, const uint64_t* src) {
+    uint64_t v = src[0];
+    switch (kind) {
+        case A_SUM_I64:
+        case A_COUNT: if (v) atomicAdd((unsigned long long*)dst, (unsigned long long)v); break;
+        case A_SUM_F64: atomicAdd((double*)dst, as_f64(v)); break;
+        case A_AVG:
+            atomicAdd((double*)dst, as_f64(v));
+            if (src[1]) atomicAdd((unsigned long long*)dst + 1, (unsigned long long)src[1]);
+            break;
+        case A_MIN_I64: atomicMin((long long*)dst, (long long)v); break;
+        case A_MAX_I64: atomicMax((long long*)dst, (long long)v); break;
+        case A_MIN_F64: atomicMin((unsigned long long*)dst, (unsigned long long)v); break;
+        case A_MAX_F64: atomicMax((unsigned long long*)dst, (unsigned long long)v); break;
+    }
+}
+
+__device__ inline void record_overflow(const PipeArgs& P, const AggArgs& A, const RowCtx& x) {
+    unsigned long long k = atomicAdd(A.ovf_count, 1ull);
+    if (k >= A.ovf_cap) {
+        atomicOr(P.err, (uint32_t)DE_OVERFLOW_LOST);
+        return;
+    }
+    int w = 1 + P.nprobes;
+    uint32_t* o = A.ovf + k * (uint64_t)w;
+    o[0] = x.r;
+    if (w > 1) o[1] = x.b0;
+    if (w > 2) o[2] = x.b1;
+    if (w > 3) o[3] = x.b2;
+    if (w > 4) o[4] = x.b3;
+}
+
+__device__ inline void smem_setup(const AggArgs& A, uint64_t* smem) {
+    for (int g = threadIdx.x; g < A.smem_groups; g += blockDim.x) {
+        uint64_t* b = smem + (uint64_t)g * A.stride;
+        for (int w = 0; w < A.stride; w++) b[w] = 0;
+        for (int k = 0; k < A.nagg; k++)
+            if (A.aggs[k].func != ML_AGG_COUNT_STAR) b[A.aggs[k].off] = agg_identity(A.aggs[k].kind);
+    }
+}
+
+__device__ inline void smem_flush(const AggArgs& A, const uint64_t* smem) {
+    for (int g = threadIdx.x; g < A.smem_groups; g += blockDim.x) {
+        const uint64_t* b = smem + (uint64_t)g * A.stride;
+        if (!b[0]) continue;
+        uint64_t* d = A.acc + (uint64_t)g * A.stride;
+        atomicAdd((unsigned long long*)d, (unsigned long long)b[0]);
+        for (int k = 0; k < A.nagg; k++) {
+            const AggDev& a = A.aggs[k];
+            if (a.func == ML_AGG_COUNT_STAR) continue;
+            acc_merge(a.kind, d + a.off, b + a.off);
+        }
+    }
+}
+
+}  // namespace mlg

@@ -4,6 +4,7 @@
 #include <cstring>
 #include <shared_mutex>
 
+#include "ml_jit.hpp"
 #include "ml_pipeline.hpp"
 
 using namespace mlg;
@@ -927,8 +928,19 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
     CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
     LA.P.err = ew.d.get<uint32_t>();
     {
+        void* jit = n ? jit_join_insert_kernel(ctx, kp, LA.P, L) : nullptr;
         KernelTimer kt(ctx, s, "join_insert");
-        launch_join_insert(LA.P, L, jt->view(), jt->next.get<uint32_t>(), jt->dup.get<uint32_t>(), n, s);
+        if (jit) {
+            TableView tv = jt->view();
+            uint32_t* next = jt->next.get<uint32_t>();
+            uint32_t* dup = jt->dup.get<uint32_t>();
+            int64_t nn = n;
+            void* args[] = {&LA.P, &L, &tv, &next, &dup, &nn};
+            jit_launch(jit, pipeline_grid(n), kPipelineThreads, 0, s, args);
+            ctx->add_profile("jit_launch", 0);
+        } else {
+            launch_join_insert(LA.P, L, jt->view(), jt->next.get<uint32_t>(), jt->dup.get<uint32_t>(), n, s);
+        }
         kt.stop();
     }
     ctx->count_launch();
@@ -1357,8 +1369,17 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
         L.P.err = local->ew.d.get<uint32_t>();
         L.P.head_probe = h->group_probe;
         AggArgs A = h->args(local->ovf_count.get<unsigned long long>(), ovf.get<uint32_t>(), ovf_cap);
+        void* jit = jit_agg_kernel(ctx, h->pipe, L.P, A);
         KernelTimer kt(ctx, s, "pipeline_aggregate");
-        launch_agg(L.P, A, agg_smem_bytes(A), s);
+        if (jit) {
+            if (L.P.n) {
+                void* args[] = {&L.P, &A};
+                jit_launch(jit, pipeline_grid(L.P.n), kPipelineThreads, agg_smem_bytes(A), s, args);
+            }
+            ctx->add_profile("jit_launch", 0);
+        } else {
+            launch_agg(L.P, A, agg_smem_bytes(A), s);
+        }
         kt.stop();
         ctx->count_launch();
         CK(cudaMemcpyAsync(local->h_count, local->ovf_count.get(), 8, cudaMemcpyDeviceToHost, s));

@@ -3,8 +3,9 @@
 // keys and the open-addressing hash table.
 #pragma once
 
-#include <cuda/atomic>
+#ifndef __CUDACC_RTC__
 #include <stdint.h>
+#endif
 
 #include "ml_internal.hpp"
 
@@ -88,17 +89,17 @@ __device__ __forceinline__ uint64_t l2_evict_last() {
 }
 __device__ __forceinline__ uint32_t ld_stream_u32(const void* a) {
     uint32_t v;
-    asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(l2_evict_first()));
+    asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(l2_evict_first()));
     return v;
 }
 __device__ __forceinline__ uint64_t ld_stream_u64(const void* a) {
     uint64_t v;
-    asm volatile("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
+    asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
     return v;
 }
 __device__ __forceinline__ uint32_t ld_stream_u8(const void* a) {
     uint16_t v;
-    asm volatile("ld.global.nc.L2::cache_hint.u8 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(l2_evict_first()));
+    asm("ld.global.nc.L2::cache_hint.u8 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(l2_evict_first()));
     return v;
 }
 
@@ -489,12 +490,12 @@ __device__ __forceinline__ uint64_t key_hash(const uint64_t* w, int nwords, uint
 constexpr uint32_t kSpinLimit = 1u << 22;
 
 __device__ __forceinline__ uint32_t load_state(uint32_t* p) {
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(*p);
-    return a.load(cuda::memory_order_acquire);
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
 }
 __device__ __forceinline__ void publish_state(uint32_t* p, uint32_t v) {
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(*p);
-    a.store(v, cuda::memory_order_release);
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ uint64_t* slot_at(const TableView& t, uint64_t i) { return t.slots + i * t.stride; }
 
@@ -503,7 +504,7 @@ __device__ inline uint32_t table_find(const TableView& t, const uint64_t* w, uin
     uint64_t i = h & t.mask;
     for (uint64_t n = 0; n <= t.mask; n++, i = (i + 1) & t.mask) {
         ulonglong2 v;
-        asm volatile("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
+        asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
                      : "=l"(v.x), "=l"(v.y)
                      : "l"(slot_at(t, i)), "l"(l2_evict_last()));
         if ((uint32_t)v.x == 0) return kNone;

@@ -1,0 +1,29 @@
+// Runtime specialization of the fused pipeline kernels.
+//
+// The ahead-of-time kernels interpret each pipeline's programs (a uniform-dispatch stack
+// machine).  For the hot sinks the pipeline is also turned into CUDA C++ source in which
+// every instruction, key field and accumulator is a straight-line statement over the
+// same device helpers (ml_device.cuh, ml_agg.cuh), compiled once per pipeline shape with
+// NVRTC for sm_100a and cached for the process.  Literal values, arena offsets and all
+// pointers stay kernel arguments, so pipelines that differ only in constants share one
+// kernel.  Both forms compute the same results; ML_CTX_INTERPRET selects the interpreter.
+#pragma once
+
+#include "ml_pipeline.hpp"
+
+namespace mlg {
+
+// Specialized fused filter/probe/aggregate kernel (signature of k_agg) for this launch,
+// or nullptr when runtime compilation is unavailable or disabled for the context.
+void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A);
+
+// Specialized join-build insert kernel (signature of k_join_insert), or nullptr.
+void* jit_join_insert_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L);
+
+// Launch a specialized kernel with `args` (pointers to the kernel's parameters).
+void jit_launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream_t s, void** args);
+
+// The generated source of the aggregate kernel (exposed for tests of the generator).
+std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArgs& A);
+
+}  // namespace mlg

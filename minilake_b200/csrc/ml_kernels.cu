@@ -6,9 +6,7 @@
 // kernels on B200: one pass over each column with coalesced loads, grids sized
 // as a multiple of the 148 SMs, state that fits in L2 (126 MB) kept there, and
 // shared-memory privatization wherever many rows hit few addresses.
-#include <cuda/atomic>
-
-#include "ml_device.cuh"
+#include "ml_agg.cuh"
 #include "ml_kernels.cuh"
 
 namespace mlg {
@@ -132,66 +130,6 @@ __device__ __forceinline__ void run_stages(const PipeArgs& P, const EvalEnv& env
     }
 }
 
-// ---- hash aggregation ---------------------------------------------------------------------
-__device__ __forceinline__ uint64_t agg_identity(int kind) {
-    switch (kind) {
-        case A_MIN_I64: return 0x7FFFFFFFFFFFFFFFull;
-        case A_MAX_I64: return 0x8000000000000000ull;
-        case A_MIN_F64: return ~0ull;
-        case A_MAX_F64: return 0ull;
-        default: return 0ull;
-    }
-}
-
-// Fold value v into the accumulator word(s) at `w` (shared or global memory).
-__device__ __forceinline__ void acc_apply(int kind, uint64_t* w, uint64_t v) {
-    switch (kind) {
-        case A_SUM_I64: atomicAdd((unsigned long long*)w, (unsigned long long)v); break;
-        case A_SUM_F64: atomicAdd((double*)w, as_f64(v)); break;
-        case A_AVG:
-            atomicAdd((double*)w, as_f64(v));
-            atomicAdd((unsigned long long*)w + 1, 1ull);
-            break;
-        case A_MIN_I64: atomicMin((long long*)w, (long long)v); break;
-        case A_MAX_I64: atomicMax((long long*)w, (long long)v); break;
-        case A_MIN_F64: atomicMin((unsigned long long*)w, (unsigned long long)f64_order(as_f64(v))); break;
-        case A_MAX_F64: atomicMax((unsigned long long*)w, (unsigned long long)f64_order(as_f64(v))); break;
-        default: atomicAdd((unsigned long long*)w, 1ull); break;  // COUNT(x)
-    }
-}
-// Merge a shared-memory partial (word(s) at src) into the global block word(s) at dst.
-__device__ __forceinline__ void acc_merge(int kind, uint64_t* dst, const uint64_t* src) {
-    uint64_t v = src[0];
-    switch (kind) {
-        case A_SUM_I64:
-        case A_COUNT: if (v) atomicAdd((unsigned long long*)dst, (unsigned long long)v); break;
-        case A_SUM_F64: atomicAdd((double*)dst, as_f64(v)); break;
-        case A_AVG:
-            atomicAdd((double*)dst, as_f64(v));
-            if (src[1]) atomicAdd((unsigned long long*)dst + 1, (unsigned long long)src[1]);
-            break;
-        case A_MIN_I64: atomicMin((long long*)dst, (long long)v); break;
-        case A_MAX_I64: atomicMax((long long*)dst, (long long)v); break;
-        case A_MIN_F64: atomicMin((unsigned long long*)dst, (unsigned long long)v); break;
-        case A_MAX_F64: atomicMax((unsigned long long*)dst, (unsigned long long)v); break;
-    }
-}
-
-__device__ void record_overflow(const PipeArgs& P, const AggArgs& A, const RowCtx& x) {
-    unsigned long long k = atomicAdd(A.ovf_count, 1ull);
-    if (k >= A.ovf_cap) {
-        atomicOr(P.err, (uint32_t)DE_OVERFLOW_LOST);
-        return;
-    }
-    int w = 1 + P.nprobes;
-    uint32_t* o = A.ovf + k * (uint64_t)w;
-    o[0] = x.r;
-    if (w > 1) o[1] = x.b0;
-    if (w > 2) o[2] = x.b1;
-    if (w > 3) o[3] = x.b2;
-    if (w > 4) o[4] = x.b3;
-}
-
 __device__ __forceinline__ void agg_fold(const PipeArgs& P, const AggArgs& A, const EvalEnv& env, const RowCtx& x,
                                          uint64_t* blk, uint32_t g) {
     atomicAdd((unsigned long long*)blk, 1ull);
@@ -240,29 +178,6 @@ __device__ __forceinline__ void agg_update(const PipeArgs& P, const AggArgs& A, 
     }
     if ((int)g < A.smem_groups) agg_fold(P, A, env, x, smem + (uint64_t)g * A.stride, g);
     else agg_fold(P, A, env, x, A.acc + (uint64_t)g * A.stride, g);
-}
-
-__device__ void smem_setup(const AggArgs& A, uint64_t* smem) {
-    for (int g = threadIdx.x; g < A.smem_groups; g += blockDim.x) {
-        uint64_t* b = smem + (uint64_t)g * A.stride;
-        for (int w = 0; w < A.stride; w++) b[w] = 0;
-        for (int k = 0; k < A.nagg; k++)
-            if (A.aggs[k].func != ML_AGG_COUNT_STAR) b[A.aggs[k].off] = agg_identity(A.aggs[k].kind);
-    }
-}
-
-__device__ void smem_flush(const AggArgs& A, const uint64_t* smem) {
-    for (int g = threadIdx.x; g < A.smem_groups; g += blockDim.x) {
-        const uint64_t* b = smem + (uint64_t)g * A.stride;
-        if (!b[0]) continue;
-        uint64_t* d = A.acc + (uint64_t)g * A.stride;
-        atomicAdd((unsigned long long*)d, (unsigned long long)b[0]);
-        for (int k = 0; k < A.nagg; k++) {
-            const AggDev& a = A.aggs[k];
-            if (a.func == ML_AGG_COUNT_STAR) continue;
-            acc_merge(a.kind, d + a.off, b + a.off);
-        }
-    }
 }
 
 __global__ void __launch_bounds__(kThreads) k_agg(const __grid_constant__ PipeArgs P, const __grid_constant__ AggArgs A) {
@@ -840,27 +755,56 @@ __device__ int cmp_rows(const SortDev& S, uint32_t a, uint32_t b) {
     return 0;
 }
 
+// Order-preserving 64-bit prefix of the first sort key: prefix(a) < prefix(b) implies
+// cmp_rows(a, b) < 0, so rows are compared through shared memory and cmp_rows runs
+// only on equal prefixes (ties, NULLs and padding).
+__device__ __forceinline__ uint64_t sort_prefix(const SortDev& S, uint32_t r) {
+    if (r == kNone) return ~0ull;
+    const DCol& c = S.cols[0];
+    if (!valid_bit(c.valid, r)) return S.nulls_first[0] ? 0ull : ~0ull;
+    uint64_t p;
+    if (c.kind == CK_UTF8) {
+        Str s = col_str(c, r);
+        p = 0;
+        uint32_t m = s.n < 8 ? s.n : 8;
+        for (uint32_t j = 0; j < m; j++) p |= (uint64_t)__ldg(s.p + j) << (56 - 8 * j);
+    } else {
+        uint64_t x = load_value(c, r);
+        if (c.dt == ML_TYPE_FLOAT64) p = (uint64_t)total_key(as_f64(x)) ^ 0x8000000000000000ull;
+        else if (c.dt == ML_TYPE_BOOL) p = x;
+        else p = x ^ 0x8000000000000000ull;
+    }
+    return S.asc[0] ? p : ~p;
+}
+
+// One block sorts kTopNChunk rows (bitonic, ascending by compare_rows) and writes the
+// first k.  Keys are compared by their shared-memory prefix first.
 __global__ void __launch_bounds__(1024) k_topn_chunk(const __grid_constant__ SortDev S, const uint32_t* in, int64_t n,
                                                     int k, uint32_t* out) {
+    __shared__ uint64_t pre[kTopNChunk];
     __shared__ uint32_t idx[kTopNChunk];
     int64_t base = (int64_t)blockIdx.x * kTopNChunk;
     for (int j = threadIdx.x; j < kTopNChunk; j += blockDim.x) {
         int64_t i = base + j;
-        idx[j] = i < n ? (in ? in[i] : (uint32_t)i) : kNone;
+        uint32_t r = i < n ? (in ? in[i] : (uint32_t)i) : kNone;
+        idx[j] = r;
+        pre[j] = sort_prefix(S, r);
     }
     __syncthreads();
-    // bitonic sort, ascending by cmp_rows
     for (int size = 2; size <= kTopNChunk; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
             for (int t = threadIdx.x; t < kTopNChunk / 2; t += blockDim.x) {
                 int lo = 2 * t - (t & (stride - 1));
                 int hi = lo + stride;
                 bool up = (lo & size) == 0;
-                uint32_t a = idx[lo], b = idx[hi];
-                int c = cmp_rows(S, a, b);
+                uint64_t pa = pre[lo], pb = pre[hi];
+                int c = pa < pb ? -1 : (pa > pb ? 1 : cmp_rows(S, idx[lo], idx[hi]));
                 if ((c > 0) == up && c != 0) {
-                    idx[lo] = b;
+                    uint32_t a = idx[lo];
+                    idx[lo] = idx[hi];
                     idx[hi] = a;
+                    pre[lo] = pb;
+                    pre[hi] = pa;
                 }
             }
             __syncthreads();
@@ -872,6 +816,7 @@ __global__ void __launch_bounds__(1024) k_topn_chunk(const __grid_constant__ Sor
 }  // namespace
 
 // ---- launch wrappers -------------------------------------------------------------------------------
+int pipeline_grid(int64_t n) { return grid_for(n, 8); }
 int agg_smem_bytes(const AggArgs& A) { return (int)((size_t)A.smem_groups * A.stride * 8); }
 void launch_agg(const PipeArgs& P, const AggArgs& A, int smem_bytes, cudaStream_t s) {
     k_agg<<<grid_for(P.n, 8), kThreads, smem_bytes, s>>>(P, A);

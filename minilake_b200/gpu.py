@@ -118,6 +118,7 @@ def _ptr(a: Optional[np.ndarray]):
 
 
 PROFILE = 2  # ML_CTX_PROFILE
+INTERPRET = 4  # ML_CTX_INTERPRET: ahead-of-time interpreter kernels instead of specialized ones
 
 
 class Context:

@@ -16,10 +16,13 @@ pytestmark = pytest.mark.gpu
 F64_TOL = 1e-12
 
 
-@pytest.fixture(scope="module")
-def ctx():
-    from minilake_b200.gpu import Context
-    c = Context(0)
+@pytest.fixture(scope="module", params=["specialized", "interpreter"])
+def ctx(request):
+    """Every parity test runs twice: with the runtime-specialized pipeline kernels (the
+    default) and with the ahead-of-time interpreter kernels (ML_CTX_INTERPRET)."""
+    from minilake_b200.gpu import INTERPRET, Context
+    c = Context(0, flags=INTERPRET if request.param == "interpreter" else 0)
+    c.mode = request.param
     yield c
     c.close()
 
@@ -191,6 +194,22 @@ def test_hashagg_matches_oracle(gpu_engine, keys):
         nk = len(keys)
         fl = {nk + 2, nk + 4}
         assert_same_rows(got, want, nk, fl)
+
+
+def test_predicates_in_fused_aggregate(ctx, gpu_engine):
+    """Every expression form as the filter of a fused aggregate (the pipeline kernel
+    evaluates it per row), against the oracle."""
+    rng = np.random.default_rng(9)
+    t = Table("t", [str(i) for i in range(7)], [random_batch(rng, n) for n in (7000, 3000)])
+    aggs = [AggSpec(COUNT_STAR), AggSpec(SUM, Col(2), FLOAT64), AggSpec(MIN, Col(1), INT64)]
+    oracle = orc.OracleEngine(threads=2)
+    before = ctx.profile("jit_launch")[0]
+    for pred in PREDICATES:
+        got = gpu_engine.fetch(gpu_engine.hashagg(t, TYPES, [(Col(0), INT32)], aggs, [Filter(pred)]))
+        want = oracle.fetch(oracle.hashagg(t, TYPES, [(Col(0), INT32)], aggs, [Filter(pred)]))
+        assert_same_rows(got, want, 1, {2})
+    launched = ctx.profile("jit_launch")[0] - before
+    assert launched > 0 if ctx.mode == "specialized" else launched == 0
 
 
 def test_hashagg_resize_on_overflow_is_exact(gpu_engine):
