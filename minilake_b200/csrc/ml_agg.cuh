@@ -34,6 +34,31 @@ __device__ __forceinline__ void acc_apply(int kind, uint64_t* w, uint64_t v) {
         default: atomicAdd((unsigned long long*)w, 1ull); break;  // COUNT(x)
     }
 }
+// acc_apply for accumulators known to be in global memory: fire-and-forget reductions
+// (red.global), so no thread waits for the L2 to answer.
+__device__ __forceinline__ void acc_apply_global(int kind, uint64_t* w, uint64_t v) {
+    switch (kind) {
+        case A_SUM_I64: asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(w), "l"(v) : "memory"); break;
+        case A_SUM_F64: asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(w), "d"(as_f64(v)) : "memory"); break;
+        case A_AVG:
+            asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(w), "d"(as_f64(v)) : "memory");
+            asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(w + 1), "l"(1ull) : "memory");
+            break;
+        case A_MIN_I64: asm volatile("red.relaxed.gpu.global.min.s64 [%0], %1;" ::"l"(w), "l"(v) : "memory"); break;
+        case A_MAX_I64: asm volatile("red.relaxed.gpu.global.max.s64 [%0], %1;" ::"l"(w), "l"(v) : "memory"); break;
+        case A_MIN_F64:
+            asm volatile("red.relaxed.gpu.global.min.u64 [%0], %1;" ::"l"(w), "l"(f64_order(as_f64(v))) : "memory");
+            break;
+        case A_MAX_F64:
+            asm volatile("red.relaxed.gpu.global.max.u64 [%0], %1;" ::"l"(w), "l"(f64_order(as_f64(v))) : "memory");
+            break;
+        default: asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(w), "l"(1ull) : "memory"); break;
+    }
+}
+__device__ __forceinline__ void count_global(uint64_t* w) {
+    asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(w), "l"(1ull) : "memory");
+}
+
 // Merge a shared-memory partial (word(s) at src) into the global block word(s) at dst.
 __device__ __forceinline__ void acc_merge(int kind, uint64_t* dst, const uint64_t* src) {
     uint64_t v = src[0];

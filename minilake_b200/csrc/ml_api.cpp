@@ -907,7 +907,7 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
     KeyLayout L = kp.key_layout(j->keys.exprs.data(), (int)j->keys.exprs.size(), kp.out, false, nullptr);
     kp.upload();
     jt->nwords = L.nwords;
-    jt->cap = pow2_at_least(std::max<uint64_t>(16, ((uint64_t)n * 4 + 2) / 3));  // load factor <= 3/4
+    jt->cap = pow2_at_least(std::max<uint64_t>(16, (uint64_t)n * 2));  // load factor <= 1/2: short probes
     size_t slot_bytes = jt->cap * 8 * (L.nwords == 1 ? 2 : 4);
     jt->slots = DevBuf(ctx, slot_bytes, jt->res.get());
     jt->next = DevBuf(ctx, std::max<size_t>((size_t)n * 4, 4), jt->res.get());
@@ -1062,6 +1062,8 @@ struct AggState {
 };
 }  // namespace
 
+constexpr uint32_t kSmemPreaggMaxGroups = 65536;
+
 struct ml_hashagg {
     Ctx* ctx;
     std::unique_ptr<Reservation> res;  // declared before everything charged to it
@@ -1100,7 +1102,9 @@ struct ml_hashagg {
         A.group_probe = group_probe;
         A.stride = stride;
         A.acc = acc.get<uint64_t>();
-        A.smem_groups = std::min<int>(smem_groups, (int)gid_cap);
+        // shared-memory pre-aggregation pays off when the group space is small enough that
+        // the first groups take a large share of the rows
+        A.smem_groups = (ungrouped || gid_cap <= kSmemPreaggMaxGroups) ? std::min<int>(smem_groups, (int)gid_cap) : 0;
         A.ovf = ovf;
         A.ovf_count = ovf_count;
         A.ovf_cap = ovf_cap;
@@ -1374,7 +1378,8 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
         if (jit) {
             if (L.P.n) {
                 void* args[] = {&L.P, &A};
-                jit_launch(jit, pipeline_grid(L.P.n), kPipelineThreads, agg_smem_bytes(A), s, args);
+                int64_t k = jit_rows_per_thread(L.P);
+                jit_launch(jit, pipeline_grid((L.P.n + k - 1) / k), kPipelineThreads, agg_smem_bytes(A), s, args);
             }
             ctx->add_profile("jit_launch", 0);
         } else {

@@ -499,17 +499,66 @@ __device__ __forceinline__ void publish_state(uint32_t* p, uint32_t v) {
 }
 __device__ __forceinline__ uint64_t* slot_at(const TableView& t, uint64_t i) { return t.slots + i * t.stride; }
 
-// Read-only lookup in a finished table (join probe): one 128-bit load per slot.
-__device__ inline uint32_t table_find(const TableView& t, const uint64_t* w, uint64_t h) {
+// Read-only lookup in a finished table (join probe): one 128-bit load per slot.  The
+// first slot's load is separate so a caller can issue it for several rows before
+// resolving any of them.
+__device__ __forceinline__ ulonglong2 slot_load(const TableView& t, uint64_t i) {
+    ulonglong2 v;
+    asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
+        : "=l"(v.x), "=l"(v.y)
+        : "l"(slot_at(t, i)), "l"(l2_evict_last()));
+    return v;
+}
+__device__ __forceinline__ uint32_t table_find_from(const TableView& t, const uint64_t* w, uint64_t h, ulonglong2 v) {
     uint64_t i = h & t.mask;
-    for (uint64_t n = 0; n <= t.mask; n++, i = (i + 1) & t.mask) {
-        ulonglong2 v;
-        asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
-                     : "=l"(v.x), "=l"(v.y)
-                     : "l"(slot_at(t, i)), "l"(l2_evict_last()));
+    for (uint64_t n = 0; n <= t.mask; n++) {
         if ((uint32_t)v.x == 0) return kNone;
         if (v.y == w[0] && (t.nwords == 1 || __ldg((const unsigned long long*)slot_at(t, i) + 2) == w[1]))
             return (uint32_t)(v.x >> 32);
+        i = (i + 1) & t.mask;
+        v = slot_load(t, i);
+    }
+    return kNone;
+}
+__device__ __forceinline__ uint32_t table_find(const TableView& t, const uint64_t* w, uint64_t h) {
+    return table_find_from(t, w, h, slot_load(t, h & t.mask));
+}
+
+// 128-bit compare-and-swap (sm_90+): returns the slot's previous contents.
+__device__ __forceinline__ ulonglong2 cas128(uint64_t* p, ulonglong2 expect, ulonglong2 desired) {
+    ulonglong2 old;
+    asm volatile(
+        "{\n\t.reg .b128 c, d, o;\n\t"
+        "mov.b128 c, {%2, %3};\n\t"
+        "mov.b128 d, {%4, %5};\n\t"
+        "atom.relaxed.gpu.global.cas.b128 o, [%6], c, d;\n\t"
+        "mov.b128 {%0, %1}, o;\n\t}"
+        : "=l"(old.x), "=l"(old.y)
+        : "l"(expect.x), "l"(expect.y), "l"(desired.x), "l"(desired.y), "l"(p)
+        : "memory");
+    return old;
+}
+
+// Insert one build row under a one-word key (join build, 16-byte slots): the slot's
+// state, payload and key are written by one 128-bit CAS, so there is no claimed state
+// and no waiting.  Returns the payload stored for the key: `row` when this thread
+// inserted it (*inserted = true), else the current chain head.
+__device__ inline uint32_t table_insert_row1(const TableView& t, uint64_t key, uint64_t h, uint32_t row, bool* inserted,
+                                             uint64_t* slot_out) {
+    const ulonglong2 want = make_ulonglong2(2ull | ((uint64_t)row << 32), key);
+    uint64_t i = h & t.mask;
+    *inserted = false;
+    for (uint64_t n = 0; n <= t.mask; n++, i = (i + 1) & t.mask) {
+        ulonglong2 old = cas128(slot_at(t, i), make_ulonglong2(0ull, 0ull), want);
+        if (old.x == 0 && old.y == 0) {
+            *inserted = true;
+            *slot_out = i;
+            return row;
+        }
+        if (old.y == key) {
+            *slot_out = i;
+            return (uint32_t)(old.x >> 32);
+        }
     }
     return kNone;
 }

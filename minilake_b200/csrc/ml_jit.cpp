@@ -159,6 +159,16 @@ CUfunction get_kernel(Ctx* ctx, const std::string& src, const char* name) {
 
 // ---- source generation --------------------------------------------------------------------------
 std::string num(int64_t v) { return std::to_string(v); }
+std::string hex(uint64_t v) {
+    char b[32];
+    snprintf(b, sizeof b, "0x%llxull", (unsigned long long)v);
+    return b;
+}
+
+// Rows a thread carries through the stages together in the batched form: the loads of
+// each stage are issued for all of them before any is used, so every thread keeps
+// several HBM / L2 requests in flight instead of one dependent chain per row.
+constexpr int kRowsPerThread = 4;
 
 class Gen {
    public:
@@ -181,7 +191,13 @@ class Gen {
     }
     int fresh() { return nv_++; }
 
-    static std::string row(int src) { return src == 0 ? "x.r" : "x.b" + num(src - 1); }
+    // The row context the generated statements read (x, or x<j> in the batched form), the
+    // statement that abandons the current row combination, and preloaded columns.
+    std::string x = "x";
+    std::string fail = "continue;";
+    std::map<int, V> cols;
+
+    std::string row(int src) const { return src == 0 ? x + ".r" : x + ".b" + num(src - 1); }
 
     // Typed load of column slot `a` (load_value, specialized on the column's kind and type).
     std::string col_value(int a) const {
@@ -209,6 +225,25 @@ class Gen {
         return c.valid ? "valid_bit(P.cols[" + num(a) + "].valid, " + row(c.src) + ")" : "true";
     }
 
+    // Column slots a program reads through I_COL.
+    void slots_of(const Prog& p, std::set<int>& out) const {
+        for (int i = 0; i < p.len; i++)
+            if (code_[p.start + i].op == I_COL) out.insert(code_[p.start + i].a);
+    }
+    // Load `slots` of the current row into registers, only when `alive` holds.
+    void preload(const std::set<int>& slots, const std::string& alive) {
+        for (int a : slots) {
+            std::string n = num(fresh()), v = "c" + n, k = "n" + n;
+            line("uint64_t " + v + " = 0;");
+            line("bool " + k + " = false;");
+            open("if (" + alive + ") {");
+            line(v + " = " + col_value(a) + ";");
+            line(k + " = " + col_valid(a) + ";");
+            close();
+            cols[a] = V{v, k};
+        }
+    }
+
     // Hoisted per-thread load of an instruction field (literal bits, arena offsets, counts).
     std::string field(int idx, const char* f, const char* type) {
         std::string name = std::string("f_") + f + num(idx);
@@ -230,11 +265,17 @@ class Gen {
             const Instr& in = code_[idx];
             const std::string n = num(fresh()), v = "v" + n, k = "k" + n;
             switch (in.op) {
-                case I_COL:
+                case I_COL: {
+                    auto it = cols.find(in.a);
+                    if (it != cols.end()) {
+                        st.push_back(it->second);
+                        break;
+                    }
                     line("const uint64_t " + v + " = " + col_value(in.a) + ";");
                     line("const bool " + k + " = " + col_valid(in.a) + ";");
                     st.push_back({v, k});
                     break;
+                }
                 case I_LIT: st.push_back({field(idx, "bits", "uint64_t"), in.lit_valid ? "true" : "false"}); break;
                 case I_BIN: {
                     V r = pop(), l = pop();
@@ -323,39 +364,32 @@ class Gen {
         return st.back();
     }
 
-    // Normalized key words of layout L into w<tag>0/1 (and null mask nm<tag> when NULLs
-    // group): make_key.  With null_kills a NULL key skips the row combination (`continue`).
-    void key(const KeyLayout& L, bool null_kills, const std::string& tag) {
-        line("uint64_t w" + tag + "0 = 0, w" + tag + "1 = 0;");
-        if (!null_kills) line("uint32_t nm" + tag + " = 0;");
+    // Normalized key words of layout L (make_key) into `wk` (a declared uint64_t[2], zeroed).
+    // A NULL key runs `on_null` (join keys) or sets its bit in `nm` (GROUP BY keys).
+    void key(const KeyLayout& L, const std::string& wk, const std::string& on_null, const std::string& nm) {
         for (int k = 0; k < L.nkeys; k++) {
             V e = expr(L.prog[k]);
             const KeyField& f = L.f[k];
             uint64_t mask = f.width >= 64 ? ~0ull : ((1ull << f.width) - 1);
-            std::string bits = "(uint64_t)";
-            std::string word = "w" + tag + num(f.word);
             std::string val = e.v;
             if (f.type == ML_TYPE_FLOAT64) val = "(as_f64(" + e.v + ") == 0.0 ? 0ull : " + e.v + ")";
-            char hex[32];
-            snprintf(hex, sizeof hex, "0x%llxull", (unsigned long long)mask);
-            std::string pack = word + " |= ((" + val + ") & " + hex + ") << " + num(f.shift) + ";";
-            if (null_kills) {
-                line("if (!(" + e.k + ")) continue;");
+            std::string pack = wk + "[" + num(f.word) + "] |= ((" + val + ") & " + hex(mask) + ") << " + num(f.shift) + ";";
+            if (nm.empty()) {
+                line("if (!(" + e.k + ")) { " + on_null + " }");
                 line(pack);
             } else {
                 open("if (!(" + e.k + ")) {");
-                line("nm" + tag + " |= " + num(1u << k) + "u;");
+                line(nm + " |= " + num(1u << k) + "u;");
                 close("} else {");
                 ind_++;
                 line(pack);
                 close();
             }
         }
-        line("const uint64_t wk" + tag + "[2] = {w" + tag + "0, w" + tag + "1};");
     }
 
-    // Streaming stages from `s` on (run_stages): filters `continue` on failure; probes
-    // look up the build table and walk duplicate-key chains as nested loops.
+    // Streaming stages from `s` on for one row (run_stages): filters and probes `continue`
+    // on failure; duplicate-key chains are walked as nested loops.
     template <class Sink> void stages(int s, Sink&& sink) {
         if (s == P_.nstages) {
             sink();
@@ -373,7 +407,8 @@ class Gen {
         const ProbeDev& pd = P_.probes[st.idx];
         std::string tag = "p" + num(s), p = num(st.idx);
         open("{  // probe " + p);
-        key(pd.keys, true, tag);
+        line("uint64_t wk" + tag + "[2] = {0ull, 0ull};");
+        key(pd.keys, "wk" + tag, "continue;", "");
         line("const uint32_t hb" + tag + " = table_find(P.probes[" + p + "].t, wk" + tag + ", key_hash(wk" + tag + ", " +
              num(pd.keys.nwords) + "));");
         line("if (hb" + tag + " == kNone) continue;");
@@ -390,6 +425,77 @@ class Gen {
         close();
     }
 
+    // The same stages for kRowsPerThread rows x0.. with liveness flags a0..: each stage first
+    // loads its columns for every live row, then evaluates (no chains: one match per probe).
+    template <class Sink> void batched_stages(Sink&& sink) {
+        const int K = kRowsPerThread;
+        auto rows = [&](auto&& f) {
+            for (int j = 0; j < K; j++) {
+                x = "x" + num(j);
+                f(j, "a" + num(j));
+            }
+            x = "x";
+        };
+        for (int s = 0; s < P_.nstages; s++) {
+            const Stage st = P_.stages[s];
+            std::set<int> slots;
+            if (st.kind == 0) {
+                slots_of(P_.filters[st.idx], slots);
+                std::vector<std::map<int, V>> pre(K);
+                rows([&](int j, const std::string& a) {
+                    cols.clear();
+                    preload(slots, a);
+                    pre[j] = cols;
+                });
+                rows([&](int j, const std::string& a) {
+                    cols = pre[j];
+                    open("if (" + a + ") {  // filter " + num(st.idx));
+                    V e = expr(P_.filters[st.idx]);
+                    line(a + " = (" + e.k + ") && ((" + e.v + ") & 1);");
+                    close();
+                });
+                cols.clear();
+                continue;
+            }
+            const ProbeDev& pd = P_.probes[st.idx];
+            const std::string p = num(st.idx);
+            for (int k = 0; k < pd.keys.nkeys; k++) slots_of(pd.keys.prog[k], slots);
+            std::vector<std::map<int, V>> pre(K);
+            rows([&](int j, const std::string& a) {
+                cols.clear();
+                preload(slots, a);
+                pre[j] = cols;
+            });
+            rows([&](int j, const std::string& a) {
+                cols = pre[j];
+                std::string tag = "p" + num(s) + "_" + num(j);
+                line("uint64_t wk" + tag + "[2] = {0ull, 0ull};");
+                line("uint64_t h" + tag + " = 0;");
+                open("if (" + a + ") {  // probe " + p + " key");
+                key(pd.keys, "wk" + tag, a + " = false;", "");
+                line("h" + tag + " = key_hash(wk" + tag + ", " + num(pd.keys.nwords) + ");");
+                close();
+            });
+            cols.clear();
+            rows([&](int j, const std::string& a) {
+                std::string tag = "p" + num(s) + "_" + num(j);
+                line("ulonglong2 s" + tag + " = make_ulonglong2(0ull, 0ull);");
+                line("if (" + a + ") s" + tag + " = slot_load(P.probes[" + p + "].t, h" + tag + " & P.probes[" + p +
+                     "].t.mask);");
+            });
+            rows([&](int j, const std::string& a) {
+                std::string tag = "p" + num(s) + "_" + num(j);
+                open("if (" + a + ") {  // probe " + p);
+                line("const uint32_t b = table_find_from(P.probes[" + p + "].t, wk" + tag + ", h" + tag + ", s" + tag + ");");
+                line(a + " = b != kNone;");
+                line(x + ".b" + p + " = b;");
+                if (st.idx == P_.head_probe) line(x + ".head = b;");
+                close();
+            });
+        }
+        sink(rows);
+    }
+
    private:
     const std::vector<Instr>& code_;
     const PipeArgs& P_;
@@ -398,82 +504,142 @@ class Gen {
     int nv_ = 0, ind_ = 2;
 };
 
-std::string row_loop_head(const PipeArgs& P) {
+// Batched form applies when no probe walks chains (at most one match per probe row).
+bool batchable(const PipeArgs& P) { return !P.has_chains; }
+
+std::string row_loop(const PipeArgs& P, bool batched, const std::string& body) {
     std::string s;
-    s += "    const int64_t stride = (int64_t)gridDim.x * blockDim.x;\n";
-    s += "    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {\n";
-    s += "        RowCtx x;\n";
-    s += P.sel ? "        x.r = __ldg(P.sel + i);\n" : "        x.r = (uint32_t)i;\n";
-    s += "        x.b0 = x.b1 = x.b2 = x.b3 = 0;\n        x.head = 0;\n";
+    if (!batched) {
+        s += "    const int64_t stride = (int64_t)gridDim.x * blockDim.x;\n";
+        s += "    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {\n";
+        s += "        RowCtx x;\n";
+        s += P.sel ? "        x.r = __ldg(P.sel + i);\n" : "        x.r = (uint32_t)i;\n";
+        s += "        x.b0 = x.b1 = x.b2 = x.b3 = 0;\n        x.head = 0;\n";
+    } else {
+        const int K = kRowsPerThread;
+        s += "    const int64_t tile = (int64_t)" + num(K) + " * blockDim.x;\n";
+        s += "    for (int64_t base = (int64_t)blockIdx.x * tile; base < P.n; base += (int64_t)gridDim.x * tile) {\n";
+        for (int j = 0; j < K; j++) {
+            std::string J = num(j), x = "x" + J, a = "a" + J;
+            s += "        RowCtx " + x + ";\n";
+            s += "        const int64_t i" + J + " = base + " + J + " * (int64_t)blockDim.x + threadIdx.x;\n";
+            s += "        bool " + a + " = i" + J + " < P.n;\n";
+            s += "        " + x + ".r = " + a + " ? " + (P.sel ? "__ldg(P.sel + i" + J + ")" : "(uint32_t)i" + J) + " : 0u;\n";
+            s += "        " + x + ".b0 = " + x + ".b1 = " + x + ".b2 = " + x + ".b3 = 0;\n";
+            s += "        " + x + ".head = 0;\n";
+        }
+    }
+    s += body;
+    s += "    }\n";
     return s;
 }
+
+// The aggregate update of one row combination (agg_update + agg_fold), in `g`'s current
+// row context; `g.fail` abandons the combination.
+void emit_aggregate(Gen& g, const AggArgs& A) {
+    const bool smem = A.smem_groups > 0;
+    const std::string S = num(A.stride);
+    if (A.group_probe >= 0) {
+        g.line("const uint32_t g = " + g.x + ".head;");
+    } else if (A.ungrouped) {
+        g.line("const uint32_t g = 0;");
+    } else {
+        g.line("uint64_t wkg[2] = {0ull, 0ull};");
+        g.line("uint32_t nmg = 0;");
+        g.key(A.keys, "wkg", "", "nmg");
+        g.line("bool ins;");
+        g.line("uint64_t slot;");
+        g.line("const uint32_t g = table_upsert(A.t, wkg, nmg, key_hash(wkg, " + num(A.keys.nwords) +
+               ", nmg), P.err, [&]() -> uint32_t { const uint32_t id = atomicAdd(A.ngroups, 1u); "
+               "return id < A.gid_cap ? id : kNone; }, &ins, &slot);");
+        g.open("if (g == kNone) {");
+        g.line("record_overflow(P, A, " + g.x + ");");
+        g.line(g.fail);
+        g.close();
+        g.open("if (ins) {");
+        g.line("A.gkeys[g] = wkg[0];");
+        if (A.keys.nwords > 1) g.line("A.gkeys[(uint64_t)A.gid_cap + g] = wkg[1];");
+        g.line("A.gnull[g] = nmg;");
+        g.close();
+    }
+    if (smem) {
+        g.line("uint64_t* blk = (int)g < A.smem_groups ? smem + (uint64_t)g * " + S + " : A.acc + (uint64_t)g * " + S + ";");
+        g.line("atomicAdd((unsigned long long*)blk, 1ull);");
+    } else {
+        g.line("uint64_t* blk = A.acc + (uint64_t)g * " + S + ";");
+        g.line("count_global(blk);");
+    }
+    for (int k = 0; k < A.nagg; k++) {
+        const AggDev& a = A.aggs[k];
+        if (a.func == ML_AGG_COUNT_STAR) continue;  // the group's row counter (word 0)
+        g.open("{  // aggregate " + num(k));
+        std::string v = "0ull";
+        if (a.has_arg) {
+            Gen::V e = g.expr(a.arg);
+            g.open("if (" + e.k + ") {");
+            v = e.v;
+        }
+        g.line(std::string(smem ? "acc_apply(" : "acc_apply_global(") + num(a.kind) + ", blk + " + num(a.off) + ", " + v +
+               ");");
+        if (a.count_valid) {
+            if (smem) g.line("atomicAdd((unsigned long long*)A.aggs[" + num(k) + "].vcnt + g, 1ull);");
+            else g.line("count_global(A.aggs[" + num(k) + "].vcnt + g);");
+        }
+        if (a.has_arg) g.close();
+        g.close();
+    }
+}
+
+const char* kPrelude = "#include \"ml_agg.cuh\"\nusing namespace mlg;\n";
 
 }  // namespace
 
 std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {
     Gen g(pipe.C.code, P);
     const bool smem = A.smem_groups > 0;
-    const std::string S = num(A.stride);
-    g.stages(0, [&]() {
-        g.open("{  // aggregate");
-        if (A.group_probe >= 0) {
-            g.line("const uint32_t g = x.head;");
-        } else if (A.ungrouped) {
-            g.line("const uint32_t g = 0;");
-        } else {
-            g.key(A.keys, false, "g");
-            g.line("bool ins;");
-            g.line("uint64_t slot;");
-            g.line("const uint32_t g = table_upsert(A.t, wkg, nmg, key_hash(wkg, " + num(A.keys.nwords) +
-                   ", nmg), P.err, [&]() -> uint32_t { const uint32_t id = atomicAdd(A.ngroups, 1u); "
-                   "return id < A.gid_cap ? id : kNone; }, &ins, &slot);");
-            g.open("if (g == kNone) {");
-            g.line("record_overflow(P, A, x);");
-            g.line("continue;");
+    const bool batched = batchable(P);
+    if (batched) {
+        g.fail = "break;";
+        g.batched_stages([&](auto&& rows) {
+            std::set<int> slots;
+            if (A.group_probe < 0 && !A.ungrouped)
+                for (int k = 0; k < A.keys.nkeys; k++) g.slots_of(A.keys.prog[k], slots);
+            for (int k = 0; k < A.nagg; k++)
+                if (A.aggs[k].has_arg && A.aggs[k].func != ML_AGG_COUNT_STAR) g.slots_of(A.aggs[k].arg, slots);
+            std::vector<std::map<int, Gen::V>> pre(kRowsPerThread);
+            rows([&](int j, const std::string& a) {
+                g.cols.clear();
+                g.preload(slots, a);
+                pre[j] = g.cols;
+            });
+            rows([&](int j, const std::string& a) {
+                g.cols = pre[j];
+                g.open("if (" + a + ") do {  // aggregate");
+                emit_aggregate(g, A);
+                g.close("} while (0);");
+            });
+            g.cols.clear();
+        });
+    } else {
+        g.stages(0, [&]() {
+            g.open("{  // aggregate");
+            emit_aggregate(g, A);
             g.close();
-            g.open("if (ins) {");
-            g.line("A.gkeys[g] = wg0;");
-            if (A.keys.nwords > 1) g.line("A.gkeys[(uint64_t)A.gid_cap + g] = wg1;");
-            g.line("A.gnull[g] = nmg;");
-            g.close();
-        }
-        if (smem)
-            g.line("uint64_t* blk = (int)g < A.smem_groups ? smem + (uint64_t)g * " + S + " : A.acc + (uint64_t)g * " + S +
-                   ";");
-        else
-            g.line("uint64_t* blk = A.acc + (uint64_t)g * " + S + ";");
-        g.line("atomicAdd((unsigned long long*)blk, 1ull);");
-        for (int k = 0; k < A.nagg; k++) {
-            const AggDev& a = A.aggs[k];
-            if (a.func == ML_AGG_COUNT_STAR) continue;  // the group's row counter (word 0)
-            g.open("{  // aggregate " + num(k));
-            std::string v = "0ull";
-            if (a.has_arg) {
-                Gen::V e = g.expr(a.arg);
-                g.open("if (" + e.k + ") {");
-                v = e.v;
-            }
-            g.line("acc_apply(" + num(a.kind) + ", blk + " + num(a.off) + ", " + v + ");");
-            if (a.count_valid) g.line("atomicAdd((unsigned long long*)A.aggs[" + num(k) + "].vcnt + g, 1ull);");
-            if (a.has_arg) g.close();
-            g.close();
-        }
-        g.close();
-    });
-    std::string src;
-    src += "#include \"ml_agg.cuh\"\nusing namespace mlg;\n";
+        });
+    }
+    std::string src = kPrelude;
     src += "extern \"C\" __global__ void __launch_bounds__(256) ml_pipeline_aggregate(const __grid_constant__ PipeArgs P, "
            "const __grid_constant__ AggArgs A) {\n";
     src += "    extern __shared__ __align__(16) uint64_t smem[];\n";
     if (smem) src += "    smem_setup(A, smem);\n    __syncthreads();\n";
     src += g.pre();
-    src += row_loop_head(P);
-    src += g.body();
-    src += "    }\n";
+    src += row_loop(P, batched, g.body());
     if (smem) src += "    __syncthreads();\n    smem_flush(A, smem);\n";
     src += "}\n";
     return src;
 }
+
+int jit_rows_per_thread(const PipeArgs& P) { return batchable(P) ? kRowsPerThread : 1; }
 
 void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {
     if (!jit_enabled(ctx)) return nullptr;
@@ -482,15 +648,20 @@ void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const Ag
 
 void* jit_join_insert_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L) {
     if (!jit_enabled(ctx)) return nullptr;
-    // build_table (join.rs:160-203): distinct keys in the table, duplicates chained in `next`
+    // build_table (join.rs:160-203): distinct keys in the table, duplicates chained in `next`.
+    // One-word keys insert with a single 128-bit CAS; wider keys use the claim protocol.
     Gen g(pipe.C.code, P);
     g.open("{  // insert");
-    g.key(L, true, "k");
+    g.line("uint64_t wkk[2] = {0ull, 0ull};");
+    g.key(L, "wkk", "continue;", "");
     g.line("bool ins;");
     g.line("uint64_t slot;");
     g.line("const uint32_t r = x.r;");
-    g.line("const uint32_t p = table_upsert(t, wkk, 0u, key_hash(wkk, " + num(L.nwords) +
-           "), P.err, [&]() { return r; }, &ins, &slot);");
+    if (L.nwords == 1)
+        g.line("const uint32_t p = table_insert_row1(t, wkk[0], key_hash(wkk, 1), r, &ins, &slot);");
+    else
+        g.line("const uint32_t p = table_upsert(t, wkk, 0u, key_hash(wkk, " + num(L.nwords) +
+               "), P.err, [&]() { return r; }, &ins, &slot);");
     g.line("if (p == kNone) continue;");
     g.open("if (!ins) {");
     g.line("const uint32_t old = atomicExch((uint32_t*)slot_at(t, slot) + 1, r);");
@@ -498,8 +669,7 @@ void* jit_join_insert_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, 
     g.line("if (*dup_flag == 0) atomicExch(dup_flag, 1u);");
     g.close();
     g.close();
-    std::string src;
-    src += "#include \"ml_agg.cuh\"\nusing namespace mlg;\n";
+    std::string src = kPrelude;
     src += "extern \"C\" __global__ void __launch_bounds__(256) ml_join_insert(const __grid_constant__ PipeArgs P, "
            "const __grid_constant__ KeyLayout L, TableView t, uint32_t* next, uint32_t* dup_flag, int64_t n) {\n";
     src += g.pre();
@@ -517,8 +687,9 @@ void jit_launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream
         N.set_attr((CUfunction)fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem) != CUDA_SUCCESS)
         raise(ML_ERR_CUDA, "cuFuncSetAttribute failed for a pipeline kernel");
     CUresult r = N.launch((CUfunction)fn, grid, 1, 1, block, 1, 1, (unsigned)smem, (CUstream)s, args, nullptr);
-    if (r != CUDA_SUCCESS) raise(ML_ERR_CUDA, "launch of a runtime-specialized pipeline kernel failed (CUresult " +
-                                                  std::to_string((int)r) + ")");
+    if (r != CUDA_SUCCESS)
+        raise(ML_ERR_CUDA, "launch of a runtime-specialized pipeline kernel failed (CUresult " + std::to_string((int)r) +
+                               ")");
 }
 
 }  // namespace mlg

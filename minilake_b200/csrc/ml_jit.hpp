@@ -20,6 +20,10 @@ void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const Ag
 // Specialized join-build insert kernel (signature of k_join_insert), or nullptr.
 void* jit_join_insert_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L);
 
+// Rows one thread of the specialized aggregate kernel handles per iteration (its grid
+// needs n / rows-per-thread threads).
+int jit_rows_per_thread(const PipeArgs& P);
+
 // Launch a specialized kernel with `args` (pointers to the kernel's parameters).
 void jit_launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream_t s, void** args);
 
