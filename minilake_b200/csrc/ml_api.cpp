@@ -421,12 +421,14 @@ std::unique_ptr<ml_batch> topn_batch(Ctx* ctx, ml_batch& b, const std::vector<So
     const uint32_t* in = nullptr;
     int64_t m = n;
     for (;;) {
-        int64_t nb = (m + kTopNChunk - 1) / kTopNChunk;
+        const bool warp = k <= kTopNWarpMax;  // small limits: one sorted list per warp
+        int64_t nb = warp ? topn_warp_blocks(m) : (m + kTopNChunk - 1) / kTopNChunk;
         DevBuf& dst = (in == a.get<uint32_t>() && in) ? bb : a;
         dst = DevBuf(ctx, (size_t)nb * k * 4, nullptr);
         {
             KernelTimer kt(ctx, st, "topn");
-            launch_topn_chunk(S, in, m, (int)k, dst.get<uint32_t>(), st);
+            if (warp) launch_topn_warp(S, in, m, (int)k, (int)nb, dst.get<uint32_t>(), st);
+            else launch_topn_chunk(S, in, m, (int)k, dst.get<uint32_t>(), st);
             kt.stop();
         }
         ctx->count_launch();

@@ -6,6 +6,8 @@
 // kernels on B200: one pass over each column with coalesced loads, grids sized
 // as a multiple of the 148 SMs, state that fits in L2 (126 MB) kept there, and
 // shared-memory privatization wherever many rows hit few addresses.
+#include <algorithm>
+
 #include "ml_agg.cuh"
 #include "ml_kernels.cuh"
 
@@ -813,6 +815,68 @@ __global__ void __launch_bounds__(1024) k_topn_chunk(const __grid_constant__ Sor
     for (int j = threadIdx.x; j < k; j += blockDim.x) out[(int64_t)blockIdx.x * k + j] = idx[j];
 }
 
+// ---- top-N for small limits (k <= 32): one sorted list per warp ------------------------------
+// Each lane holds one entry of the warp's current best 32 (ascending); a batch of 32 new
+// rows is skipped unless one of them beats the k-th entry, else it is sorted with a
+// shuffle bitonic network and merged in.  The CTA then merges its warps' lists.
+struct TopEntry {
+    uint64_t p;  // sort_prefix
+    uint32_t r;  // row (kNone = padding)
+};
+__device__ __forceinline__ bool entry_less(const SortDev& S, TopEntry a, TopEntry b) {
+    if (a.p != b.p) return a.p < b.p;
+    return cmp_rows(S, a.r, b.r) < 0;
+}
+__device__ __forceinline__ TopEntry shfl_entry(TopEntry e, int src) {
+    return TopEntry{__shfl_sync(0xFFFFFFFFu, e.p, src), __shfl_sync(0xFFFFFFFFu, e.r, src)};
+}
+// Compare-exchange with the lane `lane ^ j`; the lower lane keeps the smaller entry when
+// `ascending`.  Both lanes evaluate entry_less(upper, lower), so ties resolve consistently.
+__device__ __forceinline__ TopEntry cmp_exchange(const SortDev& S, TopEntry e, int lane, int j, bool ascending) {
+    TopEntry o = shfl_entry(e, lane ^ j);
+    bool lower = (lane & j) == 0;
+    TopEntry lo = lower ? e : o, hi = lower ? o : e;
+    bool swap = entry_less(S, hi, lo);
+    bool keep_min = lower == ascending;
+    if (keep_min) return swap ? hi : lo;
+    return swap ? lo : hi;
+}
+__device__ __forceinline__ TopEntry warp_sort32(const SortDev& S, TopEntry e, int lane) {
+    for (int k = 2; k <= 32; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) e = cmp_exchange(S, e, lane, j, (lane & k) == 0);
+    return e;
+}
+// Merge sorted `n` into sorted `l`: keep the 32 smallest of both, sorted ascending.
+__device__ __forceinline__ TopEntry warp_merge32(const SortDev& S, TopEntry l, TopEntry n, int lane) {
+    TopEntry rev = shfl_entry(n, 31 - lane);
+    TopEntry e = entry_less(S, rev, l) ? rev : l;  // bitonic: the 32 smallest of the union
+    for (int j = 16; j > 0; j >>= 1) e = cmp_exchange(S, e, lane, j, true);
+    return e;
+}
+
+__global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortDev S, const uint32_t* in, int64_t n,
+                                                   int k, uint32_t* out) {
+    __shared__ TopEntry lists[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    TopEntry best{~0ull, kNone};
+    const int64_t warps = (int64_t)gridDim.x * 8;
+    for (int64_t base = ((int64_t)blockIdx.x * 8 + warp) * 32; base < n; base += warps * 32) {
+        int64_t i = base + lane;
+        TopEntry e;
+        e.r = i < n ? (in ? in[i] : (uint32_t)i) : kNone;
+        e.p = sort_prefix(S, e.r);
+        TopEntry kth = shfl_entry(best, k - 1);
+        if (!__any_sync(0xFFFFFFFFu, e.r != kNone && entry_less(S, e, kth))) continue;
+        best = warp_merge32(S, best, warp_sort32(S, e, lane), lane);
+    }
+    lists[warp][lane] = best;
+    __syncthreads();
+    if (warp == 0) {
+        for (int w = 1; w < 8; w++) best = warp_merge32(S, best, lists[w][lane], lane);
+        if (lane < k) out[(int64_t)blockIdx.x * k + lane] = best.r;
+    }
+}
+
 }  // namespace
 
 // ---- launch wrappers -------------------------------------------------------------------------------
@@ -908,6 +972,15 @@ void launch_utf8_copy(const uint32_t* off, const uint8_t* bytes, const uint32_t*
 }
 void launch_u64_to_u32(const uint64_t* in, uint32_t* out, int64_t n, cudaStream_t s) {
     if (n) k_u64_to_u32<<<grid_for(n, 8), kThreads, 0, s>>>(in, out, n);
+}
+int topn_warp_blocks(int64_t n) {
+    if (n <= 65536) return 1;  // one CTA finishes the candidates of the previous round
+    int64_t want = (n + 255) / 256;
+    int64_t cap = (int64_t)num_sms() * 4;
+    return (int)std::max<int64_t>(1, std::min(want, cap));
+}
+void launch_topn_warp(const SortDev& S, const uint32_t* in, int64_t n, int k, int blocks, uint32_t* out, cudaStream_t s) {
+    k_topn_warp<<<blocks, 256, 0, s>>>(S, in, n, k, out);
 }
 void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, uint32_t* out, cudaStream_t s) {
     int64_t nb = (n + kTopNChunk - 1) / kTopNChunk;

@@ -80,6 +80,10 @@ void launch_u64_to_u32(const uint64_t* in, uint32_t* out, int64_t n, cudaStream_
 
 // Top-N: each CTA sorts a chunk of candidate rows and keeps the best k.
 void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, uint32_t* out, cudaStream_t s);
+// Top-k for k <= kTopNWarpMax: each CTA writes its best k rows (sorted) to out[block * k ..].
+constexpr int kTopNWarpMax = 32;
+int topn_warp_blocks(int64_t n);
+void launch_topn_warp(const SortDev& S, const uint32_t* in, int64_t n, int k, int blocks, uint32_t* out, cudaStream_t s);
 
 // Fill / concatenation helpers
 void launch_fill_u32(uint32_t* p, uint32_t v, int64_t n, cudaStream_t s);
