@@ -26,7 +26,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -68,43 +67,64 @@ def make_data(rank: int, world: int):
     return key, fk, d, v
 
 
-def clocks_sampler():
-    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-           "--format=csv,noheader,nounits", "-lms", "200"]
-    try:
-        return subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-    except OSError:
-        return None
+class ClockSampler:
+    """SM clock and clock-event reasons of this rank's GPU, sampled through NVML every
+    2 ms from a thread while the timed region runs (reads only; changes no setting)."""
 
 
-def clocks_summary(proc, device_index: int):
-    if proc is None:
-        return None
-    proc.terminate()
-    try:
-        out, _ = proc.communicate(timeout=5)
-    except subprocess.TimeoutExpired:
-        proc.kill()
-        out, _ = proc.communicate()
-    sm, mx, reasons = [], 0.0, set()
-    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-    for line in out.strip().splitlines():
-        p = [x.strip() for x in line.split(",")]
-        if len(p) < 9 or p[0] != str(device_index):
-            continue
+    def __init__(self, device_index: int):
+        self.samples, self.reasons, self.max_mhz = [], set(), 0.0
+        self._stop = threading.Event()
+        self._thread = None
         try:
-            sm.append(float(p[1]))
-            mx = max(mx, float(p[2]))
-        except ValueError:
-            continue
-        for n, flag in zip(names, p[5:9]):
-            if flag.lower() == "active":
-                reasons.add(n)
-    if not sm:
-        return None
-    return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            try:
+                uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+                h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self._reasons_fn = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            self._bits = {"hw_slowdown": pynvml.nvmlClocksThrottleReasonHwSlowdown,
+                          "hw_thermal_slowdown": pynvml.nvmlClocksThrottleReasonHwThermalSlowdown,
+                          "sw_thermal_slowdown": pynvml.nvmlClocksThrottleReasonSwThermalSlowdown,
+                          "sw_power_cap": pynvml.nvmlClocksThrottleReasonSwPowerCap}
+            self._nvml, self._h = pynvml, h
+        except Exception:
+            self._nvml = None
+
+    def __enter__(self):
+        if self._nvml is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def _run(self):
+        n, h = self._nvml, self._h
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM)))
+                bits = self._reasons_fn(h)
+                for name, bit in self._bits.items():
+                    if bits & bit:
+                        self.reasons.add(name)
+            except Exception:
+                return
+            time.sleep(0.002)
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join()
+
+    def summary(self):
+        if not self.samples:
+            return None
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples), "source": "NVML, 2 ms period, during the timed steps"}
 
 
 def measured_peak():
@@ -116,12 +136,15 @@ def measured_peak():
 
 
 def profiled_traffic():
-    """DRAM bytes per launch of the aggregate kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "pipeline_aggregate_join_groupby.json")
+    """DRAM bytes (read + write) per launch of the aggregate kernel on this workload, from
+    the committed ncu summary (line `dram_bytes_per_launch: N`)."""
+    import re
+    p = os.path.join(ROOT, "profiles", "pipeline_aggregate_join_groupby.md")
     try:
         with open(p) as f:
-            return json.load(f).get("dram_bytes_per_launch_full_size")
-    except (OSError, ValueError):
+            m = re.search(r"^dram_bytes_per_launch:\s*([0-9]+)", f.read(), re.M)
+        return int(m.group(1)) if m else None
+    except OSError:
         return None
 
 
@@ -190,17 +213,17 @@ def gpu_arm(args):
         q.run(q.dim_dev, [q.fact_dev])
     ctx.profile("pipeline_aggregate", reset=True)
     l0 = ctx.kernel_launches()
-    clk = clocks_sampler() if rank == 0 else None
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    top = None
-    for _ in range(args.steps):
-        top = q.run(q.dim_dev, [q.fact_dev])
-    e1.record()
-    barrier()
+    with ClockSampler(local) as clk:
+        e0.record()
+        top = None
+        for _ in range(args.steps):
+            top = q.run(q.dim_dev, [q.fact_dev])
+        e1.record()
+        barrier()
     ms = e0.elapsed_time(e1)
-    clocks = clocks_summary(clk, local) if rank == 0 else None
+    clocks = clk.summary()
     launches = ctx.kernel_launches() - l0
     n_agg, agg_ms = ctx.profile("pipeline_aggregate", reset=True)
     ms_t = torch.tensor([ms], device="cuda")
@@ -285,7 +308,8 @@ def gpu_arm(args):
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "kernel": "k_agg (fused filter + join probe + hash aggregate)",
+                         "kernel": "ml_pipeline_aggregate (runtime-specialized fused filter + join probe + "
+                                   "hash aggregate)",
                          "kernel_ms_per_launch": per_launch_ms,
                          "algorithmic_bytes_per_launch": FACT_ROWS * BYTES_PER_ROW,
                          "traffic": profiled_traffic()},

@@ -909,43 +909,76 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
     KeyLayout L = kp.key_layout(j->keys.exprs.data(), (int)j->keys.exprs.size(), kp.out, false, nullptr);
     kp.upload();
     jt->nwords = L.nwords;
-    jt->cap = pow2_at_least(std::max<uint64_t>(16, (uint64_t)n * 2));  // load factor <= 1/2: short probes
-    size_t slot_bytes = jt->cap * 8 * (L.nwords == 1 ? 2 : 4);
-    jt->slots = DevBuf(ctx, slot_bytes, jt->res.get());
-    jt->next = DevBuf(ctx, std::max<size_t>((size_t)n * 4, 4), jt->res.get());
-    jt->dup = DevBuf(ctx, 8, nullptr);
-    CK(cudaMemsetAsync(jt->slots.get(), 0, slot_bytes, s));
     for (auto& k : j->keys.exprs) {  // which build column each key reads (for GROUP BY the join key)
         ExprNode e = parse_expr(k);
         auto o = kp.C.column_origin(e, kp.out);
         jt->key_cols.push_back(o && e.kind == ML_EXPR_COLUMN ? o->index : -1);
     }
+    jt->next = DevBuf(ctx, std::max<size_t>((size_t)n * 4, 4), jt->res.get());
+    jt->dup = DevBuf(ctx, 8, nullptr);
     CK(cudaMemsetAsync(jt->next.get(), 0xFF, std::max<size_t>((size_t)n * 4, 4), s));
     CK(cudaMemsetAsync(jt->dup.get(), 0, 8, s));
-    Staging st(ctx);
-    Pipeline::Launch LA;
-    auto views = device_views(jt->batch);
-    kp.prepare(LA, views.data(), (int)views.size(), n, nullptr, 0, s, st, nullptr);
+    // A single integer key that is a build column, with a value range of at most 4 entries
+    // per build row, is indexed directly (no hashing, one 4-byte load per probe).
+    const DevColumn* kc = nullptr;
+    if (n > 0 && jt->key_types.size() == 1 && jt->key_cols[0] >= 0) {
+        const DevColumn* c = jt->batch.cols[jt->key_cols[0]].get();
+        int t = jt->key_types[0];
+        if (c->kind == CK_FIXED && c->dtype == t && (t == ML_TYPE_INT32 || t == ML_TYPE_DATE || t == ML_TYPE_INT64)) kc = c;
+    }
+    if (kc) {
+        DevBuf mm(ctx, 16, nullptr);
+        uint64_t init[2] = {~0ull, 0ull}, got[2];
+        CK(cudaMemcpyAsync(mm.get(), init, 16, cudaMemcpyHostToDevice, s));
+        launch_key_range(kc->dptr(), kc->dtype, kc->vptr(), n, mm.get<unsigned long long>(), s);
+        ctx->count_launch();
+        CK(cudaMemcpyAsync(got, mm.get(), 16, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (got[0] <= got[1] && got[1] - got[0] < std::min<uint64_t>(4 * (uint64_t)n + 1024, 0xFFFFFFFFull)) {
+            jt->dmin = got[0];
+            jt->drange = got[1] - got[0] + 1;
+        } else {
+            kc = nullptr;  // no valid key, or too sparse: hash table
+        }
+    }
+    if (kc) {
+        jt->dense = DevBuf(ctx, jt->drange * 4, jt->res.get());
+        CK(cudaMemsetAsync(jt->dense.get(), 0xFF, jt->drange * 4, s));
+        KernelTimer kt(ctx, s, "join_insert");
+        launch_dense_insert(kc->dptr(), kc->dtype, kc->vptr(), n, jt->dmin, jt->dense.get<uint32_t>(),
+                            jt->next.get<uint32_t>(), jt->dup.get<uint32_t>(), s);
+        kt.stop();
+        ctx->count_launch();
+    }
+    const int64_t nh = kc ? 0 : n;  // rows the hash table takes
+    jt->cap = pow2_at_least(std::max<uint64_t>(16, ((uint64_t)nh * 4 + 2) / 3));  // load factor <= 3/4
+    size_t slot_bytes = jt->cap * 8 * (L.nwords == 1 ? 2 : 4);
+    jt->slots = DevBuf(ctx, slot_bytes, jt->res.get());
+    CK(cudaMemsetAsync(jt->slots.get(), 0, slot_bytes, s));
     ErrWord ew(ctx);
     CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
-    LA.P.err = ew.d.get<uint32_t>();
-    {
-        void* jit = n ? jit_join_insert_kernel(ctx, kp, LA.P, L) : nullptr;
+    if (nh) {
+        Staging st(ctx);
+        Pipeline::Launch LA;
+        auto views = device_views(jt->batch);
+        kp.prepare(LA, views.data(), (int)views.size(), nh, nullptr, 0, s, st, nullptr);
+        LA.P.err = ew.d.get<uint32_t>();
+        void* jit = jit_join_insert_kernel(ctx, kp, LA.P, L);
         KernelTimer kt(ctx, s, "join_insert");
         if (jit) {
             TableView tv = jt->view();
             uint32_t* next = jt->next.get<uint32_t>();
             uint32_t* dup = jt->dup.get<uint32_t>();
-            int64_t nn = n;
+            int64_t nn = nh;
             void* args[] = {&LA.P, &L, &tv, &next, &dup, &nn};
-            jit_launch(jit, pipeline_grid(n), kPipelineThreads, 0, s, args);
+            jit_launch(jit, pipeline_grid(nh), kPipelineThreads, 0, s, args);
             ctx->add_profile("jit_launch", 0);
         } else {
-            launch_join_insert(LA.P, L, jt->view(), jt->next.get<uint32_t>(), jt->dup.get<uint32_t>(), n, s);
+            launch_join_insert(LA.P, L, jt->view(), jt->next.get<uint32_t>(), jt->dup.get<uint32_t>(), nh, s);
         }
         kt.stop();
+        ctx->count_launch();
     }
-    ctx->count_launch();
     // canonical ids of the build side's strings (GROUP BY on a build-side string column)
     for (auto& c : jt->batch.cols) {
         if (c->kind != CK_UTF8 || n == 0) continue;
@@ -974,11 +1007,12 @@ int ml_gpu_join_table_stats(const ml_join_table* t, int64_t* build_rows, int64_t
     REQUIRE(t, "null table");
     t->ctx->set_current();
     if (build_rows) *build_rows = t->batch.nrows;
-    if (capacity) *capacity = (int64_t)t->cap;
+    if (capacity) *capacity = (int64_t)(t->dense ? t->drange : t->cap);
     if (distinct_keys) {
         DevBuf c(t->ctx, 8, nullptr);
         CK(cudaMemset(c.get(), 0, 8));
-        launch_count_slots(t->view(), c.get<unsigned long long>(), t->ctx->stream);
+        if (t->dense) launch_count_dense(t->dense.get<uint32_t>(), t->drange, c.get<unsigned long long>(), t->ctx->stream);
+        else launch_count_slots(t->view(), c.get<unsigned long long>(), t->ctx->stream);
         t->ctx->count_launch();
         unsigned long long d = 0;
         CK(cudaMemcpyAsync(&d, c.get(), 8, cudaMemcpyDeviceToHost, t->ctx->stream));

@@ -16,6 +16,11 @@ struct ProbeDev {
     TableView t;
     const uint32_t* next;  // chain links, nullptr when every build key is distinct
     KeyLayout keys;
+    // Direct-mapped index for a dense integer key: dense[key - dmin] is the chain head of
+    // the build rows with that key (kNone = no row), for key - dmin < drange.  nullptr
+    // when the build side uses the hash table `t`.
+    const uint32_t* dense;
+    uint64_t dmin, drange;
 };
 
 // The streaming part of a pipeline (Filter / Projection folded into expressions /

@@ -524,6 +524,17 @@ __device__ __forceinline__ uint32_t table_find(const TableView& t, const uint64_
     return table_find_from(t, w, h, slot_load(t, h & t.mask));
 }
 
+// Chain head of a dense join index entry (kept in L2 like the hash tables).
+__device__ __forceinline__ uint32_t dense_load(const uint32_t* p) {
+    uint32_t v;
+    asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_evict_last()));
+    return v;
+}
+__device__ __forceinline__ uint32_t dense_find(const uint32_t* dense, uint64_t dmin, uint64_t drange, uint64_t key) {
+    const uint64_t off = key - dmin;
+    return off < drange ? dense_load(dense + off) : kNone;
+}
+
 // 128-bit compare-and-swap (sm_90+): returns the slot's previous contents.
 __device__ __forceinline__ ulonglong2 cas128(uint64_t* p, ulonglong2 expect, ulonglong2 desired) {
     ulonglong2 old;

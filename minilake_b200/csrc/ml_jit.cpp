@@ -409,8 +409,12 @@ class Gen {
         open("{  // probe " + p);
         line("uint64_t wk" + tag + "[2] = {0ull, 0ull};");
         key(pd.keys, "wk" + tag, "continue;", "");
-        line("const uint32_t hb" + tag + " = table_find(P.probes[" + p + "].t, wk" + tag + ", key_hash(wk" + tag + ", " +
-             num(pd.keys.nwords) + "));");
+        if (pd.dense)
+            line("const uint32_t hb" + tag + " = dense_find(P.probes[" + p + "].dense, P.probes[" + p + "].dmin, P.probes[" +
+                 p + "].drange, wk" + tag + "[0]);");
+        else
+            line("const uint32_t hb" + tag + " = table_find(P.probes[" + p + "].t, wk" + tag + ", key_hash(wk" + tag +
+                 ", " + num(pd.keys.nwords) + "));");
         line("if (hb" + tag + " == kNone) continue;");
         if (st.idx == P_.head_probe) line("x.head = hb" + tag + ";");
         if (P_.has_chains && pd.next) {
@@ -466,6 +470,29 @@ class Gen {
                 preload(slots, a);
                 pre[j] = cols;
             });
+            if (pd.dense) {  // direct index: one 4-byte load per row, issued for every row first
+                rows([&](int j, const std::string& a) {
+                    cols = pre[j];
+                    std::string tag = "p" + num(s) + "_" + num(j);
+                    line("uint64_t wk" + tag + "[2] = {0ull, 0ull};");
+                    line("uint32_t d" + tag + " = kNone;");
+                    open("if (" + a + ") {  // probe " + p + " (dense index)");
+                    key(pd.keys, "wk" + tag, a + " = false;", "");
+                    line("d" + tag + " = dense_find(P.probes[" + p + "].dense, P.probes[" + p + "].dmin, P.probes[" + p +
+                         "].drange, wk" + tag + "[0]);");
+                    close();
+                });
+                cols.clear();
+                rows([&](int j, const std::string& a) {
+                    std::string tag = "p" + num(s) + "_" + num(j);
+                    open("if (" + a + ") {");
+                    line(a + " = d" + tag + " != kNone;");
+                    line(x + ".b" + p + " = d" + tag + ";");
+                    if (st.idx == P_.head_probe) line(x + ".head = d" + tag + ";");
+                    close();
+                });
+                continue;
+            }
             rows([&](int j, const std::string& a) {
                 cols = pre[j];
                 std::string tag = "p" + num(s) + "_" + num(j);

@@ -57,6 +57,12 @@ struct Cursors {
     }
 };
 
+// Build row matching the normalized key `w` through probe `pd` (dense index or hash table).
+__device__ __forceinline__ uint32_t probe_find(const ProbeDev& pd, const uint64_t* w) {
+    if (pd.dense) return dense_find(pd.dense, pd.dmin, pd.drange, w[0]);
+    return table_find(pd.t, w, key_hash(w, pd.t.nwords));
+}
+
 // Run the streaming stages for one source row; call sink(ctx) for every surviving
 // (row, build matches...) combination.  Duplicate build keys are walked through their
 // chains with backtracking, like HashJoinProbe's chain walk (join.rs:297-309).
@@ -75,7 +81,7 @@ __device__ __forceinline__ void run_stages(const PipeArgs& P, const EvalEnv& env
                 uint64_t w[2];
                 uint32_t nm;
                 if (!make_key(env, pd.keys, x, w, &nm, true)) return;
-                uint32_t b = table_find(pd.t, w, key_hash(w, pd.t.nwords));
+                uint32_t b = probe_find(pd, w);
                 if (b == kNone) return;
                 x.set_build(st.idx, b);
                 if (st.idx == P.head_probe) x.head = b;
@@ -102,7 +108,7 @@ __device__ __forceinline__ void run_stages(const PipeArgs& P, const EvalEnv& env
                 uint64_t w[2];
                 uint32_t nm;
                 if (make_key(env, pd.keys, x, w, &nm, true)) {
-                    uint32_t b = table_find(pd.t, w, key_hash(w, pd.t.nwords));
+                    uint32_t b = probe_find(pd, w);
                     if (b != kNone) {
                         x.set_build(st.idx, b);
                         if (st.idx == P.head_probe) x.head = b;
@@ -591,6 +597,54 @@ __global__ void k_probe_write(const __grid_constant__ PipeArgs P, const uint64_t
     }
 }
 
+// Range of a one-column integer join key over the valid build rows, as normalized key
+// words (int32/date keys zero-extended from 32 bits, int64 keys as is).
+__device__ __forceinline__ uint64_t norm_int_key(const void* data, int dt, uint32_t r) {
+    if (dt == ML_TYPE_INT64) return (uint64_t)__ldg((const unsigned long long*)data + r);
+    return (uint64_t)(uint32_t)__ldg((const int32_t*)data + r);
+}
+__global__ void k_key_range(const void* data, int dt, const uint64_t* valid, int64_t n, unsigned long long* mm) {
+    unsigned long long lo = ~0ull, hi = 0;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if (!valid_bit(valid, (uint32_t)i)) continue;
+        unsigned long long k = norm_int_key(data, dt, (uint32_t)i);
+        lo = k < lo ? k : lo;
+        hi = k > hi ? k : hi;
+    }
+    for (int o = 16; o; o >>= 1) {
+        unsigned long long l2 = __shfl_xor_sync(0xFFFFFFFFu, lo, o), h2 = __shfl_xor_sync(0xFFFFFFFFu, hi, o);
+        lo = l2 < lo ? l2 : lo;
+        hi = h2 > hi ? h2 : hi;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(mm, lo);
+        atomicMax(mm + 1, hi);
+    }
+}
+// build_table (join.rs:160-203) over a dense key: the index entry holds the chain head,
+// later rows with the same key push the previous head into `next`.
+__global__ void k_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint32_t* dense,
+                               uint32_t* next, uint32_t* dup_flag) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        uint32_t r = (uint32_t)i;
+        if (!valid_bit(valid, r)) continue;  // NULL keys never match
+        uint32_t old = atomicExch(dense + (norm_int_key(data, dt, r) - dmin), r);
+        if (old != kNone) {
+            next[r] = old;
+            if (*dup_flag == 0) atomicExch(dup_flag, 1u);
+        }
+    }
+}
+__global__ void k_count_dense(const uint32_t* dense, uint64_t n, unsigned long long* out) {
+    unsigned long long c = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        c += dense[i] != kNone;
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
 __global__ void k_count_slots(TableView t, unsigned long long* out) {
     uint64_t n = t.mask + 1;
     unsigned long long c = 0;
@@ -946,6 +1000,16 @@ void launch_hash_columns(const PipeArgs& P, int ncols, const uint64_t* const* di
 void launch_join_insert(const PipeArgs& P, const KeyLayout& L, TableView t, uint32_t* next, uint32_t* dup_flag,
                         int64_t n, cudaStream_t s) {
     if (n) k_join_insert<<<grid_for(n, 8), kThreads, 0, s>>>(P, L, t, next, dup_flag, n);
+}
+void launch_key_range(const void* data, int dt, const uint64_t* valid, int64_t n, unsigned long long* mm, cudaStream_t s) {
+    if (n) k_key_range<<<grid_for(n, 4), kThreads, 0, s>>>(data, dt, valid, n, mm);
+}
+void launch_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint32_t* dense,
+                         uint32_t* next, uint32_t* dup_flag, cudaStream_t s) {
+    if (n) k_dense_insert<<<grid_for(n, 8), kThreads, 0, s>>>(data, dt, valid, n, dmin, dense, next, dup_flag);
+}
+void launch_count_dense(const uint32_t* dense, uint64_t n, unsigned long long* out, cudaStream_t s) {
+    if (n) k_count_dense<<<grid_for((int64_t)n, 8), kThreads, 0, s>>>(dense, n, out);
 }
 void launch_probe_count(const PipeArgs& P, uint32_t* counts, cudaStream_t s) {
     if (P.n) k_probe_count<<<grid_for(P.n, 8), kThreads, 0, s>>>(P, counts);

@@ -79,6 +79,12 @@ void launch_utf8_copy(const uint32_t* off, const uint8_t* bytes, const uint32_t*
 void launch_u64_to_u32(const uint64_t* in, uint32_t* out, int64_t n, cudaStream_t s);
 
 // Top-N: each CTA sorts a chunk of candidate rows and keeps the best k.
+// Dense join index: key range of a one-column integer build key (mm[0] = min, mm[1] = max,
+// initialized to ~0 / 0), the insert, and the count of distinct keys.
+void launch_key_range(const void* data, int dt, const uint64_t* valid, int64_t n, unsigned long long* mm, cudaStream_t s);
+void launch_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint32_t* dense,
+                         uint32_t* next, uint32_t* dup_flag, cudaStream_t s);
+void launch_count_dense(const uint32_t* dense, uint64_t n, unsigned long long* out, cudaStream_t s);
 void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, uint32_t* out, cudaStream_t s);
 // Top-k for k <= kTopNWarpMax: each CTA writes its best k rows (sorted) to out[block * k ..].
 constexpr int kTopNWarpMax = 32;

@@ -243,6 +243,9 @@ void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrow
         P.probes[p].t = jt->view();
         P.probes[p].next = jt->has_dups ? jt->next.get<uint32_t>() : nullptr;
         P.probes[p].keys = probes[p].keys;
+        P.probes[p].dense = jt->dense ? jt->dense.get<uint32_t>() : nullptr;
+        P.probes[p].dmin = jt->dmin;
+        P.probes[p].drange = jt->drange;
         P.has_chains |= jt->has_dups ? 1 : 0;
     }
     // scratch: dictionary id maps and predicate tables for this batch

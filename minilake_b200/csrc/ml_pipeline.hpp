@@ -85,6 +85,9 @@ struct ml_join_table {
     mlg::DevBuf slots, next, dup;
     uint64_t cap = 0;
     bool has_dups = false;
+    // Dense integer key: a direct-mapped index replaces the hash table (see ProbeDev).
+    mlg::DevBuf dense;
+    uint64_t dmin = 0, drange = 0;
     mlg::TableView view() const {
         mlg::TableView t{};
         t.slots = slots.get<uint64_t>();

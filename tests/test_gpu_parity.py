@@ -373,3 +373,59 @@ def test_group_by_join_key_with_duplicate_and_null_build_keys(gpu_engine, by_bui
             assert out.sink_stats["capacity"] == 0, "expected the join-key group mode (no aggregate table)"
         res[name] = eng.fetch(out)
     assert_same_rows(res["gpu"], res["oracle"], 1, {1})
+
+
+@pytest.mark.parametrize("kind", ["dense", "sparse", "negative_i32", "compound", "utf8"])
+def test_join_index_kinds_match_oracle(gpu_engine, kind):
+    """Dense integer keys use the direct index, all other keys the hash table; both must
+    give the oracle's matches (through the fused aggregate) and distinct-key counts."""
+    rng = np.random.default_rng(12)
+    nd, nf = 4000, 30_000
+    valid = rng.random(nd) > 0.03
+    if kind == "dense":
+        pool = np.arange(100, 2100, dtype=np.int64)
+        types, mk = [INT64], lambda v, m=None: [fixed(INT64, v, m)]
+    elif kind == "sparse":
+        pool = rng.integers(-2**62, 2**62, 1500, dtype=np.int64)
+        types, mk = [INT64], lambda v, m=None: [fixed(INT64, v, m)]
+    elif kind == "negative_i32":
+        pool = np.arange(-1000, 1000, dtype=np.int32)
+        types, mk = [INT32], lambda v, m=None: [fixed(INT32, v, m)]
+    elif kind == "compound":
+        pool = np.arange(3000, dtype=np.int64)
+        types = [INT32, INT32]
+        mk = lambda v, m=None: [fixed(INT32, (v % 50).astype(np.int32), m), fixed(INT32, (v // 50).astype(np.int32))]
+    else:
+        pool = np.array([b"k%05d" % i for i in range(1200)], dtype=object)
+        types = [UTF8]
+        mk = lambda v, m=None: [utf8_plain(list(v), m)]
+    dk = pool[rng.integers(0, len(pool), nd)]
+    # fact keys: mostly from the pool, some misses
+    fk = pool[rng.integers(0, len(pool), nf)]
+    if kind == "dense":  # probe keys below, inside and above the indexed range
+        fk = rng.integers(0, 2300, nf).astype(np.int64)
+    nkey = len(types)
+    dim = Table("d", [f"k{i}" for i in range(nkey)] + ["x"], [mk(dk, valid) + [fixed(INT32, rng.integers(0, 13, nd))]])
+    fact = Table("f", [f"f{i}" for i in range(nkey)] + ["v"], [mk(fk) + [fixed(FLOAT64, rng.random(nf))]])
+    keys = [(Col(i), t) for i, t in enumerate(types)]
+    # fact columns [f.., v] then build columns [k.., x]: x is column 2 * nkey + 1
+    group = [(Col(2 * nkey + 1), INT32)]
+    aggs = [AggSpec(SUM, Col(nkey), FLOAT64), AggSpec(COUNT_STAR)]
+    if kind == "utf8":  # string join keys are refused with Unsupported on the GPU
+        from minilake_b200.gpu import MiniLakeError
+        with pytest.raises(MiniLakeError, match="string join keys"):
+            gpu_engine.join_build(dim, types + [INT32], keys)
+        return
+    res, stats = {}, {}
+    for name, eng in (("gpu", gpu_engine), ("oracle", orc.OracleEngine(threads=2))):
+        j = eng.join_build(dim, types + [INT32], keys)
+        stats[name] = j.stats()
+        out = eng.hashagg(fact, types + [FLOAT64], group, aggs, prologue=[Probe(j.handle, keys)])
+        res[name] = eng.fetch(out)
+    assert stats["gpu"]["distinct_keys"] == stats["oracle"]["distinct_keys"]
+    if kind == "dense":
+        assert stats["gpu"]["capacity"] == 2000  # value range 100..2099: direct index
+    else:
+        cap = stats["gpu"]["capacity"]
+        assert cap & (cap - 1) == 0, "hash table capacity is a power of two"
+    assert_same_rows(res["gpu"], res["oracle"], 1, {1})
