@@ -908,21 +908,43 @@ __device__ __forceinline__ TopEntry warp_merge32(const SortDev& S, TopEntry l, T
     return e;
 }
 
+// Rows that beat the warp's current k-th entry are queued in shared memory; a full queue
+// (32 entries) is sorted and merged into the list, so the sort runs once per 32
+// candidates, not once per 32 rows (about k * ln(rows / k) candidates reach a warp).
 __global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortDev S, const uint32_t* in, int64_t n,
                                                    int k, uint32_t* out) {
     __shared__ TopEntry lists[8][32];
+    __shared__ TopEntry queue[8][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     TopEntry best{~0ull, kNone};
+    TopEntry kth = best;
+    int qn = 0;  // entries in this warp's queue (warp-uniform)
+    auto flush = [&]() {
+        TopEntry e = lane < qn ? queue[warp][lane] : TopEntry{~0ull, kNone};
+        __syncwarp();
+        best = warp_merge32(S, best, warp_sort32(S, e, lane), lane);
+        kth = shfl_entry(best, k - 1);
+        qn = 0;
+    };
     const int64_t warps = (int64_t)gridDim.x * 8;
     for (int64_t base = ((int64_t)blockIdx.x * 8 + warp) * 32; base < n; base += warps * 32) {
         int64_t i = base + lane;
         TopEntry e;
         e.r = i < n ? (in ? in[i] : (uint32_t)i) : kNone;
         e.p = sort_prefix(S, e.r);
-        TopEntry kth = shfl_entry(best, k - 1);
-        if (!__any_sync(0xFFFFFFFFu, e.r != kNone && entry_less(S, e, kth))) continue;
-        best = warp_merge32(S, best, warp_sort32(S, e, lane), lane);
+        bool take = e.r != kNone && entry_less(S, e, kth);
+        unsigned m = __ballot_sync(0xFFFFFFFFu, take);
+        if (!m) continue;
+        if (qn + __popc(m) > 32) {
+            flush();
+            take = take && entry_less(S, e, kth);
+            m = __ballot_sync(0xFFFFFFFFu, take);
+        }
+        if (take) queue[warp][qn + __popc(m & ((1u << lane) - 1))] = e;
+        qn += __popc(m);
+        __syncwarp();
     }
+    if (qn) flush();
     lists[warp][lane] = best;
     __syncthreads();
     if (warp == 0) {
