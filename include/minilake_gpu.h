@@ -225,6 +225,29 @@ int ml_gpu_filter(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32
                   int64_t nrows, const uint32_t* sel_in, int64_t nsel_in, int32_t location,
                   uint32_t* sel_out, int64_t* nsel_out);
 
+/* ---- FilterOperator without allocation (no counterpart in the reference) ----------- */
+/* ml_gpu_filter for callers that cannot allocate device memory: a query whose HBM budget
+ * is spent (every new reservation would fail with ML_ERR_BUDGET) but that still has to
+ * filter, and latency-critical callers for which cudaMalloc / cudaFree are off limits
+ * because they can synchronize the whole device.  Same predicate semantics, inputs and
+ * result as ml_gpu_filter (ordered selection, count on the host), with these limits:
+ *  - every column is device resident (ML_LOC_DEVICE); sel_in (optional) and sel_out are
+ *    device pointers; sel_out has room for nsel_in (or nrows) entries;
+ *  - at most 16,777,216 rows per call (selected rows when sel_in is given), 2048 program
+ *    instructions, 64 KiB of literals and 512 KiB of dictionary tables; a larger call fails
+ *    with ML_ERR_INVALID and a message that names the limit;
+ *  - its temporaries live in one static device array of 2,953,472 bytes per device, whose
+ *    address the first call on a device looks up (cudaGetSymbolAddress, with that device
+ *    current): make that first call before any stream capture.  Nothing in the array has
+ *    to start at zero (each call clears its own error word);
+ *  - calls on the same device share the array, so overlapping calls would race on it: each
+ *    call holds a per-device lock until its result is on the host.
+ * It allocates no device memory and no pinned host memory; the predicate is compiled on the
+ * host heap. */
+int ml_gpu_filter_static(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32_t ncols,
+                         int64_t nrows, const uint32_t* sel_in, int64_t nsel_in, uint32_t* sel_out,
+                         int64_t* nsel_out);
+
 /* ---- Operator: ProjectionOperator (operators/projection.rs:21-32) -------------- */
 /* Evaluate `expr` over ALL physical rows into a new device column (batch of 1 column). */
 int ml_gpu_project(ml_ctx* ctx, const ml_expr* expr, const ml_column* cols, int32_t ncols,

@@ -669,6 +669,75 @@ int ml_gpu_filter(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32
     API_END
 }
 
+// ml_gpu_filter with every temporary in the device's static scratch array (no allocation).
+namespace {
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu[kStaticMaxDevices];  // one call at a time per device: they share the array
+uint8_t* g_static_base[kStaticMaxDevices];
+}  // namespace
+
+int ml_gpu_filter_static(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32_t ncols, int64_t nrows,
+                         const uint32_t* sel_in, int64_t nsel_in, uint32_t* sel_out, int64_t* nsel_out) {
+    API_BEGIN
+    REQUIRE(ctx && pred && sel_out && nsel_out && (cols || ncols == 0) && ncols >= 0 && nrows >= 0, "bad arguments");
+    REQUIRE(ctx->device >= 0 && ctx->device < kStaticMaxDevices, "device index out of range");
+    for (int c = 0; c < ncols; c++)
+        REQUIRE(cols[c].location == ML_LOC_DEVICE, "ml_gpu_filter_static reads device-resident columns only");
+    const int64_t n = sel_in ? nsel_in : nrows;
+    REQUIRE(nsel_in >= 0, "bad selection length");
+    if (n > kStaticFilterMaxRows || nrows > 0xFFFFFFFFll)
+        raise(ML_ERR_INVALID, "ml_gpu_filter_static: " + std::to_string(n) + " rows exceed the static scratch limit of " +
+                                  std::to_string(kStaticFilterMaxRows) + " rows per call");
+    ctx->set_current();
+    std::lock_guard<std::mutex> dev_lock(g_static_mu[ctx->device]);
+    if (!g_static_base[ctx->device]) {  // first call on this device: look the array up (device is current)
+        g_static_base[ctx->device] = (uint8_t*)static_filter_scratch();
+        REQUIRE(g_static_base[ctx->device], "cudaGetSymbolAddress failed for the static filter scratch");
+    }
+    uint8_t* base = g_static_base[ctx->device];
+    std::lock_guard<std::mutex> g(ctx->op_mu);
+    cudaStream_t s = ctx->stream;
+    std::vector<int32_t> types;
+    for (int c = 0; c < ncols; c++) types.push_back(cols[c].dtype);
+    Pipeline p(ctx);
+    ml_pipe_op op{};
+    op.kind = ML_PIPE_FILTER;
+    op.nexprs = 1;
+    op.exprs = pred;
+    p.build(&op, 1, types.data(), ncols);
+    const size_t pbytes = p.C.code.size() * sizeof(Instr), abytes = p.C.arena.size();
+    if (pbytes > kStaticProgBytes || abytes > kStaticArenaBytes)
+        raise(ML_ERR_INVALID, "ml_gpu_filter_static: the predicate compiles to " + std::to_string(pbytes) +
+                                  " bytes of program and " + std::to_string(abytes) + " bytes of literals; the limits are " +
+                                  std::to_string(kStaticProgBytes) + " and " + std::to_string(kStaticArenaBytes));
+    if (pbytes) CK(cudaMemcpyAsync(base + kStaticProgOff, p.C.code.data(), pbytes, cudaMemcpyHostToDevice, s));
+    if (abytes) CK(cudaMemcpyAsync(base + kStaticArenaOff, p.C.arena.data(), abytes, cudaMemcpyHostToDevice, s));
+    Staging st(ctx);  // unused: device-resident columns are read in place
+    Pipeline::Launch L;
+    p.prepare(L, cols, ncols, nrows, sel_in, nsel_in, s, st, nullptr, base + kStaticTablesOff, kStaticTablesBytes);
+    L.P.prog = (const Instr*)(base + kStaticProgOff);
+    L.P.arena = base + kStaticArenaOff;
+    uint32_t* err = (uint32_t*)(base + kStaticErrOff);
+    CK(cudaMemsetAsync(err, 0, 4, s));
+    L.P.err = err;
+    uint32_t* bits = (uint32_t*)(base + kStaticBitsOff);
+    uint32_t* counts = (uint32_t*)(base + kStaticCountsOff);
+    uint64_t* offs = (uint64_t*)(base + kStaticOffsetsOff);
+    const int nb = select_blocks(n);
+    launch_select_flags(L.P, bits, counts, s);
+    launch_scan_u32(counts, offs, nb, (uint64_t*)(base + kStaticScanOff), s);
+    launch_select_write(L.P, bits, offs, sel_out, s);
+    ctx->count_launch(5);
+    uint64_t total = 0;
+    uint32_t errw = 0;
+    CK(cudaMemcpyAsync(&total, offs + nb, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&errw, err, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    check_device_error(ctx, errw);
+    *nsel_out = (int64_t)total;
+    API_END
+}
+
 int ml_gpu_project(ml_ctx* ctx, const ml_expr* expr, const ml_column* cols, int32_t ncols, int64_t nrows, ml_batch** out) {
     API_BEGIN
     REQUIRE(ctx && expr && out, "null argument");

@@ -955,6 +955,20 @@ __global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortD
 
 }  // namespace
 
+// Temporaries of ml_gpu_filter_static: a fixed-size device array, so that call allocates no
+// device memory.  Nothing in it has to start at zero: the error word is cleared by each call
+// and every other region is written before it is read.
+static __device__ __align__(256) uint8_t g_static_filter_scratch[kStaticScratchBytes];
+static_assert(kStaticCountsBytes >= 4 * (kStaticFilterMaxRows / kSelRowsPerBlock + 1), "block counts");
+static_assert(kStaticOffsetsBytes >= 8 * (kStaticFilterMaxRows / kSelRowsPerBlock + 2), "block offsets");
+static_assert(kStaticScanBytes >= 8 * ((kStaticFilterMaxRows / kSelRowsPerBlock + 1) / kScanBlock + 3), "scan scratch");
+
+void* static_filter_scratch() {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_static_filter_scratch) != cudaSuccess) return nullptr;
+    return p;
+}
+
 // ---- launch wrappers -------------------------------------------------------------------------------
 int pipeline_grid(int64_t n) { return grid_for(n, 8); }
 int agg_smem_bytes(const AggArgs& A) { return (int)((size_t)A.smem_groups * A.stride * 8); }

@@ -91,6 +91,30 @@ constexpr int kTopNWarpMax = 32;
 int topn_warp_blocks(int64_t n);
 void launch_topn_warp(const SortDev& S, const uint32_t* in, int64_t n, int k, int blocks, uint32_t* out, cudaStream_t s);
 
+// ---- static scratch of ml_gpu_filter_static ----------------------------------------------
+// One file-scope device array per device holds every temporary of the no-allocation filter:
+// error word, program, arena, per-batch dictionary tables, flag words, block counts, scan.
+constexpr int64_t kStaticFilterMaxRows = 1 << 24;  // rows (or selected input rows) per call
+constexpr size_t kStaticAlign = 256;
+constexpr size_t kStaticErrOff = 0;
+constexpr size_t kStaticProgOff = 256;
+constexpr size_t kStaticProgBytes = 64 << 10;       // 2048 instructions
+constexpr size_t kStaticArenaOff = kStaticProgOff + kStaticProgBytes;
+constexpr size_t kStaticArenaBytes = 64 << 10;      // literals, patterns, IN lists
+constexpr size_t kStaticTablesOff = kStaticArenaOff + kStaticArenaBytes;
+constexpr size_t kStaticTablesBytes = 512 << 10;    // dictionary id maps and predicate tables
+constexpr size_t kStaticBitsOff = kStaticTablesOff + kStaticTablesBytes;
+constexpr size_t kStaticBitsBytes = (size_t)kStaticFilterMaxRows / 8;
+constexpr size_t kStaticCountsOff = kStaticBitsOff + kStaticBitsBytes;
+constexpr size_t kStaticCountsBytes = 64 << 10;     // u32 per 2048-row block
+constexpr size_t kStaticOffsetsOff = kStaticCountsOff + kStaticCountsBytes;
+constexpr size_t kStaticOffsetsBytes = 128 << 10;   // u64 per block, + 1
+constexpr size_t kStaticScanOff = kStaticOffsetsOff + kStaticOffsetsBytes;
+constexpr size_t kStaticScanBytes = 4 << 10;
+constexpr size_t kStaticScratchBytes = kStaticScanOff + kStaticScanBytes;  // 2,953,472 bytes
+// Device address of the scratch array on the current device (cudaGetSymbolAddress).
+void* static_filter_scratch();
+
 // Fill / concatenation helpers
 void launch_fill_u32(uint32_t* p, uint32_t v, int64_t n, cudaStream_t s);
 // dst[i] = src[i] - src[0] + base for i in 0..=n

@@ -213,7 +213,7 @@ static bool dict_pred(const LutSpec& L, const std::string& s) {  // per-entry pr
 }
 
 void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrows, const uint32_t* sel, int64_t nsel,
-                       cudaStream_t s, Staging& st, Reservation* res) {
+                       cudaStream_t s, Staging& st, Reservation* res, uint8_t* tables_dst, size_t tables_cap) {
     if (ncols != (int)input_types.size())
         raise(ML_ERR_INVALID, "batch has " + std::to_string(ncols) + " columns, the pipeline expects " +
                                   std::to_string(input_types.size()));
@@ -307,12 +307,21 @@ void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrow
         lut_at.push_back({(int)l, put(t.data(), t.size())});
     }
     if (!scratch.empty()) {
-        L.scratch = DevBuf(ctx, scratch.size(), nullptr);
-        void* h = st.get(scratch.size());
-        CK(cudaStreamSynchronize(s));  // the staging buffer may still feed an earlier copy
-        memcpy(h, scratch.data(), scratch.size());
-        CK(cudaMemcpyAsync(L.scratch.get(), h, scratch.size(), cudaMemcpyHostToDevice, s));
-        uint8_t* base = L.scratch.get<uint8_t>();
+        uint8_t* base;
+        if (tables_dst) {
+            if (scratch.size() > tables_cap)
+                raise(ML_ERR_INVALID, "dictionary tables of this batch need " + std::to_string(scratch.size()) +
+                                          " bytes, more than the " + std::to_string(tables_cap) + " the call provides");
+            CK(cudaMemcpyAsync(tables_dst, scratch.data(), scratch.size(), cudaMemcpyHostToDevice, s));
+            base = tables_dst;
+        } else {
+            L.scratch = DevBuf(ctx, scratch.size(), nullptr);
+            void* h = st.get(scratch.size());
+            CK(cudaStreamSynchronize(s));  // the staging buffer may still feed an earlier copy
+            memcpy(h, scratch.data(), scratch.size());
+            CK(cudaMemcpyAsync(L.scratch.get(), h, scratch.size(), cudaMemcpyHostToDevice, s));
+            base = L.scratch.get<uint8_t>();
+        }
         for (auto& g : gid_at) P.cols[g.first].gid = (const uint32_t*)(base + g.second);
         for (auto& g : dict_at) P.cols[g.first].off = (const uint32_t*)(base + g.second);
         for (auto& g : dbytes_at) P.cols[g.first].dbytes = base + g.second;

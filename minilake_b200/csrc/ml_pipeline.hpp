@@ -56,8 +56,10 @@ class Pipeline {
         PipeArgs P{};
         std::vector<int> col_valid;  // slot has a validity bitmap in this launch
     };
+    // With `tables_dst`, the per-batch tables are copied there (at most `tables_cap` bytes,
+    // from pageable memory) instead of into a new device buffer.
     void prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrows, const uint32_t* sel, int64_t nsel,
-                 cudaStream_t s, Staging& st, Reservation* res);
+                 cudaStream_t s, Staging& st, Reservation* res, uint8_t* tables_dst = nullptr, size_t tables_cap = 0);
     // Slot mask check: does program `p` read a column with a validity bitmap?
     bool reads_nullable(const Prog& p, const Launch& L) const;
 };

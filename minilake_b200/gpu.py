@@ -65,6 +65,7 @@ def _load():
         "ml_gpu_batch_fetch": ([VP, I32, VP, VP, VP], C.c_int),
         "ml_gpu_batch_destroy": ([VP], C.c_int),
         "ml_gpu_filter": ([VP, P(abi.MlExpr), P(abi.MlColumn), I32, I64, VP, I64, I32, VP, P(I64)], C.c_int),
+        "ml_gpu_filter_static": ([VP, P(abi.MlExpr), P(abi.MlColumn), I32, I64, VP, I64, VP, P(I64)], C.c_int),
         "ml_gpu_project": ([VP, P(abi.MlExpr), P(abi.MlColumn), I32, I64, P(VP)], C.c_int),
         "ml_gpu_hash_columns": ([VP, P(abi.MlColumn), I32, I64, VP, I64, I32, VP], C.c_int),
         "ml_gpu_hashagg_create": ([VP, P(abi.MlPipeOp), I32, VP, I32, P(abi.MlExpr), I32, P(abi.MlAggSpec), I32,

@@ -1,0 +1,85 @@
+"""ml_gpu_filter_static — the filter whose temporaries live in a static device array —
+against ml_gpu_filter on the same device-resident inputs, through the C ABI.  Selections
+are index work: they must be identical."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from minilake_b200 import abi
+from minilake_b200.abi import FLOAT64, INT32, IsNull, Like, Col, Lit
+from minilake_b200.columns import encode_strings, fixed, utf8_plain
+
+pytestmark = pytest.mark.gpu
+
+WORDS = [b"apple", b"abricot", b"banana", b"ab", b"", b"zeta"]
+
+
+def _device_u32(n):
+    import torch
+    return torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
+
+
+def _filter(lib, ctx, pred, cols, nc, nrows, sel, nsel, out, static):
+    keep = abi.Keep()
+    e = abi.encode_expr(pred, abi.BOOL, keep)
+    k = C.c_int64()
+    sp = C.c_void_p(sel.data_ptr()) if sel is not None else None
+    if static:
+        st = lib.ml_gpu_filter_static(ctx.h, C.byref(e), cols, nc, nrows, sp, nsel, C.c_void_p(out.data_ptr()),
+                                      C.byref(k))
+    else:
+        st = lib.ml_gpu_filter(ctx.h, C.byref(e), cols, nc, nrows, sp, nsel, abi.LOC_DEVICE,
+                               C.c_void_p(out.data_ptr()), C.byref(k))
+    return st, k.value
+
+
+def test_static_filter_matches_filter_on_two_calls_in_a_row():
+    import torch
+    from minilake_b200.gpu import LIB, Context
+    ctx = Context(0)
+    rng = np.random.default_rng(31)
+    n = 250_000
+    valid = rng.random(n) > 0.1
+    batch = ctx.upload([fixed(INT32, rng.integers(-100, 100, n, dtype=np.int32), valid),
+                        fixed(FLOAT64, rng.random(n)),
+                        encode_strings(WORDS, rng.integers(0, len(WORDS), n), rng.random(n) > 0.05),
+                        utf8_plain([WORDS[i] for i in rng.integers(0, len(WORDS), n)])])
+    cols, nc = batch.ml_columns()
+    sel = torch.from_numpy(np.sort(rng.choice(n, n // 3, replace=False)).astype(np.int32)).cuda()
+    calls = [((Col(0) > Lit(10)) & Like(Col(2), "ab%"), None, 0),
+             ((Col(1) < Lit(0.25)) | IsNull(Col(0)) | Like(Col(3), "%an%"), sel, len(sel))]
+    free_after = []
+    for pred, s, ns in calls:
+        ref, got = _device_u32(n), _device_u32(n)
+        st, k_ref = _filter(LIB, ctx, pred, cols, nc, n, s, ns, ref, static=False)
+        assert st == 0
+        torch.cuda.synchronize()
+        before = torch.cuda.mem_get_info()[0]
+        st, k = _filter(LIB, ctx, pred, cols, nc, n, s, ns, got, static=True)
+        assert st == 0, LIB.ml_gpu_last_error()
+        free_after.append((before, torch.cuda.mem_get_info()[0]))
+        assert k == k_ref and k > 0
+        assert torch.equal(got[:k], ref[:k])
+    # the second call finds its scratch in place: the device's free memory does not move
+    assert free_after[1][0] == free_after[1][1]
+    batch.close()
+    ctx.close()
+
+
+def test_static_filter_rejects_calls_over_its_limit():
+    import torch
+    from minilake_b200.gpu import LIB, Context
+    ctx = Context(0)
+    dummy = torch.zeros(16, dtype=torch.int32, device="cuda")
+    rows = (1 << 24) + 1
+    col = (abi.MlColumn * 1)()
+    col[0].dtype, col[0].encoding, col[0].location, col[0].len = INT32, abi.ENC_PLAIN, abi.LOC_DEVICE, rows
+    col[0].data = C.c_void_p(dummy.data_ptr())
+    keep = abi.Keep()
+    e = abi.encode_expr(Col(0) > Lit(0), abi.BOOL, keep)
+    k = C.c_int64()
+    st = LIB.ml_gpu_filter_static(ctx.h, C.byref(e), col, 1, rows, None, 0, C.c_void_p(dummy.data_ptr()), C.byref(k))
+    assert st == abi.ERR_INVALID
+    assert b"16777216 rows" in LIB.ml_gpu_last_error()
+    ctx.close()
