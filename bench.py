@@ -53,7 +53,7 @@ def dist_env():
     return ws, rank, local
 
 
-def make_data(rank: int, world: int):
+def make_data(rank: int, world: int, fact_rows: int = FACT_ROWS):
     """Dimension table (replicated) and this rank's fact shard, as flat arrays."""
     rng = np.random.Generator(np.random.PCG64(43))
     key = (rng.permutation(DIM_ROWS) + 1).astype(np.int64)
@@ -61,9 +61,9 @@ def make_data(rank: int, world: int):
     # rank r's fact rows reference the keys k in 1..DIM_ROWS with k % world == r
     first = rank if rank > 0 else world
     count = (DIM_ROWS - first) // world + 1
-    fk = first + frng.integers(0, count, FACT_ROWS, dtype=np.int64) * world
-    d = frng.integers(0, 2557, FACT_ROWS, dtype=np.int32)
-    v = frng.uniform(900.0, 105000.0, FACT_ROWS)
+    fk = first + frng.integers(0, count, fact_rows, dtype=np.int64) * world
+    d = frng.integers(0, 2557, fact_rows, dtype=np.int32)
+    v = frng.uniform(900.0, 105000.0, fact_rows)
     return key, fk, d, v
 
 
@@ -197,7 +197,8 @@ def gpu_arm(args):
     from minilake_b200.columns import fixed
     from minilake_b200.gpu import PROFILE, Context
     log(f"[rank {rank}] generating data")
-    key, fk, d, v = make_data(rank, world)
+    key, fk, d, v = make_data(rank, world, args.fact_rows)
+    rows = args.fact_rows
     ctx = Context(local, flags=PROFILE)
     log(f"[rank {rank}] uploading tables")
     q = GpuQuery(ctx, key, fk, d, v)
@@ -242,7 +243,7 @@ def gpu_arm(args):
     keep.append(tkey)
     from minilake_b200 import abi
     nmorsel = 16
-    bounds = np.linspace(0, FACT_ROWS, nmorsel + 1).astype(np.int64)
+    bounds = np.linspace(0, rows, nmorsel + 1).astype(np.int64)
     morsels = [[fixed(abi.INT64, pinned[0][bounds[i]:bounds[i + 1]]), fixed(abi.INT32, pinned[1][bounds[i]:bounds[i + 1]]),
                 fixed(abi.FLOAT64, pinned[2][bounds[i]:bounds[i + 1]])] for i in range(nmorsel)]
     dim_host = [fixed(abi.INT64, pkey)]
@@ -274,12 +275,12 @@ def gpu_arm(args):
             log("merged top-10 fk:", merged[order, 0].astype(np.int64).tolist())
 
     if rank == 0:
-        rows_total = FACT_ROWS * world
+        rows_total = rows * world
         value = rows_total / (ms_max / 1e3 / args.steps)
         e2e = rows_total / (e2e_ms / 1e3 / args.steps)
         peak, peak_kind = measured_peak()
         per_launch_ms = agg_ms / max(n_agg, 1)
-        achieved = FACT_ROWS * BYTES_PER_ROW / (per_launch_ms / 1e3) / 1e9
+        achieved = rows * BYTES_PER_ROW / (per_launch_ms / 1e3) / 1e9
         log("CPU baseline")
         cpu = cpu_baseline(key, fk, d, v) if world == 1 and not args.skip_cpu else None
         line = {
@@ -296,13 +297,13 @@ def gpu_arm(args):
             "dtype": "f64",
             "data": "synthetic (seeded numpy PCG64; BASELINE shapes)",
             "config": {"workload": "join + high-cardinality GROUP BY + top-10: dim 1.5M rows (key i64), "
-                                   "fact 60M rows per GPU (fk i64, d i32, v f64), d > 1200, GROUP BY fk, "
+                                   f"fact {rows / 1e6:g}M rows per GPU (fk i64, d i32, v f64), d > 1200, GROUP BY fk, "
                                    "SUM(v), COUNT(*), ORDER BY SUM(v) DESC, fk LIMIT 10",
-                       "fact_rows_per_gpu": FACT_ROWS, "dim_rows": DIM_ROWS,
+                       "fact_rows_per_gpu": rows, "dim_rows": DIM_ROWS,
                        "l2": "inputs larger than L2 (1.2 GB fact table per step)",
                        "parallelism": f"weak, fact partitioned on the join key over {world} GPU(s)"},
             "e2e": {"value": e2e, "unit": "rows/s",
-                    "h2d_bytes_per_step": int(FACT_ROWS * BYTES_PER_ROW + DIM_ROWS * 8),
+                    "h2d_bytes_per_step": int(rows * BYTES_PER_ROW + DIM_ROWS * 8),
                     "d2h_bytes_per_step": int(10 * 24),
                     "ms_per_step": e2e_ms / args.steps},
             "gpu_launches": int(launches),
@@ -311,8 +312,8 @@ def gpu_arm(args):
                          "kernel": "ml_pipeline_aggregate (runtime-specialized fused filter + join probe + "
                                    "hash aggregate)",
                          "kernel_ms_per_launch": per_launch_ms,
-                         "algorithmic_bytes_per_launch": FACT_ROWS * BYTES_PER_ROW,
-                         "traffic": profiled_traffic()},
+                         "algorithmic_bytes_per_launch": rows * BYTES_PER_ROW,
+                         "traffic": profiled_traffic() if rows == FACT_ROWS else None},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "top10_fk": [int(x) for x in top[0].values],
@@ -399,6 +400,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--fact-rows", type=int, default=FACT_ROWS,
+                    help="fact rows per GPU (smaller cases are for profiling; the benchmark is 60M)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
