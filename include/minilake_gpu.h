@@ -321,6 +321,45 @@ int ml_gpu_topn_combine(ml_topn_local* local);
 int ml_gpu_topn_finalize(ml_topn* sink, ml_batch** out);
 int ml_gpu_topn_destroy(ml_topn* sink);
 
+/* ---- learned cardinality estimator (no counterpart in the reference) ------------- */
+/* Predicts log2 of the number of distinct keys (GROUP BY groups, join-build keys; a NULL key
+ * counts as one group) from scan statistics, to presize hash tables.  Sizing never changes a
+ * result: an underestimate falls back to resize-on-overflow. */
+enum { ML_CARD_FEATURES = 72, ML_CARD_PARAMS = 13057 };
+
+/* One pass over the key expressions of the active rows: a HyperLogLog sketch (2^14 registers
+ * of the engine's key hash) and scan statistics, as the estimator's 72 FP32 features:
+ *   [0, 64)  fraction of registers holding each value 0..63;
+ *   64 log2(rows + 1) / 32;   65 log2(max - min + 1) / 64 of the first normalized key word
+ *   over non-NULL rows;  66 NULL-key fraction;  67 log2(HLL estimate + 1) / 32;
+ *   68 key expressions / 4;  69 normalized key bits / 128;
+ *   70 log2(min(rows, max - min + 1) + 1) / 32;  71 1 if any key is NULL, else 0.
+ * hll_estimate (optional) receives the HyperLogLog estimate (linear counting when small). */
+int ml_gpu_card_features(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64_t nrows,
+                         const uint32_t* sel, int64_t nsel, int32_t location, const ml_expr* keys,
+                         int32_t nkeys, float* features, double* hll_estimate);
+
+typedef struct ml_card_model ml_card_model;
+/* FP32 MLP 72 -> 64 -> 64 -> 64 -> 1 (ReLU); the prediction of log2(distinct) is the MLP's
+ * output plus 32 * feature 67 (= log2(HLL estimate + 1)), so the network learns the sketch's
+ * correction.  Parameters are laid out
+ * [W1 (64x72, row-major [out][in]), b1, W2 (64x64), b2, W3 (64x64), b3, W4 (1x64), b4];
+ * the hidden layers start U(-1/sqrt(fan_in), 1/sqrt(fan_in)) from `seed`, W4 and b4 at zero
+ * (an untrained model predicts the sketch's estimate). */
+int ml_gpu_card_model_create(ml_ctx* ctx, uint64_t seed, ml_card_model** out);
+/* Copy the ML_CARD_PARAMS parameters out (get != NULL) and/or in (set != NULL, also resets Adam). */
+int ml_gpu_card_model_params(ml_card_model* m, float* get, const float* set);
+/* One Adam step (lr, betas 0.9/0.999, eps 1e-8) on a batch of `batch` host rows (x: batch x 72,
+ * y: log2 targets) under mean squared error; *loss = the batch loss before the step. */
+int ml_gpu_card_model_step(ml_card_model* m, const float* x, const float* y, int32_t batch, float lr, float* loss);
+/* `epochs` passes over n host rows in batches, shuffled per epoch from `seed`;
+ * *final_loss = mean batch loss of the last epoch. */
+int ml_gpu_card_model_train(ml_card_model* m, const float* x, const float* y, int64_t n, int32_t epochs,
+                            int32_t batch, float lr, uint64_t seed, float* final_loss);
+/* out[i] = predicted log2(distinct) of host row x[i]. */
+int ml_gpu_card_model_predict(ml_card_model* m, const float* x, int64_t n, float* out);
+int ml_gpu_card_model_destroy(ml_card_model* m);
+
 /* ---- profiling ------------------------------------------------------------------ */
 /* Number of kernels this library has launched since the context was created. */
 int ml_gpu_kernel_launches(ml_ctx* ctx, uint64_t* count);

@@ -77,8 +77,15 @@ __device__ __forceinline__ void acc_merge(int kind, uint64_t* dst, const uint64_
     }
 }
 
+// Append the row combination to the overflow list.  The lanes that overflow together take
+// their slots with one atomic per warp (a full table sends every new key here).
 __device__ inline void record_overflow(const PipeArgs& P, const AggArgs& A, const RowCtx& x) {
-    unsigned long long k = atomicAdd(A.ovf_count, 1ull);
+    const unsigned m = __activemask();
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(A.ovf_count, (unsigned long long)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    const unsigned long long k = base + __popc(m & ((1u << lane) - 1u));
     if (k >= A.ovf_cap) {
         atomicOr(P.err, (uint32_t)DE_OVERFLOW_LOST);
         return;

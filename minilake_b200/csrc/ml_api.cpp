@@ -4,35 +4,13 @@
 #include <cstring>
 #include <shared_mutex>
 
+#include "ml_api_common.hpp"
 #include "ml_jit.hpp"
 #include "ml_pipeline.hpp"
 
 using namespace mlg;
 
-struct ml_ctx : Ctx {
-    using Ctx::Ctx;
-    std::mutex op_mu;  // serializes the standalone operators on the context stream
-};
 
-#define API_BEGIN try {
-#define API_END                                       \
-    }                                                 \
-    catch (const MlError& e) {                        \
-        set_last_error(e.what());                     \
-        return e.code;                                \
-    }                                                 \
-    catch (const std::bad_alloc&) {                   \
-        set_last_error("host allocation failed");    \
-        return ML_ERR_INTERNAL;                       \
-    }                                                 \
-    catch (const std::exception& e) {                 \
-        set_last_error(e.what());                     \
-        return ML_ERR_INTERNAL;                       \
-    }                                                 \
-    return ML_OK;
-
-#define REQUIRE(c, msg) \
-    if (!(c)) raise(ML_ERR_INVALID, msg)
 
 namespace {
 
@@ -1513,7 +1491,17 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
         CK(cudaMemsetAsync(local->ew.d.get(), 0, 4, s));
         L.P.err = local->ew.d.get<uint32_t>();
         AggArgs A = h->args(local->ovf_count.get<unsigned long long>(), ovf2.get<uint32_t>(), count);
-        launch_agg_resume(L.P, A, ovf.get<uint32_t>(), count, w, agg_smem_bytes(A), s);
+        void* jit = jit_agg_resume_kernel(ctx, h->pipe, L.P, A);
+        if (jit) {
+            const uint32_t* rows = ovf.get<uint32_t>();
+            uint64_t cnt = count;
+            int ww = w;
+            void* args[] = {&L.P, &A, &rows, &cnt, &ww};
+            jit_launch(jit, pipeline_grid((int64_t)count), kPipelineThreads, agg_smem_bytes(A), s, args);
+            ctx->add_profile("jit_launch", 0);
+        } else {
+            launch_agg_resume(L.P, A, ovf.get<uint32_t>(), count, w, agg_smem_bytes(A), s);
+        }
         ctx->count_launch();
         CK(cudaMemcpyAsync(local->h_count, local->ovf_count.get(), 8, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(local->ew.h, local->ew.d.get(), 4, cudaMemcpyDeviceToHost, s));

@@ -577,9 +577,12 @@ __device__ inline uint32_t table_insert_row1(const TableView& t, uint64_t key, u
 // Find or insert under concurrent insertion.  On insert, `assign` produces the payload
 // (kNone = refuse: the slot is released and kNone returned).  *inserted tells the caller
 // whether this thread created the entry.
+// With `count` set, a new key is refused without touching the slot once *count has reached
+// `limit` (a full aggregation table: the row goes to the overflow list at once).
 template <class Assign>
 __device__ inline uint32_t table_upsert(const TableView& t, const uint64_t* w, uint32_t nm, uint64_t h, uint32_t* err,
-                                        Assign assign, bool* inserted, uint64_t* slot_out) {
+                                        Assign assign, bool* inserted, uint64_t* slot_out,
+                                        const uint32_t* count = nullptr, uint32_t limit = 0) {
     uint64_t i = h & t.mask;
     const uint32_t full = 2u | (nm << 8);
     *inserted = false;
@@ -588,6 +591,7 @@ __device__ inline uint32_t table_upsert(const TableView& t, const uint64_t* w, u
         uint32_t* st_p = (uint32_t*)s;
         uint32_t st = load_state(st_p);
         if (st == 0) {
+            if (count && *(const volatile uint32_t*)count >= limit) return kNone;
             uint32_t old = atomicCAS(st_p, 0u, 1u);
             if (old == 0) {
                 uint32_t p = assign();

@@ -578,7 +578,7 @@ void emit_aggregate(Gen& g, const AggArgs& A) {
         g.line("uint64_t slot;");
         g.line("const uint32_t g = table_upsert(A.t, wkg, nmg, key_hash(wkg, " + num(A.keys.nwords) +
                ", nmg), P.err, [&]() -> uint32_t { const uint32_t id = atomicAdd(A.ngroups, 1u); "
-               "return id < A.gid_cap ? id : kNone; }, &ins, &slot);");
+               "return id < A.gid_cap ? id : kNone; }, &ins, &slot, A.ngroups, A.gid_cap);");
         g.open("if (g == kNone) {");
         g.line("record_overflow(P, A, " + g.x + ");");
         g.line(g.fail);
@@ -671,6 +671,33 @@ int jit_rows_per_thread(const PipeArgs& P) { return batchable(P) ? kRowsPerThrea
 void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {
     if (!jit_enabled(ctx)) return nullptr;
     return (void*)get_kernel(ctx, jit_agg_source(pipe, P, A), "ml_pipeline_aggregate");
+}
+
+void* jit_agg_resume_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {
+    if (!jit_enabled(ctx)) return nullptr;
+    // the rows a full table sent to the overflow list, aggregated again after the table grew
+    Gen g(pipe.C.code, P);
+    g.fail = "break;";
+    g.open("do {  // aggregate");
+    emit_aggregate(g, A);
+    g.close("} while (0);");
+    const bool smem = A.smem_groups > 0;
+    std::string src = kPrelude;
+    src += "extern \"C\" __global__ void __launch_bounds__(256) ml_pipeline_aggregate_resume(const __grid_constant__ "
+           "PipeArgs P, const __grid_constant__ AggArgs A, const uint32_t* rows, uint64_t count, int w) {\n";
+    src += "    extern __shared__ __align__(16) uint64_t smem[];\n";
+    if (smem) src += "    smem_setup(A, smem);\n    __syncthreads();\n";
+    src += g.pre();
+    src += "    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;\n";
+    src += "    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {\n";
+    src += "        const uint32_t* c = rows + i * (uint64_t)w;\n";
+    src += "        RowCtx x;\n        x.r = c[0];\n        x.b0 = w > 1 ? c[1] : 0;\n        x.b1 = w > 2 ? c[2] : 0;\n";
+    src += "        x.b2 = w > 3 ? c[3] : 0;\n        x.b3 = w > 4 ? c[4] : 0;\n        x.head = 0;\n";
+    src += g.body();
+    src += "    }\n";
+    if (smem) src += "    __syncthreads();\n    smem_flush(A, smem);\n";
+    src += "}\n";
+    return (void*)get_kernel(ctx, src, "ml_pipeline_aggregate_resume");
 }
 
 void* jit_join_insert_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L) {

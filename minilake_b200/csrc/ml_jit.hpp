@@ -17,6 +17,9 @@ namespace mlg {
 // or nullptr when runtime compilation is unavailable or disabled for the context.
 void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A);
 
+// Specialized overflow-resume kernel (signature of k_agg_resume), or nullptr.
+void* jit_agg_resume_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A);
+
 // Specialized join-build insert kernel (signature of k_join_insert), or nullptr.
 void* jit_join_insert_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L);
 

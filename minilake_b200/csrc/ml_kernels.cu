@@ -173,7 +173,7 @@ __device__ __forceinline__ void agg_update(const PipeArgs& P, const AggArgs& A, 
                 uint32_t id = atomicAdd(A.ngroups, 1u);
                 return id < A.gid_cap ? id : kNone;
             },
-            &inserted, &slot);
+            &inserted, &slot, A.ngroups, A.gid_cap);
         if (g == kNone) {
             record_overflow(P, A, x);
             return;

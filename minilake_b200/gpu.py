@@ -57,6 +57,14 @@ def _load():
         "ml_gpu_ctx_synchronize": ([VP], C.c_int),
         "ml_gpu_kernel_launches": ([VP, P(U64)], C.c_int),
         "ml_gpu_profile_read": ([VP, C.c_char_p, P(U64), P(C.c_double), I32], C.c_int),
+        "ml_gpu_card_features": ([VP, P(abi.MlColumn), I32, I64, VP, I64, I32, P(abi.MlExpr), I32, VP,
+                                  P(C.c_double)], C.c_int),
+        "ml_gpu_card_model_create": ([VP, U64, P(VP)], C.c_int),
+        "ml_gpu_card_model_params": ([VP, VP, VP], C.c_int),
+        "ml_gpu_card_model_step": ([VP, VP, VP, I32, C.c_float, P(C.c_float)], C.c_int),
+        "ml_gpu_card_model_train": ([VP, VP, VP, I64, I32, I32, C.c_float, U64, P(C.c_float)], C.c_int),
+        "ml_gpu_card_model_predict": ([VP, VP, I64, VP], C.c_int),
+        "ml_gpu_card_model_destroy": ([VP], C.c_int),
         "ml_gpu_batch_upload": ([VP, P(abi.MlColumn), I32, I64, P(VP)], C.c_int),
         "ml_gpu_batch_num_rows": ([VP, P(I64)], C.c_int),
         "ml_gpu_batch_num_columns": ([VP, P(I32)], C.c_int),
@@ -482,6 +490,78 @@ class SortSink:
     def close(self):
         if self.h:
             LIB.ml_gpu_topn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- learned cardinality estimator ----------------------------------------------------------
+CARD_FEATURES, CARD_PARAMS = 72, 13057
+
+
+def card_features(ctx: Context, cols, keys: Sequence[tuple], sel=None):
+    """(72 FP32 features, HyperLogLog estimate) of the key expressions over a morsel's active
+    rows; `cols` is a DeviceBatch, a list of HostColumns or an (MlColumn array, ncols, nrows)."""
+    keep = abi.Keep()
+    k, nk = abi.encode_exprs(keys, keep)
+    arr, nc, n, _hold = _cols_arg(cols)
+    sp, ns, _s = _sel_arg(sel)
+    f = np.zeros(CARD_FEATURES, dtype=np.float32)
+    est = C.c_double()
+    _check(LIB.ml_gpu_card_features(ctx.h, arr, nc, n, sp, ns, abi.LOC_HOST, k, nk, _ptr(f), C.byref(est)))
+    return f, est.value
+
+
+class CardinalityModel:
+    """FP32 MLP 72-64-64-64-1 predicting log2(distinct keys), trained and run by the library's
+    own CUDA kernels (forward, backward, Adam)."""
+
+    def __init__(self, ctx: Context, seed: int = 0):
+        self.ctx = ctx
+        h = C.c_void_p()
+        _check(LIB.ml_gpu_card_model_create(ctx.h, seed, C.byref(h)))
+        self.h = h
+        ctx._own(self)
+
+    @property
+    def params(self) -> np.ndarray:
+        out = np.zeros(CARD_PARAMS, dtype=np.float32)
+        _check(LIB.ml_gpu_card_model_params(self.h, _ptr(out), None))
+        return out
+
+    @params.setter
+    def params(self, values):
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        assert v.shape == (CARD_PARAMS,)
+        _check(LIB.ml_gpu_card_model_params(self.h, None, _ptr(v)))
+
+    def step(self, x, y, lr: float = 1e-3) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        loss = C.c_float()
+        _check(LIB.ml_gpu_card_model_step(self.h, _ptr(x), _ptr(y), len(y), lr, C.byref(loss)))
+        return loss.value
+
+    def train(self, x, y, epochs: int = 200, batch: int = 64, lr: float = 1e-3, seed: int = 0) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        loss = C.c_float()
+        _check(LIB.ml_gpu_card_model_train(self.h, _ptr(x), _ptr(y), len(y), epochs, batch, lr, seed, C.byref(loss)))
+        return loss.value
+
+    def predict(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, CARD_FEATURES)
+        out = np.zeros(len(x), dtype=np.float32)
+        _check(LIB.ml_gpu_card_model_predict(self.h, _ptr(x), len(x), _ptr(out)))
+        return out
+
+    def close(self):
+        if self.h:
+            LIB.ml_gpu_card_model_destroy(self.h)
             self.h = None
 
     def __del__(self):
