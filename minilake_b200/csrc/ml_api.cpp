@@ -177,6 +177,48 @@ struct ErrWord {  // a device error word plus a pinned readback slot
     ~ErrWord() { ctx->release_slot(h); }
 };
 
+// The streams a sink's work runs on: its live local sinks' streams and one stream of its
+// own (finalize, reset).  Waiting for a sink waits for these only, never for the device work
+// of other sinks (other queries in flight).
+class SinkStreams {
+   public:
+    explicit SinkStreams(Ctx* c) : ctx_(c) {}
+    ~SinkStreams() {
+        if (own_) {
+            cudaStreamSynchronize(own_);
+            ctx_->free_stream(own_);
+        }
+    }
+    cudaStream_t own() {
+        std::lock_guard<std::mutex> g(mu_);
+        if (!own_) own_ = ctx_->new_stream();
+        return own_;
+    }
+    void add(cudaStream_t s) {
+        std::lock_guard<std::mutex> g(mu_);
+        live_.push_back(s);
+    }
+    void remove(cudaStream_t s) {
+        std::lock_guard<std::mutex> g(mu_);
+        live_.erase(std::find(live_.begin(), live_.end(), s));
+    }
+    void sync() {
+        std::vector<cudaStream_t> ss;
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            ss = live_;
+            if (own_) ss.push_back(own_);
+        }
+        for (auto s : ss) CK(cudaStreamSynchronize(s));
+    }
+
+   private:
+    Ctx* ctx_;
+    std::mutex mu_;
+    std::vector<cudaStream_t> live_;
+    cudaStream_t own_ = nullptr;
+};
+
 // The prologue's output for one batch, materialized as owned device columns.
 std::unique_ptr<ml_batch> materialize(Ctx* ctx, Pipeline& pipe, const std::vector<Prog>& out_progs, Pipeline::Launch& L,
                                       cudaStream_t st, Reservation* res, ErrWord& ew) {
@@ -832,15 +874,21 @@ struct ml_join_build {
     std::mutex mu;
     std::vector<std::unique_ptr<ml_batch>> parts;
     std::unique_ptr<ml_join_table> table;
-    ml_join_build(Ctx* c) : ctx(c), pipe(c) {}
+    SinkStreams streams;
+    ml_join_build(Ctx* c) : ctx(c), pipe(c), streams(c) {}
 };
 struct ml_join_build_local {
     ml_join_build* sink;
     cudaStream_t s;
     Staging st;
     std::unique_ptr<ErrWord> ew;
-    ml_join_build_local(ml_join_build* k) : sink(k), s(k->ctx->new_stream()), st(k->ctx), ew(new ErrWord(k->ctx)) {}
-    ~ml_join_build_local() { sink->ctx->free_stream(s); }
+    ml_join_build_local(ml_join_build* k) : sink(k), s(k->ctx->new_stream()), st(k->ctx), ew(new ErrWord(k->ctx)) {
+        sink->streams.add(s);
+    }
+    ~ml_join_build_local() {
+        sink->streams.remove(s);
+        sink->ctx->free_stream(s);
+    }
 };
 
 extern "C" {
@@ -917,8 +965,8 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
         *table = j->table.get();
         return ML_OK;
     }
-    ctx->sync_all();
-    cudaStream_t s = ctx->stream;
+    j->streams.sync();
+    cudaStream_t s = j->streams.own();
     auto jt = std::make_unique<ml_join_table>();
     jt->ctx = ctx;
     jt->res = std::make_unique<Reservation>(ctx, "HashJoinBuild(table)");
@@ -1073,7 +1121,7 @@ int ml_gpu_join_build_destroy(ml_join_build* j) {
     API_BEGIN
     if (j) {
         j->ctx->set_current();
-        j->ctx->sync_all();
+        j->streams.sync();
         delete j;
     }
     API_END
@@ -1166,7 +1214,24 @@ struct ml_hashagg {
     int64_t resizes = 0;
     int64_t final_groups = -1;  // set by finalize
     int smem_groups = 256;
-    ml_hashagg(Ctx* c) : ctx(c), pipe(c) {}
+    // ml_gpu_hashagg_run_resident: persistent launch state and the captured launch graphs
+    struct Resident {
+        DevBuf tables, ovf, count;  // per-batch dictionary tables, overflow rows, overflow count
+        std::unique_ptr<ErrWord> ew;
+        uint64_t* host_count = nullptr;  // pinned
+        cudaStream_t s = nullptr;
+        std::vector<std::pair<std::string, cudaGraphExec_t>> graphs;  // launch parameters -> graph
+        uint64_t hits = 0, builds = 0;
+    } run;
+    SinkStreams streams;
+    ml_hashagg(Ctx* c) : ctx(c), pipe(c), streams(c) {}
+    void resume_overflow(Pipeline::Launch& L, uint64_t count, DevBuf& ovf, int w, cudaStream_t s,
+                         unsigned long long* d_count, uint64_t* h_count, ErrWord& ew);
+    ~ml_hashagg() {
+        for (auto& g : run.graphs) cudaGraphExecDestroy(g.second);
+        if (run.host_count) ctx->release_slot(run.host_count);
+        if (run.s) ctx->free_stream(run.s);
+    }
 
     TableView table() const {
         return TableView{slots.get<uint64_t>(), cap ? cap - 1 : 0, keys.nwords, keys.nwords == 1 ? 2 : 4};
@@ -1299,34 +1364,50 @@ struct ml_hashagg {
     }
 };
 
-struct ml_hashagg_local {
-    ml_hashagg* sink;
-    cudaStream_t s;
-    Staging st;
-    ErrWord ew;
-    DevBuf ovf_count;  // u64
-    uint64_t* h_count;
-    ml_hashagg_local(ml_hashagg* k)
-        : sink(k), s(k->ctx->new_stream()), st(k->ctx), ew(k->ctx), ovf_count(k->ctx, 16, nullptr) {
-        h_count = (uint64_t*)k->ctx->pinned_slot();
+// resize-on-overflow (swiss.rs:219-232 grows by doubling; here the table grows to hold
+// the groups so far plus the rows that did not fit), then aggregate those rows again
+void ml_hashagg::resume_overflow(Pipeline::Launch& L, uint64_t count, DevBuf& ovf, int w, cudaStream_t s,
+                                 unsigned long long* d_count, uint64_t* h_count, ErrWord& ew) {
+    while (count) {
+        std::unique_lock<std::shared_mutex> lk(rw);
+        streams.sync();
+        if (run.s) CK(cudaStreamSynchronize(run.s));
+        CK(cudaMemcpyAsync(ew.h, ngroups.get(), 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        uint32_t ng = std::min(*ew.h, gid_cap);
+        uint64_t want = std::max<uint64_t>((uint64_t)gid_cap * 2, (uint64_t)ng + std::min<uint64_t>(count, 1ull << 30));
+        grow(std::min<uint64_t>(want, 0x7FFFFFFFull), s, ew);
+        resizes++;
+        DevBuf ovf2(ctx, count * w * 4, nullptr);
+        CK(cudaMemsetAsync(d_count, 0, 8, s));
+        CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
+        L.P.err = ew.d.get<uint32_t>();
+        AggArgs A = args(d_count, ovf2.get<uint32_t>(), count);
+        void* jit = jit_agg_resume_kernel(ctx, pipe, L.P, A);
+        if (jit) {
+            const uint32_t* rows = ovf.get<uint32_t>();
+            uint64_t cnt = count;
+            int ww = w;
+            void* args[] = {&L.P, &A, &rows, &cnt, &ww};
+            jit_launch(jit, pipeline_grid((int64_t)count), kPipelineThreads, agg_smem_bytes(A), s, args);
+            ctx->add_profile("jit_launch", 0);
+        } else {
+            launch_agg_resume(L.P, A, ovf.get<uint32_t>(), count, w, agg_smem_bytes(A), s);
+        }
+        ctx->count_launch();
+        CK(cudaMemcpyAsync(h_count, d_count, 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(ew.h, ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        check_device_error(ctx, *ew.h);
+        count = *h_count;
+        ovf = std::move(ovf2);
     }
-    ~ml_hashagg_local() {
-        sink->ctx->release_slot(h_count);
-        sink->ctx->free_stream(s);
-    }
-};
+}
 
-extern "C" {
-
-int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue, const int32_t* input_types, int32_t ninput,
-                          const ml_expr* group_exprs, int32_t ngroup, const ml_agg_spec* aggs, int32_t nagg, int64_t size_hint,
-                          ml_hashagg** out) {
-    API_BEGIN
-    REQUIRE(ctx && out, "null argument");
-    REQUIRE(ngroup >= 0 && nagg >= 0 && (ngroup == 0 || group_exprs) && (nagg == 0 || aggs), "bad arguments");
-    REQUIRE(nagg <= kMaxAggs, "too many aggregates");
-    ctx->set_current();
-    auto h = std::make_unique<ml_hashagg>(ctx);
+// The host side of HashAggregateSink::new: compile the prologue, the GROUP BY keys and the
+// aggregate arguments into the sink's pipeline, and lay out the group blocks.
+void compile_hashagg(ml_hashagg* h, const ml_pipe_op* prologue, int32_t nprologue, const int32_t* input_types,
+                     int32_t ninput, const ml_expr* group_exprs, int32_t ngroup, const ml_agg_spec* aggs, int32_t nagg) {
     h->pipe.build(prologue, nprologue, input_types, ninput);
     h->ungrouped = ngroup == 0;
     if (!h->ungrouped) {
@@ -1390,6 +1471,39 @@ int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprol
         h->aggs.push_back(std::move(a));
     }
     h->stride = words;
+}
+
+struct ml_hashagg_local {
+    ml_hashagg* sink;
+    cudaStream_t s;
+    Staging st;
+    ErrWord ew;
+    DevBuf ovf_count;  // u64
+    uint64_t* h_count;
+    ml_hashagg_local(ml_hashagg* k)
+        : sink(k), s(k->ctx->new_stream()), st(k->ctx), ew(k->ctx), ovf_count(k->ctx, 16, nullptr) {
+        h_count = (uint64_t*)k->ctx->pinned_slot();
+        sink->streams.add(s);
+    }
+    ~ml_hashagg_local() {
+        sink->streams.remove(s);
+        sink->ctx->release_slot(h_count);
+        sink->ctx->free_stream(s);
+    }
+};
+
+extern "C" {
+
+int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue, const int32_t* input_types, int32_t ninput,
+                          const ml_expr* group_exprs, int32_t ngroup, const ml_agg_spec* aggs, int32_t nagg, int64_t size_hint,
+                          ml_hashagg** out) {
+    API_BEGIN
+    REQUIRE(ctx && out, "null argument");
+    REQUIRE(ngroup >= 0 && nagg >= 0 && (ngroup == 0 || group_exprs) && (nagg == 0 || aggs), "bad arguments");
+    REQUIRE(nagg <= kMaxAggs, "too many aggregates");
+    ctx->set_current();
+    auto h = std::make_unique<ml_hashagg>(ctx);
+    compile_hashagg(h.get(), prologue, nprologue, input_types, ninput, group_exprs, ngroup, aggs, nagg);
     h->pipe.upload();
     h->res = std::make_unique<Reservation>(ctx, "HashAggregate");
     h->ngroups = DevBuf(ctx, 16, nullptr);
@@ -1434,7 +1548,7 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
         if (a.arg.maybe_null || h->pipe.reads_nullable(a.arg, L)) {
             std::unique_lock<std::shared_mutex> lk(h->rw);
             if (!a.vcnt_on) {
-                ctx->sync_all();
+                h->streams.sync();
                 a.vcnt = DevBuf(ctx, (size_t)h->gid_cap * 8, h->res.get());
                 // every contribution so far was valid: start from the groups' row counts
                 CK(cudaMemcpy2DAsync(a.vcnt.get(), 8, h->acc.get(), (size_t)h->stride * 8, 8, h->gid_cap,
@@ -1477,39 +1591,175 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
         count = *local->h_count;
     }
     // resize-on-overflow: grow the table, then aggregate the rows that did not fit
-    while (count) {
-        std::unique_lock<std::shared_mutex> lk(h->rw);
-        ctx->sync_all();
-        CK(cudaMemcpyAsync(local->ew.h, h->ngroups.get(), 4, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        uint32_t ng = std::min(*local->ew.h, h->gid_cap);
-        uint64_t want = std::max<uint64_t>((uint64_t)h->gid_cap * 2, (uint64_t)ng + std::min<uint64_t>(count, 1ull << 30));
-        h->grow(std::min<uint64_t>(want, 0x7FFFFFFFull), s, local->ew);
-        h->resizes++;
-        DevBuf ovf2(ctx, count * w * 4, nullptr);
-        CK(cudaMemsetAsync(local->ovf_count.get(), 0, 8, s));
-        CK(cudaMemsetAsync(local->ew.d.get(), 0, 4, s));
-        L.P.err = local->ew.d.get<uint32_t>();
-        AggArgs A = h->args(local->ovf_count.get<unsigned long long>(), ovf2.get<uint32_t>(), count);
-        void* jit = jit_agg_resume_kernel(ctx, h->pipe, L.P, A);
-        if (jit) {
-            const uint32_t* rows = ovf.get<uint32_t>();
-            uint64_t cnt = count;
-            int ww = w;
-            void* args[] = {&L.P, &A, &rows, &cnt, &ww};
-            jit_launch(jit, pipeline_grid((int64_t)count), kPipelineThreads, agg_smem_bytes(A), s, args);
-            ctx->add_profile("jit_launch", 0);
-        } else {
-            launch_agg_resume(L.P, A, ovf.get<uint32_t>(), count, w, agg_smem_bytes(A), s);
-        }
-        ctx->count_launch();
-        CK(cudaMemcpyAsync(local->h_count, local->ovf_count.get(), 8, cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(local->ew.h, local->ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        check_device_error(ctx, *local->ew.h);
-        count = *local->h_count;
-        ovf = std::move(ovf2);
+    h->resume_overflow(L, count, ovf, w, s, local->ovf_count.get<unsigned long long>(), local->h_count, local->ew);
+    API_END
+}
+
+int ml_gpu_hashagg_rebind(ml_hashagg* h, const ml_pipe_op* prologue, int32_t nprologue, const int32_t* input_types,
+                          int32_t ninput, const ml_expr* group_exprs, int32_t ngroup, const ml_agg_spec* aggs,
+                          int32_t nagg) {
+    API_BEGIN
+    REQUIRE(h, "null sink");
+    REQUIRE(nagg <= kMaxAggs && nagg == (int32_t)h->aggs.size(), "rebind: the aggregates differ from the sink's");
+    Ctx* ctx = h->ctx;
+    ctx->set_current();
+    ml_hashagg fresh(ctx);
+    compile_hashagg(&fresh, prologue, nprologue, input_types, ninput, group_exprs, ngroup, aggs, nagg);
+    const Compiler &a = h->pipe.C, &b = fresh.pipe.C;
+    bool same = a.code.size() == b.code.size() && a.arena.size() == b.arena.size() && a.slots.size() == b.slots.size() &&
+                a.luts.size() == b.luts.size() && fresh.stride == h->stride && fresh.group_probe == h->group_probe &&
+                fresh.ungrouped == h->ungrouped && fresh.pipe.nstages == h->pipe.nstages &&
+                fresh.pipe.probes.size() == h->pipe.probes.size() && memcmp(&fresh.keys, &h->keys, sizeof(KeyLayout)) == 0;
+    for (size_t i = 0; same && i < a.code.size(); i++) {
+        const Instr &x = a.code[i], &y = b.code[i];
+        same = x.op == y.op && x.sub == y.sub && x.t == y.t && x.flag == y.flag && x.a == y.a && x.b == y.b && x.c == y.c &&
+               x.lit_valid == y.lit_valid;
     }
+    for (size_t i = 0; same && i < a.slots.size(); i++)
+        same = a.slots[i].src == b.slots[i].src && a.slots[i].index == b.slots[i].index && a.slots[i].dtype == b.slots[i].dtype;
+    for (size_t i = 0; same && i < a.luts.size(); i++)
+        same = a.luts[i].slot == b.luts[i].slot && a.luts[i].what == b.luts[i].what && a.luts[i].op == b.luts[i].op;
+    if (!same) raise(ML_ERR_INVALID, "rebind: the pipeline's shape differs from the sink's (only constants may change)");
+    std::unique_lock<std::shared_mutex> lk(h->rw);
+    h->streams.sync();
+    if (h->run.s) CK(cudaStreamSynchronize(h->run.s));
+    h->pipe.C.code = b.code;
+    h->pipe.C.arena = b.arena;
+    h->pipe.C.luts = b.luts;
+    for (size_t p = 0; p < h->pipe.probes.size(); p++) h->pipe.probes[p].jt = fresh.pipe.probes[p].jt;
+    for (size_t k = 0; k < h->aggs.size(); k++) h->aggs[k].arg = fresh.aggs[k].arg;
+    cudaStream_t s = h->streams.own();
+    if (!b.code.empty())
+        CK(cudaMemcpyAsync(h->pipe.d_prog.get(), b.code.data(), b.code.size() * sizeof(Instr), cudaMemcpyHostToDevice, s));
+    if (!b.arena.empty()) CK(cudaMemcpyAsync(h->pipe.d_arena.get(), b.arena.data(), b.arena.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    API_END
+}
+
+int ml_gpu_hashagg_reset(ml_hashagg* h) {
+    API_BEGIN
+    REQUIRE(h, "null sink");
+    Ctx* ctx = h->ctx;
+    ctx->set_current();
+    std::unique_lock<std::shared_mutex> lk(h->rw);
+    h->streams.sync();
+    if (h->run.s) CK(cudaStreamSynchronize(h->run.s));
+    cudaStream_t s = h->streams.own();
+    CK(cudaMemsetAsync(h->ngroups.get(), 0, 16, s));
+    if (h->cap) CK(cudaMemsetAsync(h->slots.get(), 0, h->cap * 8 * (h->keys.nwords == 1 ? 2 : 4), s));
+    launch_acc_init(h->args(nullptr, nullptr, 0), 0, h->gid_cap, s);
+    ctx->count_launch();
+    CK(cudaStreamSynchronize(s));
+    h->final_groups = -1;
+    API_END
+}
+
+// One device-resident batch through the sink, launched as a CUDA graph: the graph (reset of
+// the group state when asked, overflow counter and error word, the fused pipeline kernel,
+// read-back of both words) is captured once per set of launch parameters and replayed.
+int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t ncols, int64_t nrows, int32_t reset) {
+    API_BEGIN
+    REQUIRE(h && (cols || ncols == 0) && nrows >= 0, "bad arguments");
+    for (int c = 0; c < ncols; c++)
+        REQUIRE(cols[c].location == ML_LOC_DEVICE, "ml_gpu_hashagg_run_resident reads device-resident columns only");
+    Ctx* ctx = h->ctx;
+    ctx->set_current();
+    std::unique_lock<std::shared_mutex> lk(h->rw);  // one resident run at a time per sink
+    ml_hashagg::Resident& R = h->run;
+    if (!R.s) {
+        R.s = ctx->new_stream();
+        R.ew = std::make_unique<ErrWord>(ctx);
+        R.host_count = (uint64_t*)ctx->pinned_slot();
+        R.count = DevBuf(ctx, 16, nullptr);
+        R.tables = DevBuf(ctx, 64 << 10, nullptr);
+    }
+    cudaStream_t s = R.s;
+    Staging st(ctx);
+    Pipeline::Launch L;
+    h->pipe.prepare(L, cols, ncols, nrows, nullptr, 0, s, st, nullptr, R.tables.get<uint8_t>(), R.tables.bytes());
+    for (const KeyDecode& d : h->dec)
+        if (d.str_kind == 1 && L.P.cols[d.slot].kind != CK_DICT)
+            raise(ML_ERR_UNSUPPORTED, "GROUP BY on a plain (not dictionary-encoded) string column of the source");
+    for (auto& a : h->aggs)
+        if (a.has_arg && !a.vcnt_on && a.kind != A_COUNT && (a.arg.maybe_null || h->pipe.reads_nullable(a.arg, L)))
+            raise(ML_ERR_UNSUPPORTED, "ml_gpu_hashagg_run_resident: an aggregate input can be NULL; use a local sink");
+    const int w = 1 + (int)h->pipe.probes.size();
+    const bool can_overflow = !h->ungrouped && h->group_probe < 0;
+    const uint64_t ovf_cap = can_overflow ? std::max<uint64_t>((uint64_t)L.P.n, 1024) : 0;
+    if (R.ovf.bytes() < std::max<uint64_t>(ovf_cap * w * 4, 16)) R.ovf = DevBuf(ctx, std::max<uint64_t>(ovf_cap * w * 4, 16), nullptr);
+    L.P.err = R.ew->d.get<uint32_t>();
+    L.P.head_probe = h->group_probe;
+    AggArgs A = h->args(R.count.get<unsigned long long>(), R.ovf.get<uint32_t>(), ovf_cap);
+    void* jit = jit_agg_kernel(ctx, h->pipe, L.P, A);
+    const int64_t k = jit ? jit_rows_per_thread(L.P) : 1;
+    const int grid = pipeline_grid((L.P.n + k - 1) / k);
+    const int smem = agg_smem_bytes(A);
+    // the graph is keyed by everything its nodes capture
+    std::string key((const char*)&L.P, sizeof(PipeArgs));
+    key.append((const char*)&A, sizeof(AggArgs));
+    key.append((const char*)&jit, sizeof(jit));
+    key.append(1, (char)(reset != 0));
+    cudaGraphExec_t exec = nullptr;
+    for (auto& g : R.graphs)
+        if (g.first == key) exec = g.second;
+    if (exec) {
+        R.hits++;
+    } else {
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        if (reset) {
+            CK(cudaMemsetAsync(h->ngroups.get(), 0, 16, s));
+            if (h->cap) CK(cudaMemsetAsync(h->slots.get(), 0, h->cap * 8 * (h->keys.nwords == 1 ? 2 : 4), s));
+            launch_acc_init(A, 0, h->gid_cap, s);
+        }
+        CK(cudaMemsetAsync(R.count.get(), 0, 8, s));
+        CK(cudaMemsetAsync(R.ew->d.get(), 0, 4, s));
+        if (L.P.n) {
+            if (jit) {
+                void* args[] = {&L.P, &A};
+                jit_launch(jit, grid, kPipelineThreads, smem, s, args);
+            } else {
+                launch_agg(L.P, A, smem, s);
+            }
+        }
+        CK(cudaMemcpyAsync(R.host_count, R.count.get(), 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(R.ew->h, R.ew->d.get(), 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamEndCapture(s, &graph));
+        cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(e);
+        if (R.graphs.size() >= 32) {  // keep the most recent shapes
+            cudaGraphExecDestroy(R.graphs.front().second);
+            R.graphs.erase(R.graphs.begin());
+        }
+        R.graphs.emplace_back(key, exec);
+        R.builds++;
+    }
+    {
+        KernelTimer kt(ctx, s, "pipeline_aggregate");
+        CK(cudaGraphLaunch(exec, s));
+        kt.stop();
+    }
+    ctx->count_launch(reset ? 2 : 1);
+    if (jit) ctx->add_profile("jit_launch", 0);
+    CK(cudaStreamSynchronize(s));
+    check_device_error(ctx, *R.ew->h);
+    if (reset) h->final_groups = -1;
+    uint64_t count = *R.host_count;
+    lk.unlock();
+    if (count) {
+        DevBuf ovf(ctx, count * w * 4, nullptr);
+        CK(cudaMemcpyAsync(ovf.get(), R.ovf.get(), count * w * 4, cudaMemcpyDeviceToDevice, s));
+        h->resume_overflow(L, count, ovf, w, s, R.count.get<unsigned long long>(), R.host_count, *R.ew);
+    }
+    API_END
+}
+
+int ml_gpu_hashagg_graph_stats(ml_hashagg* h, uint64_t* built, uint64_t* replayed) {
+    API_BEGIN
+    REQUIRE(h, "null sink");
+    if (built) *built = h->run.builds;
+    if (replayed) *replayed = h->run.hits;
     API_END
 }
 
@@ -1530,8 +1780,9 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
     Ctx* ctx = h->ctx;
     ctx->set_current();
     std::unique_lock<std::shared_mutex> lk(h->rw);
-    ctx->sync_all();
-    cudaStream_t s = ctx->stream;
+    h->streams.sync();
+    if (h->run.s) CK(cudaStreamSynchronize(h->run.s));
+    cudaStream_t s = h->streams.own();
     uint32_t ng = 1;
     DevBuf gids;  // output row -> group id (GROUP BY the join key: the non-empty build rows)
     if (h->group_probe >= 0) {
@@ -1678,7 +1929,8 @@ int ml_gpu_hashagg_destroy(ml_hashagg* h) {
     API_BEGIN
     if (h) {
         h->ctx->set_current();
-        h->ctx->sync_all();
+        h->streams.sync();
+        if (h->run.s) CK(cudaStreamSynchronize(h->run.s));
         delete h;
     }
     API_END
@@ -1699,15 +1951,21 @@ struct ml_topn {
     int64_t limit;
     std::mutex mu;
     std::vector<std::unique_ptr<ml_batch>> cands;
-    ml_topn(Ctx* c) : ctx(c), pipe(c) {}
+    SinkStreams streams;
+    ml_topn(Ctx* c) : ctx(c), pipe(c), streams(c) {}
 };
 struct ml_topn_local {
     ml_topn* sink;
     cudaStream_t s;
     Staging st;
     std::unique_ptr<ErrWord> ew;
-    ml_topn_local(ml_topn* k) : sink(k), s(k->ctx->new_stream()), st(k->ctx), ew(new ErrWord(k->ctx)) {}
-    ~ml_topn_local() { sink->ctx->free_stream(s); }
+    ml_topn_local(ml_topn* k) : sink(k), s(k->ctx->new_stream()), st(k->ctx), ew(new ErrWord(k->ctx)) {
+        sink->streams.add(s);
+    }
+    ~ml_topn_local() {
+        sink->streams.remove(s);
+        sink->ctx->free_stream(s);
+    }
 };
 
 extern "C" {
@@ -1774,13 +2032,13 @@ int ml_gpu_topn_finalize(ml_topn* t, ml_batch** out) {
     REQUIRE(t && out, "null argument");
     Ctx* ctx = t->ctx;
     ctx->set_current();
-    ctx->sync_all();
+    t->streams.sync();
     std::vector<std::unique_ptr<ml_batch>> cands;
     {
         std::lock_guard<std::mutex> g(t->mu);
         cands = std::move(t->cands);
     }
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = t->streams.own();
     std::unique_ptr<ml_batch> all;
     if (cands.empty()) {
         all = std::make_unique<ml_batch>();
@@ -1811,7 +2069,7 @@ int ml_gpu_topn_destroy(ml_topn* t) {
     API_BEGIN
     if (t) {
         t->ctx->set_current();
-        t->ctx->sync_all();
+        t->streams.sync();
         delete t;
     }
     API_END
