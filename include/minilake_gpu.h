@@ -279,6 +279,27 @@ int ml_gpu_hashagg_finalize(ml_hashagg* sink, ml_batch** out);
 int ml_gpu_hashagg_stats(ml_hashagg* sink, int64_t* groups, int64_t* capacity, int64_t* resizes);
 int ml_gpu_hashagg_destroy(ml_hashagg* sink);
 
+/* ---- resident hash aggregates for a serving loop (no counterpart in the reference) ---- */
+/* Re-point a sink at new constants: the arguments are those of ml_gpu_hashagg_create (minus
+ * the size hint) and must compile to the same pipeline shape, differing only in literal
+ * values, LIKE patterns of the same length, and the join tables probed.  ML_ERR_INVALID
+ * otherwise.  The sink's device state is kept. */
+int ml_gpu_hashagg_rebind(ml_hashagg* sink, const ml_pipe_op* prologue, int32_t nprologue,
+                          const int32_t* input_types, int32_t ninput, const ml_expr* group_exprs,
+                          int32_t ngroup, const ml_agg_spec* aggs, int32_t nagg);
+/* Empty the sink's groups and accumulators, keeping its tables allocated (size included). */
+int ml_gpu_hashagg_reset(ml_hashagg* sink);
+/* Sink one batch of device-resident columns from the calling thread (one call at a time per
+ * sink), as a CUDA graph: with `reset` the graph first empties the group state, then runs the
+ * fused pipeline kernel and reads back its overflow count and error word.  The graph is
+ * captured on the first call with a given set of launch parameters (columns, the constants'
+ * buffers, table size) and replayed by later calls; a table that overflows grows and the
+ * rows that did not fit are aggregated again outside the graph.  Finalize as usual. */
+int ml_gpu_hashagg_run_resident(ml_hashagg* sink, const ml_column* cols, int32_t ncols, int64_t nrows,
+                                int32_t reset);
+/* Graphs captured and graph launches replayed by ml_gpu_hashagg_run_resident. */
+int ml_gpu_hashagg_graph_stats(ml_hashagg* sink, uint64_t* built, uint64_t* replayed);
+
 /* ---- Sink: JoinBuildSink (operators/join.rs:72-242) --------------------------- */
 /* `build_input_types`: columns of the batches pushed into the build side (after the
  * prologue, these become the build batch whose columns HashJoinProbe gathers). */

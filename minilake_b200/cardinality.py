@@ -153,6 +153,22 @@ def q_error(pred, true):
     return np.maximum(pred / true, true / pred)
 
 
+def train_model(ctx, instances: int = 200, seed: int = 45, min_rows: int = 1_000_000, max_rows: int = 20_000_000,
+                epochs: int = 200):
+    """A cardinality model trained on a fresh sweep of `instances` (all used for training)."""
+    from .gpu import CardinalityModel, card_features
+    feats = np.zeros((instances, 72), dtype=np.float32)
+    truth = np.zeros(instances)
+    for i, inst in enumerate(make_instances(instances, seed, min_rows, max_rows)):
+        di = DeviceInstance(inst)
+        feats[i], est = card_features(ctx, di.ml, di.keys)
+        truth[i] = aggregate(ctx, di, int(est * 1.5) + 16, fetch=False)[1]
+        del di
+    model = CardinalityModel(ctx, seed=seed)
+    model.train(feats, np.log2(truth).astype(np.float32), epochs=epochs, batch=64, lr=1e-3, seed=seed)
+    return model
+
+
 def run(instances: int = 2000, train: int = 1500, seed: int = 45, min_rows: int = 1_000_000,
         max_rows: int = 100_000_000, epochs: int = 400, log=print):
     from .gpu import CardinalityModel, Context, card_features

@@ -99,23 +99,44 @@ const char kStdint[] =
     "typedef unsigned long uint64_t;\n";
 const char kStddef[] = "#pragma once\ntypedef unsigned long size_t;\n";
 
+// One entry per (device, source): the first thread to ask compiles it while later askers for
+// the same source wait on the entry; other sources are looked up and compiled meanwhile.
+struct CacheEntry {
+    std::mutex mu;
+    bool done = false;
+    CUfunction fn = nullptr;
+};
 struct Cache {
     std::mutex mu;
-    std::map<std::pair<int, std::string>, CUfunction> fns;
+    std::map<std::pair<int, std::string>, std::shared_ptr<CacheEntry>> fns;
 };
 Cache& cache() {
     static Cache c;
     return c;
 }
 
+CUfunction compile_kernel(Ctx* ctx, const std::string& src, const char* name);
+
 // Compile `src` (defining extern "C" kernel `name`) for this device, or return the cached kernel.
 CUfunction get_kernel(Ctx* ctx, const std::string& src, const char* name) {
-    Nvrtc& N = nvrtc();
     Cache& C = cache();
-    std::lock_guard<std::mutex> g(C.mu);
-    auto key = std::make_pair(ctx->device, src);
-    auto it = C.fns.find(key);
-    if (it != C.fns.end()) return it->second;
+    std::shared_ptr<CacheEntry> e;
+    {
+        std::lock_guard<std::mutex> g(C.mu);
+        auto& slot = C.fns[std::make_pair(ctx->device, src)];
+        if (!slot) slot = std::make_shared<CacheEntry>();
+        e = slot;
+    }
+    std::lock_guard<std::mutex> g(e->mu);
+    if (!e->done) {
+        e->fn = compile_kernel(ctx, src, name);  // throws on failure: the next asker tries again
+        e->done = true;
+    }
+    return e->fn;
+}
+
+CUfunction compile_kernel(Ctx* ctx, const std::string& src, const char* name) {
+    Nvrtc& N = nvrtc();
     auto t0 = std::chrono::steady_clock::now();
     std::vector<const char*> texts, names;
     for (int i = 0; i < kJitHeaderCount; i++) {
@@ -151,7 +172,6 @@ CUfunction get_kernel(Ctx* ctx, const std::string& src, const char* name) {
     CUfunction fn;
     if (N.load(&mod, bin.data()) != CUDA_SUCCESS) raise(ML_ERR_CUDA, "cuModuleLoadData failed for a pipeline kernel");
     if (N.get_fn(&fn, mod, name) != CUDA_SUCCESS) raise(ML_ERR_CUDA, "cuModuleGetFunction failed");
-    C.fns.emplace(key, fn);
     double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     ctx->add_profile("jit_compile", ms);
     return fn;

@@ -57,6 +57,11 @@ def _load():
         "ml_gpu_ctx_synchronize": ([VP], C.c_int),
         "ml_gpu_kernel_launches": ([VP, P(U64)], C.c_int),
         "ml_gpu_profile_read": ([VP, C.c_char_p, P(U64), P(C.c_double), I32], C.c_int),
+        "ml_gpu_hashagg_rebind": ([VP, P(abi.MlPipeOp), I32, VP, I32, P(abi.MlExpr), I32, P(abi.MlAggSpec), I32],
+                                  C.c_int),
+        "ml_gpu_hashagg_reset": ([VP], C.c_int),
+        "ml_gpu_hashagg_run_resident": ([VP, P(abi.MlColumn), I32, I64, I32], C.c_int),
+        "ml_gpu_hashagg_graph_stats": ([VP, P(U64), P(U64)], C.c_int),
         "ml_gpu_card_features": ([VP, P(abi.MlColumn), I32, I64, VP, I64, I32, P(abi.MlExpr), I32, VP,
                                   P(C.c_double)], C.c_int),
         "ml_gpu_card_model_create": ([VP, U64, P(VP)], C.c_int),
@@ -360,6 +365,7 @@ class HashAggregateSink:
         g, ng = abi.encode_exprs(group_exprs, keep)
         a, na = abi.encode_aggs(aggs, keep)
         types = np.asarray(input_types, dtype=np.int32)
+        self.input_types = types
         h = C.c_void_p()
         _check(LIB.ml_gpu_hashagg_create(ctx.h, ops, nops, _ptr(types), len(types), g, ng, a, na, size_hint,
                                           C.byref(h)))
@@ -368,6 +374,29 @@ class HashAggregateSink:
 
     def create_local(self):
         return _local(self, LIB.ml_gpu_hashagg_local_create, LIB.ml_gpu_hashagg_sink, LIB.ml_gpu_hashagg_combine)
+
+    # ---- resident use (serving): one query after another through the same device state ----
+    def rebind(self, prologue: Sequence[abi.PipeOp], group_exprs: Sequence[tuple], aggs: Sequence[abi.AggSpec]):
+        """New constants (same pipeline shape) for the next query."""
+        keep = abi.Keep()
+        ops, nops = abi.encode_ops(prologue, keep)
+        g, ng = abi.encode_exprs(group_exprs, keep)
+        a, na = abi.encode_aggs(aggs, keep)
+        _check(LIB.ml_gpu_hashagg_rebind(self.h, ops, nops, _ptr(self.input_types), len(self.input_types), g, ng,
+                                         a, na))
+
+    def reset(self):
+        _check(LIB.ml_gpu_hashagg_reset(self.h))
+
+    def run_resident(self, cols, reset: bool = True):
+        """Sink a device-resident batch (DeviceBatch or MlColumn tuple) as a replayed CUDA graph."""
+        arr, nc, n, _hold = _cols_arg(cols)
+        _check(LIB.ml_gpu_hashagg_run_resident(self.h, arr, nc, n, int(reset)))
+
+    def graph_stats(self):
+        b, r = C.c_uint64(), C.c_uint64()
+        _check(LIB.ml_gpu_hashagg_graph_stats(self.h, C.byref(b), C.byref(r)))
+        return {"built": b.value, "replayed": r.value}
 
     def finalize(self) -> DeviceBatch:
         h = C.c_void_p()
