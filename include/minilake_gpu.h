@@ -387,7 +387,9 @@ int ml_gpu_kernel_launches(ml_ctx* ctx, uint64_t* count);
 /* With ML_CTX_PROFILE: launches and summed device time (ms, CUDA events) of one kernel
  * family: "pipeline_aggregate" (fused filter/probe/aggregate), "join_insert", "topn",
  * "select" (filter compaction).  Always recorded: "jit_compile" (runtime compilations and
- * their host time) and "jit_launch" (launches of runtime-specialized kernels; time 0).
+ * their host time), "jit_launch" (launches of runtime-specialized kernels; time 0),
+ * "device_alloc" / "pinned_alloc" (cudaMalloc / cudaHostAlloc calls the context made and
+ * their host time) and "graph_capture" (CUDA graphs captured and instantiated).
  * `reset` clears the counters after reading. */
 int ml_gpu_profile_read(ml_ctx* ctx, const char* kernel, uint64_t* launches, double* total_ms, int32_t reset);
 

@@ -1,5 +1,6 @@
 // C ABI of the MiniLake B200 execution core (include/minilake_gpu.h).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <shared_mutex>
@@ -1705,6 +1706,7 @@ int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t nc
     if (exec) {
         R.hits++;
     } else {
+        const auto t_cap = std::chrono::steady_clock::now();
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         if (reset) {
@@ -1734,6 +1736,8 @@ int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t nc
         }
         R.graphs.emplace_back(key, exec);
         R.builds++;
+        ctx->add_profile("graph_capture",
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_cap).count());
     }
     {
         KernelTimer kt(ctx, s, "pipeline_aggregate");

@@ -3,6 +3,7 @@
 #include "ml_runtime.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 
@@ -149,7 +150,9 @@ void* Ctx::dalloc(size_t bytes, size_t* cap) {
         }
     }
     void* p = nullptr;
+    auto t0 = std::chrono::steady_clock::now();
     cudaError_t e = cudaMalloc(&p, c);
+    add_profile("device_alloc", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
     if (e != cudaSuccess) {
         cudaGetLastError();
         std::lock_guard<std::mutex> g(mu_);  // release the cache and retry once
@@ -172,7 +175,9 @@ void Ctx::dfree(void* p, size_t cap) {
 }
 void* Ctx::halloc(size_t bytes) {
     void* p = nullptr;
+    auto t0 = std::chrono::steady_clock::now();
     CK(cudaHostAlloc(&p, bytes, cudaHostAllocDefault));
+    add_profile("pinned_alloc", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
     return p;
 }
 void Ctx::hfree(void* p) { cudaFreeHost(p); }

@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import gc
 import json
 import math
 import queue
@@ -257,16 +258,27 @@ class Server:
         from .gpu import ResourcesExhausted
         pending: "queue.Queue[Optional[Query]]" = queue.Queue()
         sinks_per_slot = [dict() for _ in range(self.slots)]
-        if warmup:  # compile and capture every slot's kernels on the first query of each shape
-            for k in range(self.slots):
-                for s in range(3):
-                    for i in range(len(self.tables[s])):
-                        self.execute(Query(-1, 0.0, s, i, 1200 if s < 2 else "ab"), sinks_per_slot[k])
+        if warmup:
             # the star join's filtered dimension is indexed directly or hashed depending on the
             # prefix: compile both kernel variants (the kernel cache is shared by all slots)
             for p in range(26 * 26):
                 prefix = chr(97 + p // 26) + chr(97 + p % 26)
                 self.execute(Query(-1, 0.0, 2, 0, prefix), sinks_per_slot[0])
+
+            # every slot runs every shape and table, all slots at once: kernels compiled, graphs
+            # captured, and the device allocator's cache grown to what concurrent queries hold
+            def warm(k):
+                for rep in range(2):
+                    for s in range(3):
+                        for i in range(len(self.tables[s])):
+                            c = (600 + 1100 * rep) if s < 2 else ("ab", "qx")[rep]
+                            self.execute(Query(-1, 0.0, s, i, c), sinks_per_slot[k])
+
+            ws = [threading.Thread(target=warm, args=(k,)) for k in range(self.slots)]
+            for th in ws:
+                th.start()
+            for th in ws:
+                th.join()
         used, _, limit = self.ctx.pool_stats()
         room = self.admit_limit if self.admit_limit is not None else limit - used
         t0 = time.perf_counter() + 0.05
@@ -313,6 +325,12 @@ class Server:
                 q.done = time.perf_counter() - t0
                 release(need)
 
+        # no garbage-collector pauses while queries are timed: the objects made so far are frozen
+        # out of collection and collection waits until the stream is done
+        gc.collect()
+        gc.freeze()
+        gc_was_enabled = gc.isenabled()
+        gc.disable()
         threads = [threading.Thread(target=worker, args=(k,), daemon=True) for k in range(self.slots)]
         for th in threads:
             th.start()
@@ -325,6 +343,9 @@ class Server:
             pending.put(None)
         for th in threads:
             th.join()
+        if gc_was_enabled:
+            gc.enable()
+        gc.unfreeze()
         for d in sinks_per_slot:
             for s in d.values():
                 g = s.graph_stats()
