@@ -59,8 +59,8 @@ def make_data(rank: int, world: int, fact_rows: int = FACT_ROWS):
     key = (rng.permutation(DIM_ROWS) + 1).astype(np.int64)
     frng = np.random.Generator(np.random.PCG64(43 + 1000 * rank))
     # rank r's fact rows reference the keys k in 1..DIM_ROWS with k % world == r
-    first = rank if rank > 0 else world
-    count = (DIM_ROWS - first) // world + 1
+    from minilake_b200.exchange import shard_keys
+    first, count = shard_keys(rank, world, DIM_ROWS)
     fk = first + frng.integers(0, count, fact_rows, dtype=np.int64) * world
     d = frng.integers(0, 2557, fact_rows, dtype=np.int32)
     v = frng.uniform(900.0, 105000.0, fact_rows)
@@ -265,14 +265,10 @@ def gpu_arm(args):
 
     # ---- exchange: gather the per-rank top-10 candidates, merge on rank 0 -------------
     if world > 1:
-        cand = np.stack([top[0].values.astype(np.float64), top[1].values, top[2].values.astype(np.float64)], 1)
-        ct = torch.tensor(cand, device="cuda", dtype=torch.float64)
-        allc = [torch.zeros_like(ct) for _ in range(world)]
-        torch.distributed.all_gather(allc, ct)
+        from minilake_b200.exchange import exchange_topn
+        mk, ms, mc = exchange_topn(top[0].values, top[1].values, top[2].values, 10, device="cuda")
         if rank == 0:
-            merged = np.concatenate([c.cpu().numpy() for c in allc])
-            order = np.lexsort((merged[:, 0], -merged[:, 1]))[:10]
-            log("merged top-10 fk:", merged[order, 0].astype(np.int64).tolist())
+            log("merged top-10 fk:", mk.tolist())
 
     if rank == 0:
         rows_total = rows * world
