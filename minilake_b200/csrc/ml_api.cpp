@@ -221,8 +221,10 @@ class SinkStreams {
 };
 
 // The prologue's output for one batch, materialized as owned device columns.
+// With `borrow`, a pipeline that keeps every row and only passes source columns through returns
+// views of the launch's source columns (no copy); the caller must be done with them before L goes.
 std::unique_ptr<ml_batch> materialize(Ctx* ctx, Pipeline& pipe, const std::vector<Prog>& out_progs, Pipeline::Launch& L,
-                                      cudaStream_t st, Reservation* res, ErrWord& ew) {
+                                      cudaStream_t st, Reservation* res, ErrWord& ew, bool borrow = false) {
     DevBuf idx;
     const uint32_t* rows = L.P.sel;
     int64_t k = L.P.n;
@@ -235,6 +237,23 @@ std::unique_ptr<ml_batch> materialize(Ctx* ctx, Pipeline& pipe, const std::vecto
     auto b = std::make_unique<ml_batch>();
     b->ctx = ctx;
     b->nrows = k;
+    bool plain = borrow && rows == nullptr;  // every row, every output a source column: no copy
+    for (const ColRef& r : pipe.out) plain = plain && r.kind == 0;
+    if (plain) {
+        for (const ColRef& r : pipe.out) {
+            const DevColumn& src = *L.src[r.index];
+            auto d = std::make_unique<DevColumn>();
+            d->dtype = src.dtype;
+            d->kind = src.kind;
+            d->n = src.n;
+            d->dict = src.dict;
+            d->data_p = src.dptr();
+            d->off_p = src.optr();
+            d->valid_p = src.vptr();
+            b->cols.push_back(std::move(d));
+        }
+        return b;
+    }
     PipeArgs Q = L.P;
     Q.sel = rows;
     Q.n = k;
@@ -1204,7 +1223,8 @@ struct ml_hashagg {
     std::vector<KeyDecode> dec;
     std::vector<AggState> aggs;
     bool ungrouped = false;
-    int group_probe = -1;  // GROUP BY the join key of this probe: group id = matched build row
+    int group_probe = -1;
+    bool dense_groups = false;  // group id = the join key's dense-index position (ProbeDev::late)  // GROUP BY the join key of this probe: group id = matched build row
     std::vector<int> group_build_cols;
     double max_load = 0.5;
     int stride = 1;        // u64 words per group block
@@ -1472,6 +1492,16 @@ void compile_hashagg(ml_hashagg* h, const ml_pipe_op* prologue, int32_t nprologu
         h->aggs.push_back(std::move(a));
     }
     h->stride = words;
+    // GROUP BY a dense, distinct join key whose probe ends the pipeline, with nothing reading
+    // that probe's build row: group by the index position and check membership at finalize
+    if (h->group_probe >= 0) {
+        const int p = h->group_probe;
+        const ml_join_table* jt = h->pipe.probes[p].jt;
+        bool ok = jt->dense && !jt->has_dups && h->pipe.nstages > 0 && h->pipe.stages[h->pipe.nstages - 1].kind == 1 &&
+                  h->pipe.stages[h->pipe.nstages - 1].idx == p;
+        for (const SlotInfo& si : h->pipe.C.slots) ok = ok && si.src != p + 1;
+        h->dense_groups = ok;
+    }
 }
 
 struct ml_hashagg_local {
@@ -1512,6 +1542,7 @@ int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprol
     ErrWord ew(ctx);
     uint64_t want;
     if (h->ungrouped) want = 1;
+    else if (h->dense_groups) want = h->pipe.probes[h->group_probe].jt->drange;
     else if (h->group_probe >= 0) want = (uint64_t)std::max<int64_t>(h->pipe.probes[h->group_probe].jt->batch.nrows, 1);
     else want = (uint64_t)std::min<int64_t>(std::max<int64_t>(size_hint > 0 ? size_hint : 1024, 16), 0x7FFFFFFF);
     h->grow(want, ctx->stream, ew);
@@ -1570,6 +1601,7 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
         CK(cudaMemsetAsync(local->ew.d.get(), 0, 4, s));
         L.P.err = local->ew.d.get<uint32_t>();
         L.P.head_probe = h->group_probe;
+        if (h->dense_groups) L.P.probes[h->group_probe].late = 1;
         AggArgs A = h->args(local->ovf_count.get<unsigned long long>(), ovf.get<uint32_t>(), ovf_cap);
         void* jit = jit_agg_kernel(ctx, h->pipe, L.P, A);
         KernelTimer kt(ctx, s, "pipeline_aggregate");
@@ -1609,7 +1641,8 @@ int ml_gpu_hashagg_rebind(ml_hashagg* h, const ml_pipe_op* prologue, int32_t npr
     const Compiler &a = h->pipe.C, &b = fresh.pipe.C;
     bool same = a.code.size() == b.code.size() && a.arena.size() == b.arena.size() && a.slots.size() == b.slots.size() &&
                 a.luts.size() == b.luts.size() && fresh.stride == h->stride && fresh.group_probe == h->group_probe &&
-                fresh.ungrouped == h->ungrouped && fresh.pipe.nstages == h->pipe.nstages &&
+                fresh.ungrouped == h->ungrouped && fresh.dense_groups == h->dense_groups &&
+                fresh.pipe.nstages == h->pipe.nstages &&
                 fresh.pipe.probes.size() == h->pipe.probes.size() && memcmp(&fresh.keys, &h->keys, sizeof(KeyLayout)) == 0;
     for (size_t i = 0; same && i < a.code.size(); i++) {
         const Instr &x = a.code[i], &y = b.code[i];
@@ -1620,6 +1653,9 @@ int ml_gpu_hashagg_rebind(ml_hashagg* h, const ml_pipe_op* prologue, int32_t npr
         same = a.slots[i].src == b.slots[i].src && a.slots[i].index == b.slots[i].index && a.slots[i].dtype == b.slots[i].dtype;
     for (size_t i = 0; same && i < a.luts.size(); i++)
         same = a.luts[i].slot == b.luts[i].slot && a.luts[i].what == b.luts[i].what && a.luts[i].op == b.luts[i].op;
+    // the group state is sized for the grouping join table: it cannot change
+    if (same && h->group_probe >= 0)
+        same = fresh.pipe.probes[h->group_probe].jt == h->pipe.probes[h->group_probe].jt;
     if (!same) raise(ML_ERR_INVALID, "rebind: the pipeline's shape differs from the sink's (only constants may change)");
     std::unique_lock<std::shared_mutex> lk(h->rw);
     h->streams.sync();
@@ -1690,6 +1726,7 @@ int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t nc
     if (R.ovf.bytes() < std::max<uint64_t>(ovf_cap * w * 4, 16)) R.ovf = DevBuf(ctx, std::max<uint64_t>(ovf_cap * w * 4, 16), nullptr);
     L.P.err = R.ew->d.get<uint32_t>();
     L.P.head_probe = h->group_probe;
+        if (h->dense_groups) L.P.probes[h->group_probe].late = 1;
     AggArgs A = h->args(R.count.get<unsigned long long>(), R.ovf.get<uint32_t>(), ovf_cap);
     void* jit = jit_agg_kernel(ctx, h->pipe, L.P, A);
     const int64_t k = jit ? jit_rows_per_thread(L.P) : 1;
@@ -1794,7 +1831,8 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
         int nb = select_blocks(n);
         DevBuf bits(ctx, std::max<size_t>((size_t)(n + 31) / 32 * 4, 4), nullptr);
         DevBuf counts(ctx, std::max<size_t>((size_t)nb * 4, 4), nullptr);
-        launch_group_flags(h->acc.get<uint64_t>(), h->stride, n, bits.get<uint32_t>(), counts.get<uint32_t>(), s);
+        const uint32_t* member = h->dense_groups ? h->pipe.probes[h->group_probe].jt->dense.get<uint32_t>() : nullptr;
+        launch_group_flags(h->acc.get<uint64_t>(), h->stride, n, member, bits.get<uint32_t>(), counts.get<uint32_t>(), s);
         DevBuf offs;
         uint64_t total = scan_counts(ctx, counts.get<uint32_t>(), nb, offs, s);
         gids = DevBuf(ctx, std::max<size_t>(total * 4, 4), nullptr);
@@ -1842,7 +1880,17 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
         F.key_valid[k] = d->validity.get<uint32_t>();
         keycols.push_back(std::move(d));
     }
-    if (h->group_probe >= 0) {  // the keys are the build keys of the matched rows
+    if (h->dense_groups) {  // the key is the index position plus the index's smallest key
+        const ml_join_table* jt = h->pipe.probes[h->group_probe].jt;
+        auto d = std::make_unique<DevColumn>();
+        d->dtype = jt->key_types[0];
+        d->kind = CK_FIXED;
+        d->n = ng;
+        d->data = DevBuf(ctx, std::max<size_t>((size_t)ng * width_of(d->dtype), 8), b->res.get());
+        launch_dense_keys(gids.get<uint32_t>(), ng, jt->dmin, d->dtype, d->data.get(), s);
+        ctx->count_launch();
+        keycols.push_back(std::move(d));
+    } else if (h->group_probe >= 0) {  // the keys are the build keys of the matched rows
         const ml_batch& bb = h->pipe.probes[h->group_probe].jt->batch;
         for (int c : h->group_build_cols) keycols.push_back(gather_column(ctx, *bb.cols[c], gids.get<uint32_t>(), ng, s, b->res.get()));
     }
@@ -2014,7 +2062,7 @@ int ml_gpu_topn_sink(ml_topn_local* local, const ml_column* cols, int32_t ncols,
     const uint32_t* dsel = device_sel(ctx, sel, nsel, sel_hold, local->s);
     Pipeline::Launch L;
     t->pipe.prepare(L, cols, ncols, nrows, dsel, nsel, local->s, local->st, nullptr);
-    auto part = materialize(ctx, t->pipe, t->out_progs, L, local->s, nullptr, *local->ew);
+    auto part = materialize(ctx, t->pipe, t->out_progs, L, local->s, nullptr, *local->ew, true);
     auto best = topn_batch(ctx, *part, t->keys, t->limit, local->s, t->res.get());
     std::lock_guard<std::mutex> g(t->mu);
     t->cands.push_back(std::move(best));

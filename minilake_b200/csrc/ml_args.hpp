@@ -21,6 +21,11 @@ struct ProbeDev {
     // when the build side uses the hash table `t`.
     const uint32_t* dense;
     uint64_t dmin, drange;
+    // With a dense index whose keys are distinct, when nothing after this probe reads the build
+    // row (a GROUP BY of the join key that is the pipeline's last stage): the probe yields the
+    // key's index position (key - dmin) without reading the index, and membership in the build
+    // side is checked once per group when the aggregate is finalized.
+    int32_t late, pad;
 };
 
 // The streaming part of a pipeline (Filter / Projection folded into expressions /

@@ -535,6 +535,12 @@ __device__ __forceinline__ uint32_t dense_find(const uint32_t* dense, uint64_t d
     return off < drange ? dense_load(dense + off) : kNone;
 }
 
+// Index position of a key in a dense index's range (kNone outside it), without reading it.
+__device__ __forceinline__ uint32_t dense_slot(uint64_t dmin, uint64_t drange, uint64_t key) {
+    const uint64_t off = key - dmin;
+    return off < drange ? (uint32_t)off : kNone;
+}
+
 // 128-bit compare-and-swap (sm_90+): returns the slot's previous contents.
 __device__ __forceinline__ ulonglong2 cas128(uint64_t* p, ulonglong2 expect, ulonglong2 desired) {
     ulonglong2 old;

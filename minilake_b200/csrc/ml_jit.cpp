@@ -429,7 +429,10 @@ class Gen {
         open("{  // probe " + p);
         line("uint64_t wk" + tag + "[2] = {0ull, 0ull};");
         key(pd.keys, "wk" + tag, "continue;", "");
-        if (pd.dense)
+        if (pd.dense && pd.late)
+            line("const uint32_t hb" + tag + " = dense_slot(P.probes[" + p + "].dmin, P.probes[" + p + "].drange, wk" +
+                 tag + "[0]);");
+        else if (pd.dense)
             line("const uint32_t hb" + tag + " = dense_find(P.probes[" + p + "].dense, P.probes[" + p + "].dmin, P.probes[" +
                  p + "].drange, wk" + tag + "[0]);");
         else
@@ -498,8 +501,12 @@ class Gen {
                     line("uint32_t d" + tag + " = kNone;");
                     open("if (" + a + ") {  // probe " + p + " (dense index)");
                     key(pd.keys, "wk" + tag, a + " = false;", "");
-                    line("d" + tag + " = dense_find(P.probes[" + p + "].dense, P.probes[" + p + "].dmin, P.probes[" + p +
-                         "].drange, wk" + tag + "[0]);");
+                    if (pd.late)  // membership is checked per group at finalize: no index read per row
+                        line("d" + tag + " = dense_slot(P.probes[" + p + "].dmin, P.probes[" + p + "].drange, wk" + tag +
+                             "[0]);");
+                    else
+                        line("d" + tag + " = dense_find(P.probes[" + p + "].dense, P.probes[" + p + "].dmin, P.probes[" +
+                             p + "].drange, wk" + tag + "[0]);");
                     close();
                 });
                 cols.clear();

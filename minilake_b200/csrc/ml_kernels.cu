@@ -59,6 +59,7 @@ struct Cursors {
 
 // Build row matching the normalized key `w` through probe `pd` (dense index or hash table).
 __device__ __forceinline__ uint32_t probe_find(const ProbeDev& pd, const uint64_t* w) {
+    if (pd.dense && pd.late) return dense_slot(pd.dmin, pd.drange, w[0]);
     if (pd.dense) return dense_find(pd.dense, pd.dmin, pd.drange, w[0]);
     return table_find(pd.t, w, key_hash(w, pd.t.nwords));
 }
@@ -383,13 +384,14 @@ __global__ void __launch_bounds__(kThreads) k_index_write(int64_t n, const uint3
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_group_flags(const uint64_t* acc, int stride, int64_t n, uint32_t* bits,
+__global__ void __launch_bounds__(kThreads) k_group_flags(const uint64_t* acc, int stride, int64_t n,
+                                                          const uint32_t* member, uint32_t* bits,
                                                           uint32_t* block_counts) {
     int64_t base = (int64_t)blockIdx.x * kSelRowsPerBlock;
     uint32_t cnt = 0;
     for (int it = 0; it < 8; it++) {
         int64_t i = base + it * kThreads + threadIdx.x;
-        bool pass = i < n && acc[i * stride] != 0;
+        bool pass = i < n && acc[i * stride] != 0 && (member == nullptr || member[i] != kNone);
         uint32_t b = __ballot_sync(0xFFFFFFFFu, pass);
         if ((threadIdx.x & 31) == 0 && base + it * kThreads + (threadIdx.x & ~31) < n) bits[(base + it * kThreads + threadIdx.x) >> 5] = b;
         cnt += pass;
@@ -1007,10 +1009,21 @@ void launch_index_write(int64_t n, const uint32_t* bits, const uint64_t* block_o
     int nb = select_blocks(n);
     if (nb) k_index_write<<<nb, kThreads, 0, s>>>(n, nullptr, bits, block_offsets, out);
 }
-void launch_group_flags(const uint64_t* acc, int stride, int64_t n, uint32_t* bits, uint32_t* block_counts,
-                        cudaStream_t s) {
+__global__ void k_dense_keys(const uint32_t* gids, int64_t n, uint64_t dmin, int dt, void* out) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t k = dmin + gids[i];  // the normalized key word
+        if (dt == ML_TYPE_INT64) ((int64_t*)out)[i] = (int64_t)k;
+        else ((int32_t*)out)[i] = (int32_t)(uint32_t)k;
+    }
+}
+void launch_dense_keys(const uint32_t* gids, int64_t n, uint64_t dmin, int dt, void* out, cudaStream_t s) {
+    if (n) k_dense_keys<<<grid_for(n, 8), kThreads, 0, s>>>(gids, n, dmin, dt, out);
+}
+void launch_group_flags(const uint64_t* acc, int stride, int64_t n, const uint32_t* member, uint32_t* bits,
+                        uint32_t* block_counts, cudaStream_t s) {
     int nb = select_blocks(n);
-    if (nb) k_group_flags<<<nb, kThreads, 0, s>>>(acc, stride, n, bits, block_counts);
+    if (nb) k_group_flags<<<nb, kThreads, 0, s>>>(acc, stride, n, member, bits, block_counts);
 }
 void launch_count_slots(TableView t, unsigned long long* out, cudaStream_t s) {
     k_count_slots<<<grid_for((int64_t)t.mask + 1, 8), kThreads, 0, s>>>(t, out);

@@ -43,10 +43,13 @@ int select_blocks(int64_t n);
 void launch_select_flags(const PipeArgs& P, uint32_t* bits, uint32_t* block_counts, cudaStream_t s);
 void launch_select_write(const PipeArgs& P, const uint32_t* bits, const uint64_t* block_offsets, uint32_t* out,
                          cudaStream_t s);
-// Groups with at least one row (group blocks' word 0 > 0): pass bits + per-block counts;
-// then launch_index_write turns bits into the ordered list of group ids.
-void launch_group_flags(const uint64_t* acc, int stride, int64_t n, uint32_t* bits, uint32_t* block_counts,
-                        cudaStream_t s);
+// Groups with at least one row (group blocks' word 0 > 0) and, with `member`, whose entry
+// there is not kNone: pass bits + per-block counts; then launch_index_write turns bits into
+// the ordered list of group ids.
+void launch_group_flags(const uint64_t* acc, int stride, int64_t n, const uint32_t* member, uint32_t* bits,
+                        uint32_t* block_counts, cudaStream_t s);
+// Key values of dense-index groups: out[i] = dmin + gids[i] as int64, or as int32 / date.
+void launch_dense_keys(const uint32_t* gids, int64_t n, uint64_t dmin, int dt, void* out, cudaStream_t s);
 void launch_index_write(int64_t n, const uint32_t* bits, const uint64_t* block_offsets, uint32_t* out, cudaStream_t s);
 // Exclusive scan of u32 counts into u64 offsets (offsets[n] = total).
 void launch_scan_u32(const uint32_t* in, uint64_t* out, int64_t n, uint64_t* scratch, cudaStream_t s);

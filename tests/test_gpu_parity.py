@@ -429,3 +429,26 @@ def test_join_index_kinds_match_oracle(gpu_engine, kind):
         cap = stats["gpu"]["capacity"]
         assert cap & (cap - 1) == 0, "hash table capacity is a power of two"
     assert_same_rows(res["gpu"], res["oracle"], 1, {1})
+
+
+def test_group_by_dense_join_key_checks_membership_per_group(ctx, gpu_engine):
+    """GROUP BY a dense, distinct join key at the end of the pipeline: rows aggregate by the
+    key's index position and only keys present in the build side are emitted (fact keys that
+    are in the key range but not in the dimension, outside it, or NULL never appear)."""
+    rng = np.random.default_rng(13)
+    dk = np.sort(rng.choice(4000, 3000, replace=False)).astype(np.int64) + 100
+    dim = Table("d", ["k"], [[fixed(INT64, rng.permutation(dk))]])
+    n = 50_000
+    fact = Table("f", ["fk", "d", "v"], [[fixed(INT64, rng.integers(-20, 4200, n).astype(np.int64), rng.random(n) > 0.02),
+                                          fixed(INT32, rng.integers(0, 100, n)), fixed(FLOAT64, rng.random(n))]
+                                         for _ in range(2)])
+    aggs = [AggSpec(SUM, Col(2), FLOAT64), AggSpec(COUNT_STAR), AggSpec(MIN, Col(1), INT32), AggSpec(AVG, Col(2), FLOAT64)]
+    res = {}
+    for name, eng in (("gpu", gpu_engine), ("oracle", orc.OracleEngine(threads=2))):
+        j = eng.join_build(dim, [INT64], [(Col(0), INT64)])
+        out = eng.hashagg(fact, [INT64, INT32, FLOAT64], [(Col(0), INT64)], aggs,
+                          prologue=[Filter(Col(1) < Lit(80)), Probe(j.handle, [(Col(0), INT64)])])
+        if name == "gpu":
+            assert j.stats()["capacity"] <= 4000  # the direct (dense) index
+        res[name] = eng.fetch(out)
+    assert_same_rows(res["gpu"], res["oracle"], 1, {1, 4})
