@@ -456,27 +456,43 @@ std::unique_ptr<ml_batch> topn_batch(Ctx* ctx, ml_batch& b, const std::vector<So
         S.asc[i] = keys[i].asc;
         S.nulls_first[i] = keys[i].nulls_first;
     }
-    // rounds of chunk sorts until one chunk remains
     DevBuf a, bb;
     const uint32_t* in = nullptr;
-    int64_t m = n;
-    for (;;) {
-        const bool warp = k <= kTopNWarpMax;  // small limits: one sorted list per warp
-        int64_t nb = warp ? topn_warp_blocks(m) : (m + kTopNChunk - 1) / kTopNChunk;
-        DevBuf& dst = (in == a.get<uint32_t>() && in) ? bb : a;
-        dst = DevBuf(ctx, (size_t)nb * k * 4, nullptr);
-        {
-            KernelTimer kt(ctx, st, "topn");
-            if (warp) launch_topn_warp(S, in, m, (int)k, (int)nb, dst.get<uint32_t>(), st);
-            else launch_topn_chunk(S, in, m, (int)k, dst.get<uint32_t>(), st);
-            kt.stop();
+    if (k <= kTopNWarpMax) {  // small limits: one sorted list per warp, one launch
+        const int nb = topn_warp_blocks(n);
+        const size_t rows_b = ((size_t)nb * k * 4 + 15) & ~(size_t)15, cand_b = (size_t)nb * k * topn_entry_bytes();
+        a = DevBuf(ctx, rows_b + (nb > 1 ? cand_b + 16 + (size_t)k * 4 : 0), nullptr);
+        void* cand = nullptr;
+        unsigned int* done = nullptr;
+        uint32_t* final_out = nullptr;
+        if (nb > 1) {
+            cand = a.get<uint8_t>() + rows_b;
+            done = (unsigned int*)(a.get<uint8_t>() + rows_b + cand_b);
+            final_out = (uint32_t*)(done + 4);
+            CK(cudaMemsetAsync(done, 0, 4, st));
         }
+        KernelTimer kt(ctx, st, "topn");
+        launch_topn_warp(S, n, (int)k, nb, a.get<uint32_t>(), cand, done, final_out, st);
+        kt.stop();
         ctx->count_launch();
-        in = dst.get<uint32_t>();
-        if (nb == 1) break;
-        m = nb * k;
+        in = nb > 1 ? final_out : a.get<uint32_t>();
+    } else {  // rounds of chunk sorts until one chunk remains
+        int64_t m = n;
+        for (;;) {
+            int64_t nb = (m + kTopNChunk - 1) / kTopNChunk;
+            DevBuf& dst = (in == a.get<uint32_t>() && in) ? bb : a;
+            dst = DevBuf(ctx, (size_t)nb * k * 4, nullptr);
+            {
+                KernelTimer kt(ctx, st, "topn");
+                launch_topn_chunk(S, in, m, (int)k, dst.get<uint32_t>(), st);
+                kt.stop();
+            }
+            ctx->count_launch();
+            in = dst.get<uint32_t>();
+            if (nb == 1) break;
+            m = nb * k;
+        }
     }
-    CK(cudaStreamSynchronize(st));
     for (auto& c : b.cols) out->cols.push_back(gather_column(ctx, *c, in, k, st, res));
     CK(cudaStreamSynchronize(st));
     return out;
@@ -615,6 +631,7 @@ int ml_gpu_batch_column_info(const ml_batch* b, int32_t col, int32_t* dtype, int
 
 int ml_gpu_batch_fetch(const ml_batch* b, int32_t col, void* values, uint32_t* offsets, uint64_t* validity) {
     API_BEGIN
+    HostTimer host_timer_(b ? b->ctx : nullptr, "host:batch_fetch");
     REQUIRE(b, "null batch");
     REQUIRE(col >= 0 && col < (int32_t)b->cols.size(), "column out of range");
     b->ctx->set_current();
@@ -916,6 +933,7 @@ extern "C" {
 int ml_gpu_join_build_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue, const int32_t* input_types,
                              int32_t ninput, const ml_expr* key_exprs, int32_t nkeys, ml_join_build** out) {
     API_BEGIN
+    HostTimer host_timer_(ctx, "host:join_build_create");
     REQUIRE(ctx && out && key_exprs && nkeys > 0, "bad arguments");
     REQUIRE(nkeys <= kMaxKeys, "too many join keys");
     ctx->set_current();
@@ -946,6 +964,7 @@ int ml_gpu_join_build_local_create(ml_join_build* sink, ml_join_build_local** ou
 int ml_gpu_join_build_sink(ml_join_build_local* local, const ml_column* cols, int32_t ncols, int64_t nrows, const uint32_t* sel,
                            int64_t nsel) {
     API_BEGIN
+    HostTimer host_timer_(local ? local->sink->ctx : nullptr, "host:join_build_sink");
     REQUIRE(local, "null local sink");
     ml_join_build* j = local->sink;
     REQUIRE(!j->table, "join build sink already finalized");
@@ -978,6 +997,7 @@ int ml_gpu_join_build_combine(ml_join_build_local* local) {
 // build_table (join.rs:160-203)
 int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
     API_BEGIN
+    HostTimer host_timer_(j ? j->ctx : nullptr, "host:join_build_finalize");
     REQUIRE(j && table, "null argument");
     Ctx* ctx = j->ctx;
     ctx->set_current();
@@ -1529,6 +1549,7 @@ int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprol
                           const ml_expr* group_exprs, int32_t ngroup, const ml_agg_spec* aggs, int32_t nagg, int64_t size_hint,
                           ml_hashagg** out) {
     API_BEGIN
+    HostTimer host_timer_(ctx, "host:hashagg_create");
     REQUIRE(ctx && out, "null argument");
     REQUIRE(ngroup >= 0 && nagg >= 0 && (ngroup == 0 || group_exprs) && (nagg == 0 || aggs), "bad arguments");
     REQUIRE(nagg <= kMaxAggs, "too many aggregates");
@@ -1561,6 +1582,7 @@ int ml_gpu_hashagg_local_create(ml_hashagg* sink, ml_hashagg_local** out) {
 int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t ncols, int64_t nrows, const uint32_t* sel,
                         int64_t nsel) {
     API_BEGIN
+    HostTimer host_timer_(local ? local->sink->ctx : nullptr, "host:hashagg_sink");
     REQUIRE(local, "null local sink");
     ml_hashagg* h = local->sink;
     Ctx* ctx = h->ctx;
@@ -1817,6 +1839,7 @@ int ml_gpu_hashagg_combine(ml_hashagg_local* local) {
 // Sink::finalize -> final_batches (aggregate/hash.rs:307-314)
 int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
     API_BEGIN
+    HostTimer host_timer_(h ? h->ctx : nullptr, "host:hashagg_finalize");
     REQUIRE(h && out, "null argument");
     Ctx* ctx = h->ctx;
     ctx->set_current();
@@ -2025,6 +2048,7 @@ extern "C" {
 int ml_gpu_topn_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue, const int32_t* input_types, int32_t ninput,
                        const ml_sort_key* keys, int32_t nkeys, int64_t limit, ml_topn** out) {
     API_BEGIN
+    HostTimer host_timer_(ctx, "host:topn_create");
     REQUIRE(ctx && out && keys && nkeys > 0, "bad arguments");
     REQUIRE(nkeys <= kMaxKeys, "too many sort keys");
     REQUIRE(limit >= 0 && limit <= kMaxTopN, "limit out of range (0..2048)");
@@ -2053,6 +2077,7 @@ int ml_gpu_topn_local_create(ml_topn* sink, ml_topn_local** out) {
 // SortLocal::sink + truncate: keep only this batch's best `limit` rows
 int ml_gpu_topn_sink(ml_topn_local* local, const ml_column* cols, int32_t ncols, int64_t nrows, const uint32_t* sel, int64_t nsel) {
     API_BEGIN
+    HostTimer host_timer_(local ? local->sink->ctx : nullptr, "host:topn_sink");
     REQUIRE(local, "null local sink");
     ml_topn* t = local->sink;
     Ctx* ctx = t->ctx;
@@ -2063,7 +2088,9 @@ int ml_gpu_topn_sink(ml_topn_local* local, const ml_column* cols, int32_t ncols,
     Pipeline::Launch L;
     t->pipe.prepare(L, cols, ncols, nrows, dsel, nsel, local->s, local->st, nullptr);
     auto part = materialize(ctx, t->pipe, t->out_progs, L, local->s, nullptr, *local->ew, true);
-    auto best = topn_batch(ctx, *part, t->keys, t->limit, local->s, t->res.get());
+    auto r = std::make_unique<Reservation>(ctx, "Sort(candidates)");
+    auto best = topn_batch(ctx, *part, t->keys, t->limit, local->s, r.get());
+    best->res = std::move(r);  // the candidates own their memory: one of them may be the output
     std::lock_guard<std::mutex> g(t->mu);
     t->cands.push_back(std::move(best));
     API_END
@@ -2081,6 +2108,7 @@ int ml_gpu_topn_combine(ml_topn_local* local) {
 
 int ml_gpu_topn_finalize(ml_topn* t, ml_batch** out) {
     API_BEGIN
+    HostTimer host_timer_(t ? t->ctx : nullptr, "host:topn_finalize");
     REQUIRE(t && out, "null argument");
     Ctx* ctx = t->ctx;
     ctx->set_current();
@@ -2091,6 +2119,10 @@ int ml_gpu_topn_finalize(ml_topn* t, ml_batch** out) {
         cands = std::move(t->cands);
     }
     cudaStream_t s = t->streams.own();
+    if (cands.size() == 1) {  // one local sink: its candidates are the sorted top N already
+        *out = cands[0].release();
+        return ML_OK;
+    }
     std::unique_ptr<ml_batch> all;
     if (cands.empty()) {
         all = std::make_unique<ml_batch>();

@@ -1,6 +1,8 @@
 // Shared by the C-ABI translation units: the context handle and the status wrappers.
 #pragma once
 
+#include <chrono>
+
 #include "ml_runtime.hpp"
 
 struct ml_ctx : mlg::Ctx {
@@ -29,3 +31,15 @@ struct ml_ctx : mlg::Ctx {
 
 #define REQUIRE(c, msg) \
     if (!(c)) mlg::raise(ML_ERR_INVALID, msg)
+
+// Host time of one C-ABI call, recorded as "host:<name>" when the context profiles.
+struct HostTimer {
+    mlg::Ctx* ctx;
+    const char* name;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    HostTimer(mlg::Ctx* c, const char* n) : ctx(c), name(n) {}
+    ~HostTimer() {
+        if (ctx && ctx->profiling())
+            ctx->add_profile(name, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    }
+};

@@ -913,27 +913,24 @@ __device__ __forceinline__ TopEntry warp_merge32(const SortDev& S, TopEntry l, T
 // Rows that beat the warp's current k-th entry are queued in shared memory; a full queue
 // (32 entries) is sorted and merged into the list, so the sort runs once per 32
 // candidates, not once per 32 rows (about k * ln(rows / k) candidates reach a warp).
-__global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortDev S, const uint32_t* in, int64_t n,
-                                                   int k, uint32_t* out) {
-    __shared__ TopEntry lists[8][32];
-    __shared__ TopEntry queue[8][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// One warp's best k of n entries (batches of 32 from batch index `batch` on, every `batches`
+// batches), as a sorted list across the lanes; get(i) yields entry i.
+template <class Get>
+__device__ TopEntry warp_topk(const SortDev& S, int64_t n, int k, int64_t batch, int64_t batches, TopEntry* queue,
+                              int lane, Get get) {
     TopEntry best{~0ull, kNone};
     TopEntry kth = best;
-    int qn = 0;  // entries in this warp's queue (warp-uniform)
+    int qn = 0;  // entries in the warp's queue (warp-uniform)
     auto flush = [&]() {
-        TopEntry e = lane < qn ? queue[warp][lane] : TopEntry{~0ull, kNone};
+        TopEntry e = lane < qn ? queue[lane] : TopEntry{~0ull, kNone};
         __syncwarp();
         best = warp_merge32(S, best, warp_sort32(S, e, lane), lane);
         kth = shfl_entry(best, k - 1);
         qn = 0;
     };
-    const int64_t warps = (int64_t)gridDim.x * 8;
-    for (int64_t base = ((int64_t)blockIdx.x * 8 + warp) * 32; base < n; base += warps * 32) {
+    for (int64_t base = batch * 32; base < n; base += batches * 32) {
         int64_t i = base + lane;
-        TopEntry e;
-        e.r = i < n ? (in ? in[i] : (uint32_t)i) : kNone;
-        e.p = sort_prefix(S, e.r);
+        TopEntry e = i < n ? get(i) : TopEntry{~0ull, kNone};
         bool take = e.r != kNone && entry_less(S, e, kth);
         unsigned m = __ballot_sync(0xFFFFFFFFu, take);
         if (!m) continue;
@@ -942,16 +939,51 @@ __global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortD
             take = take && entry_less(S, e, kth);
             m = __ballot_sync(0xFFFFFFFFu, take);
         }
-        if (take) queue[warp][qn + __popc(m & ((1u << lane) - 1))] = e;
+        if (take) queue[qn + __popc(m & ((1u << lane) - 1))] = e;
         qn += __popc(m);
         __syncwarp();
     }
     if (qn) flush();
+    return best;
+}
+
+// Each CTA writes its best k rows to out[block * k ..].  With `final_out`, CTAs also write
+// their (prefix, row) entries to `cand`, and the last CTA to finish (the counter `done` starts
+// at zero) merges all CTAs' entries into final_out[0 .. k): the whole top-k in one launch.
+__global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortDev S, int64_t n, int k, uint32_t* out,
+                                                   TopEntry* cand, unsigned int* done, uint32_t* final_out) {
+    __shared__ TopEntry lists[8][32];
+    __shared__ TopEntry queue[8][32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    TopEntry best = warp_topk(S, n, k, (int64_t)blockIdx.x * 8 + warp, (int64_t)gridDim.x * 8, queue[warp], lane,
+                              [&](int64_t i) { return TopEntry{sort_prefix(S, (uint32_t)i), (uint32_t)i}; });
     lists[warp][lane] = best;
     __syncthreads();
     if (warp == 0) {
         for (int w = 1; w < 8; w++) best = warp_merge32(S, best, lists[w][lane], lane);
-        if (lane < k) out[(int64_t)blockIdx.x * k + lane] = best.r;
+        if (lane < k) {
+            out[(int64_t)blockIdx.x * k + lane] = best.r;
+            if (final_out) cand[(int64_t)blockIdx.x * k + lane] = best;
+        }
+    }
+    if (!final_out) return;
+    __threadfence();  // this CTA's entries are visible before it counts itself done
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int64_t m = (int64_t)gridDim.x * k;
+    best = warp_topk(S, m, k, warp, 8, queue[warp], lane, [&](int64_t i) {
+        const TopEntry* e = cand + i;
+        return TopEntry{__ldcg((const unsigned long long*)&e->p), __ldcg(&e->r)};
+    });
+    lists[warp][lane] = best;
+    __syncthreads();
+    if (warp == 0) {
+        for (int w = 1; w < 8; w++) best = warp_merge32(S, best, lists[w][lane], lane);
+        if (lane < k) final_out[lane] = best.r;
     }
 }
 
@@ -1092,8 +1124,10 @@ int topn_warp_blocks(int64_t n) {
     int64_t cap = (int64_t)num_sms() * 4;
     return (int)std::max<int64_t>(1, std::min(want, cap));
 }
-void launch_topn_warp(const SortDev& S, const uint32_t* in, int64_t n, int k, int blocks, uint32_t* out, cudaStream_t s) {
-    k_topn_warp<<<blocks, 256, 0, s>>>(S, in, n, k, out);
+size_t topn_entry_bytes() { return sizeof(TopEntry); }
+void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* out, void* cand, unsigned int* done,
+                      uint32_t* final_out, cudaStream_t s) {
+    k_topn_warp<<<blocks, 256, 0, s>>>(S, n, k, out, (TopEntry*)cand, done, final_out);
 }
 void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, uint32_t* out, cudaStream_t s) {
     int64_t nb = (n + kTopNChunk - 1) / kTopNChunk;
