@@ -695,9 +695,75 @@ std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArg
 
 int jit_rows_per_thread(const PipeArgs& P) { return batchable(P) ? kRowsPerThread : 1; }
 
+namespace {
+
+// The launch arguments with every runtime-only value cleared (pointers reduced to presence,
+// sizes and constants to zero): equal signatures give equal generated sources.
+std::string signature(char kind, const PipeArgs& P, const AggArgs* A, const KeyLayout* L) {
+    PipeArgs p = P;
+    p.n = 0;
+    p.sel = P.sel ? (const uint32_t*)1 : nullptr;
+    p.prog = nullptr;
+    p.arena = nullptr;
+    p.err = nullptr;
+    for (auto& l : p.luts) l = nullptr;
+    for (auto& c : p.cols) {
+        c.data = nullptr;
+        c.off = nullptr;
+        c.valid = c.valid ? (const uint64_t*)1 : nullptr;
+        c.gid = c.gid ? (const uint32_t*)1 : nullptr;
+        c.dbytes = nullptr;
+        c.n = 0;
+        c.dict_len = 0;
+    }
+    for (auto& pd : p.probes) {
+        pd.t = TableView{};
+        pd.next = pd.next ? (const uint32_t*)1 : nullptr;
+        pd.dense = pd.dense ? (const uint32_t*)1 : nullptr;
+        pd.dmin = pd.drange = 0;
+    }
+    std::string key(1, kind);
+    key.append((const char*)&p, sizeof p);
+    if (A) {
+        AggArgs a = *A;
+        a.t = TableView{};
+        a.gkeys = nullptr;
+        a.gnull = nullptr;
+        a.ngroups = nullptr;
+        a.acc = nullptr;
+        a.ovf = nullptr;
+        a.ovf_count = nullptr;
+        a.gid_cap = 0;
+        a.ovf_cap = 0;
+        a.smem_groups = a.smem_groups > 0;
+        for (auto& g : a.aggs) g.vcnt = g.vcnt ? (uint64_t*)1 : nullptr;
+        key.append((const char*)&a, sizeof a);
+    }
+    if (L) key.append((const char*)L, sizeof *L);
+    return key;
+}
+
+template <class Make>
+void* memoized(const Pipeline& pipe, std::string key, Make make) {
+    {
+        std::lock_guard<std::mutex> g(pipe.jit_mu);
+        for (auto& e : pipe.jit_memo)
+            if (e.first == key) return e.second;
+    }
+    void* fn = make();
+    std::lock_guard<std::mutex> g(pipe.jit_mu);
+    if (pipe.jit_memo.size() >= 16) pipe.jit_memo.erase(pipe.jit_memo.begin());
+    pipe.jit_memo.emplace_back(std::move(key), fn);
+    return fn;
+}
+
+}  // namespace
+
 void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {
     if (!jit_enabled(ctx)) return nullptr;
-    return (void*)get_kernel(ctx, jit_agg_source(pipe, P, A), "ml_pipeline_aggregate");
+    return memoized(pipe, signature('a', P, &A, nullptr) + std::string((const char*)&ctx->device, sizeof(int)), [&] {
+        return (void*)get_kernel(ctx, jit_agg_source(pipe, P, A), "ml_pipeline_aggregate");
+    });
 }
 
 void* jit_agg_resume_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {

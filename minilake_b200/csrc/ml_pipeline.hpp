@@ -44,6 +44,11 @@ class Pipeline {
     std::vector<ProbeInfo> probes;
     StringIntern intern;
     DevBuf d_prog, d_arena;
+    // Runtime-specialized kernels already looked up for this pipeline, by the launch's
+    // structural signature (the fields the source generator reads), so repeated launches skip
+    // generating the source again.
+    mutable std::mutex jit_mu;
+    mutable std::vector<std::pair<std::string, void*>> jit_memo;
 
     void build(const ml_pipe_op* ops, int nops, const int32_t* types, int ntypes);
     KeyLayout key_layout(const ml_expr* exprs, int n, const Schema& schema, bool group, std::vector<KeyDecode>* dec);

@@ -102,6 +102,11 @@ Ctx::Ctx(int dev, uint64_t budget, uint32_t fl) : device(dev), flags(fl), pool(b
 Ctx::~Ctx() {
     cudaSetDevice(device);
     cudaDeviceSynchronize();
+    for (auto& t : timings_) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    for (auto e : events_) cudaEventDestroy(e);
     for (auto s : streams_) cudaStreamDestroy(s);
     for (auto s : idle_streams_) cudaStreamDestroy(s);
     if (stream) cudaStreamDestroy(stream);
@@ -225,6 +230,8 @@ void Ctx::add_profile(const std::string& k, double ms) {
 }
 void Ctx::read_profile(const std::string& k, uint64_t* n, double* ms, bool reset) {
     std::lock_guard<std::mutex> g(prof_mu_);
+    set_current();
+    drain_timings(0);
     auto& e = prof_[k];
     if (n) *n = e.first;
     if (ms) *ms = e.second;
@@ -233,21 +240,50 @@ void Ctx::read_profile(const std::string& k, uint64_t* n, double* ms, bool reset
 
 KernelTimer::KernelTimer(Ctx* ctx, cudaStream_t s, const char* name) : ctx_(ctx), s_(s), name_(name) {
     if (!ctx_->profiling()) return;
-    cudaEventCreate(&a_);
-    cudaEventCreate(&b_);
+    a_ = ctx_->get_event();
+    b_ = ctx_->get_event();
     cudaEventRecord(a_, s_);
 }
 void KernelTimer::stop() {
     if (b_) cudaEventRecord(b_, s_);
 }
 KernelTimer::~KernelTimer() {
-    if (!a_) return;
-    float ms = 0;
-    if (cudaEventSynchronize(b_) == cudaSuccess && cudaEventElapsedTime(&ms, a_, b_) == cudaSuccess)
-        ctx_->add_profile(name_, ms);
-    cudaGetLastError();
-    cudaEventDestroy(a_);
-    cudaEventDestroy(b_);
+    if (a_) ctx_->add_timing(name_, a_, b_);
+}
+
+cudaEvent_t Ctx::get_event() {
+    {
+        std::lock_guard<std::mutex> g(prof_mu_);
+        if (!events_.empty()) {
+            cudaEvent_t e = events_.back();
+            events_.pop_back();
+            return e;
+        }
+    }
+    cudaEvent_t e = nullptr;
+    CK(cudaEventCreate(&e));
+    return e;
+}
+void Ctx::add_timing(const char* name, cudaEvent_t a, cudaEvent_t b) {
+    std::lock_guard<std::mutex> g(prof_mu_);
+    timings_.push_back(Timing{name, a, b});
+    if (timings_.size() > 4096) drain_timings(1024);
+}
+void Ctx::drain_timings(size_t keep) {  // collect all but the newest `keep` timings
+    size_t n = timings_.size() > keep ? timings_.size() - keep : 0;
+    for (size_t i = 0; i < n; i++) {
+        Timing& t = timings_[i];
+        float ms = 0;
+        if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+            auto& e = prof_[t.name];
+            e.first++;
+            e.second += ms;
+        }
+        cudaGetLastError();
+        events_.push_back(t.a);
+        events_.push_back(t.b);
+    }
+    timings_.erase(timings_.begin(), timings_.begin() + n);
 }
 
 Staging::~Staging() {

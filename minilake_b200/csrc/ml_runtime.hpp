@@ -120,10 +120,21 @@ class Ctx {
     bool profiling() const { return (flags & ML_CTX_PROFILE) != 0; }
     void add_profile(const std::string& k, double ms);
     void read_profile(const std::string& k, uint64_t* n, double* ms, bool reset);
+    // Kernel timings are collected lazily: a launch's event pair waits here until the profile
+    // is read (or the list is long), so timing a kernel adds no host synchronization.
+    void add_timing(const char* name, cudaEvent_t a, cudaEvent_t b);
+    cudaEvent_t get_event();
 
    private:
     std::mutex mu_, prof_mu_;
     std::map<std::string, std::pair<uint64_t, double>> prof_;
+    struct Timing {
+        const char* name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Timing> timings_;   // under prof_mu_
+    std::vector<cudaEvent_t> events_;  // idle events, under prof_mu_
+    void drain_timings(size_t keep);  // prof_mu_ held
     std::multimap<size_t, void*> free_;  // cached device blocks by capacity
     std::vector<cudaStream_t> streams_, idle_streams_;
     std::vector<void*> slabs_, free_slots_;
@@ -135,7 +146,7 @@ class KernelTimer {
    public:
     KernelTimer(Ctx* ctx, cudaStream_t s, const char* name);
     ~KernelTimer();
-    void stop();  // records the end event; the time is collected at destruction (after a sync)
+    void stop();  // records the end event; the time is collected when the profile is read
 
    private:
     Ctx* ctx_;
