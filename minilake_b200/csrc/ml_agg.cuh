@@ -99,12 +99,24 @@ __device__ inline void record_overflow(const PipeArgs& P, const AggArgs& A, cons
     if (w > 4) o[4] = x.b3;
 }
 
+// The CTA's direct group index (AggArgs::dslots): entry = group id + 1, 0 until a thread of
+// this CTA has looked the slot's key up in the global table.  Every writer of an entry writes
+// the same value (a slot stands for one key), so readers need no ordering: a 0 read only sends
+// the row to the global table.
+__device__ __forceinline__ uint32_t* direct_slots(const AggArgs& A, uint64_t* smem) {
+    return (uint32_t*)(smem + (uint64_t)A.smem_groups * A.stride + (uint64_t)A.priv_groups * A.stride * 256);
+}
+
 __device__ inline void smem_setup(const AggArgs& A, uint64_t* smem) {
     for (int g = threadIdx.x; g < A.smem_groups; g += blockDim.x) {
         uint64_t* b = smem + (uint64_t)g * A.stride;
         for (int w = 0; w < A.stride; w++) b[w] = 0;
         for (int k = 0; k < A.nagg; k++)
             if (A.aggs[k].func != ML_AGG_COUNT_STAR) b[A.aggs[k].off] = agg_identity(A.aggs[k].kind);
+    }
+    if (agg_direct_on(A)) {
+        uint32_t* d = direct_slots(A, smem);
+        for (int i = threadIdx.x; i < kDirectSlots; i += blockDim.x) d[i] = 0;
     }
 }
 

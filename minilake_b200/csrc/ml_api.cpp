@@ -1231,6 +1231,14 @@ struct AggState {
     bool vcnt_on = false;  // valid-input counts maintained
     DevBuf vcnt;
 };
+
+// Grid of a runtime-specialized aggregate launch: the CTAs the rows need, at most one wave of
+// resident CTAs (each CTA sets up and flushes its shared-memory groups once).
+int agg_grid(void* jit, const PipeArgs& P, int smem) {
+    const int64_t k = jit_rows_per_thread(P);
+    return std::min<int64_t>(pipeline_grid((P.n + k - 1) / k),
+                             (int64_t)jit_resident_blocks(jit, kPipelineThreads, smem) * num_sms());
+}
 }  // namespace
 
 constexpr uint32_t kSmemPreaggMaxGroups = 65536;
@@ -1278,6 +1286,37 @@ struct ml_hashagg {
         return TableView{slots.get<uint64_t>(), cap ? cap - 1 : 0, keys.nwords, keys.nwords == 1 ? 2 : 4};
     }
 
+    // Direct group slots of this launch (AggArgs::dslots), for the runtime-specialized kernel:
+    // every key a dictionary-coded string column of the scanned batch or a BOOL value, and the
+    // product of the keys' value counts (NULL included) at most kDirectSlots.
+    void direct_slots(AggArgs& A, const Pipeline::Launch& L) const {
+        A.dslots = 0;
+        if (!agg_direct_on(A)) return;
+        uint64_t total = 1;
+        uint32_t mul[kMaxKeys], base[kMaxKeys];
+        for (int k = 0; k < A.keys.nkeys; k++) {
+            const Prog& p = A.keys.prog[k];
+            uint64_t range;
+            if (A.keys.f[k].type == ML_TYPE_BOOL) {
+                base[k] = 0;
+                range = 3;
+            } else {
+                if (p.len != 1 || p.start < 0 || p.start >= (int)pipe.C.code.size()) return;
+                const Instr& in = pipe.C.code[p.start];
+                if (in.op != I_COL || in.a < 0 || in.a >= (int)L.gid_range.size()) return;
+                const auto r = L.gid_range[in.a];
+                if (r.first > r.second) return;  // not a dictionary-coded source column
+                base[k] = r.first;
+                range = (uint64_t)(r.second - r.first) + 2;
+            }
+            mul[k] = (uint32_t)total;
+            total *= range;
+            if (total > (uint64_t)kDirectSlots) return;
+        }
+        A.dslots = (uint32_t)total;
+        for (int k = 0; k < A.keys.nkeys; k++) A.dmul[k] = mul[k], A.dbase[k] = base[k];
+    }
+
     AggArgs args(unsigned long long* ovf_count, uint32_t* ovf, uint64_t ovf_cap) {
         AggArgs A{};
         A.keys = keys;
@@ -1294,6 +1333,14 @@ struct ml_hashagg {
         // shared-memory pre-aggregation pays off when the group space is small enough that
         // the first groups take a large share of the rows
         A.smem_groups = (ungrouped || gid_cap <= kSmemPreaggMaxGroups) ? std::min<int>(smem_groups, (int)gid_cap) : 0;
+        // the first groups get per-thread accumulators (no atomics) in what the shared-memory
+        // budget leaves (three CTAs per SM)
+        bool vcnt = false;
+        for (const AggState& a : aggs) vcnt = vcnt || (a.vcnt_on && a.kind != A_AVG);
+        const int fixed = (int)((size_t)A.smem_groups * stride * 8 + agg_direct_bytes(A));
+        A.priv_groups = vcnt || !A.smem_groups
+                            ? 0
+                            : std::max(0, std::min({A.smem_groups, 8, (kAggSmemBudget - fixed) / (stride * 256 * 8)}));
         A.ovf = ovf;
         A.ovf_count = ovf_count;
         A.ovf_cap = ovf_cap;
@@ -1424,6 +1471,7 @@ void ml_hashagg::resume_overflow(Pipeline::Launch& L, uint64_t count, DevBuf& ov
         CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
         L.P.err = ew.d.get<uint32_t>();
         AggArgs A = args(d_count, ovf2.get<uint32_t>(), count);
+        A.priv_groups = 0;  // the few rows that overflowed: shared-memory atomics suffice
         void* jit = jit_agg_resume_kernel(ctx, pipe, L.P, A);
         if (jit) {
             const uint32_t* rows = ovf.get<uint32_t>();
@@ -1625,13 +1673,15 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
         L.P.head_probe = h->group_probe;
         if (h->dense_groups) L.P.probes[h->group_probe].late = 1;
         AggArgs A = h->args(local->ovf_count.get<unsigned long long>(), ovf.get<uint32_t>(), ovf_cap);
+        h->direct_slots(A, L);
         void* jit = jit_agg_kernel(ctx, h->pipe, L.P, A);
+        if (!jit) A.priv_groups = 0, A.dslots = 0;  // both exist in specialized kernels only
         KernelTimer kt(ctx, s, "pipeline_aggregate");
         if (jit) {
             if (L.P.n) {
                 void* args[] = {&L.P, &A};
-                int64_t k = jit_rows_per_thread(L.P);
-                jit_launch(jit, pipeline_grid((L.P.n + k - 1) / k), kPipelineThreads, agg_smem_bytes(A), s, args);
+                const int smem = agg_smem_bytes(A);
+                jit_launch(jit, agg_grid(jit, L.P, smem), kPipelineThreads, smem, s, args);
             }
             ctx->add_profile("jit_launch", 0);
         } else {
@@ -1750,10 +1800,11 @@ int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t nc
     L.P.head_probe = h->group_probe;
         if (h->dense_groups) L.P.probes[h->group_probe].late = 1;
     AggArgs A = h->args(R.count.get<unsigned long long>(), R.ovf.get<uint32_t>(), ovf_cap);
+    h->direct_slots(A, L);
     void* jit = jit_agg_kernel(ctx, h->pipe, L.P, A);
-    const int64_t k = jit ? jit_rows_per_thread(L.P) : 1;
-    const int grid = pipeline_grid((L.P.n + k - 1) / k);
+    if (!jit) A.priv_groups = 0, A.dslots = 0;  // both exist in specialized kernels only
     const int smem = agg_smem_bytes(A);
+    const int grid = jit ? agg_grid(jit, L.P, smem) : pipeline_grid(L.P.n);
     // the graph is keyed by everything its nodes capture
     std::string key((const char*)&L.P, sizeof(PipeArgs));
     key.append((const char*)&A, sizeof(AggArgs));

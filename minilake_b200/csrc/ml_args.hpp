@@ -57,13 +57,33 @@ struct AggArgs {
     int32_t ungrouped;        // no GROUP BY: every row goes to group 0
     int32_t group_probe;      // >= 0: GROUP BY the join key of this probe; group id = matched build row
     int32_t smem_groups;      // group ids below this are pre-aggregated in shared memory
+    int32_t priv_groups;      // group ids below this have per-thread accumulators in shared memory
+                              // (runtime-specialized kernels only; 0 for the interpreter)
     int32_t stride;           // u64 words per group block
     uint64_t* acc;            // group blocks (gid_cap x stride)
     uint32_t* ovf;            // overflow row contexts
     unsigned long long* ovf_count;
     uint64_t ovf_cap;
+    // Direct group slots (runtime-specialized kernels only; 0 = off): when every GROUP BY key
+    // takes few values in this launch (a dictionary-coded string: its string ids lie in
+    // [dbase, dbase + range - 2]; a BOOL), the key's slot is sum_k term_k * dmul[k] with
+    // term_k = 0 for NULL, else value - dbase[k] + 1, and dslots (<= kDirectSlots) bounds it.
+    uint32_t dslots;
+    uint32_t dmul[kMaxKeys];
+    uint32_t dbase[kMaxKeys];
     AggDev aggs[kMaxAggs];
 };
+
+// Shared memory of an aggregate launch (256 threads), in this order: the pre-aggregated group
+// blocks (smem_groups x stride words), the per-thread accumulators (priv_groups x stride x 256
+// words), then, for a keyed GROUP BY with shared-memory groups, kDirectSlots u32 entries of the
+// CTA's direct group index (group id + 1 by direct slot, 0 = not yet looked up).
+constexpr int kDirectSlots = 1024;
+// Per-CTA budget that keeps three 256-thread CTAs resident on an SM (228 KB of shared memory).
+constexpr int kAggSmemBudget = 74 << 10;
+
+ML_HD inline bool agg_direct_on(const AggArgs& A) { return A.smem_groups > 0 && !A.ungrouped && A.group_probe < 0; }
+ML_HD inline uint64_t agg_direct_bytes(const AggArgs& A) { return agg_direct_on(A) ? 4 * kDirectSlots : 0; }
 
 struct SortDev {
     int32_t nkeys, pad;

@@ -6,6 +6,12 @@
 
 #include "../../include/minilake_gpu.h"
 
+#if defined(__CUDACC__)
+#define ML_HD __host__ __device__
+#else
+#define ML_HD
+#endif
+
 namespace mlg {
 
 // ---- limits --------------------------------------------------------------------

@@ -38,6 +38,7 @@ struct Nvrtc {
     CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
                        void**, void**);
     CUresult (*set_attr)(CUfunction, CUfunction_attribute, int);
+    CUresult (*occupancy)(int*, CUfunction, int, size_t);
 
     Nvrtc() {
         const char* names[] = {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"};
@@ -73,6 +74,7 @@ struct Nvrtc {
         drv(get_fn, "cuModuleGetFunction");
         drv(launch, "cuLaunchKernel");
         drv(set_attr, "cuFuncSetAttribute");
+        drv(occupancy, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
         ok = got;
         if (!ok) why = "NVRTC or driver module entry points missing";
     }
@@ -386,7 +388,9 @@ class Gen {
 
     // Normalized key words of layout L (make_key) into `wk` (a declared uint64_t[2], zeroed).
     // A NULL key runs `on_null` (join keys) or sets its bit in `nm` (GROUP BY keys).
-    void key(const KeyLayout& L, const std::string& wk, const std::string& on_null, const std::string& nm) {
+    // `ds` (optional): also sum the key's direct slot (AggArgs::dslots) into that variable.
+    void key(const KeyLayout& L, const std::string& wk, const std::string& on_null, const std::string& nm,
+             const std::string& ds = "") {
         for (int k = 0; k < L.nkeys; k++) {
             V e = expr(L.prog[k]);
             const KeyField& f = L.f[k];
@@ -403,6 +407,10 @@ class Gen {
                 close("} else {");
                 ind_++;
                 line(pack);
+                if (!ds.empty()) {
+                    const std::string v = f.type == ML_TYPE_BOOL ? "((uint32_t)(" + e.v + ") & 1u)" : "(uint32_t)(" + e.v + ")";
+                    line(ds + " += (" + v + " - A.dbase[" + num(k) + "] + 1u) * A.dmul[" + num(k) + "];");
+                }
                 close();
             }
         }
@@ -584,6 +592,10 @@ std::string row_loop(const PipeArgs& P, bool batched, const std::string& body) {
         }
     }
     s += body;
+    // Batched tiles have the same trip count in every lane: reconverge the warp once per tile,
+    // so lanes split by a data-dependent branch (a group's first lookup, a claimed slot) do
+    // not go on issuing the next tile's loads separately.
+    if (batched) s += "        __syncwarp();\n";
     s += "    }\n";
     return s;
 }
@@ -598,14 +610,21 @@ void emit_aggregate(Gen& g, const AggArgs& A) {
     } else if (A.ungrouped) {
         g.line("const uint32_t g = 0;");
     } else {
+        const bool direct = A.dslots > 0;  // implies agg_direct_on(A)
         g.line("uint64_t wkg[2] = {0ull, 0ull};");
         g.line("uint32_t nmg = 0;");
-        g.key(A.keys, "wkg", "", "nmg");
-        g.line("bool ins;");
+        if (direct) g.line("uint32_t dsg = 0;");
+        g.key(A.keys, "wkg", "", "nmg", direct ? "dsg" : "");
+        g.line("bool ins = false;");
+        // with direct slots, the CTA's index first: the global table only on the slot's first use
+        g.line(direct ? "uint32_t g = dsg < A.dslots ? dsl[dsg] - 1u : kNone;" : "uint32_t g = kNone;");
+        g.open("if (g == kNone) {");
         g.line("uint64_t slot;");
-        g.line("const uint32_t g = table_upsert(A.t, wkg, nmg, key_hash(wkg, " + num(A.keys.nwords) +
+        g.line("g = table_upsert(A.t, wkg, nmg, key_hash(wkg, " + num(A.keys.nwords) +
                ", nmg), P.err, [&]() -> uint32_t { const uint32_t id = atomicAdd(A.ngroups, 1u); "
                "return id < A.gid_cap ? id : kNone; }, &ins, &slot, A.ngroups, A.gid_cap);");
+        if (direct) g.line("if (g != kNone && dsg < A.dslots) dsl[dsg] = g + 1u;");
+        g.close();
         g.open("if (g == kNone) {");
         g.line("record_overflow(P, A, " + g.x + ");");
         g.line(g.fail);
@@ -615,6 +634,47 @@ void emit_aggregate(Gen& g, const AggArgs& A) {
         if (A.keys.nwords > 1) g.line("A.gkeys[(uint64_t)A.gid_cap + g] = wkg[1];");
         g.line("A.gnull[g] = nmg;");
         g.close();
+    }
+    // every aggregate's argument, evaluated once for whichever accumulators the group uses
+    std::vector<Gen::V> args(A.nagg);
+    for (int k = 0; k < A.nagg; k++) {
+        const AggDev& a = A.aggs[k];
+        if (a.func != ML_AGG_COUNT_STAR && a.has_arg) args[k] = g.expr(a.arg);
+    }
+    const int priv = A.priv_groups;
+    if (priv > 0) {  // per-thread accumulators: plain updates, no atomics
+        g.open("if (g < " + num(priv) + "u) {");
+        g.line("uint64_t* pv = smem + (uint64_t)A.smem_groups * " + S + " + (uint64_t)g * " + num(A.stride * 256) +
+               " + threadIdx.x;");
+        g.line("pv[0] += 1ull;");
+        for (int k = 0; k < A.nagg; k++) {
+            const AggDev& a = A.aggs[k];
+            if (a.func == ML_AGG_COUNT_STAR) continue;
+            const std::string w = "pv[" + num(a.off * 256) + "]", v = a.has_arg ? args[k].v : "0ull";
+            if (a.has_arg) g.open("if (" + args[k].k + ") {");
+            switch (a.kind) {
+                case A_SUM_I64: g.line(w + " += " + v + ";"); break;
+                case A_SUM_F64: g.line(w + " = f64_bits(__dadd_rn(as_f64(" + w + "), as_f64(" + v + ")));"); break;
+                case A_AVG:
+                    g.line(w + " = f64_bits(__dadd_rn(as_f64(" + w + "), as_f64(" + v + ")));");
+                    g.line("pv[" + num((a.off + 1) * 256) + "] += 1ull;");
+                    break;
+                case A_MIN_I64: g.line(w + " = (uint64_t)min((long long)" + w + ", (long long)" + v + ");"); break;
+                case A_MAX_I64: g.line(w + " = (uint64_t)max((long long)" + w + ", (long long)" + v + ");"); break;
+                case A_MIN_F64:
+                    g.line(w + " = (uint64_t)min((unsigned long long)" + w + ", (unsigned long long)f64_order(as_f64(" + v +
+                           ")));");
+                    break;
+                case A_MAX_F64:
+                    g.line(w + " = (uint64_t)max((unsigned long long)" + w + ", (unsigned long long)f64_order(as_f64(" + v +
+                           ")));");
+                    break;
+                default: g.line(w + " += 1ull;"); break;  // COUNT(x)
+            }
+            if (a.has_arg) g.close();
+        }
+        g.close("} else {");
+        g.open("");
     }
     if (smem) {
         g.line("uint64_t* blk = (int)g < A.smem_groups ? smem + (uint64_t)g * " + S + " : A.acc + (uint64_t)g * " + S + ";");
@@ -629,9 +689,8 @@ void emit_aggregate(Gen& g, const AggArgs& A) {
         g.open("{  // aggregate " + num(k));
         std::string v = "0ull";
         if (a.has_arg) {
-            Gen::V e = g.expr(a.arg);
-            g.open("if (" + e.k + ") {");
-            v = e.v;
+            g.open("if (" + args[k].k + ") {");
+            v = args[k].v;
         }
         g.line(std::string(smem ? "acc_apply(" : "acc_apply_global(") + num(a.kind) + ", blk + " + num(a.off) + ", " + v +
                ");");
@@ -642,6 +701,109 @@ void emit_aggregate(Gen& g, const AggArgs& A) {
         if (a.has_arg) g.close();
         g.close();
     }
+    if (priv > 0) g.close();
+}
+
+// What each word of a group block holds: 0 = integer count or sum, 1 = f64 sum, 2/3 = signed
+// min/max, 4/5 = order-mapped f64 min/max (unsigned compare).
+std::vector<int> word_ops(const AggArgs& A) {
+    std::vector<int> ops(A.stride, 0);
+    for (int k = 0; k < A.nagg; k++) {
+        const AggDev& a = A.aggs[k];
+        if (a.func == ML_AGG_COUNT_STAR) continue;
+        switch (a.kind) {
+            case A_SUM_F64:
+            case A_AVG: ops[a.off] = 1; break;
+            case A_MIN_I64: ops[a.off] = 2; break;
+            case A_MAX_I64: ops[a.off] = 3; break;
+            case A_MIN_F64: ops[a.off] = 4; break;
+            case A_MAX_F64: ops[a.off] = 5; break;
+            default: break;
+        }
+    }
+    return ops;
+}
+
+// Start values of the per-thread accumulators, then (after the rows) their reduction over the
+// CTA's threads and one global update per group and word (skipped for groups with no rows).
+std::string priv_init(const AggArgs& A) {
+    const int S = A.stride, P = A.priv_groups;
+    std::string id = "{";
+    for (int w = 0; w < S; w++) id += (w ? ", " : "") + std::string("0ull");
+    id += "}";
+    std::string src;
+    src += "    {\n        uint64_t idw[" + num(S) + "] = " + id + ";\n";
+    for (int k = 0; k < A.nagg; k++)
+        if (A.aggs[k].func != ML_AGG_COUNT_STAR)
+            src += "        idw[" + num(A.aggs[k].off) + "] = agg_identity(" + num(A.aggs[k].kind) + ");\n";
+    src += "        uint64_t* pv = smem + (uint64_t)A.smem_groups * " + num(S) + ";\n";
+    src += "        for (int i = threadIdx.x; i < " + num(P * S * 256) + "; i += blockDim.x) pv[i] = idw[(i >> 8) % " +
+           num(S) + "];\n";
+    src += "    }\n    __syncthreads();\n";
+    return src;
+}
+
+std::string priv_flush(const AggArgs& A) {
+    const int S = A.stride, P = A.priv_groups;
+    const std::vector<int> ops = word_ops(A);
+    std::string src;
+    src += "    {\n";
+    src += "        const uint64_t* pv = smem + (uint64_t)A.smem_groups * " + num(S) + ";\n";
+    src += "        const int lane = threadIdx.x & 31;\n";
+    src += "        for (int pair = threadIdx.x >> 5; pair < " + num(P * S) + "; pair += blockDim.x >> 5) {\n";
+    src += "            const int gg = pair / " + num(S) + ", w = pair % " + num(S) + ";\n";
+    src += "            const uint64_t* c = pv + (uint64_t)gg * " + num(S * 256) + ";\n";
+    src += "            unsigned long long rows = 0;\n";
+    src += "            for (int t = lane; t < 256; t += 32) rows += c[t];\n";
+    src += "            for (int o = 16; o; o >>= 1) rows += __shfl_xor_sync(0xFFFFFFFFu, rows, o);\n";
+    src += "            if (rows == 0) continue;  // no row of this group in this CTA\n";
+    src += "            const uint64_t* x = c + w * 256;\n";
+    src += "            uint64_t* dst = A.acc + (uint64_t)gg * " + num(S) + " + w;\n";
+    src += "            switch (w) {\n";
+    for (int w = 0; w < S; w++) {
+        src += "                case " + num(w) + ": {\n";
+        switch (ops[w]) {
+            case 1:
+                src += "                    double v = 0.0;\n";
+                src += "                    for (int t = lane; t < 256; t += 32) v = __dadd_rn(v, as_f64(x[t]));\n";
+                src += "                    for (int o = 16; o; o >>= 1) v = __dadd_rn(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));\n";
+                src += "                    if (lane == 0) atomicAdd((double*)dst, v);\n";
+                break;
+            case 2:
+            case 3: {
+                const char* f = ops[w] == 2 ? "min" : "max";
+                src += "                    long long v = (long long)x[lane];\n";
+                src += std::string("                    for (int t = lane + 32; t < 256; t += 32) v = ") + f +
+                       "(v, (long long)x[t]);\n";
+                src += std::string("                    for (int o = 16; o; o >>= 1) v = ") + f +
+                       "(v, (long long)__shfl_xor_sync(0xFFFFFFFFu, (unsigned long long)v, o));\n";
+                src += std::string("                    if (lane == 0) atomic") + (ops[w] == 2 ? "Min" : "Max") +
+                       "((long long*)dst, v);\n";
+                break;
+            }
+            case 4:
+            case 5: {
+                const char* f = ops[w] == 4 ? "min" : "max";
+                src += "                    unsigned long long v = x[lane];\n";
+                src += std::string("                    for (int t = lane + 32; t < 256; t += 32) v = ") + f +
+                       "(v, (unsigned long long)x[t]);\n";
+                src += std::string("                    for (int o = 16; o; o >>= 1) v = ") + f +
+                       "(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));\n";
+                src += std::string("                    if (lane == 0) atomic") + (ops[w] == 4 ? "Min" : "Max") +
+                       "((unsigned long long*)dst, v);\n";
+                break;
+            }
+            default:
+                src += "                    unsigned long long v = 0;\n";
+                src += "                    for (int t = lane; t < 256; t += 32) v += x[t];\n";
+                src += "                    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);\n";
+                src += "                    if (lane == 0 && v) atomicAdd((unsigned long long*)dst, v);\n";
+                break;
+        }
+        src += "                    break;\n                }\n";
+    }
+    src += "            }\n        }\n    }\n";
+    return src;
 }
 
 const char* kPrelude = "#include \"ml_agg.cuh\"\nusing namespace mlg;\n";
@@ -686,9 +848,12 @@ std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArg
            "const __grid_constant__ AggArgs A) {\n";
     src += "    extern __shared__ __align__(16) uint64_t smem[];\n";
     if (smem) src += "    smem_setup(A, smem);\n    __syncthreads();\n";
+    if (A.dslots > 0) src += "    uint32_t* const dsl = direct_slots(A, smem);\n";
+    if (A.priv_groups > 0) src += priv_init(A);
     src += g.pre();
     src += row_loop(P, batched, g.body());
     if (smem) src += "    __syncthreads();\n    smem_flush(A, smem);\n";
+    if (A.priv_groups > 0) src += priv_flush(A);
     src += "}\n";
     return src;
 }
@@ -736,6 +901,8 @@ std::string signature(char kind, const PipeArgs& P, const AggArgs* A, const KeyL
         a.gid_cap = 0;
         a.ovf_cap = 0;
         a.smem_groups = a.smem_groups > 0;
+        a.dslots = a.dslots > 0;
+        for (int k = 0; k < kMaxKeys; k++) a.dmul[k] = a.dbase[k] = 0;
         for (auto& g : a.aggs) g.vcnt = g.vcnt ? (uint64_t*)1 : nullptr;
         key.append((const char*)&a, sizeof a);
     }
@@ -780,6 +947,7 @@ void* jit_agg_resume_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, c
            "PipeArgs P, const __grid_constant__ AggArgs A, const uint32_t* rows, uint64_t count, int w) {\n";
     src += "    extern __shared__ __align__(16) uint64_t smem[];\n";
     if (smem) src += "    smem_setup(A, smem);\n    __syncthreads();\n";
+    if (A.dslots > 0) src += "    uint32_t* const dsl = direct_slots(A, smem);\n";
     src += g.pre();
     src += "    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;\n";
     src += "    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {\n";
@@ -826,6 +994,23 @@ void* jit_join_insert_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, 
     src += g.body();
     src += "    }\n}\n";
     return (void*)get_kernel(ctx, src, "ml_join_insert");
+}
+
+int jit_resident_blocks(void* fn, unsigned block, size_t smem) {
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<void*, size_t>, int>> memo;
+    std::lock_guard<std::mutex> g(mu);
+    for (auto& e : memo)
+        if (e.first.first == fn && e.first.second == smem) return e.second;
+    Nvrtc& N = nvrtc();
+    if (smem > 48 * 1024 &&
+        N.set_attr((CUfunction)fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem) != CUDA_SUCCESS)
+        raise(ML_ERR_CUDA, "cuFuncSetAttribute failed for a pipeline kernel");
+    int n = 0;
+    if (N.occupancy(&n, (CUfunction)fn, (int)block, smem) != CUDA_SUCCESS || n < 1) n = 1;
+    if (memo.size() >= 256) memo.erase(memo.begin());
+    memo.push_back({{fn, smem}, n});
+    return n;
 }
 
 void jit_launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream_t s, void** args) {

@@ -29,6 +29,8 @@ int jit_rows_per_thread(const PipeArgs& P);
 
 // Launch a specialized kernel with `args` (pointers to the kernel's parameters).
 void jit_launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream_t s, void** args);
+// CTAs of `block` threads with `smem` bytes of dynamic shared memory resident on one SM.
+int jit_resident_blocks(void* fn, unsigned block, size_t smem);
 
 // The generated source of the aggregate kernel (exposed for tests of the generator).
 std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArgs& A);

@@ -13,18 +13,18 @@
 
 namespace mlg {
 
+int num_sms() {
+    static const int sms = [] {
+        int dev = 0, n = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n > 0 ? n : 148;
+    }();
+    return sms;
+}
+
 namespace {
 constexpr int kThreads = 256;
-int g_sms = 0;
-int num_sms() {
-    if (!g_sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-        if (g_sms <= 0) g_sms = 148;
-    }
-    return g_sms;
-}
 int grid_for(int64_t n, int per_sm = 8) {
     int64_t want = (n + kThreads - 1) / kThreads;
     int64_t cap = (int64_t)num_sms() * per_sm;
@@ -1005,8 +1005,12 @@ void* static_filter_scratch() {
 
 // ---- launch wrappers -------------------------------------------------------------------------------
 int pipeline_grid(int64_t n) { return grid_for(n, 8); }
-int agg_smem_bytes(const AggArgs& A) { return (int)((size_t)A.smem_groups * A.stride * 8); }
+int agg_smem_bytes(const AggArgs& A) {
+    return (int)((size_t)A.smem_groups * A.stride * 8 + (size_t)A.priv_groups * A.stride * kThreads * 8 +
+                 agg_direct_bytes(A));
+}
 void launch_agg(const PipeArgs& P, const AggArgs& A, int smem_bytes, cudaStream_t s) {
+    if (smem_bytes > (48 << 10)) cudaFuncSetAttribute(k_agg, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     k_agg<<<grid_for(P.n, 8), kThreads, smem_bytes, s>>>(P, A);
 }
 void launch_agg_resume(const PipeArgs& P, const AggArgs& A, const uint32_t* ctx, uint64_t count, int w, int smem_bytes,

@@ -14,6 +14,7 @@ void launch_agg_resume(const PipeArgs& P, const AggArgs& A, const uint32_t* ctx,
 int agg_smem_bytes(const AggArgs& A);
 // Grid of the row-parallel pipeline kernels for n rows (8 CTAs of 256 threads per SM at most).
 int pipeline_grid(int64_t n);
+int num_sms();  // of the current device
 constexpr int kPipelineThreads = 256;
 void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                        int nwords, uint32_t* err, cudaStream_t s);

@@ -260,6 +260,7 @@ void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrow
         return o;
     };
     L.col_valid.assign(C.slots.size(), 0);
+    L.gid_range.assign(C.slots.size(), {1u, 0u});
     for (size_t i = 0; i < C.slots.size(); i++) {
         const SlotInfo& si = C.slots[i];
         DCol& d = P.cols[i];
@@ -289,6 +290,7 @@ void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrow
                 g[hd.len()] = intern.id(std::string());  // spare entry for clamped codes
             }
             d.dict_len = (uint32_t)hd.len();
+            if (si.src == 0) L.gid_range[i] = {*std::min_element(g.begin(), g.end()), *std::max_element(g.begin(), g.end())};
             gid_at.push_back({(int)i, put(g.data(), g.size() * 4)});
             std::vector<uint32_t> doff(hd.off);
             doff.push_back(hd.off.back());  // the spare entry is the empty string

@@ -60,6 +60,9 @@ class Pipeline {
         DevBuf scratch;
         PipeArgs P{};
         std::vector<int> col_valid;  // slot has a validity bitmap in this launch
+        // dictionary-coded source slots: the least and greatest string id of this batch's
+        // dictionary (clamp entry included); first > second for every other slot
+        std::vector<std::pair<uint32_t, uint32_t>> gid_range;
     };
     // With `tables_dst`, the per-batch tables are copied there (at most `tables_cap` bytes,
     // from pageable memory) instead of into a new device buffer.

@@ -182,6 +182,7 @@ AGG_FLOAT_COLS = (2, 4, 6)  # offsets after the keys: SUM f64, AVG, MAX f64 (MAX
 
 
 @pytest.mark.parametrize("keys", [[(Col(0), INT32)], [(Col(5), UTF8)], [(Col(4), BOOL), (Col(3), DATE)],
+                                  [(Col(5), UTF8), (Col(4), BOOL)],
                                   [(Col(1), INT64), (Col(0), INT32)], [(Cast(Col(2), INT64), INT64)], []])
 def test_hashagg_matches_oracle(gpu_engine, keys):
     rng = np.random.default_rng(4)
@@ -239,7 +240,9 @@ def test_join_probe_pairs_match_oracle(ctx, gpu_engine):
     build = Table("b", ["k", "x"], [[fixed(INT64, bkey[:2500], bvalid[:2500]), fixed(INT32, np.arange(2500))],
                                     [fixed(INT64, bkey[2500:], bvalid[2500:]), fixed(INT32, np.arange(2500, nb))]])
     g = gpu_engine.join_build(build, [INT64, INT32], [(Col(0), INT64)])
-    o = orc.OracleEngine(threads=2).join_build(build, [INT64, INT32], [(Col(0), INT64)])
+    # one oracle thread: its build batch keeps the row groups in order, as the single-threaded
+    # GPU engine's does, so build row ids of both sides index `bkey` the same way
+    o = orc.OracleEngine(threads=1).join_build(build, [INT64, INT32], [(Col(0), INT64)])
     assert g.stats()["build_rows"] == o.stats()["build_rows"] == nb
     assert g.stats()["distinct_keys"] == o.stats()["distinct_keys"]
     pk = rng.integers(-5, 2100, 20_000).astype(np.int64)
@@ -452,3 +455,25 @@ def test_group_by_dense_join_key_checks_membership_per_group(ctx, gpu_engine):
             assert j.stats()["capacity"] <= 4000  # the direct (dense) index
         res[name] = eng.fetch(out)
     assert_same_rows(res["gpu"], res["oracle"], 1, {1, 4})
+
+
+@pytest.mark.parametrize("groups", [3, 20])
+def test_low_cardinality_group_by_every_aggregate(gpu_engine, groups):
+    """Few groups and no NULLs: the first groups take per-thread accumulators in the
+    specialized kernel (the rest shared-memory atomics); every aggregate kind against the oracle."""
+    rng = np.random.default_rng(14 + groups)
+    n = 60_000
+    cols = lambda: [fixed(INT32, rng.integers(0, groups, n).astype(np.int32)), fixed(INT64, rng.integers(-10**6, 10**6, n)),
+                    fixed(FLOAT64, np.round(rng.normal(0, 50, n), 2)), fixed(DATE, rng.integers(9000, 9500, n).astype(np.int32))]
+    t = Table("t", ["g", "i", "f", "d"], [cols() for _ in range(3)])
+    types = [INT32, INT64, FLOAT64, DATE]
+    pro = [Filter(Col(1) > Lit(-900_000))]
+    oracle = orc.OracleEngine(threads=2)
+    for aggs in ([AggSpec(COUNT_STAR), AggSpec(COUNT, Col(2), FLOAT64), AggSpec(SUM, Col(1), INT64),
+                  AggSpec(SUM, Col(2), FLOAT64), AggSpec(AVG, Col(2), FLOAT64), AggSpec(MIN, Col(1), INT64),
+                  AggSpec(MAX, Col(1), INT64)],
+                 [AggSpec(MIN, Col(2), FLOAT64), AggSpec(MAX, Col(2), FLOAT64), AggSpec(MIN, Col(3), DATE),
+                  AggSpec(MAX, Col(3), DATE), AggSpec(COUNT_STAR)]):
+        got = gpu_engine.fetch(gpu_engine.hashagg(t, types, [(Col(0), INT32)], aggs, pro))
+        want = oracle.fetch(oracle.hashagg(t, types, [(Col(0), INT32)], aggs, pro))
+        assert_same_rows(got, want, 1, {4, 5} if len(aggs) == 7 else set())
