@@ -279,6 +279,11 @@ def gpu_arm(args):
         achieved = rows * BYTES_PER_ROW / (per_launch_ms / 1e3) / 1e9
         log("CPU baseline")
         cpu = cpu_baseline(key, fk, d, v) if world == 1 and not args.skip_cpu else None
+        ops = None
+        if world == 1 and not args.skip_ops:
+            log("per-operator throughput")
+            from minilake_b200 import opbench
+            ops = opbench.run(iters=5, log=log)["ops"]
         line = {
             "metric": METRIC,
             "value": value,
@@ -311,6 +316,7 @@ def gpu_arm(args):
                          "algorithmic_bytes_per_launch": rows * BYTES_PER_ROW,
                          "traffic": profiled_traffic() if rows == FACT_ROWS else None},
             "cpu_baseline": cpu,
+            "ops": ops,
             "clocks": clocks,
             "top10_fk": [int(x) for x in top[0].values],
         }
@@ -396,6 +402,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-ops", action="store_true", help="leave out the per-operator throughput lines")
     ap.add_argument("--fact-rows", type=int, default=FACT_ROWS,
                     help="fact rows per GPU (smaller cases are for profiling; the benchmark is 60M)")
     args = ap.parse_args()

@@ -386,7 +386,8 @@ int ml_gpu_card_model_destroy(ml_card_model* m);
 int ml_gpu_kernel_launches(ml_ctx* ctx, uint64_t* count);
 /* With ML_CTX_PROFILE: launches and summed device time (ms, CUDA events) of one kernel
  * family: "pipeline_aggregate" (fused filter/probe/aggregate), "join_insert", "topn",
- * "select" (filter compaction).  Always recorded: "jit_compile" (runtime compilations and
+ * "select" (filter flags and counts), "select_write" (filter compaction), "card_hll"
+ * (cardinality features scan).  Always recorded: "jit_compile" (runtime compilations and
  * their host time), "jit_launch" (launches of runtime-specialized kernels; time 0),
  * "device_alloc" / "pinned_alloc" (cudaMalloc / cudaHostAlloc calls the context made and
  * their host time) and "graph_capture" (CUDA graphs captured and instantiated).

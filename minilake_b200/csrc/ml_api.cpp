@@ -231,7 +231,7 @@ std::unique_ptr<ml_batch> materialize(Ctx* ctx, Pipeline& pipe, const std::vecto
     if (pipe.nstages > 0) {
         CK(cudaMemsetAsync(ew.d.get(), 0, 4, st));
         L.P.err = ew.d.get<uint32_t>();
-        k = run_select(ctx, L.P, idx, st);
+        k = run_select(ctx, pipe, L.P, idx, st);
         rows = idx.get<uint32_t>();
     }
     auto b = std::make_unique<ml_batch>();
@@ -716,7 +716,7 @@ int ml_gpu_filter(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32
     CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
     L.P.err = ew.d.get<uint32_t>();
     DevBuf out;
-    int64_t k = run_select(ctx, L.P, out, s);
+    int64_t k = run_select(ctx, p, L.P, out, s);
     CK(cudaMemcpyAsync(ew.h, ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
     if (k) CK(cudaMemcpyAsync(sel_out, out.get(), (size_t)k * 4,
                               location == ML_LOC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));

@@ -65,6 +65,15 @@ __global__ void __launch_bounds__(256) k_hll(const __grid_constant__ PipeArgs P,
         if (regs[i]) atomicMax(o.regs + i, regs[i]);
 }
 
+// Register-wise max over the CTAs' byte registers (4 per word) -> the u32 registers.
+__global__ void k_hll_merge(const uint32_t* __restrict__ cta_regs, int ctas, uint32_t* regs) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= kHllRegisters / 4) return;
+    uint32_t m = 0;
+    for (int c = 0; c < ctas; c++) m = __vmaxu4(m, __ldg(cta_regs + (size_t)c * (kHllRegisters / 4) + w));
+    for (int b = 0; b < 4; b++) regs[4 * w + b] = (m >> (8 * b)) & 0xFFu;
+}
+
 __global__ void k_dense_fwd(const float* __restrict__ X, int in, const float* __restrict__ W, const float* __restrict__ b,
                             float* __restrict__ Y, int out, int B, int relu) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -163,6 +172,10 @@ void launch_hll(const PipeArgs& P, const KeyLayout& L, HllOut o, cudaStream_t s)
     long long want = (P.n + 255) / 256;
     int grid = (int)(want < 2LL * sms ? (want > 0 ? want : 1) : 2LL * sms);
     k_hll<<<grid, 256, smem, s>>>(P, L, o);
+}
+
+void launch_hll_merge(const uint32_t* cta_regs, int ctas, uint32_t* regs, cudaStream_t s) {
+    k_hll_merge<<<(kHllRegisters / 4 + 255) / 256, 256, 0, s>>>(cta_regs, ctas, regs);
 }
 
 void launch_dense_fwd(const float* X, int in, const float* W, const float* bias, float* Y, int out, int B, bool relu,

@@ -29,6 +29,9 @@ struct HllOut {
     unsigned long long* minmax;    // 2: ~0 and 0 on entry
 };
 void launch_hll(const PipeArgs& P, const KeyLayout& L, HllOut o, cudaStream_t s);
+// Registers of the runtime-specialized scan: max over `ctas` CTAs' byte registers
+// (kHllRegisters / 4 words each) into the u32 registers.
+void launch_hll_merge(const uint32_t* cta_regs, int ctas, uint32_t* regs, cudaStream_t s);
 
 // Y[b][o] = act(bias[o] + sum_i W[o][i] X[b][i]) for b < B.
 void launch_dense_fwd(const float* X, int in, const float* W, const float* bias, float* Y, int out, int B, bool relu,

@@ -5,6 +5,8 @@
 #include <cstring>
 
 #include "ml_api_common.hpp"
+#include "ml_jit.hpp"
+#include "ml_kernels.cuh"
 #include "ml_card.hpp"
 #include "ml_pipeline.hpp"
 
@@ -131,7 +133,26 @@ int ml_gpu_card_features(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int6
     o.nulls = (unsigned long long*)(buf.get<uint8_t>() + kHllRegisters * 4);
     o.minmax = o.nulls + 1;
     CK(cudaMemsetAsync(o.minmax, 0xFF, 8, s));  // min starts at ~0, max at 0
-    launch_hll(La.P, L, o, s);
+    void* jit = jit_hll_kernel(ctx, p, La.P, L);
+    DevBuf cta_regs;
+    {
+        KernelTimer kt(ctx, s, "card_hll");
+        if (jit && La.P.n) {
+            const int smem = kHllRegisters * 4;
+            const int64_t tiles = (La.P.n + 8 * kPipelineThreads - 1) / (8 * kPipelineThreads);
+            const int grid = (int)std::min<int64_t>(tiles, (int64_t)jit_resident_blocks(jit, kPipelineThreads, smem) * num_sms());
+            cta_regs = DevBuf(ctx, (size_t)grid * kHllRegisters, nullptr);
+            uint32_t* cr = cta_regs.get<uint32_t>();
+            void* args[] = {&La.P, &L, &cr, &o.nulls, &o.minmax};
+            jit_launch(jit, grid, kPipelineThreads, smem, s, args);
+            launch_hll_merge(cr, grid, o.regs, s);
+            ctx->add_profile("jit_launch", 0);
+            ctx->count_launch();
+        } else {
+            launch_hll(La.P, L, o, s);
+        }
+        kt.stop();
+    }
     ctx->count_launch();
     std::vector<uint32_t> regs(kHllRegisters);
     uint64_t tail[3];

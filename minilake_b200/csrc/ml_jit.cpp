@@ -213,6 +213,8 @@ class Gen {
     }
     int fresh() { return nv_++; }
 
+    // Rows per thread of the batched form.
+    int rows_per_thread = kRowsPerThread;
     // The row context the generated statements read (x, or x<j> in the batched form), the
     // statement that abandons the current row combination, and preloaded columns.
     std::string x = "x";
@@ -463,7 +465,7 @@ class Gen {
     // The same stages for kRowsPerThread rows x0.. with liveness flags a0..: each stage first
     // loads its columns for every live row, then evaluates (no chains: one match per probe).
     template <class Sink> void batched_stages(Sink&& sink) {
-        const int K = kRowsPerThread;
+        const int K = rows_per_thread;
         auto rows = [&](auto&& f) {
             for (int j = 0; j < K; j++) {
                 x = "x" + num(j);
@@ -569,7 +571,7 @@ class Gen {
 // Batched form applies when no probe walks chains (at most one match per probe row).
 bool batchable(const PipeArgs& P) { return !P.has_chains; }
 
-std::string row_loop(const PipeArgs& P, bool batched, const std::string& body) {
+std::string row_loop(const PipeArgs& P, bool batched, const std::string& body, int K = kRowsPerThread) {
     std::string s;
     if (!batched) {
         s += "    const int64_t stride = (int64_t)gridDim.x * blockDim.x;\n";
@@ -578,7 +580,6 @@ std::string row_loop(const PipeArgs& P, bool batched, const std::string& body) {
         s += P.sel ? "        x.r = __ldg(P.sel + i);\n" : "        x.r = (uint32_t)i;\n";
         s += "        x.b0 = x.b1 = x.b2 = x.b3 = 0;\n        x.head = 0;\n";
     } else {
-        const int K = kRowsPerThread;
         s += "    const int64_t tile = (int64_t)" + num(K) + " * blockDim.x;\n";
         s += "    for (int64_t base = (int64_t)blockIdx.x * tile; base < P.n; base += (int64_t)gridDim.x * tile) {\n";
         for (int j = 0; j < K; j++) {
@@ -994,6 +995,124 @@ void* jit_join_insert_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, 
     src += g.body();
     src += "    }\n}\n";
     return (void*)get_kernel(ctx, src, "ml_join_insert");
+}
+
+void* jit_select_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P) {
+    if (!jit_enabled(ctx) || !batchable(P)) return nullptr;
+    return memoized(pipe, signature('s', P, nullptr, nullptr) + std::string((const char*)&ctx->device, sizeof(int)),
+                    [&] { return (void*)get_kernel(ctx, jit_select_source(pipe, P), "ml_select_flags"); });
+}
+
+std::string jit_select_source(const Pipeline& pipe, const PipeArgs& P) {
+    {
+        // Pass bits and per-chunk pass counts of 2048-row chunks (the layout of the ahead-of-time
+        // k_select_flags), 8 rows per thread with every chunk's loads issued together.  CTAs stride
+        // over the chunks; each warp adds its count to the chunk's (zeroed) counter.
+        Gen g(pipe.C.code, P);
+        g.rows_per_thread = 8;
+        g.fail = "break;";
+        g.batched_stages([&](auto&&) {});
+        const int K = g.rows_per_thread;
+        std::string src = kPrelude;
+        src += "extern \"C\" __global__ void __launch_bounds__(256) ml_select_flags(const __grid_constant__ PipeArgs P, "
+               "uint32_t* bits, uint32_t* chunk_counts) {\n";
+        src += g.pre();
+        src += "    const int lane = threadIdx.x & 31;\n";
+        src += "    const int64_t chunks = (P.n + 2047) / 2048;\n";
+        src += "    for (int64_t c = blockIdx.x; c < chunks; c += gridDim.x) {\n";
+        src += "        const int64_t base = c * 2048;\n";
+        for (int j = 0; j < K; j++) {
+            std::string J = num(j), x = "x" + J, a = "a" + J;
+            src += "        RowCtx " + x + ";\n";
+            src += "        const int64_t i" + J + " = base + " + J + " * 256 + threadIdx.x;\n";
+            src += "        bool " + a + " = i" + J + " < P.n;\n";
+            src += "        " + x + ".r = " + a + " ? " + (P.sel ? "__ldg(P.sel + i" + J + ")" : "(uint32_t)i" + J) + " : 0u;\n";
+            src += "        " + x + ".b0 = " + x + ".b1 = " + x + ".b2 = " + x + ".b3 = 0;\n";
+            src += "        " + x + ".head = 0;\n";
+        }
+        src += g.body();
+        src += "        uint32_t cnt = 0;\n";
+        for (int j = 0; j < K; j++) {
+            std::string J = num(j);
+            src += "        {\n            const uint32_t b = __ballot_sync(0xFFFFFFFFu, a" + J + ");\n";
+            src += "            const int64_t w0 = base + " + J + " * 256 + (threadIdx.x & ~31);\n";
+            src += "            if (lane == 0 && w0 < P.n) bits[w0 >> 5] = b;\n";
+            src += "            cnt += __popc(b);\n        }\n";
+        }
+        src += "        if (lane == 0 && cnt) atomicAdd(chunk_counts + c, cnt);\n";
+        src += "        __syncwarp();\n";
+        src += "    }\n}\n";
+        return src;
+    }
+}
+
+void* jit_hll_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L) {
+    if (!jit_enabled(ctx) || !batchable(P)) return nullptr;
+    std::string key = signature('h', P, nullptr, &L) + std::string((const char*)&ctx->device, sizeof(int));
+    return memoized(pipe, key, [&] { return (void*)get_kernel(ctx, jit_hll_source(pipe, P, L), "ml_card_hll"); });
+}
+
+std::string jit_hll_source(const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L) {
+    {
+        // The cardinality features scan: every row's key hashed into 2^14 HyperLogLog registers
+        // privatized in shared memory, NULL count and the first key word's range; each CTA
+        // leaves its registers as bytes in cta_regs[blockIdx.x][4096 words] for the merge kernel.
+        Gen g(pipe.C.code, P);
+        g.rows_per_thread = 8;
+        g.fail = "break;";
+        g.batched_stages([&](auto&& rows) {
+            std::set<int> slots;
+            for (int k = 0; k < L.nkeys; k++) g.slots_of(L.prog[k], slots);
+            std::vector<std::map<int, Gen::V>> pre(g.rows_per_thread);
+            rows([&](int j, const std::string& a) {
+                g.cols.clear();
+                g.preload(slots, a);
+                pre[j] = g.cols;
+            });
+            rows([&](int j, const std::string& a) {
+                g.cols = pre[j];
+                g.open("if (" + a + ") {  // key " + num(j));
+                g.line("uint64_t wk[2] = {0ull, 0ull};");
+                g.line("uint32_t nmk = 0;");
+                g.key(L, "wk", "", "nmk");
+                g.open("if (nmk) {");
+                g.line("nulls++;");
+                g.close("} else {");
+                g.open("");
+                g.line("lo = wk[0] < lo ? wk[0] : lo;");
+                g.line("hi = wk[0] > hi ? wk[0] : hi;");
+                g.close();
+                g.line("const uint64_t h = hll_mix(key_hash(wk, " + num(L.nwords) + ", nmk));");
+                g.line("const uint64_t rest = (h << 14) | (1ull << 13);  // guard bit: rank <= 51");
+                g.line("atomicMax(&regs[(uint32_t)(h >> 50)], (uint32_t)__clzll((long long)rest) + 1u);");
+                g.close();
+            });
+            g.cols.clear();
+        });
+        std::string src = kPrelude;
+        src += "// MurmurHash3's 64-bit finalizer (fmix64) over the engine's key hash.\n";
+        src += "__device__ __forceinline__ uint64_t hll_mix(uint64_t k) {\n"
+               "    k ^= k >> 33;\n    k *= 0xff51afd7ed558ccdull;\n    k ^= k >> 33;\n"
+               "    k *= 0xc4ceb9fe1a85ec53ull;\n    k ^= k >> 33;\n    return k;\n}\n";
+        src += "extern \"C\" __global__ void __launch_bounds__(256) ml_card_hll(const __grid_constant__ PipeArgs P, "
+               "const __grid_constant__ KeyLayout L, uint32_t* cta_regs, unsigned long long* nulls_out, "
+               "unsigned long long* minmax) {\n";
+        src += "    extern __shared__ uint32_t regs[];\n";
+        src += "    for (int i = threadIdx.x; i < 16384; i += blockDim.x) regs[i] = 0;\n    __syncthreads();\n";
+        src += "    unsigned long long nulls = 0, lo = ~0ull, hi = 0;\n";
+        src += g.pre();
+        src += row_loop(P, true, g.body(), g.rows_per_thread);
+        src += "    for (int o = 16; o; o >>= 1) {\n"
+               "        nulls += __shfl_xor_sync(0xFFFFFFFFu, nulls, o);\n"
+               "        const unsigned long long l2 = __shfl_xor_sync(0xFFFFFFFFu, lo, o), h2 = __shfl_xor_sync(0xFFFFFFFFu, hi, o);\n"
+               "        lo = l2 < lo ? l2 : lo;\n        hi = h2 > hi ? h2 : hi;\n    }\n";
+        src += "    if ((threadIdx.x & 31) == 0) {\n        if (nulls) atomicAdd(nulls_out, nulls);\n"
+               "        if (lo != ~0ull) atomicMin(minmax, lo);\n        if (hi) atomicMax(minmax + 1, hi);\n    }\n";
+        src += "    __syncthreads();\n    uint32_t* dst = cta_regs + (uint64_t)blockIdx.x * 4096;\n";
+        src += "    for (int w = threadIdx.x; w < 4096; w += blockDim.x)\n"
+               "        dst[w] = regs[4 * w] | (regs[4 * w + 1] << 8) | (regs[4 * w + 2] << 16) | (regs[4 * w + 3] << 24);\n}\n";
+        return src;
+    }
 }
 
 int jit_resident_blocks(void* fn, unsigned block, size_t smem) {

@@ -22,6 +22,15 @@ void* jit_agg_resume_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, c
 
 // Specialized join-build insert kernel (signature of k_join_insert), or nullptr.
 void* jit_join_insert_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L);
+// Filter pass bits and per-CTA counts (the layout of launch_select_flags), or nullptr when the
+// pipeline has duplicate-key probes or specialization is off.  Arguments: P, bits, block_counts.
+void* jit_select_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P);
+// Cardinality features scan of the key layout L (64 KB of dynamic shared memory per CTA).
+// Arguments: P, L, cta_regs (gridDim x 4096 words), nulls, minmax.
+void* jit_hll_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L);
+// Sources of the kernels above.
+std::string jit_select_source(const Pipeline& pipe, const PipeArgs& P);
+std::string jit_hll_source(const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L);
 
 // Rows one thread of the specialized aggregate kernel handles per iteration (its grid
 // needs n / rows-per-thread threads).

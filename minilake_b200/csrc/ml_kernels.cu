@@ -363,13 +363,16 @@ __global__ void __launch_bounds__(kThreads) k_index_write(int64_t n, const uint3
         if (lane == 0) warp_tot[it * (kThreads / 32) + warp] = __popc(w[it]);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {  // exclusive scan over the 64 words in row order
-        uint32_t s = 0;
-        for (int k = 0; k < 8 * (kThreads / 32); k++) {
-            uint32_t t = warp_tot[k];
-            warp_tot[k] = s;
-            s += t;
+    static_assert(8 * (kThreads / 32) == 64, "two words per lane in the scan below");
+    if (warp == 0) {  // exclusive scan over the 64 words in row order, two per lane
+        const uint32_t a = warp_tot[2 * lane], b = warp_tot[2 * lane + 1];
+        uint32_t x = a + b;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= o) x += y;
         }
+        warp_tot[2 * lane] = x - a - b;
+        warp_tot[2 * lane + 1] = x - b;
     }
     __syncthreads();
     uint64_t off = block_offsets[blockIdx.x];

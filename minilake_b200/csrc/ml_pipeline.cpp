@@ -1,5 +1,6 @@
 // Pipeline construction and per-launch preparation.
 #include "ml_pipeline.hpp"
+#include "ml_jit.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -351,20 +352,37 @@ uint64_t scan_counts(Ctx* ctx, const uint32_t* counts, int64_t n, DevBuf& offset
     return total;
 }
 
-int64_t run_select(Ctx* ctx, const PipeArgs& P, DevBuf& out, cudaStream_t s) {
+int64_t run_select(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, DevBuf& out, cudaStream_t s) {
     int nb = select_blocks(P.n);
     DevBuf bits(ctx, std::max<size_t>((size_t)(P.n + 31) / 32 * 4, 4), nullptr);
     DevBuf counts(ctx, std::max<size_t>((size_t)nb * 4, 4), nullptr);
     {
+        void* jit = jit_select_kernel(ctx, pipe, P);
         KernelTimer kt(ctx, s, "select");
-        launch_select_flags(P, bits.get<uint32_t>(), counts.get<uint32_t>(), s);
+        if (jit) {
+            if (nb) {
+                uint32_t* b = bits.get<uint32_t>();
+                uint32_t* c = counts.get<uint32_t>();
+                CK(cudaMemsetAsync(c, 0, (size_t)nb * 4, s));
+                void* args[] = {(void*)&P, &b, &c};
+                const int grid = std::min<int64_t>(nb, (int64_t)jit_resident_blocks(jit, kPipelineThreads, 0) * num_sms());
+                jit_launch(jit, grid, kPipelineThreads, 0, s, args);
+            }
+            ctx->add_profile("jit_launch", 0);
+        } else {
+            launch_select_flags(P, bits.get<uint32_t>(), counts.get<uint32_t>(), s);
+        }
         kt.stop();
     }
     ctx->count_launch();
     DevBuf offs;
     uint64_t total = scan_counts(ctx, counts.get<uint32_t>(), nb, offs, s);
     out = DevBuf(ctx, std::max<size_t>(total * 4, 4), nullptr);
-    launch_select_write(P, bits.get<uint32_t>(), offs.get<uint64_t>(), out.get<uint32_t>(), s);
+    {
+        KernelTimer kt(ctx, s, "select_write");
+        launch_select_write(P, bits.get<uint32_t>(), offs.get<uint64_t>(), out.get<uint32_t>(), s);
+        kt.stop();
+    }
     ctx->count_launch();
     CK(cudaStreamSynchronize(s));
     return (int64_t)total;

@@ -74,7 +74,7 @@ class Pipeline {
 
 // Ordered selection of the rows where all of the pipeline's stages pass (no probes).
 // Returns the number of selected rows; `out` holds them (device).
-int64_t run_select(Ctx* ctx, const PipeArgs& P, DevBuf& out, cudaStream_t s);
+int64_t run_select(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, DevBuf& out, cudaStream_t s);
 
 // Exclusive scan helper (device u32 counts -> u64 offsets incl. total); returns the total.
 uint64_t scan_counts(Ctx* ctx, const uint32_t* counts, int64_t n, DevBuf& offsets, cudaStream_t s);

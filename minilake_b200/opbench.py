@@ -1,0 +1,190 @@
+"""Per-operator device throughput: rows/s and HBM GB/s of each hot operator, on tables in HBM.
+
+Each operator runs on seeded synthetic tables generated on the device (the shapes of the
+benchmark queries), twice untimed, then `--iters` times with its kernels timed by CUDA events
+on the launching stream (the library's profile counters).  GB/s counts ALGORITHMIC bytes: the
+bytes an operator must move per row, stated with each operator below; a value near the
+measured copy bandwidth means the kernel is at the HBM roofline.
+
+    filter           WHERE d <= 2467 over 100M rows -> selection vector.  Flags pass: 4 B/row read
+                     (d) + 1 bit/row written; compaction: 1 bit/row read + 4 B per selected row.
+    filter_groupby   WHERE d <= 2467 GROUP BY two dictionary strings, SUM, SUM(x*(1-y)), AVG,
+                     COUNT(*) over 100M rows: 36 B/row (d 4, two dict codes 4+4, three f64 24).
+    join_groupby     d > 1200, probe of the dense join index on fk (1.5M distinct keys),
+                     GROUP BY fk SUM(v) COUNT(*) over 60M rows: 20 B/row (fk 8, d 4, v 8).
+    join_build       1.5M distinct i64 keys -> dense join index: 8 B/row read + 4 B/row index.
+    topn             ORDER BY v DESC LIMIT 10 over 60M f64 values: 8 B/row.
+    card_features    HyperLogLog scan of a 60M-row i64 key column: 8 B/row.
+
+    python -m minilake_b200.opbench [--iters 5] [--rows-filter 100000000] [--rows-join 60000000]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import AggSpec, Col, COUNT_STAR, FLOAT64, INT32, INT64, Lit, SortKey, SUM
+
+
+def measured_hbm_gbs() -> float:
+    """The measured HBM copy bandwidth (GB/s) on this machine's GPUs, else the fallback figure."""
+    p = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
+
+
+def _timed(ctx, keys, fn, iters):
+    """Run fn twice untimed, then `iters` times; mean device ms per run of the kernels in `keys`."""
+    for _ in range(2):
+        fn()
+    for k in keys:
+        ctx.profile(k, reset=True)
+    out = None
+    for _ in range(iters):
+        out = fn()
+    ms = {k: ctx.profile(k, reset=True)[1] / iters for k in keys}
+    return ms, out
+
+
+def _line(rows, ms, nbytes, peak):
+    gbs = nbytes / (ms * 1e6) if ms > 0 else 0.0
+    return {"rows": int(rows), "ms": round(ms, 4), "rows_per_s": rows / (ms * 1e-3) if ms > 0 else 0.0,
+            "algorithmic_bytes": int(nbytes), "gbs": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 3)}
+
+
+def run(iters: int = 5, rows_filter: int = 100_000_000, rows_join: int = 60_000_000, dim_rows: int = 1_500_000,
+        seed: int = 1234, log=print):
+    import torch
+
+    from . import serving, workloads
+    from .gpu import LIB, PROFILE, Context, HashAggregateSink, JoinBuildSink, SortSink, _check, card_features
+
+    ctx = Context(0, flags=PROFILE)
+    peak = measured_hbm_gbs()
+    res = {}
+
+    # ---- filter and filter + low-cardinality GROUP BY ------------------------------------
+    t0 = serving.gen_fact(0, rows_filter, seed)
+    keep = abi.Keep()
+    pred = abi.encode_expr(Col(0) <= Lit(2467), abi.BOOL, keep)
+    arr, nc, n = t0.ml
+    sel = torch.empty(n, dtype=torch.int32, device="cuda")
+    k = C.c_int64()
+
+    def filt():
+        _check(LIB.ml_gpu_filter(ctx.h, C.byref(pred), arr, nc, n, None, 0, abi.LOC_DEVICE,
+                                 C.c_void_p(sel.data_ptr()), C.byref(k)))
+        return k.value
+
+    ms, nsel = _timed(ctx, ("select", "select_write"), filt, iters)
+    tot = ms["select"] + ms["select_write"]
+    res["filter"] = _line(n, tot, 4 * n + n / 8 + n / 8 + 4 * nsel, peak)
+    res["filter"]["selected"] = int(nsel)
+    res["filter"]["flags_ms"], res["filter"]["compact_ms"] = round(ms["select"], 4), round(ms["select_write"], 4)
+    log(f"filter: {res['filter']}")
+
+    prologue, group, aggs = workloads.filter_groupby_plan(2467)
+
+    def fg():
+        sink = HashAggregateSink(ctx, t0.types, group, aggs, prologue)
+        loc = sink.create_local()
+        loc.sink(t0.ml)
+        loc.combine()
+        out = sink.finalize()
+        g = out.num_rows
+        out.close()
+        sink.close()
+        return g
+
+    ms, groups = _timed(ctx, ("pipeline_aggregate",), fg, iters)
+    res["filter_groupby"] = _line(n, ms["pipeline_aggregate"], 36 * n, peak)
+    res["filter_groupby"]["groups"] = int(groups)
+    log(f"filter_groupby: {res['filter_groupby']}")
+    del t0, sel
+    torch.cuda.empty_cache()
+
+    # ---- join build, join + high-cardinality GROUP BY, top-N, cardinality features ----------
+    t1 = serving.gen_fact(1, rows_join, seed + 1, dim_rows=dim_rows)
+    dim = serving.DeviceTable([(INT64, torch.arange(1, dim_rows + 1, device="cuda", dtype=torch.int64), None)])
+
+    def build():
+        j = JoinBuildSink(ctx, [INT64], [(Col(0), INT64)])
+        loc = j.create_local()
+        loc.sink(dim.ml)
+        loc.combine()
+        j.finalize()
+        return j
+
+    joins = []
+    ms, _ = _timed(ctx, ("join_insert",), lambda: joins.append(build()), iters)
+    res["join_build"] = _line(dim_rows, ms["join_insert"], 12 * dim_rows, peak)
+    log(f"join_build: {res['join_build']}")
+    j = joins[-1]
+    for other in joins[:-1]:
+        other.close()
+
+    jp, jg, ja = workloads.join_groupby_plan(j.handle, 1200)
+
+    def jgb():
+        sink = HashAggregateSink(ctx, t1.types, jg, ja, jp, size_hint=dim_rows)
+        loc = sink.create_local()
+        loc.sink(t1.ml)
+        loc.combine()
+        out = sink.finalize()
+        g = out.num_rows
+        out.close()
+        sink.close()
+        return g
+
+    ms, groups = _timed(ctx, ("pipeline_aggregate",), jgb, iters)
+    res["join_groupby"] = _line(rows_join, ms["pipeline_aggregate"], 20 * rows_join, peak)
+    res["join_groupby"]["groups"] = int(groups)
+    log(f"join_groupby: {res['join_groupby']}")
+    j.close()
+
+    v_only = serving.DeviceTable([(FLOAT64, t1.keep[2][1], None)])
+
+    def topn():
+        ts = SortSink(ctx, [FLOAT64], [SortKey(Col(0), FLOAT64, asc=False)], 10)
+        loc = ts.create_local()
+        loc.sink(v_only.ml)
+        loc.combine()
+        out = ts.finalize()
+        m = out.num_rows
+        out.close()
+        ts.close()
+        return m
+
+    ms, _ = _timed(ctx, ("topn",), topn, iters)
+    res["topn"] = _line(rows_join, ms["topn"], 8 * rows_join, peak)
+    log(f"topn: {res['topn']}")
+
+    ms, (_, est) = _timed(ctx, ("card_hll",), lambda: card_features(ctx, t1.ml, [(Col(0), INT64)]), iters)
+    res["card_features"] = _line(rows_join, ms["card_hll"], 8 * rows_join, peak)
+    res["card_features"]["hll_estimate"] = round(float(est))
+    log(f"card_features: {res['card_features']}")
+    ctx.close()
+    return {"peak_gbs": peak, "ops": res}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--iters", type=int, default=5)
+    ap.add_argument("--rows-filter", type=int, default=100_000_000)
+    ap.add_argument("--rows-join", type=int, default=60_000_000)
+    a = ap.parse_args()
+    import sys
+    out = run(a.iters, a.rows_filter, a.rows_join, log=lambda *m: print(*m, file=sys.stderr, flush=True))
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()
