@@ -97,6 +97,15 @@ __device__ __forceinline__ uint64_t ld_stream_u64(const void* a) {
     asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
     return v;
 }
+// Consecutive values of a streamed column in one 16-byte load (16-byte aligned address).
+__device__ __forceinline__ void ld_stream_v4_u32(const void* a, uint32_t* v) {
+    asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+        : "l"(a), "l"(l2_evict_first()));
+}
+__device__ __forceinline__ void ld_stream_v2_u64(const void* a, uint64_t* v) {
+    asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(v[0]), "=l"(v[1]) : "l"(a), "l"(l2_evict_first()));
+}
 __device__ __forceinline__ uint32_t ld_stream_u8(const void* a) {
     uint16_t v;
     asm("ld.global.nc.L2::cache_hint.u8 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(l2_evict_first()));

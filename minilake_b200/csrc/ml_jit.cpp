@@ -213,8 +213,11 @@ class Gen {
     }
     int fresh() { return nv_++; }
 
-    // Rows per thread of the batched form.
+    // Rows per thread of the batched form, and whether a thread's rows are consecutive
+    // (x<j>.r = r0 + j, `full` when all are in range): then the source columns of the rows are
+    // read with vector loads, one validity word per thread.
     int rows_per_thread = kRowsPerThread;
+    bool contig = false;
     // The row context the generated statements read (x, or x<j> in the batched form), the
     // statement that abandons the current row combination, and preloaded columns.
     std::string x = "x";
@@ -265,6 +268,90 @@ class Gen {
             line(k + " = " + col_valid(a) + ";");
             close();
             cols[a] = V{v, k};
+        }
+    }
+
+    // Load `slots` for the batched rows x0.. (alive a0..) into pre[j].  With consecutive rows a
+    // fixed-width or dictionary-coded source column is read with one vector load per thread when
+    // all its rows are in range, its validity with one word.
+    void preload_rows(const std::set<int>& slots, std::vector<std::map<int, V>>& pre) {
+        const int K = rows_per_thread;
+        pre.assign(K, {});
+        auto per_row = [&](const std::set<int>& sl) {
+            for (int j = 0; j < K; j++) {
+                x = "x" + num(j);
+                cols.clear();
+                preload(sl, "a" + num(j));
+                for (auto& e : cols) pre[j][e.first] = e.second;
+            }
+            x = "x";
+            cols.clear();
+        };
+        if (!contig) {
+            per_row(slots);
+            return;
+        }
+        std::string any = "(";
+        for (int j = 0; j < K; j++) any += (j ? " || a" : "a") + num(j);
+        any += ")";
+        for (int a : slots) {
+            const DCol& c = P_.cols[a];
+            const bool vec = c.src == 0 && (c.kind == CK_FIXED || c.kind == CK_DICT);
+            if (!vec) {
+                per_row({a});
+                continue;
+            }
+            const int W = c.kind == CK_DICT ? 4 : (c.dt == ML_TYPE_BOOL ? 1 : (c.dt == ML_TYPE_INT32 || c.dt == ML_TYPE_DATE) ? 4 : 8);
+            const std::string n = num(fresh()), C = "P.cols[" + num(a) + "]", t = "t" + n;
+            for (int j = 0; j < K; j++) {
+                line("uint64_t c" + n + "_" + num(j) + " = 0;");
+                line("bool n" + n + "_" + num(j) + " = false;");
+            }
+            open("if (full && " + any + ") {");
+            if (W == 4) {  // 16-byte loads (the widest this toolchain's runtime compiler accepts)
+                line("uint32_t " + t + "[" + num(K) + "];");
+                for (int q = 0; q < K; q += 4)
+                    line("ld_stream_v4_u32((const uint32_t*)" + C + ".data + x0.r + " + num(q) + ", " + t + " + " + num(q) +
+                         ");");
+            } else if (W == 8) {
+                line("uint64_t " + t + "[" + num(K) + "];");
+                for (int q = 0; q < K; q += 2)
+                    line("ld_stream_v2_u64((const unsigned long long*)" + C + ".data + x0.r + " + num(q) + ", " + t + " + " +
+                         num(q) + ");");
+            } else {
+                line(std::string("const uint64_t ") + t + " = " +
+                     (K == 8 ? "ld_stream_u64((const unsigned long long*)(" : "(uint64_t)ld_stream_u32((const uint32_t*)(") +
+                     "(const uint8_t*)" + C + ".data + x0.r));");
+            }
+            for (int j = 0; j < K; j++) {
+                const std::string J = num(j), v = "c" + n + "_" + J;
+                if (c.kind == CK_DICT)
+                    line(v + " = (uint64_t)__ldg(" + C + ".gid + (" + t + "[" + J + "] < " + C + ".dict_len ? " + t + "[" + J +
+                         "] : " + C + ".dict_len));");
+                else if (W == 4)
+                    line(v + " = (uint64_t)(int64_t)(int32_t)" + t + "[" + J + "];");
+                else if (W == 8)
+                    line(v + " = " + t + "[" + J + "];");
+                else
+                    line(v + " = (" + t + " >> " + num(8 * j) + ") & 0xFFull;");
+            }
+            close("} else {");
+            ind_++;
+            for (int j = 0; j < K; j++) {
+                x = "x" + num(j);
+                line("if (a" + num(j) + ") c" + n + "_" + num(j) + " = " + col_value(a) + ";");
+            }
+            x = "x";
+            close();
+            if (c.valid) {
+                line("const uint64_t w" + n + " = " + any + " ? __ldg(" + C + ".valid + (x0.r >> 6)) : 0ull;");
+                for (int j = 0; j < K; j++)
+                    line("n" + n + "_" + num(j) + " = a" + num(j) + " && ((w" + n + " >> ((x0.r & 63u) + " + num(j) +
+                         "u)) & 1ull);");
+            } else {
+                for (int j = 0; j < K; j++) line("n" + n + "_" + num(j) + " = a" + num(j) + ";");
+            }
+            for (int j = 0; j < K; j++) pre[j][a] = V{"c" + n + "_" + num(j), "n" + n + "_" + num(j)};
         }
     }
 
@@ -478,12 +565,8 @@ class Gen {
             std::set<int> slots;
             if (st.kind == 0) {
                 slots_of(P_.filters[st.idx], slots);
-                std::vector<std::map<int, V>> pre(K);
-                rows([&](int j, const std::string& a) {
-                    cols.clear();
-                    preload(slots, a);
-                    pre[j] = cols;
-                });
+                std::vector<std::map<int, V>> pre;
+                preload_rows(slots, pre);
                 rows([&](int j, const std::string& a) {
                     cols = pre[j];
                     open("if (" + a + ") {  // filter " + num(st.idx));
@@ -497,12 +580,8 @@ class Gen {
             const ProbeDev& pd = P_.probes[st.idx];
             const std::string p = num(st.idx);
             for (int k = 0; k < pd.keys.nkeys; k++) slots_of(pd.keys.prog[k], slots);
-            std::vector<std::map<int, V>> pre(K);
-            rows([&](int j, const std::string& a) {
-                cols.clear();
-                preload(slots, a);
-                pre[j] = cols;
-            });
+            std::vector<std::map<int, V>> pre;
+            preload_rows(slots, pre);
             if (pd.dense) {  // direct index: one 4-byte load per row, issued for every row first
                 rows([&](int j, const std::string& a) {
                     cols = pre[j];
@@ -571,7 +650,43 @@ class Gen {
 // Batched form applies when no probe walks chains (at most one match per probe row).
 bool batchable(const PipeArgs& P) { return !P.has_chains; }
 
-std::string row_loop(const PipeArgs& P, bool batched, const std::string& body, int K = kRowsPerThread) {
+// Declarations of the batched rows x0.. / a0.. of the tile at `base`: strided (x<j>.r = base +
+// j * 256 + thread) or, with `contig`, consecutive (x<j>.r = r0 + j, r0 = base + K * thread, and
+// `full` when all K are rows).
+std::string tile_rows(const PipeArgs& P, int K, bool contig, const std::string& ind) {
+    std::string s;
+    if (contig) {
+        s += ind + "const int64_t r0 = base + (int64_t)threadIdx.x * " + num(K) + ";\n";
+        s += ind + "const bool full = r0 + " + num(K) + " <= P.n;\n";
+    }
+    for (int j = 0; j < K; j++) {
+        std::string J = num(j), x = "x" + J, a = "a" + J;
+        s += ind + "RowCtx " + x + ";\n";
+        if (contig) {
+            s += ind + "bool " + a + " = r0 + " + J + " < P.n;\n";
+            s += ind + x + ".r = (uint32_t)(r0 + " + J + ");\n";
+        } else {
+            s += ind + "const int64_t i" + J + " = base + " + J + " * (int64_t)blockDim.x + threadIdx.x;\n";
+            s += ind + "bool " + a + " = i" + J + " < P.n;\n";
+            s += ind + x + ".r = " + a + " ? " + (P.sel ? "__ldg(P.sel + i" + J + ")" : "(uint32_t)i" + J) + " : 0u;\n";
+        }
+        s += ind + x + ".b0 = " + x + ".b1 = " + x + ".b2 = " + x + ".b3 = 0;\n";
+        s += ind + x + ".head = 0;\n";
+    }
+    return s;
+}
+
+// Consecutive rows per thread need no selection vector and every fixed-width or dictionary
+// source column aligned to 16 bytes (the vector loads' width).
+bool contig_ok(const PipeArgs& P) {
+    if (P.sel) return false;
+    for (const DCol& c : P.cols)
+        if (c.src == 0 && (c.kind == CK_FIXED || c.kind == CK_DICT) && ((uintptr_t)c.data & 15)) return false;
+    return true;
+}
+
+std::string row_loop(const PipeArgs& P, bool batched, const std::string& body, int K = kRowsPerThread,
+                     bool contig = false) {
     std::string s;
     if (!batched) {
         s += "    const int64_t stride = (int64_t)gridDim.x * blockDim.x;\n";
@@ -582,15 +697,7 @@ std::string row_loop(const PipeArgs& P, bool batched, const std::string& body, i
     } else {
         s += "    const int64_t tile = (int64_t)" + num(K) + " * blockDim.x;\n";
         s += "    for (int64_t base = (int64_t)blockIdx.x * tile; base < P.n; base += (int64_t)gridDim.x * tile) {\n";
-        for (int j = 0; j < K; j++) {
-            std::string J = num(j), x = "x" + J, a = "a" + J;
-            s += "        RowCtx " + x + ";\n";
-            s += "        const int64_t i" + J + " = base + " + J + " * (int64_t)blockDim.x + threadIdx.x;\n";
-            s += "        bool " + a + " = i" + J + " < P.n;\n";
-            s += "        " + x + ".r = " + a + " ? " + (P.sel ? "__ldg(P.sel + i" + J + ")" : "(uint32_t)i" + J) + " : 0u;\n";
-            s += "        " + x + ".b0 = " + x + ".b1 = " + x + ".b2 = " + x + ".b3 = 0;\n";
-            s += "        " + x + ".head = 0;\n";
-        }
+        s += tile_rows(P, K, contig, "        ");
     }
     s += body;
     // Batched tiles have the same trip count in every lane: reconverge the warp once per tile,
@@ -811,10 +918,11 @@ const char* kPrelude = "#include \"ml_agg.cuh\"\nusing namespace mlg;\n";
 
 }  // namespace
 
-std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {
+std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArgs& A, bool contig) {
     Gen g(pipe.C.code, P);
     const bool smem = A.smem_groups > 0;
     const bool batched = batchable(P);
+    g.contig = contig && batched;
     if (batched) {
         g.fail = "break;";
         g.batched_stages([&](auto&& rows) {
@@ -823,12 +931,8 @@ std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArg
                 for (int k = 0; k < A.keys.nkeys; k++) g.slots_of(A.keys.prog[k], slots);
             for (int k = 0; k < A.nagg; k++)
                 if (A.aggs[k].has_arg && A.aggs[k].func != ML_AGG_COUNT_STAR) g.slots_of(A.aggs[k].arg, slots);
-            std::vector<std::map<int, Gen::V>> pre(kRowsPerThread);
-            rows([&](int j, const std::string& a) {
-                g.cols.clear();
-                g.preload(slots, a);
-                pre[j] = g.cols;
-            });
+            std::vector<std::map<int, Gen::V>> pre;
+            g.preload_rows(slots, pre);
             rows([&](int j, const std::string& a) {
                 g.cols = pre[j];
                 g.open("if (" + a + ") do {  // aggregate");
@@ -852,7 +956,7 @@ std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArg
     if (A.dslots > 0) src += "    uint32_t* const dsl = direct_slots(A, smem);\n";
     if (A.priv_groups > 0) src += priv_init(A);
     src += g.pre();
-    src += row_loop(P, batched, g.body());
+    src += row_loop(P, batched, g.body(), kRowsPerThread, g.contig);
     if (smem) src += "    __syncthreads();\n    smem_flush(A, smem);\n";
     if (A.priv_groups > 0) src += priv_flush(A);
     src += "}\n";
@@ -929,9 +1033,10 @@ void* memoized(const Pipeline& pipe, std::string key, Make make) {
 
 void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {
     if (!jit_enabled(ctx)) return nullptr;
-    return memoized(pipe, signature('a', P, &A, nullptr) + std::string((const char*)&ctx->device, sizeof(int)), [&] {
-        return (void*)get_kernel(ctx, jit_agg_source(pipe, P, A), "ml_pipeline_aggregate");
-    });
+    const bool contig = batchable(P) && contig_ok(P);
+    return memoized(pipe, signature('a', P, &A, nullptr) + std::string((const char*)&ctx->device, sizeof(int)) +
+                              (contig ? "c" : "s"),
+                    [&] { return (void*)get_kernel(ctx, jit_agg_source(pipe, P, A, contig), "ml_pipeline_aggregate"); });
 }
 
 void* jit_agg_resume_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {
@@ -999,17 +1104,20 @@ void* jit_join_insert_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, 
 
 void* jit_select_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P) {
     if (!jit_enabled(ctx) || !batchable(P)) return nullptr;
-    return memoized(pipe, signature('s', P, nullptr, nullptr) + std::string((const char*)&ctx->device, sizeof(int)),
-                    [&] { return (void*)get_kernel(ctx, jit_select_source(pipe, P), "ml_select_flags"); });
+    const bool contig = contig_ok(P);
+    return memoized(pipe, signature('s', P, nullptr, nullptr) + std::string((const char*)&ctx->device, sizeof(int)) +
+                              (contig ? "c" : "s"),
+                    [&] { return (void*)get_kernel(ctx, jit_select_source(pipe, P, contig), "ml_select_flags"); });
 }
 
-std::string jit_select_source(const Pipeline& pipe, const PipeArgs& P) {
+std::string jit_select_source(const Pipeline& pipe, const PipeArgs& P, bool contig) {
     {
         // Pass bits and per-chunk pass counts of 2048-row chunks (the layout of the ahead-of-time
         // k_select_flags), 8 rows per thread with every chunk's loads issued together.  CTAs stride
         // over the chunks; each warp adds its count to the chunk's (zeroed) counter.
         Gen g(pipe.C.code, P);
         g.rows_per_thread = 8;
+        g.contig = contig;
         g.fail = "break;";
         g.batched_stages([&](auto&&) {});
         const int K = g.rows_per_thread;
@@ -1021,23 +1129,29 @@ std::string jit_select_source(const Pipeline& pipe, const PipeArgs& P) {
         src += "    const int64_t chunks = (P.n + 2047) / 2048;\n";
         src += "    for (int64_t c = blockIdx.x; c < chunks; c += gridDim.x) {\n";
         src += "        const int64_t base = c * 2048;\n";
-        for (int j = 0; j < K; j++) {
-            std::string J = num(j), x = "x" + J, a = "a" + J;
-            src += "        RowCtx " + x + ";\n";
-            src += "        const int64_t i" + J + " = base + " + J + " * 256 + threadIdx.x;\n";
-            src += "        bool " + a + " = i" + J + " < P.n;\n";
-            src += "        " + x + ".r = " + a + " ? " + (P.sel ? "__ldg(P.sel + i" + J + ")" : "(uint32_t)i" + J) + " : 0u;\n";
-            src += "        " + x + ".b0 = " + x + ".b1 = " + x + ".b2 = " + x + ".b3 = 0;\n";
-            src += "        " + x + ".head = 0;\n";
-        }
-        src += g.body();
-        src += "        uint32_t cnt = 0;\n";
-        for (int j = 0; j < K; j++) {
-            std::string J = num(j);
-            src += "        {\n            const uint32_t b = __ballot_sync(0xFFFFFFFFu, a" + J + ");\n";
-            src += "            const int64_t w0 = base + " + J + " * 256 + (threadIdx.x & ~31);\n";
-            src += "            if (lane == 0 && w0 < P.n) bits[w0 >> 5] = b;\n";
-            src += "            cnt += __popc(b);\n        }\n";
+        if (contig) {
+            // thread t's rows are base + 8t .. +7 (the per-CTA tile of the strided form, 8 x 256)
+            src += tile_rows(P, K, true, "        ");
+            src += g.body();
+            src += "        uint32_t byte = 0;\n";
+            for (int j = 0; j < K; j++) src += "        byte |= (a" + num(j) + " ? 1u : 0u) << " + num(j) + ";\n";
+            // a 32-row word is the bytes of 4 consecutive lanes
+            src += "        uint32_t word = byte << (8 * (lane & 3));\n";
+            src += "        word |= __shfl_xor_sync(0xFFFFFFFFu, word, 1);\n";
+            src += "        word |= __shfl_xor_sync(0xFFFFFFFFu, word, 2);\n";
+            src += "        if ((lane & 3) == 0 && r0 < P.n) bits[r0 >> 5] = word;\n";
+            src += "        const uint32_t cnt = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)__popc(byte));\n";
+        } else {
+            src += tile_rows(P, K, false, "        ");
+            src += g.body();
+            src += "        uint32_t cnt = 0;\n";
+            for (int j = 0; j < K; j++) {
+                std::string J = num(j);
+                src += "        {\n            const uint32_t b = __ballot_sync(0xFFFFFFFFu, a" + J + ");\n";
+                src += "            const int64_t w0 = base + " + J + " * 256 + (threadIdx.x & ~31);\n";
+                src += "            if (lane == 0 && w0 < P.n) bits[w0 >> 5] = b;\n";
+                src += "            cnt += __popc(b);\n        }\n";
+            }
         }
         src += "        if (lane == 0 && cnt) atomicAdd(chunk_counts + c, cnt);\n";
         src += "        __syncwarp();\n";
@@ -1048,27 +1162,26 @@ std::string jit_select_source(const Pipeline& pipe, const PipeArgs& P) {
 
 void* jit_hll_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L) {
     if (!jit_enabled(ctx) || !batchable(P)) return nullptr;
-    std::string key = signature('h', P, nullptr, &L) + std::string((const char*)&ctx->device, sizeof(int));
-    return memoized(pipe, key, [&] { return (void*)get_kernel(ctx, jit_hll_source(pipe, P, L), "ml_card_hll"); });
+    const bool contig = contig_ok(P);
+    std::string key = signature('h', P, nullptr, &L) + std::string((const char*)&ctx->device, sizeof(int)) +
+                      (contig ? "c" : "s");
+    return memoized(pipe, key, [&] { return (void*)get_kernel(ctx, jit_hll_source(pipe, P, L, contig), "ml_card_hll"); });
 }
 
-std::string jit_hll_source(const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L) {
+std::string jit_hll_source(const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L, bool contig) {
     {
         // The cardinality features scan: every row's key hashed into 2^14 HyperLogLog registers
         // privatized in shared memory, NULL count and the first key word's range; each CTA
         // leaves its registers as bytes in cta_regs[blockIdx.x][4096 words] for the merge kernel.
         Gen g(pipe.C.code, P);
         g.rows_per_thread = 8;
+        g.contig = contig;
         g.fail = "break;";
         g.batched_stages([&](auto&& rows) {
             std::set<int> slots;
             for (int k = 0; k < L.nkeys; k++) g.slots_of(L.prog[k], slots);
-            std::vector<std::map<int, Gen::V>> pre(g.rows_per_thread);
-            rows([&](int j, const std::string& a) {
-                g.cols.clear();
-                g.preload(slots, a);
-                pre[j] = g.cols;
-            });
+            std::vector<std::map<int, Gen::V>> pre;
+            g.preload_rows(slots, pre);
             rows([&](int j, const std::string& a) {
                 g.cols = pre[j];
                 g.open("if (" + a + ") {  // key " + num(j));
@@ -1101,7 +1214,7 @@ std::string jit_hll_source(const Pipeline& pipe, const PipeArgs& P, const KeyLay
         src += "    for (int i = threadIdx.x; i < 16384; i += blockDim.x) regs[i] = 0;\n    __syncthreads();\n";
         src += "    unsigned long long nulls = 0, lo = ~0ull, hi = 0;\n";
         src += g.pre();
-        src += row_loop(P, true, g.body(), g.rows_per_thread);
+        src += row_loop(P, true, g.body(), g.rows_per_thread, contig);
         src += "    for (int o = 16; o; o >>= 1) {\n"
                "        nulls += __shfl_xor_sync(0xFFFFFFFFu, nulls, o);\n"
                "        const unsigned long long l2 = __shfl_xor_sync(0xFFFFFFFFu, lo, o), h2 = __shfl_xor_sync(0xFFFFFFFFu, hi, o);\n"

@@ -29,8 +29,10 @@ void* jit_select_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P);
 // Arguments: P, L, cta_regs (gridDim x 4096 words), nulls, minmax.
 void* jit_hll_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L);
 // Sources of the kernels above.
-std::string jit_select_source(const Pipeline& pipe, const PipeArgs& P);
-std::string jit_hll_source(const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L);
+// `contig`: consecutive rows per thread with vector loads (needs no selection vector and 16-byte
+// aligned source columns).
+std::string jit_select_source(const Pipeline& pipe, const PipeArgs& P, bool contig);
+std::string jit_hll_source(const Pipeline& pipe, const PipeArgs& P, const KeyLayout& L, bool contig);
 
 // Rows one thread of the specialized aggregate kernel handles per iteration (its grid
 // needs n / rows-per-thread threads).
@@ -42,6 +44,6 @@ void jit_launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream
 int jit_resident_blocks(void* fn, unsigned block, size_t smem);
 
 // The generated source of the aggregate kernel (exposed for tests of the generator).
-std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArgs& A);
+std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArgs& A, bool contig = false);
 
 }  // namespace mlg
