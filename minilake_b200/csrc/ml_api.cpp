@@ -469,7 +469,7 @@ std::unique_ptr<ml_batch> topn_batch(Ctx* ctx, ml_batch& b, const std::vector<So
             cand = a.get<uint8_t>() + rows_b;
             done = (unsigned int*)(a.get<uint8_t>() + rows_b + cand_b);
             final_out = (uint32_t*)(done + 4);
-            CK(cudaMemsetAsync(done, 0, 4, st));
+            CK(cudaMemsetAsync(done, 0, 16, st));  // finished-CTA counter and the shared top-k threshold
         }
         KernelTimer kt(ctx, st, "topn");
         launch_topn_warp(S, n, (int)k, nb, a.get<uint32_t>(), cand, done, final_out, st);

@@ -860,6 +860,7 @@ __global__ void __launch_bounds__(1024) k_topn_chunk(const __grid_constant__ Sor
                 bool up = (lo & size) == 0;
                 uint64_t pa = pre[lo], pb = pre[hi];
                 int c = pa < pb ? -1 : (pa > pb ? 1 : cmp_rows(S, idx[lo], idx[hi]));
+                if (c == 0) c = idx[lo] < idx[hi] ? -1 : (idx[lo] > idx[hi]);  // equal keys: input order
                 if ((c > 0) == up && c != 0) {
                     uint32_t a = idx[lo];
                     idx[lo] = idx[hi];
@@ -882,9 +883,11 @@ struct TopEntry {
     uint64_t p;  // sort_prefix
     uint32_t r;  // row (kNone = padding)
 };
+// Rows with equal keys keep their input order (the row id breaks the tie), as in a stable sort.
 __device__ __forceinline__ bool entry_less(const SortDev& S, TopEntry a, TopEntry b) {
     if (a.p != b.p) return a.p < b.p;
-    return cmp_rows(S, a.r, b.r) < 0;
+    const int c = cmp_rows(S, a.r, b.r);
+    return c ? c < 0 : a.r < b.r;
 }
 __device__ __forceinline__ TopEntry shfl_entry(TopEntry e, int src) {
     return TopEntry{__shfl_sync(0xFFFFFFFFu, e.p, src), __shfl_sync(0xFFFFFFFFu, e.r, src)};
@@ -950,17 +953,146 @@ __device__ TopEntry warp_topk(const SortDev& S, int64_t n, int k, int64_t batch,
     return best;
 }
 
+// sort_prefix of a fixed-width first key of type DT from its loaded value (load_value's form):
+// `flip` is 0 for ascending keys and ~0 for descending ones, `nullp` the prefix of a NULL.
+template <int DT>
+__device__ __forceinline__ uint64_t fixed_prefix(uint64_t x, bool valid, uint64_t flip, uint64_t nullp) {
+    uint64_t p;
+    if (DT == ML_TYPE_FLOAT64) p = (uint64_t)total_key(as_f64(x)) ^ 0x8000000000000000ull;
+    else if (DT == ML_TYPE_BOOL) p = x;
+    else p = x ^ 0x8000000000000000ull;
+    return valid ? p ^ flip : nullp;
+}
+
+// Four consecutive values of the key column (registers, not an array: no stack traffic).
+struct Quad {
+    uint64_t v0, v1, v2, v3;
+};
+
+// warp_topk over the source rows when the first sort key is a fixed-width column of type DT:
+// each lane reads 4 consecutive rows (one or two 16-byte loads when the column is aligned), the
+// next 128-row chunk is loaded before the current one is compared, and a chunk is skipped unless
+// some row beats the k-th entry.  `shared_thr` (optional, starts at 0) holds ~T for the smallest
+// full-list k-th prefix T any warp of the launch has published: k rows have prefixes <= T, so a
+// row with a larger prefix cannot be in the top k and no warp queues it.
+template <int DT>
+__device__ TopEntry warp_topk_fixed(const SortDev& S, int64_t n, int k, int64_t chunk, int64_t chunks, TopEntry* queue,
+                                    int lane, unsigned long long* shared_thr) {
+    const DCol& c = S.cols[0];
+    const bool vec = ((uintptr_t)c.data & 15) == 0;
+    const uint64_t flip = S.asc[0] ? 0ull : ~0ull, nullp = S.nulls_first[0] ? 0ull : ~0ull;
+    const uint32_t n32 = (uint32_t)n;  // row ids are 32-bit
+    TopEntry best{~0ull, kNone};
+    TopEntry kth = best;
+    int qn = 0;  // entries in the warp's queue (warp-uniform)
+    uint64_t thr = ~0ull;
+    auto flush = [&]() {
+        TopEntry e = lane < qn ? queue[lane] : TopEntry{~0ull, kNone};
+        __syncwarp();
+        best = warp_merge32(S, best, warp_sort32(S, e, lane), lane);
+        kth = shfl_entry(best, k - 1);
+        qn = 0;
+        if (shared_thr && kth.r != kNone && kth.p < thr) {
+            thr = kth.p;
+            if (lane == 0) atomicMax(shared_thr, ~kth.p);
+        }
+    };
+    auto load = [&](uint32_t r0) -> Quad {
+        Quad q{0ull, 0ull, 0ull, 0ull};
+        if (vec && r0 + 4u <= n32) {
+            if (DT == ML_TYPE_FLOAT64 || DT == ML_TYPE_INT64) {
+                uint64_t t[2], u[2];
+                ld_stream_v2_u64((const unsigned long long*)c.data + r0, t);
+                ld_stream_v2_u64((const unsigned long long*)c.data + r0 + 2, u);
+                q = Quad{t[0], t[1], u[0], u[1]};
+            } else if (DT == ML_TYPE_BOOL) {
+                const uint32_t w = ld_stream_u32((const uint8_t*)c.data + r0);
+                q = Quad{w & 0xFFu, (w >> 8) & 0xFFu, (w >> 16) & 0xFFu, w >> 24};
+            } else {
+                uint32_t w[4];
+                ld_stream_v4_u32((const uint32_t*)c.data + r0, w);
+                q = Quad{(uint64_t)(int64_t)(int32_t)w[0], (uint64_t)(int64_t)(int32_t)w[1],
+                         (uint64_t)(int64_t)(int32_t)w[2], (uint64_t)(int64_t)(int32_t)w[3]};
+            }
+        } else {
+            if (r0 < n32) q.v0 = load_value(c, r0);
+            if (r0 + 1u < n32) q.v1 = load_value(c, r0 + 1u);
+            if (r0 + 2u < n32) q.v2 = load_value(c, r0 + 2u);
+            if (r0 + 3u < n32) q.v3 = load_value(c, r0 + 3u);
+        }
+        return q;
+    };
+    auto offer = [&](TopEntry e) {  // every lane of the warp calls it with one entry
+        bool take = e.r != kNone && e.p <= thr && entry_less(S, e, kth);
+        unsigned m = __ballot_sync(0xFFFFFFFFu, take);
+        if (!m) return;
+        if (qn + __popc(m) > 32) {
+            flush();
+            take = take && e.p <= thr && entry_less(S, e, kth);
+            m = __ballot_sync(0xFFFFFFFFu, take);
+        }
+        if (take) queue[qn + __popc(m & ((1u << lane) - 1))] = e;
+        qn += __popc(m);
+        __syncwarp();
+    };
+    auto process = [&](uint32_t r0, const Quad& q, uint64_t published) {
+        const uint32_t rem = r0 < n32 ? n32 - r0 : 0u;  // rows of this lane's four that exist
+        uint32_t vb = 0xFu;
+        if (c.valid && rem) vb = (uint32_t)(__ldg(c.valid + (r0 >> 6)) >> (r0 & 63u));
+        thr = ~published < thr ? ~published : thr;
+        const uint64_t bound = kth.p < thr ? kth.p : thr;
+        const uint64_t p0 = fixed_prefix<DT>(q.v0, vb & 1u, flip, nullp);
+        const uint64_t p1 = fixed_prefix<DT>(q.v1, vb & 2u, flip, nullp);
+        const uint64_t p2 = fixed_prefix<DT>(q.v2, vb & 4u, flip, nullp);
+        const uint64_t p3 = fixed_prefix<DT>(q.v3, vb & 8u, flip, nullp);
+        const bool any = (rem > 0 && p0 <= bound) || (rem > 1 && p1 <= bound) || (rem > 2 && p2 <= bound) ||
+                         (rem > 3 && p3 <= bound);
+        if (!__any_sync(0xFFFFFFFFu, any)) return;
+        offer(rem > 0 ? TopEntry{p0, r0} : TopEntry{~0ull, kNone});
+        offer(rem > 1 ? TopEntry{p1, r0 + 1u} : TopEntry{~0ull, kNone});
+        offer(rem > 2 ? TopEntry{p2, r0 + 2u} : TopEntry{~0ull, kNone});
+        offer(rem > 3 ? TopEntry{p3, r0 + 3u} : TopEntry{~0ull, kNone});
+    };
+    // the shared threshold is read together with the next chunk's values (off the critical path)
+    int64_t base = chunk * 128;
+    Quad qc{0ull, 0ull, 0ull, 0ull};
+    uint64_t pc = 0, pn = 0;
+    if (base < n) qc = load((uint32_t)base + (uint32_t)lane * 4u);
+    for (; base < n; base += chunks * 128) {
+        const int64_t next = base + chunks * 128;
+        Quad qn4{0ull, 0ull, 0ull, 0ull};
+        if (next < n) {
+            qn4 = load((uint32_t)next + (uint32_t)lane * 4u);
+            if (shared_thr) pn = __ldcg(shared_thr);
+        }
+        process((uint32_t)base + (uint32_t)lane * 4u, qc, pc);
+        qc = qn4;
+        pc = pn;
+    }
+    if (qn) flush();
+    return best;
+}
+
 // Each CTA writes its best k rows to out[block * k ..].  With `final_out`, CTAs also write
 // their (prefix, row) entries to `cand`, and the last CTA to finish (the counter `done` starts
 // at zero) merges all CTAs' entries into final_out[0 .. k): the whole top-k in one launch.
+// DT: the first sort key's type when it is a fixed-width column (warp_topk_fixed), -1 otherwise.
+template <int DT>
 __global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortDev S, int64_t n, int k, uint32_t* out,
                                                    TopEntry* cand, unsigned int* done, uint32_t* final_out) {
     __shared__ TopEntry lists[8][32];
     __shared__ TopEntry queue[8][32];
     __shared__ bool last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    TopEntry best = warp_topk(S, n, k, (int64_t)blockIdx.x * 8 + warp, (int64_t)gridDim.x * 8, queue[warp], lane,
-                              [&](int64_t i) { return TopEntry{sort_prefix(S, (uint32_t)i), (uint32_t)i}; });
+    TopEntry best;
+    // `done` points at 16 zeroed bytes: the finished-CTA counter, then the shared threshold
+    unsigned long long* thr = done ? reinterpret_cast<unsigned long long*>(done + 2) : nullptr;
+    if (DT >= 0)
+        best = warp_topk_fixed<DT < 0 ? 0 : DT>(S, n, k, (int64_t)blockIdx.x * 8 + warp, (int64_t)gridDim.x * 8,
+                                                  queue[warp], lane, thr);
+    else
+        best = warp_topk(S, n, k, (int64_t)blockIdx.x * 8 + warp, (int64_t)gridDim.x * 8, queue[warp], lane,
+                         [&](int64_t i) { return TopEntry{sort_prefix(S, (uint32_t)i), (uint32_t)i}; });
     lists[warp][lane] = best;
     __syncthreads();
     if (warp == 0) {
@@ -1127,14 +1259,37 @@ void launch_u64_to_u32(const uint64_t* in, uint32_t* out, int64_t n, cudaStream_
 }
 int topn_warp_blocks(int64_t n) {
     if (n <= 65536) return 1;  // one CTA finishes the candidates of the previous round
+    static const int resident = [] {  // CTAs per SM that every instantiation reaches: one wave
+        int r = 8;
+        auto at_most = [&](const void* f) {
+            int b = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, 256, 0) == cudaSuccess && b > 0) r = std::min(r, b);
+        };
+        at_most((const void*)k_topn_warp<-1>);
+        at_most((const void*)k_topn_warp<ML_TYPE_FLOAT64>);
+        at_most((const void*)k_topn_warp<ML_TYPE_INT64>);
+        at_most((const void*)k_topn_warp<ML_TYPE_INT32>);
+        at_most((const void*)k_topn_warp<ML_TYPE_BOOL>);
+        return r;
+    }();
     int64_t want = (n + 255) / 256;
-    int64_t cap = (int64_t)num_sms() * 4;
+    int64_t cap = (int64_t)num_sms() * resident;
     return (int)std::max<int64_t>(1, std::min(want, cap));
 }
 size_t topn_entry_bytes() { return sizeof(TopEntry); }
 void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* out, void* cand, unsigned int* done,
                       uint32_t* final_out, cudaStream_t s) {
-    k_topn_warp<<<blocks, 256, 0, s>>>(S, n, k, out, (TopEntry*)cand, done, final_out);
+    const DCol& c = S.cols[0];
+    const int dt = S.nkeys > 0 && c.kind == CK_FIXED && c.src == 0 ? c.dt : -1;
+    TopEntry* ce = (TopEntry*)cand;
+    switch (dt) {
+        case ML_TYPE_FLOAT64: k_topn_warp<ML_TYPE_FLOAT64><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
+        case ML_TYPE_INT64: k_topn_warp<ML_TYPE_INT64><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
+        case ML_TYPE_INT32:
+        case ML_TYPE_DATE: k_topn_warp<ML_TYPE_INT32><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
+        case ML_TYPE_BOOL: k_topn_warp<ML_TYPE_BOOL><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
+        default: k_topn_warp<-1><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
+    }
 }
 void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, uint32_t* out, cudaStream_t s) {
     int64_t nb = (n + kTopNChunk - 1) / kTopNChunk;

@@ -93,8 +93,9 @@ void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, u
 // Top-k for k <= kTopNWarpMax: each CTA writes its best k rows (sorted) to out[block * k ..].
 constexpr int kTopNWarpMax = 32;
 int topn_warp_blocks(int64_t n);
-// With final_out, `cand` (blocks * k entries of topn_entry_bytes()) and a zeroed counter
-// `done`, the last CTA merges every CTA's candidates into final_out[0 .. k): one launch.
+// With final_out, `cand` (blocks * k entries of topn_entry_bytes()) and `done` (16 zeroed
+// bytes: the finished-CTA counter and the launch's shared top-k threshold), the last CTA merges
+// every CTA's candidates into final_out[0 .. k): one launch.
 size_t topn_entry_bytes();
 void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* out, void* cand, unsigned int* done,
                       uint32_t* final_out, cudaStream_t s);
