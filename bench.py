@@ -283,7 +283,7 @@ def gpu_arm(args):
         if world == 1 and not args.skip_ops:
             log("per-operator throughput")
             from minilake_b200 import opbench
-            ops = opbench.run(iters=5, log=log)["ops"]
+            ops = opbench.run(iters=5, log=log)  # {"peak_gbs", "peak_kind", "ops": {...}}
         line = {
             "metric": METRIC,
             "value": value,

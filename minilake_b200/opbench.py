@@ -3,8 +3,9 @@
 Each operator runs on seeded synthetic tables generated on the device (the shapes of the
 benchmark queries), twice untimed, then `--iters` times with its kernels timed by CUDA events
 on the launching stream (the library's profile counters).  GB/s counts ALGORITHMIC bytes: the
-bytes an operator must move per row, stated with each operator below; a value near the
-measured copy bandwidth means the kernel is at the HBM roofline.
+bytes an operator must move per row, stated with each operator below; a value near the HBM
+copy bandwidth (measured on these GPUs, or the fallback figure; `peak_kind` says which) means
+the kernel is at the HBM roofline.
 
     filter           WHERE d <= 2467 over 100M rows -> selection vector.  Flags pass: 4 B/row read
                      (d) + 1 bit/row written; compaction: 1 bit/row read + 4 B per selected row.
@@ -31,14 +32,15 @@ from . import abi
 from .abi import AggSpec, Col, COUNT_STAR, FLOAT64, INT32, INT64, Lit, SortKey, SUM
 
 
-def measured_hbm_gbs() -> float:
-    """The measured HBM copy bandwidth (GB/s) on this machine's GPUs, else the fallback figure."""
+def hbm_peak():
+    """(GB/s, kind): the measured HBM copy bandwidth of this machine's GPUs ("measured", from
+    MEASURED_PEAKS.json), else the earlier measurement on the same kind of B200 ("fallback")."""
     p = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
     try:
         with open(p) as f:
-            return float(json.load(f)["hbm_gbs"])
+            return float(json.load(f)["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
-        return 6650.0
+        return 6650.0, "fallback"
 
 
 def _timed(ctx, keys, fn, iters):
@@ -57,7 +59,7 @@ def _timed(ctx, keys, fn, iters):
 def _line(rows, ms, nbytes, peak):
     gbs = nbytes / (ms * 1e6) if ms > 0 else 0.0
     return {"rows": int(rows), "ms": round(ms, 4), "rows_per_s": rows / (ms * 1e-3) if ms > 0 else 0.0,
-            "algorithmic_bytes": int(nbytes), "gbs": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 3)}
+            "algorithmic_bytes": int(nbytes), "gbs": round(gbs, 1), "frac_of_hbm_peak": round(gbs / peak, 3)}
 
 
 def run(iters: int = 5, rows_filter: int = 100_000_000, rows_join: int = 60_000_000, dim_rows: int = 1_500_000,
@@ -68,7 +70,7 @@ def run(iters: int = 5, rows_filter: int = 100_000_000, rows_join: int = 60_000_
     from .gpu import LIB, PROFILE, Context, HashAggregateSink, JoinBuildSink, SortSink, _check, card_features
 
     ctx = Context(0, flags=PROFILE)
-    peak = measured_hbm_gbs()
+    peak, peak_kind = hbm_peak()
     res = {}
 
     # ---- filter and filter + low-cardinality GROUP BY ------------------------------------
@@ -172,7 +174,7 @@ def run(iters: int = 5, rows_filter: int = 100_000_000, rows_join: int = 60_000_
     res["card_features"]["hll_estimate"] = round(float(est))
     log(f"card_features: {res['card_features']}")
     ctx.close()
-    return {"peak_gbs": peak, "ops": res}
+    return {"peak_gbs": peak, "peak_kind": peak_kind, "ops": res}
 
 
 def main():
