@@ -181,9 +181,11 @@ typedef struct ml_topn_local ml_topn_local;
 /* flags: ML_CTX_PROFILE times the library's main kernels with CUDA events recorded on the
  * stream each kernel is launched on (read back with ml_gpu_profile_read).
  * ML_CTX_INTERPRET runs every fused pipeline through the ahead-of-time interpreter kernels;
- * by default the aggregate and join-build pipelines are specialized at run time (NVRTC,
- * compiled once per pipeline shape and cached for the process).  Both give the same results. */
-enum { ML_CTX_DETERMINISTIC = 1, ML_CTX_PROFILE = 2, ML_CTX_INTERPRET = 4 };
+ * by default the filter, aggregate, join-build and cardinality pipelines are specialized at run
+ * time (NVRTC, compiled once per pipeline shape and cached for the process).  Both give the same
+ * results.  Floating-point SUM/AVG accumulate with atomics, so they agree with a sequential sum
+ * within rounding, not bit for bit from run to run.  Any other flag bit is rejected. */
+enum { ML_CTX_PROFILE = 2, ML_CTX_INTERPRET = 4 };
 
 /* ExecConfig (context.rs:14-34) for one device: hbm_budget_bytes is the query-wide
  * MemoryPool limit (memory.rs:22-26) applied to device bytes; 0 = unlimited. */

@@ -522,6 +522,7 @@ int ml_gpu_last_budget_error(char* op, size_t op_cap, uint64_t* requested, uint6
 int ml_gpu_ctx_create(int device, uint64_t hbm_budget_bytes, uint32_t flags, ml_ctx** out) {
     API_BEGIN
     REQUIRE(out, "null output");
+    REQUIRE((flags & ~(uint32_t)(ML_CTX_PROFILE | ML_CTX_INTERPRET)) == 0, "unknown context flags");
     *out = new ml_ctx(device, hbm_budget_bytes, flags);
     API_END
 }

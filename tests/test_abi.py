@@ -38,3 +38,14 @@ def test_python_binding_loads_the_library():
 def test_build_targets_sm_100a():
     mk = open(os.path.join(ROOT, "minilake_b200", "csrc", "Makefile")).read()
     assert "arch=compute_100a,code=sm_100a" in mk
+
+
+def test_context_rejects_unknown_flags():
+    """Flag bits the library does not implement are refused before any device is touched."""
+    from minilake_b200 import abi
+    lib = ctypes.CDLL(LIB)
+    out = ctypes.c_void_p()
+    rc = lib.ml_gpu_ctx_create(0, ctypes.c_uint64(0), ctypes.c_uint32(1), ctypes.byref(out))
+    assert rc == abi.ERR_INVALID and not out.value
+    lib.ml_gpu_last_error.restype = ctypes.c_char_p
+    assert b"unknown context flags" in lib.ml_gpu_last_error()
