@@ -314,8 +314,8 @@ int ml_gpu_join_build_sink(ml_join_build_local* local, const ml_column* cols, in
 int ml_gpu_join_build_combine(ml_join_build_local* local);
 /* Sink::finalize -> build_table (join.rs:160-203).  The table stays owned by the sink.
  * A single integer key (int32/date/int64 build column) whose value range spans at most
- * 4 entries per build row (+1024) is indexed directly by value; other keys use the hash
- * table.  Both give the same matches. */
+ * 4 entries per build row (+1024), or at most 2^20 entries, is indexed directly by value;
+ * other keys use the hash table.  Both give the same matches. */
 int ml_gpu_join_build_finalize(ml_join_build* sink, ml_join_table** table);
 /* capacity: hash-table slots, or the value range of a direct (dense) index. */
 int ml_gpu_join_table_stats(const ml_join_table* t, int64_t* build_rows, int64_t* distinct_keys,

@@ -1055,7 +1055,8 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
     CK(cudaMemsetAsync(jt->next.get(), 0xFF, std::max<size_t>((size_t)n * 4, 4), s));
     CK(cudaMemsetAsync(jt->dup.get(), 0, 8, s));
     // A single integer key that is a build column, with a value range of at most 4 entries
-    // per build row, is indexed directly (no hashing, one 4-byte load per probe).
+    // per build row or at most 2^20 entries (a 4 MB index, which L2 holds), is indexed directly
+    // (no hashing, one 4-byte load per probe).
     const DevColumn* kc = nullptr;
     if (n > 0 && jt->key_types.size() == 1 && jt->key_cols[0] >= 0) {
         const DevColumn* c = jt->batch.cols[jt->key_cols[0]].get();
@@ -1070,7 +1071,8 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
         ctx->count_launch();
         CK(cudaMemcpyAsync(got, mm.get(), 16, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
-        if (got[0] <= got[1] && got[1] - got[0] < std::min<uint64_t>(4 * (uint64_t)n + 1024, 0xFFFFFFFFull)) {
+        const uint64_t limit = std::max<uint64_t>(4 * (uint64_t)n + 1024, 1ull << 20);
+        if (got[0] <= got[1] && got[1] - got[0] < std::min<uint64_t>(limit, 0xFFFFFFFFull)) {
             jt->dmin = got[0];
             jt->drange = got[1] - got[0] + 1;
         } else {

@@ -14,6 +14,9 @@ the kernel is at the HBM roofline.
     join_groupby     d > 1200, probe of the dense join index on fk (1.5M distinct keys),
                      GROUP BY fk SUM(v) COUNT(*) over 60M rows: 20 B/row (fk 8, d 4, v 8).
     join_build       1.5M distinct i64 keys -> dense join index: 8 B/row read + 4 B/row index.
+    star_join        name LIKE 'ab%' on A (150k plain strings) -> probe A on k1 (Zipf 1.1), B on k2,
+                     C on region, GROUP BY label SUM(v*(1-w)) over 60M rows: 4 B/row (k1) + 20 B
+                     per row that survives the A probe (k2 4, v 8, w 8).
     topn             ORDER BY v DESC LIMIT 10 over 60M f64 values: 8 B/row.
     card_features    HyperLogLog scan of a 60M-row i64 key column: 8 B/row.
 
@@ -67,6 +70,7 @@ def run(iters: int = 5, rows_filter: int = 100_000_000, rows_join: int = 60_000_
     import torch
 
     from . import serving, workloads
+    from .engine import GpuEngine
     from .gpu import LIB, PROFILE, Context, HashAggregateSink, JoinBuildSink, SortSink, _check, card_features
 
     ctx = Context(0, flags=PROFILE)
@@ -151,6 +155,36 @@ def run(iters: int = 5, rows_filter: int = 100_000_000, rows_join: int = 60_000_
     res["join_groupby"]["groups"] = int(groups)
     log(f"join_groupby: {res['join_groupby']}")
     j.close()
+
+    # ---- star join (fact shape 2) ------------------------------------------------------------
+    t2 = serving.gen_fact(2, rows_join, seed + 2)
+    dim_a, dim_b, dim_c, names, a_key = serving.star_dims(ctx)
+    eng = GpuEngine(ctx)
+    a, b, c = workloads.star_join_builds(eng, dim_a, dim_b, dim_c)
+    sp, sg, sa = workloads.star_join_plan(a, b, c)
+    # fact rows whose k1 is the key of a name starting with "ab" (the rows the later stages read)
+    match = torch.from_numpy(a_key[[i for i, nm in enumerate(names) if nm.startswith(b"ab")]]).to("cuda")
+    survivors = int(torch.isin(t2.keep[0][1], match).sum().item())
+
+    def star():
+        sink = HashAggregateSink(ctx, t2.types, sg, sa, sp)
+        loc = sink.create_local()
+        loc.sink(t2.ml)
+        loc.combine()
+        out = sink.finalize()
+        g = out.num_rows
+        out.close()
+        sink.close()
+        return g
+
+    ms, groups = _timed(ctx, ("pipeline_aggregate",), star, iters)
+    res["star_join"] = _line(rows_join, ms["pipeline_aggregate"], 4 * rows_join + 20 * survivors, peak)
+    res["star_join"]["groups"], res["star_join"]["rows_after_a_probe"] = int(groups), survivors
+    log(f"star_join: {res['star_join']}")
+    for j in (a, b, c):
+        j.close()
+    del t2
+    torch.cuda.empty_cache()
 
     v_only = serving.DeviceTable([(FLOAT64, t1.keep[2][1], None)])
 

@@ -78,6 +78,22 @@ class DeviceTable:
         self.nbytes = sum(int(x.numel() * x.element_size()) for _, x, _ in cols)
 
 
+def star_dims(ctx):
+    """The star join's dimension tables in HBM (seeded): A (150k keys, 18-character names),
+    B (10k keys, region in [0, 25)), C (25 keys, labels); returns (A, B, C, names, A's keys)."""
+    from .datagen import _random_words
+    srng = np.random.Generator(np.random.PCG64(44))
+    a_key = (srng.permutation(150_000) + 1).astype(np.int32)
+    names = _random_words(srng, 150_000, 18)
+    A = ctx.upload([fixed(INT32, a_key), utf8_plain(names)])
+    b_key = (srng.permutation(10_000) + 1).astype(np.int32)
+    region = srng.integers(0, 25, 10_000, dtype=np.int32)
+    B = ctx.upload([fixed(INT32, b_key), fixed(INT32, region)])
+    labels = _random_words(srng, 25, 10)
+    C = ctx.upload([fixed(INT32, np.arange(25, dtype=np.int32)), utf8_plain(labels)])
+    return A, B, C, names, a_key
+
+
 def gen_fact(shape: int, rows: int, seed: int, dim_rows: int = 1_500_000, a_rows: int = 150_000,
              b_rows: int = 10_000) -> DeviceTable:
     import torch
@@ -153,16 +169,7 @@ class Server:
         key = (drng.permutation(1_500_000) + 1).astype(np.int64)
         self.dim = ctx.upload([fixed(INT64, key)])
         self.dim_join = self._build(self.dim, [INT64], [(Col(0), INT64)])
-        srng = np.random.Generator(np.random.PCG64(44))
-        from .datagen import _random_words
-        a_key = (srng.permutation(150_000) + 1).astype(np.int32)
-        self.names = _random_words(srng, 150_000, 18)
-        self.A = ctx.upload([fixed(INT32, a_key), utf8_plain(self.names)])
-        b_key = (srng.permutation(10_000) + 1).astype(np.int32)
-        region = srng.integers(0, 25, 10_000, dtype=np.int32)
-        self.B = ctx.upload([fixed(INT32, b_key), fixed(INT32, region)])
-        labels = _random_words(srng, 25, 10)
-        self.C = ctx.upload([fixed(INT32, np.arange(25, dtype=np.int32)), utf8_plain(labels)])
+        self.A, self.B, self.C, self.names, _ = star_dims(ctx)
         self.b_join = self._build(self.B, [INT32, INT32], [(Col(0), INT32)])
         self.c_join = self._build(self.C, [INT32, UTF8], [(Col(0), INT32)])
         # learned sizing: predicted group counts per (shape, table) from scan features

@@ -378,7 +378,7 @@ def test_group_by_join_key_with_duplicate_and_null_build_keys(gpu_engine, by_bui
     assert_same_rows(res["gpu"], res["oracle"], 1, {1})
 
 
-@pytest.mark.parametrize("kind", ["dense", "sparse", "negative_i32", "compound", "utf8"])
+@pytest.mark.parametrize("kind", ["dense", "small_wide", "sparse", "negative_i32", "compound", "utf8"])
 def test_join_index_kinds_match_oracle(gpu_engine, kind):
     """Dense integer keys use the direct index, all other keys the hash table; both must
     give the oracle's matches (through the fused aggregate) and distinct-key counts."""
@@ -387,6 +387,9 @@ def test_join_index_kinds_match_oracle(gpu_engine, kind):
     valid = rng.random(nd) > 0.03
     if kind == "dense":
         pool = np.arange(100, 2100, dtype=np.int64)
+        types, mk = [INT64], lambda v, m=None: [fixed(INT64, v, m)]
+    elif kind == "small_wide":  # few keys spread over a range that still fits a 4 MB index
+        pool = np.sort(rng.choice(500_000, 300, replace=False)).astype(np.int64) + 7
         types, mk = [INT64], lambda v, m=None: [fixed(INT64, v, m)]
     elif kind == "sparse":
         pool = rng.integers(-2**62, 2**62, 1500, dtype=np.int64)
@@ -428,6 +431,9 @@ def test_join_index_kinds_match_oracle(gpu_engine, kind):
     assert stats["gpu"]["distinct_keys"] == stats["oracle"]["distinct_keys"]
     if kind == "dense":
         assert stats["gpu"]["capacity"] == 2000  # value range 100..2099: direct index
+    elif kind == "small_wide":
+        lo, hi = dk[valid].min(), dk[valid].max()
+        assert stats["gpu"]["capacity"] == hi - lo + 1  # direct index over the valid keys' range
     else:
         cap = stats["gpu"]["capacity"]
         assert cap & (cap - 1) == 0, "hash table capacity is a power of two"
