@@ -139,6 +139,15 @@ CUfunction get_kernel(Ctx* ctx, const std::string& src, const char* name) {
 
 CUfunction compile_kernel(Ctx* ctx, const std::string& src, const char* name) {
     Nvrtc& N = nvrtc();
+    // MINILAKE_GPU_JIT_DUMP=<dir>: keep each generated source there (<kernel>_<hash>.cu) to read
+    // or compile offline
+    if (const char* dir = getenv("MINILAKE_GPU_JIT_DUMP")) {
+        const std::string path = std::string(dir) + "/" + name + "_" + std::to_string(std::hash<std::string>{}(src)) + ".cu";
+        if (FILE* f = fopen(path.c_str(), "w")) {
+            fwrite(src.data(), 1, src.size(), f);
+            fclose(f);
+        }
+    }
     auto t0 = std::chrono::steady_clock::now();
     std::vector<const char*> texts, names;
     for (int i = 0; i < kJitHeaderCount; i++) {
@@ -218,6 +227,8 @@ class Gen {
     // read with vector loads, one validity word per thread.
     int rows_per_thread = kRowsPerThread;
     bool contig = false;
+    // Statement that leaves the current tile (empty: tiles are never cut short).
+    std::string tile_skip;
     // The row context the generated statements read (x, or x<j> in the batched form), the
     // statement that abandons the current row combination, and preloaded columns.
     std::string x = "x";
@@ -560,7 +571,18 @@ class Gen {
             }
             x = "x";
         };
+        // after a join probe (joins are where most rows of a star query drop out), a tile where no
+        // lane of the warp has a live row skips the rest; the decision is warp-uniform, so the
+        // warp stays converged.  Not after filters: the vote costs more than it saves when most
+        // rows pass.
+        auto skip_dead_tile = [&](int after) {
+            if (tile_skip.empty() || P_.stages[after].kind != 1) return;
+            std::string any;
+            for (int j = 0; j < K; j++) any += (j ? " || a" : "a") + num(j);
+            line("if (!__any_sync(0xFFFFFFFFu, " + any + ")) " + tile_skip);
+        };
         for (int s = 0; s < P_.nstages; s++) {
+            if (s > 0) skip_dead_tile(s - 1);
             const Stage st = P_.stages[s];
             std::set<int> slots;
             if (st.kind == 0) {
@@ -636,6 +658,7 @@ class Gen {
                 close();
             });
         }
+        if (P_.nstages > 0) skip_dead_tile(P_.nstages - 1);
         sink(rows);
     }
 
@@ -923,6 +946,7 @@ std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArg
     const bool smem = A.smem_groups > 0;
     const bool batched = batchable(P);
     g.contig = contig && batched;
+    g.tile_skip = "continue;";  // the tile loop of row_loop
     if (batched) {
         g.fail = "break;";
         g.batched_stages([&](auto&& rows) {
