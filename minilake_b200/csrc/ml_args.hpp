@@ -26,6 +26,10 @@ struct ProbeDev {
     // key's index position (key - dmin) without reading the index, and membership in the build
     // side is checked once per group when the aggregate is finalized.
     int32_t late, pad;
+    // With a dense index whose keys are distinct, when nothing after this probe reads the build
+    // row (a semi-join): one bit per index position (bit set = a build row has that key), so the
+    // probe reads 1/32 of the index's bytes; a match yields build row 0, which nothing reads.
+    const uint32_t* member;
 };
 
 // The streaming part of a pipeline (Filter / Projection folded into expressions /

@@ -543,6 +543,11 @@ __device__ __forceinline__ uint32_t dense_find(const uint32_t* dense, uint64_t d
     const uint64_t off = key - dmin;
     return off < drange ? dense_load(dense + off) : kNone;
 }
+// Membership of a key in a dense index's bitmap (ProbeDev::member): 0 when present, else kNone.
+__device__ __forceinline__ uint32_t dense_member(const uint32_t* bits, uint64_t dmin, uint64_t drange, uint64_t key) {
+    const uint64_t off = key - dmin;
+    return off < drange && ((__ldg(bits + (off >> 5)) >> (off & 31)) & 1u) ? 0u : kNone;
+}
 
 // Index position of a key in a dense index's range (kNone outside it), without reading it.
 __device__ __forceinline__ uint32_t dense_slot(uint64_t dmin, uint64_t drange, uint64_t key) {

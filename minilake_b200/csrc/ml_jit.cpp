@@ -540,6 +540,9 @@ class Gen {
         if (pd.dense && pd.late)
             line("const uint32_t hb" + tag + " = dense_slot(P.probes[" + p + "].dmin, P.probes[" + p + "].drange, wk" +
                  tag + "[0]);");
+        else if (pd.dense && pd.member)
+            line("const uint32_t hb" + tag + " = dense_member(P.probes[" + p + "].member, P.probes[" + p +
+                 "].dmin, P.probes[" + p + "].drange, wk" + tag + "[0]);");
         else if (pd.dense)
             line("const uint32_t hb" + tag + " = dense_find(P.probes[" + p + "].dense, P.probes[" + p + "].dmin, P.probes[" +
                  p + "].drange, wk" + tag + "[0]);");
@@ -615,6 +618,9 @@ class Gen {
                     if (pd.late)  // membership is checked per group at finalize: no index read per row
                         line("d" + tag + " = dense_slot(P.probes[" + p + "].dmin, P.probes[" + p + "].drange, wk" + tag +
                              "[0]);");
+                    else if (pd.member)  // semi-join: one bit per key
+                        line("d" + tag + " = dense_member(P.probes[" + p + "].member, P.probes[" + p + "].dmin, P.probes[" +
+                             p + "].drange, wk" + tag + "[0]);");
                     else
                         line("d" + tag + " = dense_find(P.probes[" + p + "].dense, P.probes[" + p + "].dmin, P.probes[" +
                              p + "].drange, wk" + tag + "[0]);");
@@ -1014,6 +1020,7 @@ std::string signature(char kind, const PipeArgs& P, const AggArgs* A, const KeyL
         pd.t = TableView{};
         pd.next = pd.next ? (const uint32_t*)1 : nullptr;
         pd.dense = pd.dense ? (const uint32_t*)1 : nullptr;
+        pd.member = pd.member ? (const uint32_t*)1 : nullptr;
         pd.dmin = pd.drange = 0;
     }
     std::string key(1, kind);

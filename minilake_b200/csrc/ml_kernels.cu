@@ -60,6 +60,7 @@ struct Cursors {
 // Build row matching the normalized key `w` through probe `pd` (dense index or hash table).
 __device__ __forceinline__ uint32_t probe_find(const ProbeDev& pd, const uint64_t* w) {
     if (pd.dense && pd.late) return dense_slot(pd.dmin, pd.drange, w[0]);
+    if (pd.dense && pd.member) return dense_member(pd.member, pd.dmin, pd.drange, w[0]);
     if (pd.dense) return dense_find(pd.dense, pd.dmin, pd.drange, w[0]);
     return table_find(pd.t, w, key_hash(w, pd.t.nwords));
 }
@@ -629,6 +630,18 @@ __global__ void k_key_range(const void* data, int dt, const uint64_t* valid, int
 }
 // build_table (join.rs:160-203) over a dense key: the index entry holds the chain head,
 // later rows with the same key push the previous head into `next`.
+// Membership bitmap of a dense index: bit i of the words = (dense[i] != kNone); one warp per word.
+__global__ void k_dense_bits(const uint32_t* dense, uint64_t n, uint32_t* bits) {
+    const uint64_t words = (n + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < words; w += warps) {
+        const uint64_t i = w * 32 + lane;
+        const unsigned b = __ballot_sync(0xFFFFFFFFu, i < n && dense[i] != kNone);
+        if (lane == 0) bits[w] = b;
+    }
+}
+
 __global__ void k_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint32_t* dense,
                                uint32_t* next, uint32_t* dup_flag) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1227,6 +1240,10 @@ void launch_key_range(const void* data, int dt, const uint64_t* valid, int64_t n
 void launch_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint32_t* dense,
                          uint32_t* next, uint32_t* dup_flag, cudaStream_t s) {
     if (n) k_dense_insert<<<grid_for(n, 8), kThreads, 0, s>>>(data, dt, valid, n, dmin, dense, next, dup_flag);
+}
+void launch_dense_bits(const uint32_t* dense, uint64_t n, uint32_t* bits, cudaStream_t s) {
+    const uint64_t words = (n + 31) / 32;
+    if (words) k_dense_bits<<<grid_for((int64_t)words * 32, 8), kThreads, 0, s>>>(dense, n, bits);
 }
 void launch_count_dense(const uint32_t* dense, uint64_t n, unsigned long long* out, cudaStream_t s) {
     if (n) k_count_dense<<<grid_for((int64_t)n, 8), kThreads, 0, s>>>(dense, n, out);

@@ -89,6 +89,8 @@ void launch_key_range(const void* data, int dt, const uint64_t* valid, int64_t n
 void launch_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint32_t* dense,
                          uint32_t* next, uint32_t* dup_flag, cudaStream_t s);
 void launch_count_dense(const uint32_t* dense, uint64_t n, unsigned long long* out, cudaStream_t s);
+// bits[i / 32] bit i % 32 = (dense[i] != kNone), for i < n.
+void launch_dense_bits(const uint32_t* dense, uint64_t n, uint32_t* bits, cudaStream_t s);
 void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, uint32_t* out, cudaStream_t s);
 // Top-k for k <= kTopNWarpMax: each CTA writes its best k rows (sorted) to out[block * k ..].
 constexpr int kTopNWarpMax = 32;

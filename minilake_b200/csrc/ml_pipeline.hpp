@@ -98,6 +98,9 @@ struct ml_join_table {
     // Dense integer key: a direct-mapped index replaces the hash table (see ProbeDev).
     mlg::DevBuf dense;
     uint64_t dmin = 0, drange = 0;
+    // One bit per dense index position (a build row has that key): the semi-join form of the
+    // index (ProbeDev::member), used when the keys are distinct.
+    mlg::DevBuf member;
     mlg::TableView view() const {
         mlg::TableView t{};
         t.slots = slots.get<uint64_t>();

@@ -483,3 +483,29 @@ def test_low_cardinality_group_by_every_aggregate(gpu_engine, groups):
         got = gpu_engine.fetch(gpu_engine.hashagg(t, types, [(Col(0), INT32)], aggs, pro))
         want = oracle.fetch(oracle.hashagg(t, types, [(Col(0), INT32)], aggs, pro))
         assert_same_rows(got, want, 1, {4, 5} if len(aggs) == 7 else set())
+
+
+@pytest.mark.parametrize("dups", [False, True])
+def test_semi_join_probe_matches_oracle(gpu_engine, dups):
+    """A probe whose build rows nothing reads (GROUP BY and aggregates over fact columns only)
+    tests membership in the dense index's bitmap when the build keys are distinct; with
+    duplicate build keys every match still counts once per build row."""
+    rng = np.random.default_rng(21)
+    nd, nf = 3000, 50_000
+    dk = rng.choice(200_000, nd, replace=False).astype(np.int64) + 11
+    if dups:
+        dk[: nd // 3] = dk[nd // 3: 2 * (nd // 3)]
+    valid = rng.random(nd) > 0.02
+    dim = Table("d", ["k", "x"], [[fixed(INT64, dk, valid), fixed(INT32, rng.integers(0, 9, nd).astype(np.int32))]])
+    fk = np.where(rng.random(nf) < 0.5, dk[rng.integers(0, nd, nf)], rng.integers(0, 200_020, nf)).astype(np.int64)
+    g = rng.integers(0, 40, nf).astype(np.int32)
+    fact = Table("f", ["fk", "g", "v"], [[fixed(INT64, fk[:20_000]), fixed(INT32, g[:20_000]), fixed(FLOAT64, rng.random(20_000))],
+                                        [fixed(INT64, fk[20_000:]), fixed(INT32, g[20_000:]), fixed(FLOAT64, rng.random(nf - 20_000))]])
+    keys = [(Col(0), INT64)]
+    aggs = [AggSpec(SUM, Col(2), FLOAT64), AggSpec(COUNT_STAR)]
+    res = {}
+    for name, eng in (("gpu", gpu_engine), ("oracle", orc.OracleEngine(threads=1))):
+        j = eng.join_build(dim, [INT64, INT32], keys)
+        out = eng.hashagg(fact, [INT64, INT32, FLOAT64], [(Col(1), INT32)], aggs, prologue=[Probe(j.handle, keys)])
+        res[name] = eng.fetch(out)
+    assert_same_rows(res["gpu"], res["oracle"], 1, {1})
