@@ -294,9 +294,10 @@ int ml_gpu_hashagg_reset(ml_hashagg* sink);
 /* Sink one batch of device-resident columns from the calling thread (one call at a time per
  * sink), as a CUDA graph: with `reset` the graph first empties the group state, then runs the
  * fused pipeline kernel and reads back its overflow count and error word.  The graph is
- * captured on the first call with a given set of launch parameters (columns, the constants'
- * buffers, table size) and replayed by later calls; a table that overflows grows and the
- * rows that did not fit are aggregated again outside the graph.  Finalize as usual. */
+ * captured on the second call with a given set of launch parameters (columns, the constants'
+ * buffers, join tables, table size; the first such call runs the same steps without a graph)
+ * and replayed by later calls; a table that overflows grows and the rows that did not fit are
+ * aggregated again outside the graph.  Finalize as usual. */
 int ml_gpu_hashagg_run_resident(ml_hashagg* sink, const ml_column* cols, int32_t ncols, int64_t nrows,
                                 int32_t reset);
 /* Graphs captured and graph launches replayed by ml_gpu_hashagg_run_resident. */

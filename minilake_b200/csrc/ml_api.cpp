@@ -1291,6 +1291,7 @@ struct ml_hashagg {
         uint64_t* host_count = nullptr;  // pinned
         cudaStream_t s = nullptr;
         std::vector<std::pair<std::string, cudaGraphExec_t>> graphs;  // launch parameters -> graph
+        std::vector<std::string> seen;  // launch parameters run once without a graph (recent 64)
         uint64_t hits = 0, builds = 0;
     } run;
     SinkStreams streams;
@@ -1833,15 +1834,8 @@ int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t nc
     key.append((const char*)&A, sizeof(AggArgs));
     key.append((const char*)&jit, sizeof(jit));
     key.append(1, (char)(reset != 0));
-    cudaGraphExec_t exec = nullptr;
-    for (auto& g : R.graphs)
-        if (g.first == key) exec = g.second;
-    if (exec) {
-        R.hits++;
-    } else {
-        const auto t_cap = std::chrono::steady_clock::now();
-        cudaGraph_t graph;
-        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    // the whole run: reset, clear the read-back words, the fused kernel, read back
+    auto enqueue = [&]() {
         if (reset) {
             CK(cudaMemsetAsync(h->ngroups.get(), 0, 16, s));
             if (h->cap) CK(cudaMemsetAsync(h->slots.get(), 0, h->cap * 8 * (h->keys.nwords == 1 ? 2 : 4), s));
@@ -1859,6 +1853,27 @@ int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t nc
         }
         CK(cudaMemcpyAsync(R.host_count, R.count.get(), 8, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(R.ew->h, R.ew->d.get(), 4, cudaMemcpyDeviceToHost, s));
+    };
+    cudaGraphExec_t exec = nullptr;
+    for (auto& g : R.graphs)
+        if (g.first == key) exec = g.second;
+    // a launch shape is captured the second time it is seen: one-off shapes (a join table built
+    // for one query) run directly instead of paying for a capture and evicting graphs that recur
+    bool seen = exec != nullptr;
+    if (!exec) {
+        for (auto& k : R.seen) seen = seen || k == key;
+        if (!seen) {
+            if (R.seen.size() >= 64) R.seen.erase(R.seen.begin());
+            R.seen.push_back(key);
+        }
+    }
+    if (exec) {
+        R.hits++;
+    } else if (seen) {
+        const auto t_cap = std::chrono::steady_clock::now();
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        enqueue();
         CK(cudaStreamEndCapture(s, &graph));
         cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
@@ -1874,7 +1889,8 @@ int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t nc
     }
     {
         KernelTimer kt(ctx, s, "pipeline_aggregate");
-        CK(cudaGraphLaunch(exec, s));
+        if (exec) CK(cudaGraphLaunch(exec, s));
+        else enqueue();
         kt.stop();
     }
     ctx->count_launch(reset ? 2 : 1);

@@ -12,8 +12,9 @@
   slot is free and its memory estimate fits the HBM pool budget (160 GB); queries that arrive
   meanwhile wait in arrival order.  Admitted queries run concurrently on the device.
 * Each query rebinds its slot's resident sink to the query's constants and runs the fused
-  pipeline kernel as a replayed CUDA graph (captured once per slot, table and join table),
-  then finalizes and takes its top-N / ORDER BY on the device.
+  pipeline kernel as a replayed CUDA graph (captured the second time a slot runs the same
+  table and join tables; a one-off combination runs without a graph), then finalizes and takes
+  its top-N / ORDER BY on the device.
 * Learned sizing on: each sink is presized with the cardinality model's prediction of the
   group count (from the table's scan features) and admission uses that estimate; off: no
   size hint (resize on overflow) and a fixed per-query estimate.

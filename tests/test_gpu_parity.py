@@ -509,3 +509,32 @@ def test_semi_join_probe_matches_oracle(gpu_engine, dups):
         out = eng.hashagg(fact, [INT64, INT32, FLOAT64], [(Col(1), INT32)], aggs, prologue=[Probe(j.handle, keys)])
         res[name] = eng.fetch(out)
     assert_same_rows(res["gpu"], res["oracle"], 1, {1})
+
+
+def test_resident_runs_match_a_local_sink(ctx, gpu_engine):
+    """ml_gpu_hashagg_run_resident: the first run of a launch shape goes without a graph, the
+    second is captured, later ones replay; every run (with reset) gives the local sink's result,
+    also after new constants are bound."""
+    from minilake_b200.gpu import HashAggregateSink
+    rng = np.random.default_rng(33)
+    n = 70_000
+    cols = [fixed(INT32, rng.integers(0, 50, n).astype(np.int32)), fixed(INT64, rng.integers(-500, 500, n)),
+            fixed(FLOAT64, np.round(rng.normal(0, 10, n), 3))]
+    dev = ctx.upload(cols)
+    types = [INT32, INT64, FLOAT64]
+    group = [(Col(0), INT32)]
+    aggs = [AggSpec(SUM, Col(2), FLOAT64), AggSpec(MAX, Col(1), INT64), AggSpec(COUNT_STAR)]
+    t = Table("t", ["g", "i", "f"], [cols])
+    sink = HashAggregateSink(ctx, types, group, aggs, [Filter(Col(1) > Lit(-400))], size_hint=128)
+    for cutoff in (-400, 100):
+        if cutoff != -400:
+            sink.rebind([Filter(Col(1) > Lit(cutoff))], group, aggs)
+        want = gpu_engine.fetch(gpu_engine.hashagg(t, types, group, aggs, [Filter(Col(1) > Lit(cutoff))]))
+        for _ in range(3):
+            sink.run_resident(dev, reset=True)
+            out = sink.finalize()
+            assert_same_rows(gpu_engine.fetch(out), want, 1, {1})
+            out.close()
+    st = sink.graph_stats()
+    assert st["built"] >= 1 and st["replayed"] >= 1, st
+    sink.close()
