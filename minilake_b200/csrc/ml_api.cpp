@@ -1153,7 +1153,7 @@ int ml_gpu_join_table_stats(const ml_join_table* t, int64_t* build_rows, int64_t
     if (capacity) *capacity = (int64_t)(t->dense ? t->drange : t->cap);
     if (distinct_keys) {
         DevBuf c(t->ctx, 8, nullptr);
-        CK(cudaMemset(c.get(), 0, 8));
+        CK(cudaMemsetAsync(c.get(), 0, 8, t->ctx->stream));
         if (t->dense) launch_count_dense(t->dense.get<uint32_t>(), t->drange, c.get<unsigned long long>(), t->ctx->stream);
         else launch_count_slots(t->view(), c.get<unsigned long long>(), t->ctx->stream);
         t->ctx->count_launch();
@@ -1629,7 +1629,7 @@ int ml_gpu_hashagg_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprol
     h->pipe.upload();
     h->res = std::make_unique<Reservation>(ctx, "HashAggregate");
     h->ngroups = DevBuf(ctx, 16, nullptr);
-    CK(cudaMemset(h->ngroups.get(), 0, 16));
+    CK(cudaMemsetAsync(h->ngroups.get(), 0, 16, ctx->stream));  // grow() below runs on ctx->stream
     ErrWord ew(ctx);
     uint64_t want;
     if (h->ungrouped) want = 1;
@@ -1762,8 +1762,8 @@ int ml_gpu_hashagg_rebind(ml_hashagg* h, const ml_pipe_op* prologue, int32_t npr
     for (size_t k = 0; k < h->aggs.size(); k++) h->aggs[k].arg = fresh.aggs[k].arg;
     cudaStream_t s = h->streams.own();
     if (!b.code.empty())
-        CK(cudaMemcpyAsync(h->pipe.d_prog.get(), b.code.data(), b.code.size() * sizeof(Instr), cudaMemcpyHostToDevice, s));
-    if (!b.arena.empty()) CK(cudaMemcpyAsync(h->pipe.d_arena.get(), b.arena.data(), b.arena.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(h->pipe.d_prog, b.code.data(), b.code.size() * sizeof(Instr), cudaMemcpyHostToDevice, s));
+    if (!b.arena.empty()) CK(cudaMemcpyAsync(h->pipe.d_arena, b.arena.data(), b.arena.size(), cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
     API_END
 }
@@ -2052,8 +2052,8 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
             }
             kc->offsets = DevBuf(ctx, (size_t)(ng + 1) * 4, b->res.get());
             kc->data = DevBuf(ctx, std::max<size_t>(bytes.size(), 1), b->res.get());
-            CK(cudaMemcpy(kc->offsets.get(), off.data(), (size_t)(ng + 1) * 4, cudaMemcpyHostToDevice));
-            if (!bytes.empty()) CK(cudaMemcpy(kc->data.get(), bytes.data(), bytes.size(), cudaMemcpyHostToDevice));
+            h2d_now(kc->offsets.get(), off.data(), (size_t)(ng + 1) * 4);
+            h2d_now(kc->data.get(), bytes.data(), bytes.size());
         } else {
             const DevColumn& src = *h->pipe.probes[d.build].jt->batch.cols[d.build_col];
             DevColumn tmp;

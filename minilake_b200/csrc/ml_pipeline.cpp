@@ -184,12 +184,15 @@ void Pipeline::build(const ml_pipe_op* ops, int nops, const int32_t* types, int 
 }
 
 void Pipeline::upload() {
-    size_t pb = std::max<size_t>(C.code.size() * sizeof(Instr), 32);
-    size_t ab = std::max<size_t>(C.arena.size(), 16);
-    d_prog = DevBuf(ctx, pb, nullptr);
-    d_arena = DevBuf(ctx, ab, nullptr);
-    if (!C.code.empty()) CK(cudaMemcpy(d_prog.get(), C.code.data(), C.code.size() * sizeof(Instr), cudaMemcpyHostToDevice));
-    if (!C.arena.empty()) CK(cudaMemcpy(d_arena.get(), C.arena.data(), C.arena.size(), cudaMemcpyHostToDevice));
+    const size_t pb = (std::max<size_t>(C.code.size() * sizeof(Instr), 32) + 255) & ~(size_t)255;
+    const size_t ab = std::max<size_t>(C.arena.size(), 16);
+    std::vector<uint8_t> host(pb + ab, 0);
+    if (!C.code.empty()) memcpy(host.data(), C.code.data(), C.code.size() * sizeof(Instr));
+    if (!C.arena.empty()) memcpy(host.data() + pb, C.arena.data(), C.arena.size());
+    d_code = DevBuf(ctx, pb + ab, nullptr);
+    d_prog = d_code.get<Instr>();
+    d_arena = d_code.get<uint8_t>() + pb;
+    h2d_now(d_code.get(), host.data(), host.size());
 }
 
 static bool dict_pred(const LutSpec& L, const std::string& s) {  // per-entry predicate
@@ -231,8 +234,8 @@ void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrow
     P = PipeArgs{};
     P.n = sel ? nsel : nrows;
     P.sel = sel;
-    P.prog = d_prog.get<Instr>();
-    P.arena = d_arena.get<uint8_t>();
+    P.prog = d_prog;
+    P.arena = d_arena;
     P.nstages = nstages;
     P.nprobes = (int)probes.size();
     P.head_probe = -1;

@@ -43,7 +43,10 @@ class Pipeline {
     std::vector<Prog> filters;
     std::vector<ProbeInfo> probes;
     StringIntern intern;
-    DevBuf d_prog, d_arena;
+    // The program and its arena in one device buffer (one copy per upload).
+    DevBuf d_code;
+    Instr* d_prog = nullptr;
+    uint8_t* d_arena = nullptr;
     // Runtime-specialized kernels already looked up for this pipeline, by the launch's
     // structural signature (the fields the source generator reads), so repeated launches skip
     // generating the source again.

@@ -298,6 +298,12 @@ void* Staging::get(size_t bytes) {
     return p_;
 }
 
+void h2d_now(void* dst, const void* src, size_t bytes) {
+    if (!bytes) return;
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, cudaStreamPerThread));
+    CK(cudaStreamSynchronize(cudaStreamPerThread));
+}
+
 int width_of(int dt) {
     switch (dt) {
         case ML_TYPE_BOOL: return 1;

@@ -213,6 +213,9 @@ namespace mlg {
 std::unique_ptr<DevColumn> stage_column(Ctx* ctx, const ml_column& c, int64_t nrows, cudaStream_t s, Staging& st,
                                         Reservation* res);
 int width_of(int dtype);
+// Host -> device copy that has landed when it returns (a pageable cudaMemcpy may return before
+// its DMA ends, and kernels on non-blocking streams do not wait for the legacy stream).
+void h2d_now(void* dst, const void* src, size_t bytes);
 
 // ---- host scalar semantics (crates/minilake-core/src/scalar.rs, kernels/scalar_ops.rs) -------
 struct HScalar {
