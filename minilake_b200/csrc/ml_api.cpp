@@ -1130,11 +1130,6 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
         CK(cudaStreamSynchronize(s));
     }
     uint32_t dup = 0;
-    if (jt->dense) {  // the semi-join form of the dense index (1/32 of its bytes)
-        jt->member = DevBuf(ctx, std::max<size_t>((jt->drange + 31) / 32 * 4, 4), jt->res.get());
-        launch_dense_bits(jt->dense.get<uint32_t>(), jt->drange, jt->member.get<uint32_t>(), s);
-        ctx->count_launch();
-    }
     CK(cudaMemcpyAsync(&dup, jt->dup.get(), 4, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(ew.h, ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -1243,13 +1238,29 @@ struct AggState {
 // Probes whose build rows nothing downstream reads (no column slot of that build side, not the
 // GROUP BY probe) test membership in the bitmap of a dense, duplicate-free index: a semi-join
 // that reads 1/32 of the index's bytes per probe row.
-void semi_probes(PipeArgs& P, const Pipeline& pipe, int head_probe) {
+// The membership bitmap of a dense join index (ml_join_table::member), built on stream `s` by
+// the first caller; later callers' streams wait for it.
+const uint32_t* member_bits(Ctx* ctx, ml_join_table* jt, cudaStream_t s) {
+    std::lock_guard<std::mutex> g(jt->member_mu);
+    if (!jt->member) {
+        jt->member = DevBuf(ctx, std::max<size_t>((jt->drange + 31) / 32 * 4, 4), jt->res.get());
+        launch_dense_bits(jt->dense.get<uint32_t>(), jt->drange, jt->member.get<uint32_t>(), s);
+        ctx->count_launch();
+        CK(cudaEventCreateWithFlags(&jt->member_ready, cudaEventDisableTiming));
+        CK(cudaEventRecord(jt->member_ready, s));
+    } else {
+        CK(cudaStreamWaitEvent(s, jt->member_ready, 0));
+    }
+    return jt->member.get<uint32_t>();
+}
+
+void semi_probes(Ctx* ctx, PipeArgs& P, const Pipeline& pipe, int head_probe, cudaStream_t s) {
     for (size_t p = 0; p < pipe.probes.size(); p++) {
-        const ml_join_table* jt = pipe.probes[p].jt;
-        if (!jt->member || jt->has_dups || (int)p == head_probe || P.probes[p].late) continue;
+        ml_join_table* jt = pipe.probes[p].jt;
+        if (!jt->dense || jt->has_dups || (int)p == head_probe || P.probes[p].late) continue;
         bool read = false;
         for (const SlotInfo& si : pipe.C.slots) read = read || si.src == (int)p + 1;
-        if (!read) P.probes[p].member = jt->member.get<uint32_t>();
+        if (!read) P.probes[p].member = member_bits(ctx, jt, s);
     }
 }
 
@@ -1694,7 +1705,7 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
         L.P.err = local->ew.d.get<uint32_t>();
         L.P.head_probe = h->group_probe;
         if (h->dense_groups) L.P.probes[h->group_probe].late = 1;
-        semi_probes(L.P, h->pipe, h->group_probe);
+        semi_probes(ctx, L.P, h->pipe, h->group_probe, s);
         AggArgs A = h->args(local->ovf_count.get<unsigned long long>(), ovf.get<uint32_t>(), ovf_cap);
         h->direct_slots(A, L);
         void* jit = jit_agg_kernel(ctx, h->pipe, L.P, A);
@@ -1822,7 +1833,7 @@ int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t nc
     L.P.err = R.ew->d.get<uint32_t>();
     L.P.head_probe = h->group_probe;
         if (h->dense_groups) L.P.probes[h->group_probe].late = 1;
-    semi_probes(L.P, h->pipe, h->group_probe);
+    semi_probes(ctx, L.P, h->pipe, h->group_probe, s);
     AggArgs A = h->args(R.count.get<unsigned long long>(), R.ovf.get<uint32_t>(), ovf_cap);
     h->direct_slots(A, L);
     void* jit = jit_agg_kernel(ctx, h->pipe, L.P, A);

@@ -102,8 +102,14 @@ struct ml_join_table {
     mlg::DevBuf dense;
     uint64_t dmin = 0, drange = 0;
     // One bit per dense index position (a build row has that key): the semi-join form of the
-    // index (ProbeDev::member), used when the keys are distinct.
+    // index (ProbeDev::member), built by the first launch that probes the table as a semi-join
+    // (member_bits); `member_ready` marks its completion for launches on other streams.
     mlg::DevBuf member;
+    cudaEvent_t member_ready = nullptr;
+    std::mutex member_mu;
+    ~ml_join_table() {
+        if (member_ready) cudaEventDestroy(member_ready);
+    }
     mlg::TableView view() const {
         mlg::TableView t{};
         t.slots = slots.get<uint64_t>();
