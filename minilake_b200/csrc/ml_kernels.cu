@@ -771,10 +771,6 @@ __global__ void k_u64_to_u32(const uint64_t* in, uint32_t* out, int64_t n) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (uint32_t)in[i];
 }
-__global__ void k_fill_u32(uint32_t* p, uint32_t v, int64_t n) {
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
-}
 
 __global__ void k_offsets_rebase(const uint32_t* src, int64_t n, uint32_t base, uint32_t* dst) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1012,7 +1008,7 @@ __device__ TopEntry warp_topk_fixed(const SortDev& S, int64_t n, int k, int64_t 
     };
     auto load = [&](uint32_t r0) -> Quad {
         Quad q{0ull, 0ull, 0ull, 0ull};
-        if (vec && r0 + 4u <= n32) {
+        if (vec && (uint64_t)r0 + 4u <= (uint64_t)n32) {
             if (DT == ML_TYPE_FLOAT64 || DT == ML_TYPE_INT64) {
                 uint64_t t[2], u[2];
                 ld_stream_v2_u64((const unsigned long long*)c.data + r0, t);
@@ -1028,10 +1024,11 @@ __device__ TopEntry warp_topk_fixed(const SortDev& S, int64_t n, int k, int64_t 
                          (uint64_t)(int64_t)(int32_t)w[2], (uint64_t)(int64_t)(int32_t)w[3]};
             }
         } else {
-            if (r0 < n32) q.v0 = load_value(c, r0);
-            if (r0 + 1u < n32) q.v1 = load_value(c, r0 + 1u);
-            if (r0 + 2u < n32) q.v2 = load_value(c, r0 + 2u);
-            if (r0 + 3u < n32) q.v3 = load_value(c, r0 + 3u);
+            const uint64_t r = r0;
+            if (r < n32) q.v0 = load_value(c, r0);
+            if (r + 1u < n32) q.v1 = load_value(c, r0 + 1u);
+            if (r + 2u < n32) q.v2 = load_value(c, r0 + 2u);
+            if (r + 3u < n32) q.v3 = load_value(c, r0 + 3u);
         }
         return q;
     };
@@ -1317,9 +1314,6 @@ void launch_offsets_rebase(const uint32_t* src, int64_t n, uint32_t base, uint32
 }
 void launch_copy_bits(const uint64_t* src, int64_t n, uint64_t* dst, int64_t dst_off, cudaStream_t s) {
     if (n) k_copy_bits<<<grid_for(n, 8), kThreads, 0, s>>>(src, n, dst, dst_off);
-}
-void launch_fill_u32(uint32_t* p, uint32_t v, int64_t n, cudaStream_t s) {
-    if (n) k_fill_u32<<<grid_for(n, 8), kThreads, 0, s>>>(p, v, n);
 }
 
 }  // namespace mlg

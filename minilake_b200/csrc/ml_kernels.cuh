@@ -126,8 +126,7 @@ constexpr size_t kStaticScratchBytes = kStaticScanOff + kStaticScanBytes;  // 2,
 // Device address of the scratch array on the current device (cudaGetSymbolAddress).
 void* static_filter_scratch();
 
-// Fill / concatenation helpers
-void launch_fill_u32(uint32_t* p, uint32_t v, int64_t n, cudaStream_t s);
+// Concatenation helpers
 // dst[i] = src[i] - src[0] + base for i in 0..=n
 void launch_offsets_rebase(const uint32_t* src, int64_t n, uint32_t base, uint32_t* dst, cudaStream_t s);
 // OR the first n validity bits of src (nullptr = all valid) into dst at bit dst_off
