@@ -684,16 +684,17 @@ bool batchable(const PipeArgs& P) { return !P.has_chains; }
 // `full` when all K are rows).
 std::string tile_rows(const PipeArgs& P, int K, bool contig, const std::string& ind) {
     std::string s;
-    if (contig) {
-        s += ind + "const int64_t r0 = base + (int64_t)threadIdx.x * " + num(K) + ";\n";
-        s += ind + "const bool full = r0 + " + num(K) + " <= P.n;\n";
+    if (contig) {  // 32-bit row arithmetic (contig_ok bounds the row count below 2^32 - 2^16)
+        s += ind + "const uint32_t r0 = (uint32_t)base + threadIdx.x * " + num(K) + "u;\n";
+        s += ind + "const uint32_t n32 = (uint32_t)P.n;\n";
+        s += ind + "const bool full = r0 + " + num(K) + "u <= n32;\n";
     }
     for (int j = 0; j < K; j++) {
         std::string J = num(j), x = "x" + J, a = "a" + J;
         s += ind + "RowCtx " + x + ";\n";
         if (contig) {
-            s += ind + "bool " + a + " = r0 + " + J + " < P.n;\n";
-            s += ind + x + ".r = (uint32_t)(r0 + " + J + ");\n";
+            s += ind + "bool " + a + " = r0 + " + J + "u < n32;\n";
+            s += ind + x + ".r = r0 + " + J + "u;\n";
         } else {
             s += ind + "const int64_t i" + J + " = base + " + J + " * (int64_t)blockDim.x + threadIdx.x;\n";
             s += ind + "bool " + a + " = i" + J + " < P.n;\n";
@@ -708,7 +709,7 @@ std::string tile_rows(const PipeArgs& P, int K, bool contig, const std::string& 
 // Consecutive rows per thread need no selection vector and every fixed-width or dictionary
 // source column aligned to 16 bytes (the vector loads' width).
 bool contig_ok(const PipeArgs& P) {
-    if (P.sel) return false;
+    if (P.sel || P.n > 0xFFFF0000ll) return false;
     for (const DCol& c : P.cols)
         if (c.src == 0 && (c.kind == CK_FIXED || c.kind == CK_DICT) && ((uintptr_t)c.data & 15)) return false;
     return true;
