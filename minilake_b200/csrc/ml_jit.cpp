@@ -285,6 +285,43 @@ class Gen {
     // Load `slots` for the batched rows x0.. (alive a0..) into pre[j].  With consecutive rows a
     // fixed-width or dictionary-coded source column is read with one vector load per thread when
     // all its rows are in range, its validity with one word.
+    // Width in bytes of a column's per-row value as the vector loads read it (0: not loaded so).
+    int vec_width(int a) const {
+        const DCol& c = P_.cols[a];
+        if (c.src != 0 || (c.kind != CK_FIXED && c.kind != CK_DICT)) return 0;
+        if (c.kind == CK_DICT) return 4;
+        if (c.dt == ML_TYPE_BOOL) return 1;
+        return (c.dt == ML_TYPE_INT32 || c.dt == ML_TYPE_DATE) ? 4 : 8;
+    }
+    void vec_decl(int W, const std::string& t) {
+        const int K = rows_per_thread;
+        if (W == 4) line("uint32_t " + t + "[" + num(K) + "];");
+        else if (W == 8) line("uint64_t " + t + "[" + num(K) + "];");
+        else line("uint64_t " + t + ";");
+    }
+    // The K consecutive values of slot `a` from x0.r on into `t` (16-byte loads: the widest this
+    // toolchain's runtime compiler accepts).
+    void vec_load(int a, int W, const std::string& t) {
+        const int K = rows_per_thread;
+        const std::string C = "P.cols[" + num(a) + "]";
+        if (W == 4) {
+            for (int q = 0; q < K; q += 4)
+                line("ld_stream_v4_u32((const uint32_t*)" + C + ".data + x0.r + " + num(q) + ", " + t + " + " + num(q) + ");");
+        } else if (W == 8) {
+            for (int q = 0; q < K; q += 2)
+                line("ld_stream_v2_u64((const unsigned long long*)" + C + ".data + x0.r + " + num(q) + ", " + t + " + " +
+                     num(q) + ");");
+        } else {
+            line(t + " = " +
+                 (K == 8 ? "ld_stream_u64((const unsigned long long*)(" : "(uint64_t)ld_stream_u32((const uint32_t*)(") +
+                 "(const uint8_t*)" + C + ".data + x0.r));");
+        }
+    }
+
+    // Load `slots` for the batched rows x0.. (alive a0..) into pre[j].  With consecutive rows a
+    // fixed-width or dictionary-coded source column is read with one vector load per thread when
+    // all its rows are in range, its validity with one word; a column loaded ahead of the tile's
+    // first stage (`spec_vals`) is reused when that speculative load ran.
     void preload_rows(const std::set<int>& slots, std::vector<std::map<int, V>>& pre) {
         const int K = rows_per_thread;
         pre.assign(K, {});
@@ -307,32 +344,29 @@ class Gen {
         any += ")";
         for (int a : slots) {
             const DCol& c = P_.cols[a];
-            const bool vec = c.src == 0 && (c.kind == CK_FIXED || c.kind == CK_DICT);
-            if (!vec) {
+            const int W = vec_width(a);
+            if (!W) {
                 per_row({a});
                 continue;
             }
-            const int W = c.kind == CK_DICT ? 4 : (c.dt == ML_TYPE_BOOL ? 1 : (c.dt == ML_TYPE_INT32 || c.dt == ML_TYPE_DATE) ? 4 : 8);
-            const std::string n = num(fresh()), C = "P.cols[" + num(a) + "]", t = "t" + n;
+            const std::string n = num(fresh()), C = "P.cols[" + num(a) + "]";
             for (int j = 0; j < K; j++) {
                 line("uint64_t c" + n + "_" + num(j) + " = 0;");
                 line("bool n" + n + "_" + num(j) + " = false;");
             }
-            open("if (full && " + any + ") {");
-            if (W == 4) {  // 16-byte loads (the widest this toolchain's runtime compiler accepts)
-                line("uint32_t " + t + "[" + num(K) + "];");
-                for (int q = 0; q < K; q += 4)
-                    line("ld_stream_v4_u32((const uint32_t*)" + C + ".data + x0.r + " + num(q) + ", " + t + " + " + num(q) +
-                         ");");
-            } else if (W == 8) {
-                line("uint64_t " + t + "[" + num(K) + "];");
-                for (int q = 0; q < K; q += 2)
-                    line("ld_stream_v2_u64((const unsigned long long*)" + C + ".data + x0.r + " + num(q) + ", " + t + " + " +
-                         num(q) + ");");
+            auto ahead = spec_vals.find(a);
+            std::string t;
+            if (ahead != spec_vals.end()) {
+                t = ahead->second;
+                open("if (specd || (full && " + any + ")) {");
+                open("if (!specd) {");
+                vec_load(a, W, t);
+                close();
             } else {
-                line(std::string("const uint64_t ") + t + " = " +
-                     (K == 8 ? "ld_stream_u64((const unsigned long long*)(" : "(uint64_t)ld_stream_u32((const uint32_t*)(") +
-                     "(const uint8_t*)" + C + ".data + x0.r));");
+                t = "t" + n;
+                open("if (full && " + any + ") {");
+                vec_decl(W, t);
+                vec_load(a, W, t);
             }
             for (int j = 0; j < K; j++) {
                 const std::string J = num(j), v = "c" + n + "_" + J;
@@ -365,6 +399,19 @@ class Gen {
             for (int j = 0; j < K; j++) pre[j][a] = V{"c" + n + "_" + num(j), "n" + n + "_" + num(j)};
         }
     }
+
+    // Speculative loads: with consecutive rows, the source columns that only later stages (and
+    // the sink: `sink_slots`) read are loaded at the start of the tile, together with the first
+    // stage's columns, when `spec` holds, so the tile waits for memory once instead of once per
+    // stage.  `spec` is each thread's own guess: at least half of its rows passed the first stage
+    // in its previous tile (rows that then fail only waste bytes that are read anyway when most
+    // rows pass).
+    // Only where the extra registers are free and the first stage is a filter: kernels whose
+    // residency shared memory already limits (per-thread accumulators); a selective first join
+    // probe or a register-limited kernel loses more than it gains (measured).
+    bool speculate = false;
+    std::set<int> sink_slots;
+    std::map<int, std::string> spec_vals;
 
     // Hoisted per-thread load of an instruction field (literal bits, arena offsets, counts).
     std::string field(int idx, const char* f, const char* type) {
@@ -584,7 +631,39 @@ class Gen {
             for (int j = 0; j < K; j++) any += (j ? " || a" : "a") + num(j);
             line("if (!__any_sync(0xFFFFFFFFu, " + any + ")) " + tile_skip);
         };
+        spec_vals.clear();
+        if (contig && speculate && P_.nstages > 0 && P_.stages[0].kind == 0) {
+            std::set<int> first, later = sink_slots;
+            const Stage s0 = P_.stages[0];
+            if (s0.kind == 0) slots_of(P_.filters[s0.idx], first);
+            else for (int k = 0; k < P_.probes[s0.idx].keys.nkeys; k++) slots_of(P_.probes[s0.idx].keys.prog[k], first);
+            for (int s = 1; s < P_.nstages; s++) {
+                const Stage st = P_.stages[s];
+                if (st.kind == 0) slots_of(P_.filters[st.idx], later);
+                else for (int k = 0; k < P_.probes[st.idx].keys.nkeys; k++) slots_of(P_.probes[st.idx].keys.prog[k], later);
+            }
+            for (int a : later) {
+                const int W = vec_width(a);
+                if (!W || first.count(a)) continue;
+                const std::string t = "sp" + num(fresh());
+                vec_decl(W, t);
+                spec_vals[a] = t;
+            }
+            if (!spec_vals.empty()) {
+                if (hoisted_.insert("spec").second) pre_ << "    bool spec = true;  // speculative loads (see Gen::spec_vals)\n";
+                // this tile's decision (spec itself is updated for the next tile after stage 0)
+                line("const bool specd = full && spec;");
+                open("if (specd) {");
+                for (auto& e : spec_vals) vec_load(e.first, vec_width(e.first), e.second);
+                close();
+            }
+        }
         for (int s = 0; s < P_.nstages; s++) {
+            if (s == 1 && !spec_vals.empty()) {  // this tile's first-stage pass rate decides the next tile
+                std::string alive;
+                for (int j = 0; j < K; j++) alive += (j ? " + (a" : "(a") + num(j) + " ? 1 : 0)";
+                line("spec = 2 * (" + alive + ") >= " + num(K) + ";");
+            }
             if (s > 0) skip_dead_tile(s - 1);
             const Stage st = P_.stages[s];
             std::set<int> slots;
@@ -663,6 +742,11 @@ class Gen {
                 if (st.idx == P_.head_probe) line(x + ".head = b;");
                 close();
             });
+        }
+        if (P_.nstages == 1 && !spec_vals.empty()) {  // a single stage: decide before the sink
+            std::string alive;
+            for (int j = 0; j < K; j++) alive += (j ? " + (a" : "(a") + num(j) + " ? 1 : 0)";
+            line("spec = 2 * (" + alive + ") >= " + num(K) + ";");
         }
         if (P_.nstages > 0) skip_dead_tile(P_.nstages - 1);
         sink(rows);
@@ -954,6 +1038,11 @@ std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArg
     const bool batched = batchable(P);
     g.contig = contig && batched;
     g.tile_skip = "continue;";  // the tile loop of row_loop
+    g.speculate = A.priv_groups > 0;
+    if (A.group_probe < 0 && !A.ungrouped)
+        for (int k = 0; k < A.keys.nkeys; k++) g.slots_of(A.keys.prog[k], g.sink_slots);
+    for (int k = 0; k < A.nagg; k++)
+        if (A.aggs[k].has_arg && A.aggs[k].func != ML_AGG_COUNT_STAR) g.slots_of(A.aggs[k].arg, g.sink_slots);
     if (batched) {
         g.fail = "break;";
         g.batched_stages([&](auto&& rows) {
