@@ -2,7 +2,8 @@
 
 tests/jit_codegen_probe.cpp asks the library for the sources it generates for the filter,
 cardinality-scan and aggregate kernels (strided and consecutive-row tiles, per-thread
-accumulators and direct group slots, a semi-join probe, GROUP BY the dense join key); each is
+accumulators, direct group slots and speculative loads, a semi-join probe, GROUP BY the dense
+join key); each is
 compiled here with NVRTC, with the device headers the library embeds, the way ml_jit.cpp does.
 """
 import os
@@ -81,3 +82,6 @@ def test_specialized_kernels_compile_for_sm_100a(tmp_path):
     assert "dense_member" in sources["aggregate_semi_join_contig"]
     assert "dense_slot" in sources["aggregate_dense_groups_contig"]
     assert "dsl[dsg]" in sources["aggregate_groups_contig"]
+    # per-thread accumulators after a filter: speculative loads in the consecutive-row form only
+    assert "specd" in sources["aggregate_groups_contig"] and "specd" not in sources["aggregate_groups_strided"]
+    assert "specd" not in sources["aggregate_dense_groups_contig"]
