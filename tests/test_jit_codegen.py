@@ -3,8 +3,8 @@
 tests/jit_codegen_probe.cpp asks the library for the sources it generates for the filter,
 cardinality-scan and aggregate kernels (strided and consecutive-row tiles, per-thread
 accumulators, direct group slots and speculative loads, a semi-join probe, GROUP BY the dense
-join key); each is
-compiled here with NVRTC, with the device headers the library embeds, the way ml_jit.cpp does.
+join key); each is compiled here with NVRTC, with the device headers the library embeds, the
+way ml_jit.cpp does.
 """
 import os
 import re
