@@ -1043,7 +1043,6 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
     Pipeline kp(ctx);
     kp.build(nullptr, 0, j->out_types.data(), (int)j->out_types.size());
     KeyLayout L = kp.key_layout(j->keys.exprs.data(), (int)j->keys.exprs.size(), kp.out, false, nullptr);
-    kp.upload();
     jt->nwords = L.nwords;
     for (auto& k : j->keys.exprs) {  // which build column each key reads (for GROUP BY the join key)
         ExprNode e = parse_expr(k);
@@ -1095,7 +1094,8 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
     CK(cudaMemsetAsync(jt->slots.get(), 0, slot_bytes, s));
     ErrWord ew(ctx);
     CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
-    if (nh) {
+    if (nh) {  // the key programs run only here (a dense index reads the key column directly)
+        kp.upload();
         Staging st(ctx);
         Pipeline::Launch LA;
         auto views = device_views(jt->batch);
