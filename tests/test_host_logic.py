@@ -70,3 +70,21 @@ def test_operator_line_arithmetic():
     assert math.isclose(line["frac_of_hbm_peak"], round(7200.0 / 6650.0, 3))
     peak, kind = opbench.hbm_peak()
     assert peak > 0 and kind in ("measured", "fallback")
+
+
+def test_bench_data_shards_and_traffic_record():
+    """bench.py: each rank's fact rows reference only its own keys (key % world == rank), the
+    dimension keys are a permutation of 1..1.5M, and the DRAM bytes per launch recorded in the
+    committed ncu summary are readable (the bench line's `roofline.traffic`)."""
+    import bench
+    for world in (1, 2, 4):
+        for rank in range(world):
+            key, fk, d, v = bench.make_data(rank, world, fact_rows=20_000)
+            assert np.array_equal(np.sort(key), np.arange(1, bench.DIM_ROWS + 1))
+            assert fk.min() >= 1 and fk.max() <= bench.DIM_ROWS
+            assert np.all(fk % world == rank)
+            assert d.min() >= 0 and d.max() < 2557 and v.min() >= 900.0 and v.max() < 105000.0
+    traffic = bench.profiled_traffic()
+    assert traffic is not None and traffic >= bench.FACT_ROWS * bench.BYTES_PER_ROW
+    peak, kind = bench.measured_peak()
+    assert peak > 0 and kind in ("measured", "fallback")
