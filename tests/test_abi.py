@@ -49,3 +49,11 @@ def test_context_rejects_unknown_flags():
     assert rc == abi.ERR_INVALID and not out.value
     lib.ml_gpu_last_error.restype = ctypes.c_char_p
     assert b"unknown context flags" in lib.ml_gpu_last_error()
+
+
+def test_rust_binding_declares_every_entry_point():
+    """INTEGRATION.md's Rust `ffi.rs` block declares each function include/*.h declares."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    rust = set(re.findall(r"pub fn (ml_gpu_\w+)\(", text))
+    missing = [n for n in declared() if n not in rust]
+    assert not missing, missing
