@@ -296,7 +296,7 @@ def gpu_arm(args):
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f64",
-            "data": "synthetic (seeded numpy PCG64; BASELINE shapes)",
+            "data": "synthetic (seeded numpy PCG64 with the workload's shapes and value distributions)",
             "config": {"workload": "join + high-cardinality GROUP BY + top-10: dim 1.5M rows (key i64), "
                                    f"fact {rows / 1e6:g}M rows per GPU (fk i64, d i32, v f64), d > 1200, GROUP BY fk, "
                                    "SUM(v), COUNT(*), ORDER BY SUM(v) DESC, fk LIMIT 10",
@@ -383,7 +383,7 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded numpy PCG64; BASELINE shapes)",
+        "data": "synthetic (seeded numpy PCG64 with the workload's shapes and value distributions)",
         "config": {"workload": "join + high-cardinality GROUP BY + top-10: dim 1.5M rows (key i64), "
                                "fact 60M rows (fk i64, d i32, v f64), d > 1200, GROUP BY fk, SUM(v), COUNT(*), "
                                "ORDER BY SUM(v) DESC, fk LIMIT 10",
