@@ -44,7 +44,7 @@ extern "C" {
 enum {
     ML_OK = 0,
     ML_ERR_INVALID = 1,     /* MiniLakeError::Internal / Execution (bad arguments, type errors) */
-    ML_ERR_BUDGET = 2,      /* MiniLakeError::ResourcesExhausted (memory.rs:326-339) */
+    ML_ERR_BUDGET = 2,      /* MiniLakeError::ResourcesExhausted (memory.rs:114-128) */
     ML_ERR_CUDA = 3,        /* a CUDA runtime call failed */
     ML_ERR_TIMEOUT = 4,     /* a bounded device-side wait ran out */
     ML_ERR_UNSUPPORTED = 5, /* MiniLakeError::Unsupported */
@@ -191,7 +191,7 @@ enum { ML_CTX_PROFILE = 2, ML_CTX_INTERPRET = 4 };
  * MemoryPool limit (memory.rs:22-26) applied to device bytes; 0 = unlimited. */
 int ml_gpu_ctx_create(int device, uint64_t hbm_budget_bytes, uint32_t flags, ml_ctx** out);
 int ml_gpu_ctx_destroy(ml_ctx* ctx);
-/* MemoryPool::used / peak / limit (memory.rs:250-263). */
+/* MemoryPool::used / peak / limit (memory.rs:39-53). */
 int ml_gpu_pool_stats(ml_ctx* ctx, uint64_t* used, uint64_t* peak, uint64_t* limit);
 /* Details of the last ML_ERR_BUDGET on this thread: ResourcesExhausted{operator, requested,
  * used, limit} (error.rs).  `op` receives a NUL-terminated operator name. */
@@ -259,7 +259,7 @@ int ml_gpu_project(ml_ctx* ctx, const ml_expr* expr, const ml_column* cols, int3
 int ml_gpu_hash_columns(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64_t nrows,
                         const uint32_t* sel, int64_t nsel, int32_t location, uint64_t* out);
 
-/* ---- Sink: HashAggregateSink (operators/aggregate/hash.rs:434-634) ------------- */
+/* ---- Sink: HashAggregateSink (operators/aggregate/hash.rs:285-484) ------------- */
 /* `input_types` describes the pipeline source's columns (the prologue's first input).
  * `size_hint` presizes the device table (expected number of groups; 0 = start small and
  * grow on overflow, swiss.rs:287-301). */

@@ -1223,7 +1223,7 @@ int ml_gpu_join_probe(ml_ctx* ctx, ml_join_table* table, const ml_expr* key_expr
 }  // extern "C"
 
 // =====================================================================================================
-// HashAggregateSink (aggregate/hash.rs:434-634)
+// HashAggregateSink (aggregate/hash.rs:285-484)
 // =====================================================================================================
 namespace {
 struct AggState {

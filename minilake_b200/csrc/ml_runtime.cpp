@@ -23,7 +23,7 @@ void check_cuda(cudaError_t e, const char* what) {
     if (e != cudaSuccess) raise(ML_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// ---- memory pool (memory.rs:265-289) ------------------------------------------------------------
+// ---- memory pool (memory.rs:58-77) ------------------------------------------------------------
 bool MemoryPool::try_grow(uint64_t bytes, uint64_t* observed) {
     uint64_t cur = used.load(std::memory_order_relaxed);
     for (;;) {

@@ -43,14 +43,14 @@ struct MemoryPool {
     uint64_t limit;
     std::atomic<uint64_t> used{0}, peak{0};
     explicit MemoryPool(uint64_t lim) : limit(lim ? lim : UINT64_MAX) {}
-    // CAS loop: check + add is one atomic step (memory.rs:265-289)
+    // CAS loop: check + add is one atomic step (memory.rs:58-77)
     bool try_grow(uint64_t bytes, uint64_t* observed);
     void shrink(uint64_t bytes) { used.fetch_sub(bytes); }
 };
 
 class Ctx;
 
-// RAII reservation (MemoryReservation, memory.rs:296-369).
+// RAII reservation (MemoryReservation, memory.rs:84-158).
 class Reservation {
    public:
     Reservation(Ctx* ctx, std::string name) : ctx_(ctx), name_(std::move(name)) {}

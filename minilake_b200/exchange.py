@@ -5,7 +5,7 @@ k % world == r (the dimension table is replicated).  Every group then lives on e
 each rank aggregates its own groups with no data-path collective, and the only exchange is the
 final one: the ranks' local top-N lists are gathered and merged (the global top N of disjoint
 groups is inside the union of the local top Ns), as MiniLake's distributed mode merges partial
-results on its coordinator (minilake-dist/src/split.rs:79-150).
+results on its coordinator (minilake-dist/src/split.rs:54-127).
 """
 from __future__ import annotations
 

@@ -35,7 +35,7 @@ class MiniLakeError(RuntimeError):
 
 
 class ResourcesExhausted(MiniLakeError):
-    """ResourcesExhausted{operator, requested, used, limit} (memory.rs:326-339)."""
+    """ResourcesExhausted{operator, requested, used, limit} (memory.rs:114-128)."""
 
     def __init__(self, code, msg, operator, requested, used, limit):
         super().__init__(code, msg)
@@ -355,7 +355,7 @@ def _local(sink, create, fn_sink, fn_combine) -> LocalSink:
 
 # ---- sinks ------------------------------------------------------------------------------------
 class HashAggregateSink:
-    """GROUP BY (operators/aggregate/hash.rs:434-634); no GROUP BY = ungrouped (ungrouped.rs)."""
+    """GROUP BY (operators/aggregate/hash.rs:285-484); no GROUP BY = ungrouped (ungrouped.rs)."""
 
     def __init__(self, ctx: Context, input_types: Sequence[int], group_exprs: Sequence[tuple],
                  aggs: Sequence[abi.AggSpec], prologue: Sequence[abi.PipeOp] = (), size_hint: int = 0):

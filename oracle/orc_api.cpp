@@ -139,7 +139,7 @@ void drive(const ml_column* cols, int nmorsels, int ncols, const int64_t* rows, 
         cancel);
 }
 
-// ---- HashAggregate sink (aggregate/hash.rs:434-634, ungrouped.rs) --------------------
+// ---- HashAggregate sink (aggregate/hash.rs:285-484, ungrouped.rs) --------------------
 struct AggShared {
     std::vector<Expr> group;
     std::vector<int> key_types;
@@ -201,7 +201,7 @@ uint64_t orc_fold_mul(uint64_t a, uint64_t b) { return fold_mul(a, b); }
 uint64_t orc_swar_match_tag(uint64_t g, uint8_t tag) { return swar_match_tag(g, tag); }
 uint64_t orc_swar_match_empty(uint64_t g) { return swar_match_empty(g); }
 
-// Property-test driver for SwissTable::find_or_insert_batch (proptest_tables.rs:97-123):
+// Property-test driver for SwissTable::find_or_insert_batch (proptest_tables.rs:14-41):
 // `keys` holds nbatch batches (sizes in `sizes`); hash_mode 0 = hash_u64, 1 = x % 4,
 // 2 = constant 42.  Writes the payload of every key into `out`; returns len via *len and
 // verifies every stored key with find() (status ML_ERR_INTERNAL on mismatch).
@@ -240,7 +240,7 @@ int orc_swiss_batches(const uint64_t* keys, const int64_t* sizes, int nbatch, in
     ORC_CATCH
 }
 
-// MemoryPool known-answer driver (memory.rs:371-412): ops[i] = (reservation id, kind, bytes)
+// MemoryPool known-answer driver (memory.rs:160-201): ops[i] = (reservation id, kind, bytes)
 // kind 0 = try_grow, 1 = try_resize, 2 = drop.  results[i] = status; used/peak after each op.
 int orc_pool_script(uint64_t limit, const int64_t* ops, int nops, int* results, uint64_t* used, uint64_t* peak) {
     ORC_TRY
@@ -327,7 +327,7 @@ int orc_hashagg_run(const ml_column* cols, int nmorsels, int ncols, const int64_
     drive<AggLocal>(
         cols, nmorsels, ncols, rows, ops, threads, (size_t)batch_size,
         [&]() { return std::make_unique<AggLocal>(&sh); },
-        [&](std::unique_ptr<AggLocal> l) {  // HashAggLocal::combine (hash.rs:589-633)
+        [&](std::unique_ptr<AggLocal> l) {  // HashAggLocal::combine (aggregate/hash.rs:439-484)
             std::lock_guard<std::mutex> g(sh.mu);
             if (sh.group.empty()) {
                 if (!sh.have_ungrouped) {

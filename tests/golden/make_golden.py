@@ -98,7 +98,7 @@ def known_answers():
             ["%special%requests%", "requests special", False], ["a_c", "abc", True], ["a_c", "abbc", False],
             ["%", "", True],
         ],
-        # kernels/string.rs:204-216
+        # kernels/string.rs:37-49
         "like_on_plain_strings": {"values": ["PROMO A", "STD", "PROMO B"], "like": [True, False, True],
                                   "in_std": [False, True, False]},
         # expr/eval.rs:548-612: a = [1, 5, 10, 20] (INT64), b = [0.5, 1.5, 2.5, 3.5]
@@ -112,7 +112,7 @@ def known_answers():
             "values": [1.0, 2.0, 3.0, 4.0], "valid": [True, True, False, True], "gids": [0, 1, 0, 1],
             "sum": [1.0, 6.0], "avg_group1": 3.0,
         },
-        # minilake-hashtable/src/swiss.rs:377-419
+        # minilake-hashtable/src/swiss.rs:308-350
         "swiss": {
             "swar_group": list(group), "swar_tag": 5, "swar_hits_include": [0, 3], "match_empty": EMPTY << 8,
             "grow_keys": 10_000, "absent_key": 99_999, "full_collision_keys": 100,
@@ -121,7 +121,7 @@ def known_answers():
         "hash": {"distinct_u64": 10_000, "bytes_differ": [["abc", "abd"], ["", "\u0000"]]},
         # kernels/scalar_ops.rs:158-164
         "scalar_kleene": {"null_and_false": False, "null_or_false": None},
-        # minilake-exec/src/memory.rs:375-392: (reservation, op, bytes) with op 0 grow, 1 resize, 2 drop
+        # minilake-exec/src/memory.rs:163-180: (reservation, op, bytes) with op 0 grow, 1 resize, 2 drop
         "memory_pool": {
             "limit": 100,
             "script": [[0, 0, 60], [1, 0, 50], [1, 0, 40], [0, 2, 0], [1, 1, 10]],

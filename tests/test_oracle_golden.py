@@ -61,7 +61,7 @@ def test_arith():  # arith.rs:136-153
     assert r.values[0] == m["out"]
 
 
-def test_like():  # like.rs:134-166, string.rs:204-216
+def test_like():  # like.rs:134-166, string.rs:37-49
     for pat, s, want in G["like_matching"]:
         r = orc.project(Like(Col(0), pat), BOOL, [utf8_plain([s.encode()])])[0]
         assert bool(r.values[0]) == want, (pat, s)
@@ -95,7 +95,7 @@ def test_accumulator_grouped_sum_avg():  # accumulator.rs:600-623
     assert out[2].values[order][1] == g["avg_group1"]
 
 
-def test_hash_and_swar():  # hash.rs:60-68, swiss.rs:377-384
+def test_hash_and_swar():  # hash.rs:60-68, swiss.rs:308-316
     g = G["hash"]
     hs = {orc.LIB.orc_hash_u64(i) for i in range(g["distinct_u64"])}
     assert len(hs) == g["distinct_u64"]
@@ -109,7 +109,7 @@ def test_hash_and_swar():  # hash.rs:60-68, swiss.rs:377-384
     assert orc.LIB.orc_swar_match_empty(group) == s["match_empty"]
 
 
-def test_swiss_growth_and_collisions():  # swiss.rs:386-419, proptest_tables.rs:194-262
+def test_swiss_growth_and_collisions():  # swiss.rs:317-350, proptest_tables.rs:14-79
     s = G["swiss"]
     keys = list(range(s["grow_keys"]))
     out, n, cap = orc.swiss_batches([keys], 0)
@@ -128,7 +128,7 @@ def test_swiss_growth_and_collisions():  # swiss.rs:386-419, proptest_tables.rs:
             assert list(out) == exp and n == len(ref)
 
 
-def test_memory_pool():  # memory.rs:375-392
+def test_memory_pool():  # memory.rs:163-180
     g = G["memory_pool"]
     res, used, peak = orc.pool_script(g["limit"], g["script"])
     names = {abi.OK: "ok", abi.ERR_BUDGET: "budget"}
