@@ -222,16 +222,17 @@ int ml_gpu_batch_destroy(ml_batch* b);
 /* ---- Operator: FilterOperator (operators/filter.rs:19-25, expr/eval.rs:167-196) --- */
 /* Rows of the selection (or of 0..n when sel_in is NULL) where `pred` is TRUE, in increasing
  * order.  sel_out must have room for n (or nsel_in) entries; sel_in/sel_out are host or
- * device memory as `location` says. */
+ * device memory as `location` says.  The call's device temporaries (flag words, counts, the
+ * selection) are charged to the context's HBM budget: ML_ERR_BUDGET when it has no room. */
 int ml_gpu_filter(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32_t ncols,
                   int64_t nrows, const uint32_t* sel_in, int64_t nsel_in, int32_t location,
                   uint32_t* sel_out, int64_t* nsel_out);
 
 /* ---- FilterOperator without allocation (no counterpart in the reference) ----------- */
 /* ml_gpu_filter for callers that cannot allocate device memory: a query whose HBM budget
- * is spent (every new reservation would fail with ML_ERR_BUDGET) but that still has to
- * filter, and latency-critical callers for which cudaMalloc / cudaFree are off limits
- * because they can synchronize the whole device.  Same predicate semantics, inputs and
+ * is spent (ml_gpu_filter, like every new reservation, would fail with ML_ERR_BUDGET) but
+ * that still has to filter, and latency-critical callers for which cudaMalloc / cudaFree are
+ * off limits because they can synchronize the whole device.  Same predicate semantics, inputs and
  * result as ml_gpu_filter (ordered selection, count on the host), with these limits:
  *  - every column is device resident (ML_LOC_DEVICE); sel_in (optional) and sel_out are
  *    device pointers; sel_out has room for nsel_in (or nrows) entries;
@@ -243,7 +244,8 @@ int ml_gpu_filter(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32
  *    current): make that first call before any stream capture.  Nothing in the array has
  *    to start at zero (each call clears its own error word);
  *  - calls on the same device share the array, so overlapping calls would race on it: each
- *    call holds a per-device lock until its result is on the host.
+ *    call holds a per-device lock until its work on the device has finished (a call that
+ *    fails part-way drains its stream before it releases the lock).
  * It allocates no device memory and no pinned host memory; the predicate is compiled on the
  * host heap. */
 int ml_gpu_filter_static(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32_t ncols,

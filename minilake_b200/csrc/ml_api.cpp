@@ -32,11 +32,12 @@ bool is_device_ptr(const void* p) {
 }
 
 // Selection vector on the device (copied when it is host memory).
-const uint32_t* device_sel(Ctx* ctx, const uint32_t* sel, int64_t nsel, DevBuf& hold, cudaStream_t s) {
+const uint32_t* device_sel(Ctx* ctx, const uint32_t* sel, int64_t nsel, DevBuf& hold, cudaStream_t s,
+                           Reservation* res = nullptr) {
     if (!sel) return nullptr;
     if (nsel < 0) raise(ML_ERR_INVALID, "negative selection length");
     if (is_device_ptr(sel)) return sel;
-    hold = DevBuf(ctx, std::max<size_t>((size_t)nsel * 4, 4), nullptr);
+    hold = DevBuf(ctx, std::max<size_t>((size_t)nsel * 4, 4), res);
     if (nsel) CK(cudaMemcpyAsync(hold.get(), sel, (size_t)nsel * 4, cudaMemcpyHostToDevice, s));
     return hold.get<uint32_t>();
 }
@@ -709,15 +710,18 @@ int ml_gpu_filter(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32
     p.build(&op, 1, types.data(), ncols);
     p.upload();
     Staging st(ctx);
+    // the call's device temporaries count against the query's HBM budget (ResourcesExhausted
+    // when it is spent); ml_gpu_filter_static allocates none
+    Reservation res(ctx, "Filter");
     DevBuf sel_hold;
-    const uint32_t* dsel = device_sel(ctx, sel_in, nsel_in, sel_hold, s);
+    const uint32_t* dsel = device_sel(ctx, sel_in, nsel_in, sel_hold, s, &res);
     Pipeline::Launch L;
     p.prepare(L, cols, ncols, nrows, dsel, nsel_in, s, st, nullptr);
     ErrWord ew(ctx);
     CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
     L.P.err = ew.d.get<uint32_t>();
     DevBuf out;
-    int64_t k = run_select(ctx, p, L.P, out, s);
+    int64_t k = run_select(ctx, p, L.P, out, s, &res);
     CK(cudaMemcpyAsync(ew.h, ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
     if (k) CK(cudaMemcpyAsync(sel_out, out.get(), (size_t)k * 4,
                               location == ML_LOC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
@@ -741,20 +745,17 @@ int ml_gpu_filter_static(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols
     REQUIRE(ctx->device >= 0 && ctx->device < kStaticMaxDevices, "device index out of range");
     for (int c = 0; c < ncols; c++)
         REQUIRE(cols[c].location == ML_LOC_DEVICE, "ml_gpu_filter_static reads device-resident columns only");
+    if (sel_in) REQUIRE(nsel_in >= 0, "bad selection length");  // nsel_in is ignored without a selection
+    if (nrows > 0xFFFFFFFFll)
+        raise(ML_ERR_INVALID, "ml_gpu_filter_static: a batch of " + std::to_string(nrows) +
+                                  " rows; row ids are 32-bit, so a batch holds at most 4294967295 rows");
     const int64_t n = sel_in ? nsel_in : nrows;
-    REQUIRE(nsel_in >= 0, "bad selection length");
-    if (n > kStaticFilterMaxRows || nrows > 0xFFFFFFFFll)
-        raise(ML_ERR_INVALID, "ml_gpu_filter_static: " + std::to_string(n) + " rows exceed the static scratch limit of " +
-                                  std::to_string(kStaticFilterMaxRows) + " rows per call");
+    if (n > kStaticFilterMaxRows)
+        raise(ML_ERR_INVALID, "ml_gpu_filter_static: " + std::to_string(n) + (sel_in ? " selected rows" : " rows") +
+                                  " exceed the static scratch limit of " + std::to_string(kStaticFilterMaxRows) +
+                                  " rows per call");
     ctx->set_current();
-    std::lock_guard<std::mutex> dev_lock(g_static_mu[ctx->device]);
-    if (!g_static_base[ctx->device]) {  // first call on this device: look the array up (device is current)
-        g_static_base[ctx->device] = (uint8_t*)static_filter_scratch();
-        REQUIRE(g_static_base[ctx->device], "cudaGetSymbolAddress failed for the static filter scratch");
-    }
-    uint8_t* base = g_static_base[ctx->device];
-    std::lock_guard<std::mutex> g(ctx->op_mu);
-    cudaStream_t s = ctx->stream;
+    // everything that is checked on the host comes before the first copy into the shared array
     std::vector<int32_t> types;
     for (int c = 0; c < ncols; c++) types.push_back(cols[c].dtype);
     Pipeline p(ctx);
@@ -768,11 +769,26 @@ int ml_gpu_filter_static(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols
         raise(ML_ERR_INVALID, "ml_gpu_filter_static: the predicate compiles to " + std::to_string(pbytes) +
                                   " bytes of program and " + std::to_string(abytes) + " bytes of literals; the limits are " +
                                   std::to_string(kStaticProgBytes) + " and " + std::to_string(kStaticArenaBytes));
-    if (pbytes) CK(cudaMemcpyAsync(base + kStaticProgOff, p.C.code.data(), pbytes, cudaMemcpyHostToDevice, s));
-    if (abytes) CK(cudaMemcpyAsync(base + kStaticArenaOff, p.C.arena.data(), abytes, cudaMemcpyHostToDevice, s));
+    std::lock_guard<std::mutex> dev_lock(g_static_mu[ctx->device]);
+    if (!g_static_base[ctx->device]) {  // first call on this device: look the array up (device is current)
+        g_static_base[ctx->device] = (uint8_t*)static_filter_scratch();
+        REQUIRE(g_static_base[ctx->device], "cudaGetSymbolAddress failed for the static filter scratch");
+    }
+    uint8_t* base = g_static_base[ctx->device];
+    std::lock_guard<std::mutex> g(ctx->op_mu);
+    cudaStream_t s = ctx->stream;
+    // Declared after the locks, so destroyed before them: whichever way the call ends (an error
+    // raised after some copies or kernels were queued included), the stream has drained before
+    // another call may touch the array.
+    struct Drain {
+        cudaStream_t s;
+        ~Drain() { cudaStreamSynchronize(s); }
+    } drain{s};
     Staging st(ctx);  // unused: device-resident columns are read in place
     Pipeline::Launch L;
     p.prepare(L, cols, ncols, nrows, sel_in, nsel_in, s, st, nullptr, base + kStaticTablesOff, kStaticTablesBytes);
+    if (pbytes) CK(cudaMemcpyAsync(base + kStaticProgOff, p.C.code.data(), pbytes, cudaMemcpyHostToDevice, s));
+    if (abytes) CK(cudaMemcpyAsync(base + kStaticArenaOff, p.C.arena.data(), abytes, cudaMemcpyHostToDevice, s));
     L.P.prog = (const Instr*)(base + kStaticProgOff);
     L.P.arena = base + kStaticArenaOff;
     uint32_t* err = (uint32_t*)(base + kStaticErrOff);

@@ -344,9 +344,9 @@ bool Pipeline::reads_nullable(const Prog& p, const Launch& L) const {
     return false;
 }
 
-uint64_t scan_counts(Ctx* ctx, const uint32_t* counts, int64_t n, DevBuf& offsets, cudaStream_t s) {
-    offsets = DevBuf(ctx, (size_t)(n + 1) * 8, nullptr);
-    DevBuf scratch(ctx, scan_scratch_words(n) * 8, nullptr);
+uint64_t scan_counts(Ctx* ctx, const uint32_t* counts, int64_t n, DevBuf& offsets, cudaStream_t s, Reservation* res) {
+    offsets = DevBuf(ctx, (size_t)(n + 1) * 8, res);
+    DevBuf scratch(ctx, scan_scratch_words(n) * 8, res);
     launch_scan_u32(counts, offsets.get<uint64_t>(), n, scratch.get<uint64_t>(), s);
     ctx->count_launch(3);
     uint64_t total = 0;
@@ -355,10 +355,10 @@ uint64_t scan_counts(Ctx* ctx, const uint32_t* counts, int64_t n, DevBuf& offset
     return total;
 }
 
-int64_t run_select(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, DevBuf& out, cudaStream_t s) {
+int64_t run_select(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, DevBuf& out, cudaStream_t s, Reservation* res) {
     int nb = select_blocks(P.n);
-    DevBuf bits(ctx, std::max<size_t>((size_t)(P.n + 31) / 32 * 4, 4), nullptr);
-    DevBuf counts(ctx, std::max<size_t>((size_t)nb * 4, 4), nullptr);
+    DevBuf bits(ctx, std::max<size_t>((size_t)(P.n + 31) / 32 * 4, 4), res);
+    DevBuf counts(ctx, std::max<size_t>((size_t)nb * 4, 4), res);
     {
         void* jit = jit_select_kernel(ctx, pipe, P);
         KernelTimer kt(ctx, s, "select");
@@ -379,8 +379,8 @@ int64_t run_select(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, DevBuf& ou
     }
     ctx->count_launch();
     DevBuf offs;
-    uint64_t total = scan_counts(ctx, counts.get<uint32_t>(), nb, offs, s);
-    out = DevBuf(ctx, std::max<size_t>(total * 4, 4), nullptr);
+    uint64_t total = scan_counts(ctx, counts.get<uint32_t>(), nb, offs, s, res);
+    out = DevBuf(ctx, std::max<size_t>(total * 4, 4), res);
     {
         KernelTimer kt(ctx, s, "select_write");
         launch_select_write(P, bits.get<uint32_t>(), offs.get<uint64_t>(), out.get<uint32_t>(), s);

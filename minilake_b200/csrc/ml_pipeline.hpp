@@ -76,11 +76,14 @@ class Pipeline {
 };
 
 // Ordered selection of the rows where all of the pipeline's stages pass (no probes).
-// Returns the number of selected rows; `out` holds them (device).
-int64_t run_select(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, DevBuf& out, cudaStream_t s);
+// Returns the number of selected rows; `out` holds them (device).  Its device buffers are
+// charged to `res` when given.
+int64_t run_select(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, DevBuf& out, cudaStream_t s,
+                   Reservation* res = nullptr);
 
 // Exclusive scan helper (device u32 counts -> u64 offsets incl. total); returns the total.
-uint64_t scan_counts(Ctx* ctx, const uint32_t* counts, int64_t n, DevBuf& offsets, cudaStream_t s);
+uint64_t scan_counts(Ctx* ctx, const uint32_t* counts, int64_t n, DevBuf& offsets, cudaStream_t s,
+                     Reservation* res = nullptr);
 
 // Gather a plain UTF8 column: strings at `idx` (or all rows) into a new column.
 void gather_utf8(Ctx* ctx, const uint32_t* off, const uint8_t* bytes, const uint32_t* idx, int64_t k, DevColumn& out,
