@@ -8,7 +8,7 @@ import pytest
 
 from minilake_b200 import abi
 from minilake_b200.abi import FLOAT64, INT32, IsNull, Like, Col, Lit
-from minilake_b200.columns import encode_strings, fixed, utf8_plain
+from minilake_b200.columns import encode_strings, fixed, utf8_dict, utf8_plain
 
 pytestmark = pytest.mark.gpu
 
@@ -129,9 +129,9 @@ def test_static_filter_limits_and_recovery():
     long_words = [bytes([97 + i % 26]) * 400 + str(i).encode() for i in range(200)]
     st, _ = _filter(LIB, ctx, InList(Col(3), long_words), cols, nc, n, None, 0, out, static=True)
     assert st == abi.ERR_INVALID and b"bytes of literals" in LIB.ml_gpu_last_error()
-    # 512 KiB of dictionary tables: a dictionary of 150,000 entries
-    pool = [b"w%06d" % i for i in range(150_000)]
-    big = ctx.upload([encode_strings(pool, np.arange(n) % len(pool))])
+    # 512 KiB of dictionary tables: a dictionary of 65,536 entries needs about 1 MB of them
+    pool = [b"w%06d" % i for i in range(65_536)]
+    big = ctx.upload([utf8_dict(pool, (np.arange(n) % len(pool)).astype(np.uint32))])
     bcols, bnc = big.ml_columns()
     st, _ = _filter(LIB, ctx, Like(Col(0), "w00%"), bcols, bnc, n, None, 0, out, static=True)
     assert st == abi.ERR_INVALID and b"dictionary tables" in LIB.ml_gpu_last_error()
