@@ -142,8 +142,11 @@ def test_static_filter_limits_and_recovery():
     st, k = _filter(LIB, ctx, pred, cols, nc, n, None, 0, got, static=True)
     assert st == 0 and torch.equal(got[:k], ref[:k])
     # no rows: nothing selected
-    st, k = _filter(LIB, ctx, pred, cols, nc, 0, None, 0, got, static=True)
-    assert st == 0 and k == 0
+    empty = (abi.MlColumn * nc)(*[cols[i] for i in range(nc)])
+    for i in range(nc):
+        empty[i].len = 0
+    st, k = _filter(LIB, ctx, pred, empty, nc, 0, None, 0, got, static=True)
+    assert st == 0 and k == 0, LIB.ml_gpu_last_error()
     big.close()
     batch.close()
     ctx.close()
