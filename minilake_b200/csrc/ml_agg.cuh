@@ -77,56 +77,6 @@ __device__ __forceinline__ void acc_merge(int kind, uint64_t* dst, const uint64_
     }
 }
 
-// ---- radix-partitioned aggregation (PartArgs) ---------------------------------------------
-// One record's update applied straight to the group's block in global memory: the path of a
-// record whose shared-memory buffer or region is full.  `val(v)` returns argument word v.
-template <class Val>
-__device__ __forceinline__ void part_apply_global(const AggArgs& A, const PartArgs& R, uint32_t g, Val val) {
-    uint64_t* blk = A.acc + (uint64_t)g * A.stride;
-    count_global(blk);
-    for (int k = 0; k < A.nagg; k++) {
-        const AggDev& a = A.aggs[k];
-        if (a.func == ML_AGG_COUNT_STAR) continue;
-        const int v = R.val_of[k];
-        acc_apply_global(a.kind, blk + a.off, v >= 0 ? val(v) : 0ull);
-    }
-}
-
-// Write every partition buffer holding at least `thresh` records to the CTA's region of that
-// partition (one warp per buffer, B <= 32 records: one coalesced store per word), then empty
-// it.  Records past the region's capacity are applied directly.  Called by the whole CTA
-// between two __syncthreads.  Record s of buffer p sits at p * B + ((s + p) & (B - 1)) (the
-// rotation spreads the buffers' first records over the banks).
-template <int B>
-__device__ inline void part_flush(const AggArgs& A, const PartArgs& R, const uint64_t* pval, const uint32_t* pgid,
-                                  uint32_t* pfill, uint32_t* pcur, uint32_t thresh) {
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const uint64_t plane = (uint64_t)R.nparts * B;
-    for (uint32_t p = warp; p < R.nparts; p += nw) {
-        const uint32_t f0 = pfill[p];
-        if (f0 < thresh) continue;  // one shared word: the branch is warp-uniform
-        const uint32_t f = f0 < (uint32_t)B ? f0 : (uint32_t)B;
-        const uint32_t c0 = pcur[p];
-        if (lane < f) {
-            const uint32_t q = p * B + ((lane + p) & (B - 1));
-            const uint32_t g = pgid[q];
-            const uint32_t j = c0 + lane;
-            if (j < R.rcap) {
-                const uint64_t at = ((uint64_t)blockIdx.x * R.nparts + p) * R.rcap + j;
-                R.rgid[at] = g;
-                for (uint32_t v = 0; v < R.nvals; v++) R.rval[v * R.rstride + at] = pval[v * plane + q];
-            } else {
-                part_apply_global(A, R, g, [&](int v) { return pval[(uint64_t)v * plane + q]; });
-            }
-        }
-        __syncwarp();
-        if (lane == 0) {
-            pcur[p] = c0 + f;
-            pfill[p] = 0;
-        }
-    }
-}
-
 // Append the row combination to the overflow list.  The lanes that overflow together take
 // their slots with one atomic per warp (a full table sends every new key here).
 __device__ inline void record_overflow(const PipeArgs& P, const AggArgs& A, const RowCtx& x) {

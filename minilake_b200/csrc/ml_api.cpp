@@ -1325,18 +1325,6 @@ struct ml_hashagg {
     ml_hashagg(Ctx* c) : ctx(c), pipe(c), streams(c) {}
     void resume_overflow(Pipeline::Launch& L, uint64_t count, DevBuf& ovf, int w, cudaStream_t s,
                          unsigned long long* d_count, uint64_t* h_count, ErrWord& ew);
-    // The partitioned aggregation of one launch (PartArgs): its kernels, layout and record
-    // buffers.  plan_partitioned returns false when the launch keeps the plain fused kernel.
-    struct PartPlan {
-        PartArgs R{};
-        void* fn = nullptr;
-        size_t smem_a = 0;
-        int64_t batch = 0;
-        DevBuf rgid, rval, counts;
-    };
-    bool plan_partitioned(const Pipeline::Launch& L, const AggArgs& A, PartPlan& pl);
-    // Phase A + phase B over the launch's rows in batches of pl.batch rows, on stream s.
-    void run_partitioned(const Pipeline::Launch& L, const AggArgs& A, PartPlan& pl, cudaStream_t s);
     ~ml_hashagg() {
         for (auto& g : run.graphs) cudaGraphExecDestroy(g.second);
         if (run.host_count) ctx->release_slot(run.host_count);
@@ -1554,112 +1542,6 @@ void ml_hashagg::resume_overflow(Pipeline::Launch& L, uint64_t count, DevBuf& ov
     }
 }
 
-namespace {
-constexpr int64_t kPartMinRows = 1 << 20;      // smaller launches keep the plain fused kernel
-constexpr uint64_t kPartSmemA = 75u << 10;     // phase A: three 256-thread CTAs per SM
-constexpr uint64_t kPartSmemB = 224u << 10;    // phase B: one 1024-thread CTA per SM
-constexpr int64_t kPartTileRows = 4 * kPipelineThreads;
-// Rows per phase A + phase B round: the records of a round (at most 12 bytes per row for one
-// SUM) stay within the 126 MB L2 between the two phases.  MINILAKE_GPU_PART_ROWS overrides it.
-constexpr int64_t kPartBatchRows = 8 << 20;
-int64_t part_batch_rows() {
-    static const int64_t v = [] {
-        const char* e = getenv("MINILAKE_GPU_PART_ROWS");
-        const long long x = e ? atoll(e) : 0;
-        return x > 0 ? (int64_t)x : kPartBatchRows;
-    }();
-    return v;
-}
-bool part_enabled() {
-    static const bool v = [] {
-        const char* e = getenv("MINILAKE_GPU_PARTITION");
-        return !(e && e[0] == '0');
-    }();
-    return v;
-}
-}  // namespace
-
-bool ml_hashagg::plan_partitioned(const Pipeline::Launch& L, const AggArgs& A, PartPlan& pl) {
-    if (!part_enabled() || group_probe < 0 || gid_cap <= kSmemPreaggMaxGroups || L.P.n < kPartMinRows ||
-        L.P.has_chains || A.smem_groups > 0)
-        return false;
-    for (int k = 0; k < A.nagg; k++)
-        if (A.aggs[k].count_valid) return false;
-    PartArgs R{};
-    R.nvals = (uint32_t)part_value_words(A, R.val_of);
-    const uint64_t sms = (uint64_t)num_sms();
-    uint64_t np = 0, gp = 0;
-    int B = 0;
-    for (uint64_t k = 1; k <= 64 && !np; k++) {  // partitions: a multiple of the SM count
-        uint64_t n = sms * k, g = (gid_cap + n - 1) / n;
-        if (g < 2) return false;
-        n = (gid_cap + g - 1) / g;
-        if (g * stride * 8 + (16 * sms + 1) * 4 > kPartSmemB) continue;  // phase B: the range's blocks
-        int b = 32;
-        while (b >= 8 && part_smem_bytes((uint32_t)n, R.nvals, b) > kPartSmemA) b >>= 1;
-        if (b < 8) return false;  // too many partitions for phase A's buffers
-        np = n, gp = g, B = b;
-    }
-    if (!np) return false;
-    R.nparts = (uint32_t)np;
-    R.gp = (uint32_t)gp;
-    R.magic = (uint32_t)(((1ull << 32) + gp - 1) / gp);
-    void* fn = jit_part_kernel(ctx, pipe, L.P, A, B);
-    if (!fn) return false;
-    const size_t smem_a = part_smem_bytes(R.nparts, R.nvals, B);
-    const int64_t n = L.P.n;
-    int64_t batch = std::min<int64_t>(n, (part_batch_rows() + kPartTileRows - 1) / kPartTileRows * kPartTileRows);
-    const int64_t tiles = (batch + kPartTileRows - 1) / kPartTileRows;
-    R.grid = (uint32_t)std::min<int64_t>((int64_t)jit_resident_blocks(fn, kPipelineThreads, smem_a) * (int64_t)sms, tiles);
-    if (part_merge_smem_bytes(A, R) > kPartSmemB) return false;
-    // a region holds its expected share of a round's rows (every row passing) with a quarter
-    // to spare; records beyond it are applied directly (skewed keys)
-    const int64_t rows_cta = (tiles + R.grid - 1) / R.grid * kPartTileRows;
-    R.rcap = (uint32_t)((rows_cta * 5 / 4 + (int64_t)np - 1) / (int64_t)np + 2 * B);
-    R.rstride = (uint64_t)R.grid * np * R.rcap;
-    try {
-        pl.rgid = DevBuf(ctx, R.rstride * 4, res.get());
-        pl.rval = DevBuf(ctx, std::max<uint64_t>(R.rstride * 8 * R.nvals, 8), res.get());
-        pl.counts = DevBuf(ctx, (size_t)R.grid * np * 4, res.get());
-    } catch (const MlError& e) {
-        if (e.code != ML_ERR_BUDGET) throw;
-        pl.rgid.release(), pl.rval.release(), pl.counts.release();
-        return false;  // no room for the records: the plain kernel needs none
-    }
-    R.rgid = pl.rgid.get<uint32_t>();
-    R.rval = pl.rval.get<uint64_t>();
-    R.counts = pl.counts.get<uint32_t>();
-    pl.R = R;
-    pl.fn = fn;
-    pl.smem_a = smem_a;
-    pl.batch = batch;
-    return true;
-}
-
-void ml_hashagg::run_partitioned(const Pipeline::Launch& L, const AggArgs& A, PartPlan& pl, cudaStream_t s) {
-    const int64_t n = L.P.n;
-    for (int64_t b0 = 0; b0 < n; b0 += pl.batch) {
-        PipeArgs Pb = L.P;
-        Pb.n = std::min<int64_t>(n, b0 + pl.batch);
-        PartArgs R = pl.R;
-        R.row_begin = b0;
-        AggArgs Ab = A;
-        void* args[] = {&Pb, &Ab, &R};
-        {
-            KernelTimer kt(ctx, s, "part_scatter");
-            jit_launch(pl.fn, R.grid, kPipelineThreads, pl.smem_a, s, args);
-            kt.stop();
-        }
-        {
-            KernelTimer kt(ctx, s, "part_merge");
-            launch_part_merge(A, R, L.P.err, s);
-            kt.stop();
-        }
-        ctx->count_launch(2);
-        ctx->add_profile("jit_launch", 0);
-    }
-}
-
 // The host side of HashAggregateSink::new: compile the prologue, the GROUP BY keys and the
 // aggregate arguments into the sink's pipeline, and lay out the group blocks.
 void compile_hashagg(ml_hashagg* h, const ml_pipe_op* prologue, int32_t nprologue, const int32_t* input_types,
@@ -1830,28 +1712,6 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
     int w = 1 + (int)h->pipe.probes.size();
     bool can_overflow = !h->ungrouped && h->group_probe < 0;
     uint64_t ovf_cap = can_overflow ? std::max<uint64_t>((uint64_t)L.P.n, 1024) : 0;
-    if (h->group_probe >= 0 && L.P.n >= kPartMinRows && h->gid_cap > kSmemPreaggMaxGroups) {
-        // a GROUP BY probe over many groups: the partitioned aggregation, which owns the group
-        // blocks while it runs (phase B rewrites them), so the sink is held exclusively
-        std::unique_lock<std::shared_mutex> lk(h->rw);
-        if (h->run.s) CK(cudaStreamSynchronize(h->run.s));
-        L.P.err = local->ew.d.get<uint32_t>();
-        L.P.head_probe = h->group_probe;
-        if (h->dense_groups) L.P.probes[h->group_probe].late = 1;
-        semi_probes(ctx, L.P, h->pipe, h->group_probe, s);
-        AggArgs A = h->args(local->ovf_count.get<unsigned long long>(), nullptr, 0);
-        ml_hashagg::PartPlan pl;
-        if (h->plan_partitioned(L, A, pl)) {
-            CK(cudaMemsetAsync(local->ew.d.get(), 0, 4, s));
-            KernelTimer kt(ctx, s, "pipeline_aggregate");
-            h->run_partitioned(L, A, pl, s);
-            kt.stop();
-            CK(cudaMemcpyAsync(local->ew.h, local->ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
-            CK(cudaStreamSynchronize(s));
-            check_device_error(ctx, *local->ew.h);
-            return ML_OK;
-        }
-    }
     DevBuf ovf(ctx, std::max<uint64_t>(ovf_cap * w * 4, 16), nullptr);
     uint64_t count;
     {

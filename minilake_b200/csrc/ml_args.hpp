@@ -89,48 +89,6 @@ constexpr int kAggSmemBudget = 74 << 10;
 ML_HD inline bool agg_direct_on(const AggArgs& A) { return A.smem_groups > 0 && !A.ungrouped && A.group_probe < 0; }
 ML_HD inline uint64_t agg_direct_bytes(const AggArgs& A) { return agg_direct_on(A) ? 4 * kDirectSlots : 0; }
 
-// Radix-partitioned aggregation of a GROUP BY whose group id each row already carries (the
-// matched build row, or the dense index position, of the GROUP BY probe) over more groups than
-// shared memory holds.  Phase A (the runtime-specialized pipeline kernel) runs the streaming
-// stages and, instead of two L2 reductions per surviving row, appends a record (group id and
-// the aggregates' argument words) to a per-partition buffer in shared memory; full buffers are
-// written as contiguous runs into the CTA's own region of each partition.  Phase B
-// (k_part_merge) gives each partition (a range of `gp` group ids) to one CTA, which loads the
-// range's accumulators into shared memory, folds in every region's records there and writes
-// the range back.  The group range of a partition fits in one CTA's shared memory, so every
-// accumulator update is a shared-memory atomic and each group block crosses L2 once per phase B.
-struct PartArgs {
-    int64_t row_begin;      // phase A: first row of this launch (a multiple of the tile)
-    uint32_t nparts;        // partitions (group ranges)
-    uint32_t gp;            // group ids per partition (>= 2)
-    uint32_t magic;         // ceil(2^32 / gp): partition = umulhi(g, magic), corrected by one
-    uint32_t rcap;          // record capacity of one (CTA, partition) region
-    uint32_t nvals;         // argument words per record
-    uint32_t grid;          // phase A CTAs (regions per partition)
-    int32_t val_of[kMaxAggs];  // aggregate k -> its argument word in a record (-1: none)
-    uint32_t* rgid;         // record group ids; region (c, p) starts at ((c * nparts) + p) * rcap
-    uint64_t* rval;         // argument word v of a record at v * rstride + its index
-    uint64_t rstride;       // grid * nparts * rcap
-    uint32_t* counts;       // records in region (c, p), at c * nparts + p
-};
-
-// Shared memory of a phase A CTA with buffers of B records per partition: argument words
-// (nvals x nparts x B u64), group ids (nparts x B), fill counts and region cursors (nparts each).
-ML_HD inline uint64_t part_smem_bytes(uint32_t nparts, uint32_t nvals, uint32_t B) {
-    return (uint64_t)nparts * B * (8ull * nvals + 4) + 8ull * nparts;
-}
-
-ML_HD inline uint32_t part_index(const PartArgs& R, uint32_t g) {
-#if defined(__CUDA_ARCH__)
-    uint32_t p = __umulhi(g, R.magic);
-#else
-    uint32_t p = (uint32_t)(((uint64_t)g * R.magic) >> 32);
-#endif
-    // magic = ceil(2^32 / gp) gives floor(g / gp) or one more (g < 2^31)
-    if (p * R.gp > g) p--;
-    return p;
-}
-
 struct SortDev {
     int32_t nkeys, pad;
     DCol cols[kMaxKeys];

@@ -1030,115 +1030,7 @@ std::string priv_flush(const AggArgs& A) {
 
 const char* kPrelude = "#include \"ml_agg.cuh\"\nusing namespace mlg;\n";
 
-// Phase A of the partitioned aggregation for one row combination: the group id (the GROUP BY
-// probe's match), the aggregates' argument words, then the record into its partition's buffer
-// in shared memory (kB records per buffer), or, when the buffer is full, the update applied to
-// the group's block in global memory as the plain kernel does.
-void emit_part_put(Gen& g, const AggArgs& A) {
-    const std::string S = num(A.stride);
-    g.line("const uint32_t g = " + g.x + ".head;");
-    std::vector<Gen::V> args(A.nagg);
-    std::string ok = "true";
-    for (int k = 0; k < A.nagg; k++) {
-        const AggDev& a = A.aggs[k];
-        if (a.func == ML_AGG_COUNT_STAR || !a.has_arg) continue;
-        args[k] = g.expr(a.arg);
-        if (args[k].k != "true") ok += " && (" + args[k].k + ")";
-    }
-    int32_t val_of[kMaxAggs];
-    part_value_words(A, val_of);
-    g.line("const uint32_t pp = part_index(R, g);");
-    g.line("uint32_t s = kB;");
-    g.line("if ((" + ok + ") && pp < R.nparts) s = atomicAdd(pfill + pp, 1u);");
-    g.open("if (s < kB) {");
-    g.line("const uint32_t q = pp * kB + ((s + pp) & (kB - 1u));");
-    g.line("pgid[q] = g;");
-    for (int k = 0; k < A.nagg; k++)
-        if (val_of[k] >= 0) g.line("pval[" + num(val_of[k]) + "ull * R.nparts * kB + q] = " + args[k].v + ";");
-    g.close("} else {");
-    g.open("");
-    g.open("if (g >= A.gid_cap) {");
-    g.line("atomicOr(P.err, (uint32_t)DE_BAD_INDEX);");
-    g.line(g.fail);
-    g.close();
-    g.line("uint64_t* blk = A.acc + (uint64_t)g * " + S + ";");
-    g.line("count_global(blk);");
-    for (int k = 0; k < A.nagg; k++) {
-        const AggDev& a = A.aggs[k];
-        if (a.func == ML_AGG_COUNT_STAR) continue;
-        if (a.has_arg) g.open("if (" + args[k].k + ") {");
-        g.line("acc_apply_global(" + num(a.kind) + ", blk + " + num(a.off) + ", " + (a.has_arg ? args[k].v : "0ull") + ");");
-        if (a.has_arg) g.close();
-    }
-    g.close();
-}
-
 }  // namespace
-
-int part_value_words(const AggArgs& A, int32_t* val_of) {
-    int nv = 0;
-    for (int k = 0; k < kMaxAggs; k++) {
-        val_of[k] = -1;
-        if (k >= A.nagg) continue;
-        const AggDev& a = A.aggs[k];
-        if (a.func != ML_AGG_COUNT_STAR && a.has_arg && a.kind != A_COUNT) val_of[k] = nv++;
-    }
-    return nv;
-}
-
-std::string jit_part_source(const Pipeline& pipe, const PipeArgs& P, const AggArgs& A, int B, bool contig) {
-    if (!batchable(P) || A.group_probe < 0 || B < 2 || B > 32 || (B & (B - 1)))
-        raise(ML_ERR_INTERNAL, "partitioned aggregation needs single-match probes and a GROUP BY probe");
-    Gen g(pipe.C.code, P);
-    g.contig = contig;
-    g.fail = "break;";
-    g.tile_skip = "break;";  // leaves the tile's do-while; the CTA still reaches the flush barriers
-    g.batched_stages([&](auto&& rows) {
-        std::set<int> slots;
-        for (int k = 0; k < A.nagg; k++)
-            if (A.aggs[k].has_arg && A.aggs[k].func != ML_AGG_COUNT_STAR) g.slots_of(A.aggs[k].arg, slots);
-        std::vector<std::map<int, Gen::V>> pre;
-        g.preload_rows(slots, pre);
-        rows([&](int j, const std::string& a) {
-            g.cols = pre[j];
-            g.open("if (" + a + ") do {  // record");
-            emit_part_put(g, A);
-            g.close("} while (0);");
-        });
-        g.cols.clear();
-    });
-    const int K = g.rows_per_thread;
-    std::string src = kPrelude;
-    src += "extern \"C\" __global__ void __launch_bounds__(256) ml_pipeline_partition(const __grid_constant__ PipeArgs P, "
-           "const __grid_constant__ AggArgs A, const __grid_constant__ PartArgs R) {\n";
-    src += "    extern __shared__ __align__(16) uint64_t smem[];\n";
-    src += "    constexpr uint32_t kB = " + num(B) + "u;\n";
-    src += "    uint64_t* const pval = smem;\n";
-    src += "    uint32_t* const pgid = (uint32_t*)(smem + (uint64_t)R.nvals * R.nparts * kB);\n";
-    src += "    uint32_t* const pfill = pgid + R.nparts * kB;\n";
-    src += "    uint32_t* const pcur = pfill + R.nparts;\n";
-    src += "    for (uint32_t i = threadIdx.x; i < 2u * R.nparts; i += blockDim.x) pfill[i] = 0u;\n";
-    src += "    __syncthreads();\n";
-    src += g.pre();
-    // every thread of a CTA runs the same tiles: the barriers around the flush are uniform
-    src += "    const int64_t tile = (int64_t)" + num(K) + " * blockDim.x;\n";
-    src += "    for (int64_t base = R.row_begin + (int64_t)blockIdx.x * tile; base < P.n; base += (int64_t)gridDim.x * tile) {\n";
-    src += "        do {\n";
-    src += tile_rows(P, K, g.contig, "            ");
-    std::istringstream in(g.body());
-    for (std::string ln; std::getline(in, ln);) src += "    " + ln + "\n";
-    src += "        } while (0);\n";
-    src += "        __syncthreads();\n";
-    src += "        part_flush<kB>(A, R, pval, pgid, pfill, pcur, kB / 2u);\n";
-    src += "        __syncthreads();\n";
-    src += "    }\n";
-    src += "    part_flush<kB>(A, R, pval, pgid, pfill, pcur, 1u);\n";
-    src += "    __syncthreads();\n";
-    src += "    for (uint32_t p = threadIdx.x; p < R.nparts; p += blockDim.x)\n";
-    src += "        R.counts[(uint64_t)blockIdx.x * R.nparts + p] = pcur[p] < R.rcap ? pcur[p] : R.rcap;\n";
-    src += "}\n";
-    return src;
-}
 
 std::string jit_agg_source(const Pipeline& pipe, const PipeArgs& P, const AggArgs& A, bool contig) {
     Gen g(pipe.C.code, P);
@@ -1266,15 +1158,6 @@ void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const Ag
     return memoized(pipe, signature('a', P, &A, nullptr) + std::string((const char*)&ctx->device, sizeof(int)) +
                               (contig ? "c" : "s"),
                     [&] { return (void*)get_kernel(ctx, jit_agg_source(pipe, P, A, contig), "ml_pipeline_aggregate"); });
-}
-
-void* jit_part_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A, int B) {
-    if (!jit_enabled(ctx) || !batchable(P) || A.group_probe < 0) return nullptr;
-    const bool contig = contig_ok(P);
-    return memoized(pipe,
-                    signature('p', P, &A, nullptr) + std::string((const char*)&ctx->device, sizeof(int)) +
-                        (contig ? "c" : "s") + num(B),
-                    [&] { return (void*)get_kernel(ctx, jit_part_source(pipe, P, A, B, contig), "ml_pipeline_partition"); });
 }
 
 void* jit_agg_resume_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {

@@ -17,16 +17,6 @@ namespace mlg {
 // or nullptr when runtime compilation is unavailable or disabled for the context.
 void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A);
 
-// Phase A of the partitioned aggregation (PartArgs) with buffers of B records per partition
-// (a power of two <= 32), or nullptr when specialization is off or the pipeline does not
-// qualify (duplicate-key probes, no GROUP BY probe).  Arguments: P, A, R; dynamic shared
-// memory part_smem_bytes(R.nparts, R.nvals, B).
-void* jit_part_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A, int B);
-std::string jit_part_source(const Pipeline& pipe, const PipeArgs& P, const AggArgs& A, int B, bool contig);
-// Argument words of a partitioned record: val_of[k] = word of aggregate k, or -1 (COUNT(*),
-// COUNT(x)); returns the number of words.
-int part_value_words(const AggArgs& A, int32_t* val_of);
-
 // Specialized overflow-resume kernel (signature of k_agg_resume), or nullptr.
 void* jit_agg_resume_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A);
 

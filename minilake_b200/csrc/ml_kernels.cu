@@ -229,100 +229,6 @@ __global__ void __launch_bounds__(kThreads) k_agg_resume(const __grid_constant__
     smem_flush(A, smem);
 }
 
-// Phase B of the partitioned aggregation: CTA p owns group ids [p * gp, (p + 1) * gp).  It
-// loads their accumulator blocks into shared memory, turns the regions' record counts into
-// offsets of one concatenated record list, folds every record in with shared-memory atomics
-// (kPartRecs records per thread and round, all their loads issued first) and writes the blocks
-// back.  The caller guarantees that no other launch updates these blocks meanwhile.
-constexpr int kPartMergeThreads = 1024;
-constexpr int kPartRecs = 8;
-__global__ void __launch_bounds__(kPartMergeThreads) k_part_merge(const __grid_constant__ AggArgs A,
-                                                                  const __grid_constant__ PartArgs R, uint32_t* err) {
-    extern __shared__ __align__(16) uint64_t st[];
-    const uint32_t p = blockIdx.x;
-    const uint64_t g0 = (uint64_t)p * R.gp;
-    if (g0 >= A.gid_cap) return;
-    const uint64_t left = A.gid_cap - g0;
-    const uint32_t ng = left < R.gp ? (uint32_t)left : R.gp;
-    const int S = A.stride;
-    uint32_t* offs = (uint32_t*)(st + (uint64_t)R.gp * S);  // R.grid + 1 entries
-    uint32_t* cnt = offs + R.grid + 1;                        // R.grid entries
-    const uint64_t* src = A.acc + g0 * S;
-    for (uint32_t i = threadIdx.x; i < ng * (uint32_t)S; i += blockDim.x) st[i] = src[i];
-    for (uint32_t c = threadIdx.x; c < R.grid; c += blockDim.x) {
-        const uint32_t n = R.counts[(uint64_t)c * R.nparts + p];
-        cnt[c] = n < R.rcap ? n : R.rcap;
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {  // exclusive offsets: one warp, consecutive entries per lane
-        const uint32_t lane = threadIdx.x, per = (R.grid + 31) / 32;
-        const uint32_t lo = min(lane * per, R.grid), hi = min(lo + per, R.grid);
-        uint32_t sum = 0;
-        for (uint32_t c = lo; c < hi; c++) sum += cnt[c];
-        uint32_t incl = sum;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= (uint32_t)o) incl += t;
-        }
-        uint32_t run = incl - sum;
-        for (uint32_t c = lo; c < hi; c++) {
-            offs[c] = run;
-            run += cnt[c];
-        }
-        if (lane == 31) offs[R.grid] = incl;
-    }
-    __syncthreads();
-    const uint32_t total = offs[R.grid];
-    const uint64_t rp = R.rcap;
-    for (uint32_t b = threadIdx.x * kPartRecs; b < total; b += blockDim.x * kPartRecs) {
-        uint32_t lo = 0, hi = R.grid;  // offs[lo] <= b < offs[hi]
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (offs[mid] <= b) lo = mid;
-            else hi = mid;
-        }
-        uint32_t c = lo;
-        uint64_t at[kPartRecs];
-        uint32_t gl[kPartRecs];
-#pragma unroll
-        for (int k = 0; k < kPartRecs; k++) {
-            const uint32_t i = b + k;
-            at[k] = ~0ull;
-            if (i < total) {
-                while (offs[c + 1] <= i) c++;
-                at[k] = ((uint64_t)c * R.nparts + p) * rp + (i - offs[c]);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kPartRecs; k++) gl[k] = at[k] != ~0ull ? __ldg(R.rgid + at[k]) : 0u;
-#pragma unroll
-        for (int k = 0; k < kPartRecs; k++) {
-            if (at[k] == ~0ull) continue;
-            gl[k] -= (uint32_t)g0;
-            if (gl[k] >= ng) {  // not this partition's group: never written so, but never trusted
-                atomicOr(err, (uint32_t)DE_BAD_INDEX);
-                at[k] = ~0ull;
-                continue;
-            }
-            atomicAdd((unsigned long long*)&st[(uint64_t)gl[k] * S], 1ull);
-        }
-        for (int a = 0; a < A.nagg; a++) {
-            const AggDev& ag = A.aggs[a];
-            if (ag.func == ML_AGG_COUNT_STAR) continue;
-            const int v = R.val_of[a];
-            uint64_t val[kPartRecs];
-#pragma unroll
-            for (int k = 0; k < kPartRecs; k++) val[k] = (v >= 0 && at[k] != ~0ull) ? __ldg(R.rval + v * R.rstride + at[k]) : 0ull;
-#pragma unroll
-            for (int k = 0; k < kPartRecs; k++)
-                if (at[k] != ~0ull) acc_apply(ag.kind, &st[(uint64_t)gl[k] * S + ag.off], val[k]);
-        }
-    }
-    __syncthreads();
-    uint64_t* dst = A.acc + g0 * S;
-    for (uint32_t i = threadIdx.x; i < ng * (uint32_t)S; i += blockDim.x) dst[i] = st[i];
-}
-
 __global__ void k_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                              int nwords, uint32_t* err) {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1255,14 +1161,6 @@ void launch_agg(const PipeArgs& P, const AggArgs& A, int smem_bytes, cudaStream_
 void launch_agg_resume(const PipeArgs& P, const AggArgs& A, const uint32_t* ctx, uint64_t count, int w, int smem_bytes,
                        cudaStream_t s) {
     k_agg_resume<<<grid_for((int64_t)count, 8), kThreads, smem_bytes, s>>>(P, A, ctx, count, w);
-}
-size_t part_merge_smem_bytes(const AggArgs& A, const PartArgs& R) {
-    return (size_t)R.gp * A.stride * 8 + ((size_t)R.grid * 2 + 1) * 4;
-}
-void launch_part_merge(const AggArgs& A, const PartArgs& R, uint32_t* err, cudaStream_t s) {
-    const size_t smem = part_merge_smem_bytes(A, R);
-    if (smem > (48 << 10)) cudaFuncSetAttribute(k_part_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_part_merge<<<R.nparts, kPartMergeThreads, smem, s>>>(A, R, err);
 }
 void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                        int nwords, uint32_t* err, cudaStream_t s) {

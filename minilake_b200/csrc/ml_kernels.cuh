@@ -18,10 +18,6 @@ int num_sms();  // of the current device
 constexpr int kPipelineThreads = 256;
 void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                        int nwords, uint32_t* err, cudaStream_t s);
-// Phase B of the partitioned aggregation (PartArgs): one CTA of 1024 threads per partition,
-// part_merge_smem_bytes of dynamic shared memory (at most 227 KB).
-size_t part_merge_smem_bytes(const AggArgs& A, const PartArgs& R);
-void launch_part_merge(const AggArgs& A, const PartArgs& R, uint32_t* err, cudaStream_t s);
 // Initialize group blocks [from, to) to the identities of the aggregates.
 void launch_acc_init(const AggArgs& A, uint32_t from, uint32_t to, cudaStream_t s);
 // Final values: keys decoded into `key_out` (fixed-width or u32 string ids), aggregates into

@@ -12,8 +12,7 @@ the kernel is at the HBM roofline.
     filter_groupby   WHERE d <= 2467 GROUP BY two dictionary strings, SUM, SUM(x*(1-y)), AVG,
                      COUNT(*) over 100M rows: 36 B/row (d 4, two dict codes 4+4, three f64 24).
     join_groupby     d > 1200, probe of the dense join index on fk (1.5M distinct keys),
-                     GROUP BY fk SUM(v) COUNT(*) over 60M rows: 20 B/row (fk 8, d 4, v 8); the
-                     radix-partitioned aggregation (both phases counted).
+                     GROUP BY fk SUM(v) COUNT(*) over 60M rows: 20 B/row (fk 8, d 4, v 8).
     join_build       1.5M distinct i64 keys -> dense join index: 8 B/row read + 4 B/row index.
     star_join        name LIKE 'ab%' on A (150k plain strings) -> probe A on k1 (Zipf 1.1), B on k2,
                      C on region, GROUP BY label SUM(v*(1-w)) over 60M rows: 4 B/row (k1) + 20 B
@@ -151,12 +150,9 @@ def run(iters: int = 5, rows_filter: int = 100_000_000, rows_join: int = 60_000_
         sink.close()
         return g
 
-    ms, groups = _timed(ctx, ("pipeline_aggregate", "part_scatter", "part_merge"), jgb, iters)
+    ms, groups = _timed(ctx, ("pipeline_aggregate",), jgb, iters)
     res["join_groupby"] = _line(rows_join, ms["pipeline_aggregate"], 20 * rows_join, peak)
     res["join_groupby"]["groups"] = int(groups)
-    # radix-partitioned form: phase A (fused filter/probe -> records) and phase B (merge) device time
-    res["join_groupby"]["scatter_ms"] = round(ms["part_scatter"], 4)
-    res["join_groupby"]["merge_ms"] = round(ms["part_merge"], 4)
     log(f"join_groupby: {res['join_groupby']}")
     j.close()
 

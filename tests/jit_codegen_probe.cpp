@@ -118,8 +118,6 @@ int main() {
         D.aggs[1] = AggDev{A_SUM_F64, ML_AGG_SUM, 1, 1, 0};
         D.aggs[1].arg = Prog{5, 1, ML_TYPE_FLOAT64, 0, 1};
         emit(("aggregate_dense_groups" + c).c_str(), jit_agg_source(pipe, G, D, contig));
-        // the same GROUP BY, radix-partitioned (phase A: records into per-partition buffers)
-        emit(("partition_dense_groups" + c).c_str(), jit_part_source(pipe, G, D, 32, contig));
     }
     return 0;
 }

@@ -3,8 +3,8 @@
 tests/jit_codegen_probe.cpp asks the library for the sources it generates for the filter,
 cardinality-scan and aggregate kernels (strided and consecutive-row tiles, per-thread
 accumulators, direct group slots and speculative loads, a semi-join probe, GROUP BY the dense
-join key, and that GROUP BY's radix-partitioned phase A); each is compiled here with NVRTC, with
-the device headers the library embeds, the way ml_jit.cpp does.
+join key); each is compiled here with NVRTC, with the device headers the library embeds, the
+way ml_jit.cpp does.
 """
 import os
 import re
@@ -62,7 +62,7 @@ def _generated_sources(tmp_path):
 def test_specialized_kernels_compile_for_sm_100a(tmp_path):
     nvrtc = _nvrtc()
     sources = _generated_sources(tmp_path)
-    assert len(sources) == 12, sorted(sources)
+    assert len(sources) == 10, sorted(sources)
     names, texts = _header_set()
     opts = [b"--gpu-architecture=sm_100a", b"-std=c++17", b"--fmad=false"]
     failed = {}
@@ -85,7 +85,3 @@ def test_specialized_kernels_compile_for_sm_100a(tmp_path):
     # per-thread accumulators after a filter: speculative loads in the consecutive-row form only
     assert "specd" in sources["aggregate_groups_contig"] and "specd" not in sources["aggregate_groups_strided"]
     assert "specd" not in sources["aggregate_dense_groups_contig"]
-    # phase A appends records to shared-memory buffers and flushes them between two barriers
-    part = sources["partition_dense_groups_contig"]
-    assert "part_flush<kB>" in part and "atomicAdd(pfill + pp, 1u)" in part
-    assert "red.relaxed" not in part.split("part_index")[0]
