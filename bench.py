@@ -135,17 +135,24 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes (read + write) per launch of the aggregate kernel on this workload, from
-    the committed ncu summary (line `dram_bytes_per_launch: N`)."""
-    import re
-    p = os.path.join(ROOT, "profiles", "pipeline_aggregate_join_groupby.md")
+# DRAM bytes (read + write) of one launch of the fused aggregate kernel on the full 60M-row
+# workload, from one ncu capture of it (`ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
+# --clock-control none -k regex:ml_pipeline_aggregate -s 3 -c 1 python bench.py --steps 3
+# --warmup 3 --skip-cpu --skip-ops`; those two metrics take one pass).  A device counter cannot be
+# read from inside the timed run, so the figure is carried here and labelled as such.
+NCU_DRAM_BYTES_PER_LAUNCH = 1_228_317_184
+
+
+def cpu_model() -> str:
     try:
-        with open(p) as f:
-            m = re.search(r"^dram_bytes_per_launch:\s*([0-9]+)", f.read(), re.M)
-        return int(m.group(1)) if m else None
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
     except OSError:
-        return None
+        pass
+    import platform
+    return platform.processor() or "unknown"
 
 
 # ---------------------------------------------------------------------------------------------
@@ -314,7 +321,9 @@ def gpu_arm(args):
                                    "hash aggregate)",
                          "kernel_ms_per_launch": per_launch_ms,
                          "algorithmic_bytes_per_launch": rows * BYTES_PER_ROW,
-                         "traffic": profiled_traffic() if rows == FACT_ROWS else None},
+                         "traffic": NCU_DRAM_BYTES_PER_LAUNCH if rows == FACT_ROWS else None,
+                         "traffic_source": "ncu capture of one full-size launch (dram__bytes_read.sum + "
+                                           "dram__bytes_write.sum), carried as a constant"},
             "cpu_baseline": cpu,
             "ops": ops,
             "clocks": clocks,
@@ -346,10 +355,8 @@ def oracle_step(eng, dim, fact):
     return workloads.run_join_groupby(eng, dim, fact)
 
 
-def cpu_baseline(key, fk, d, v, runs=3):
+def _time_oracle(dim, fact, threads, runs):
     from oracle import orc
-    threads = os.cpu_count() or 1
-    dim, fact = oracle_tables(key, fk, d, v)
     eng = orc.OracleEngine(threads=threads)
     oracle_step(eng, dim, fact)
     times = []
@@ -357,10 +364,23 @@ def cpu_baseline(key, fk, d, v, runs=3):
         t0 = time.perf_counter()
         oracle_step(eng, dim, fact)
         times.append(time.perf_counter() - t0)
-    med = float(np.median(times))
+    return float(np.median(times)), float(min(times)), float(max(times))
+
+
+def cpu_baseline(key, fk, d, v, runs=3):
+    """The oracle on this host: all cores (the line's value) and 8 threads (the configuration's
+    `--threads 8`), median of `runs` after one warm-up, like MiniLake's `bench` command."""
+    threads = os.cpu_count() or 1
+    dim, fact = oracle_tables(key, fk, d, v)
+    med, lo, hi = _time_oracle(dim, fact, threads, runs)
+    med8, lo8, hi8 = _time_oracle(dim, fact, 8, runs)
     return {"value": len(fk) / med, "unit": "rows/s", "cores": threads, "kind": "port",
             "sample": f"the full workload ({len(fk):,} fact rows), median of {runs} runs after 1 warm-up, "
-                      f"pre-decoded in-memory columns, {threads} threads"}
+                      f"pre-decoded in-memory columns, {threads} threads",
+            "ms": {"median": med * 1e3, "min": lo * 1e3, "max": hi * 1e3},
+            "threads_8": {"value": len(fk) / med8, "unit": "rows/s", "cores": 8,
+                          "ms": {"median": med8 * 1e3, "min": lo8 * 1e3, "max": hi8 * 1e3}},
+            "cpu_model": cpu_model(), "host_threads": threads}
 
 
 def reference_arm(args):
@@ -389,7 +409,8 @@ def reference_arm(args):
                                "ORDER BY SUM(v) DESC, fk LIMIT 10",
                    "engine": "C++ restatement of MiniLake's CPU engine (the Rust reference cannot be built here)"},
         "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
-                         "sample": f"the full workload per step ({FACT_ROWS:,} fact rows), {threads} threads"},
+                         "sample": f"the full workload per step ({FACT_ROWS:,} fact rows), {threads} threads",
+                         "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -1120,9 +1120,13 @@ __global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortD
     if (!last) return;
     __threadfence();
     const int64_t m = (int64_t)gridDim.x * k;
+    // k rows of some warp's full list have prefixes <= the published threshold, so a candidate
+    // above it cannot be in the top k: most CTAs' lists drop out here without a sort
+    const uint64_t bound = thr ? ~__ldcg(thr) : ~0ull;
     best = warp_topk(S, m, k, warp, 8, queue[warp], lane, [&](int64_t i) {
         const TopEntry* e = cand + i;
-        return TopEntry{__ldcg((const unsigned long long*)&e->p), __ldcg(&e->r)};
+        const TopEntry t{__ldcg((const unsigned long long*)&e->p), __ldcg(&e->r)};
+        return t.p <= bound ? t : TopEntry{~0ull, kNone};
     });
     lists[warp][lane] = best;
     __syncthreads();
@@ -1286,7 +1290,9 @@ int topn_warp_blocks(int64_t n) {
         at_most((const void*)k_topn_warp<ML_TYPE_BOOL>);
         return r;
     }();
-    int64_t want = (n + 255) / 256;
+    // at least 8 chunks of 128 rows per warp: a warp's first chunk mostly enters its list, later
+    // ones mostly fall below the list's k-th entry or the launch-wide threshold
+    int64_t want = (n + 8191) / 8192;
     int64_t cap = (int64_t)num_sms() * resident;
     return (int)std::max<int64_t>(1, std::min(want, cap));
 }
