@@ -14,12 +14,11 @@ with SUM(v) and COUNT(*), ORDER BY SUM(v) DESC, fk LIMIT 10.  Seeded synthetic d
 * cpu_baseline  the CPU oracle (a C++ restatement of MiniLake's engine) on this
           host's cores, the full workload
 
-Multi-GPU (torchrun, N ranks): weak scaling; rank r owns a 60M-row fact shard whose
-fk values are the keys with key % N == r (a fact table partitioned on the join key),
-the dimension table is replicated, every rank aggregates its disjoint groups and
-keeps its top-10; the exchange step gathers the N top-10 candidate lists to rank 0,
-which merges them (the top-10 of disjoint groups is within the union of the local
-top-10s).
+Multi-GPU (torchrun, N ranks): weak scaling; rank r scans its own 60M-row share of the fact
+table (fk uniform over every key, as a split by row group gives), the dimension table is
+replicated, every rank aggregates its share in Partial mode, the exchange step sends each
+partial group to the rank that owns its key hash (one NCCL all-to-all per state column), the
+owners merge, and the ranks' top-10 lists are gathered and merged on every rank.
 """
 from __future__ import annotations
 
@@ -54,14 +53,13 @@ def dist_env():
 
 
 def make_data(rank: int, world: int, fact_rows: int = FACT_ROWS):
-    """Dimension table (replicated) and this rank's fact shard, as flat arrays."""
+    """Dimension table (replicated) and this rank's share of the fact table, as flat arrays.
+    Every rank's fact rows reference keys uniform over all of 1..DIM_ROWS (a split by row
+    group, not by key), so the ranks' partial aggregates overlap in nearly every group."""
     rng = np.random.Generator(np.random.PCG64(43))
     key = (rng.permutation(DIM_ROWS) + 1).astype(np.int64)
     frng = np.random.Generator(np.random.PCG64(43 + 1000 * rank))
-    # rank r's fact rows reference the keys k in 1..DIM_ROWS with k % world == r
-    from minilake_b200.exchange import shard_keys
-    first, count = shard_keys(rank, world, DIM_ROWS)
-    fk = first + frng.integers(0, count, fact_rows, dtype=np.int64) * world
+    fk = frng.integers(1, DIM_ROWS + 1, fact_rows, dtype=np.int64)
     d = frng.integers(0, 2557, fact_rows, dtype=np.int32)
     v = frng.uniform(900.0, 105000.0, fact_rows)
     return key, fk, d, v
@@ -184,6 +182,25 @@ class GpuQuery:
         return out
 
 
+    def run_distributed(self, world: int, dim_source, fact_sources, threads=1):
+        """The query over this rank's share, merged across the ranks (minilake_b200.exchange):
+        the merged global top 10 as (fk, sum, count) arrays on every rank."""
+        from minilake_b200 import exchange, workloads
+        from minilake_b200.engine import GpuEngine
+        eng = GpuEngine(self.ctx, threads=threads)
+        j = workloads.join_groupby_build(eng, [dim_source] if not isinstance(dim_source, list) else dim_source)
+        prologue, group, aggs = workloads.join_groupby_plan(j.handle)
+        side = exchange.DeviceSide(eng)
+        final, proj = exchange.distributed_hashagg(eng, side, fact_sources,
+                                                   [self.abi.INT64, self.abi.INT32, self.abi.FLOAT64], group, aggs,
+                                                   prologue, world)
+        res = eng.topn(final, workloads.JG_OUT_TYPES, workloads.join_groupby_topn_keys(), 10)
+        top = res.fetch()
+        out = exchange.exchange_topn(top[0].values, top[1].values, top[2].values, 10, device="cuda")
+        j.close()
+        return out
+
+
 def pinned_like(a: np.ndarray):
     import torch
     t = torch.empty(a.shape, dtype={np.int64: torch.int64, np.int32: torch.int32,
@@ -215,10 +232,17 @@ def gpu_arm(args):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
+    def step(dim_source, fact_sources, threads=1):
+        """One query: (fk, sum, count) of the top 10; with N ranks, merged across them."""
+        if world > 1:
+            return q.run_distributed(world, dim_source, fact_sources, threads)
+        top = q.run(dim_source, fact_sources, threads)
+        return top[0].values, top[1].values, top[2].values
+
     # ---- value: HBM-resident tables, one launch over the whole fact table -------------
     log(f"[rank {rank}] warm-up")
     for _ in range(args.warmup):
-        q.run(q.dim_dev, [q.fact_dev])
+        step(q.dim_dev, [q.fact_dev])
     ctx.profile("pipeline_aggregate", reset=True)
     l0 = ctx.kernel_launches()
     barrier()
@@ -227,7 +251,7 @@ def gpu_arm(args):
         e0.record()
         top = None
         for _ in range(args.steps):
-            top = q.run(q.dim_dev, [q.fact_dev])
+            top = step(q.dim_dev, [q.fact_dev])
         e1.record()
         barrier()
     ms = e0.elapsed_time(e1)
@@ -255,12 +279,12 @@ def gpu_arm(args):
                 fixed(abi.FLOAT64, pinned[2][bounds[i]:bounds[i + 1]])] for i in range(nmorsel)]
     dim_host = [fixed(abi.INT64, pkey)]
     for _ in range(max(1, args.warmup // 2)):
-        q.run(dim_host, morsels, threads=4)
+        step(dim_host, morsels, threads=4)
     barrier()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record()
     for _ in range(args.steps):
-        top_e2e = q.run(dim_host, morsels, threads=4)
+        top_e2e = step(dim_host, morsels, threads=4)
     f1.record()
     barrier()
     e2e_ms = f0.elapsed_time(f1)
@@ -268,14 +292,7 @@ def gpu_arm(args):
     if world > 1:
         torch.distributed.all_reduce(et, op=torch.distributed.ReduceOp.MAX)
     e2e_ms = float(et.item())
-    assert np.array_equal(top_e2e[0].values, top[0].values), "e2e and HBM-resident results differ"
-
-    # ---- exchange: gather the per-rank top-10 candidates, merge on rank 0 -------------
-    if world > 1:
-        from minilake_b200.exchange import exchange_topn
-        mk, ms, mc = exchange_topn(top[0].values, top[1].values, top[2].values, 10, device="cuda")
-        if rank == 0:
-            log("merged top-10 fk:", mk.tolist())
+    assert np.array_equal(top_e2e[0], top[0]), "e2e and HBM-resident results differ"
 
     if rank == 0:
         rows_total = rows * world
@@ -309,7 +326,8 @@ def gpu_arm(args):
                                    "SUM(v), COUNT(*), ORDER BY SUM(v) DESC, fk LIMIT 10",
                        "fact_rows_per_gpu": rows, "dim_rows": DIM_ROWS,
                        "l2": "inputs larger than L2 (1.2 GB fact table per step)",
-                       "parallelism": f"weak, fact partitioned on the join key over {world} GPU(s)"},
+                       "parallelism": f"weak, fact split by row group over {world} GPU(s); partial aggregates "
+                                      "exchanged by key hash (NCCL all-to-all), merged by their owners"},
             "e2e": {"value": e2e, "unit": "rows/s",
                     "h2d_bytes_per_step": int(rows * BYTES_PER_ROW + DIM_ROWS * 8),
                     "d2h_bytes_per_step": int(10 * 24),
@@ -327,7 +345,7 @@ def gpu_arm(args):
             "cpu_baseline": cpu,
             "ops": ops,
             "clocks": clocks,
-            "top10_fk": [int(x) for x in top[0].values],
+            "top10_fk": [int(x) for x in top[0]],
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -261,6 +261,17 @@ int ml_gpu_project(ml_ctx* ctx, const ml_expr* expr, const ml_column* cols, int3
 int ml_gpu_hash_columns(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64_t nrows,
                         const uint32_t* sel, int64_t nsel, int32_t location, uint64_t* out);
 
+/* ---- exchange step of the multi-GPU plan (minilake-dist/src/split.rs:54-127) ----- */
+/* Reorder a batch's rows by partition: partition = hash_columns of the key columns
+ * (kernels/hash.rs:16-23) modulo nparts (1..64).  *out holds the rows grouped by partition,
+ * partition 0 first, each partition's rows in input order; counts[p] receives partition p's row
+ * count (nparts entries).  MiniLake's distributed mode merges every worker's partial aggregate
+ * on its coordinator; the multi-GPU plan sends each partial group to the rank that owns its key
+ * hash instead, so every rank merges 1/nparts of the groups.  Columns may be host or device
+ * memory; the output is device resident. */
+int ml_gpu_partition(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64_t nrows, const int32_t* key_cols,
+                     int32_t nkeys, int32_t nparts, ml_batch** out, int64_t* counts);
+
 /* ---- Sink: HashAggregateSink (operators/aggregate/hash.rs:285-484) ------------- */
 /* `input_types` describes the pipeline source's columns (the prologue's first input).
  * `size_hint` presizes the device table (expected number of groups; 0 = start small and

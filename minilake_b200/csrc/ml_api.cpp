@@ -164,6 +164,63 @@ std::unique_ptr<DevColumn> project_column(Ctx* ctx, const PipeArgs& P, Prog p, i
     return d;
 }
 
+// hash_columns (kernels/hash.rs:16-23) of the active rows of `cols` into `o` (one u64 per row)
+// on stream s: dictionary columns hash each entry once on the host (kernels/hash.rs:66-77).
+void hash_rows(Ctx* ctx, const ml_column* cols, int ncols, int64_t nrows, const uint32_t* dsel, int64_t nsel,
+               cudaStream_t s, Staging& st, DevBuf& o) {
+    std::vector<std::unique_ptr<DevColumn>> staged;
+    PipeArgs P{};
+    P.sel = dsel;
+    P.n = dsel ? nsel : nrows;
+    std::vector<DevBuf> dh;
+    std::vector<const uint64_t*> dh_ptr(ncols, nullptr);
+    for (int c = 0; c < ncols; c++) {
+        staged.push_back(stage_column(ctx, cols[c], nrows, s, st, nullptr));
+        const DevColumn& col = *staged.back();
+        DCol& d = P.cols[c];
+        d.dt = col.dtype;
+        d.kind = col.kind;
+        d.data = col.dptr();
+        d.off = col.optr();
+        d.valid = col.vptr();
+        d.n = col.n;
+        if (col.kind == CK_DICT) {
+            d.dict_len = (uint32_t)col.dict->len();
+            std::vector<uint64_t> hv(col.dict->len() + 1);
+            for (size_t e = 0; e < col.dict->len(); e++) {
+                uint64_t x = 0x243F6A8885A308D3ull ^ ((uint64_t)(col.dict->off[e + 1] - col.dict->off[e]) * 0x9E3779B97F4A7C15ull);
+                const uint8_t* bytes = col.dict->bytes.data() + col.dict->off[e];
+                size_t nbytes = col.dict->off[e + 1] - col.dict->off[e];
+                auto fm = [](uint64_t a, uint64_t m) {
+                    unsigned __int128 r = (unsigned __int128)a * m;
+                    return (uint64_t)r ^ (uint64_t)(r >> 64);
+                };
+                size_t full = nbytes / 8;
+                for (size_t q = 0; q < full; q++) {
+                    uint64_t w;
+                    memcpy(&w, bytes + q * 8, 8);
+                    x = fm(x ^ w, 0x9E3779B97F4A7C15ull);
+                }
+                if (nbytes % 8) {
+                    uint64_t w = 0;
+                    memcpy(&w, bytes + full * 8, nbytes % 8);
+                    x = fm(x ^ w, 0xBF58476D1CE4E5B9ull);
+                }
+                hv[e] = x;
+            }
+            dh.emplace_back(ctx, hv.size() * 8, nullptr);
+            CK(cudaMemcpyAsync(dh.back().get(), hv.data(), hv.size() * 8, cudaMemcpyHostToDevice, s));
+            dh_ptr[c] = dh.back().get<uint64_t>();
+        }
+    }
+    DevBuf ptrs(ctx, std::max<size_t>(ncols * 8, 8), nullptr);
+    if (ncols) CK(cudaMemcpyAsync(ptrs.get(), dh_ptr.data(), ncols * 8, cudaMemcpyHostToDevice, s));
+    o = DevBuf(ctx, std::max<size_t>((size_t)P.n * 8, 8), nullptr);
+    launch_hash_columns(P, ncols, ptrs.get<const uint64_t*>(), o.get<uint64_t>(), s);
+    ctx->count_launch();
+    CK(cudaStreamSynchronize(s));  // the staged columns and tables go out of scope here
+}
+
 void check_device_error(Ctx* ctx, uint32_t err) {
     (void)ctx;
     if (err & DE_TIMEOUT) raise(ML_ERR_TIMEOUT, "a bounded device-side wait ran out");
@@ -856,60 +913,55 @@ int ml_gpu_hash_columns(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64
     cudaStream_t s = ctx->stream;
     if (location == ML_LOC_HOST) check_sel_bounds(sel, nsel, nrows);
     Staging st(ctx);
-    std::vector<std::unique_ptr<DevColumn>> staged;
-    PipeArgs P{};
     DevBuf sel_hold;
-    P.sel = device_sel(ctx, sel, nsel, sel_hold, s);
-    P.n = sel ? nsel : nrows;
-    std::vector<DevBuf> dh;
-    std::vector<const uint64_t*> dh_ptr(ncols, nullptr);
-    for (int c = 0; c < ncols; c++) {
-        staged.push_back(stage_column(ctx, cols[c], nrows, s, st, nullptr));
-        const DevColumn& col = *staged.back();
-        DCol& d = P.cols[c];
-        d.dt = col.dtype;
-        d.kind = col.kind;
-        d.data = col.dptr();
-        d.off = col.optr();
-        d.valid = col.vptr();
-        d.n = col.n;
-        if (col.kind == CK_DICT) d.dict_len = (uint32_t)col.dict->len();
-        if (col.kind == CK_DICT) {  // kernels/hash.rs:66-77: hash each dictionary entry once
-            std::vector<uint64_t> h(col.dict->len() + 1);
-            for (size_t e = 0; e < col.dict->len(); e++) {
-                uint64_t x = 0x243F6A8885A308D3ull ^ ((uint64_t)(col.dict->off[e + 1] - col.dict->off[e]) * 0x9E3779B97F4A7C15ull);
-                const uint8_t* b = col.dict->bytes.data() + col.dict->off[e];
-                size_t nb = col.dict->off[e + 1] - col.dict->off[e];
-                auto fm = [](uint64_t a, uint64_t m) {
-                    unsigned __int128 r = (unsigned __int128)a * m;
-                    return (uint64_t)r ^ (uint64_t)(r >> 64);
-                };
-                size_t full = nb / 8;
-                for (size_t q = 0; q < full; q++) {
-                    uint64_t w;
-                    memcpy(&w, b + q * 8, 8);
-                    x = fm(x ^ w, 0x9E3779B97F4A7C15ull);
-                }
-                if (nb % 8) {
-                    uint64_t w = 0;
-                    memcpy(&w, b + full * 8, nb % 8);
-                    x = fm(x ^ w, 0xBF58476D1CE4E5B9ull);
-                }
-                h[e] = x;
-            }
-            dh.emplace_back(ctx, h.size() * 8, nullptr);
-            CK(cudaMemcpyAsync(dh.back().get(), h.data(), h.size() * 8, cudaMemcpyHostToDevice, s));
-            dh_ptr[c] = dh.back().get<uint64_t>();
-        }
-    }
-    DevBuf ptrs(ctx, std::max<size_t>(ncols * 8, 8), nullptr);
-    if (ncols) CK(cudaMemcpyAsync(ptrs.get(), dh_ptr.data(), ncols * 8, cudaMemcpyHostToDevice, s));
-    DevBuf o(ctx, std::max<size_t>((size_t)P.n * 8, 8), nullptr);
-    launch_hash_columns(P, ncols, ptrs.get<const uint64_t*>(), o.get<uint64_t>(), s);
-    ctx->count_launch();
-    if (P.n) CK(cudaMemcpyAsync(out, o.get(), (size_t)P.n * 8,
-                                location == ML_LOC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    const uint32_t* dsel = device_sel(ctx, sel, nsel, sel_hold, s);
+    DevBuf o;
+    hash_rows(ctx, cols, ncols, nrows, dsel, nsel, s, st, o);
+    const int64_t n = sel ? nsel : nrows;
+    if (n) CK(cudaMemcpyAsync(out, o.get(), (size_t)n * 8,
+                              location == ML_LOC_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    API_END
+}
+
+int ml_gpu_partition(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64_t nrows, const int32_t* key_cols,
+                     int32_t nkeys, int32_t nparts, ml_batch** out, int64_t* counts) {
+    API_BEGIN
+    REQUIRE(ctx && out && counts && (cols || ncols == 0) && key_cols && nkeys > 0, "null argument");
+    REQUIRE(ncols <= kMaxCols && nkeys <= ncols, "too many columns");
+    REQUIRE(nparts >= 1 && nparts <= kMaxExchangeParts, "partitions out of range (1..64)");
+    REQUIRE(nrows >= 0 && nrows < 0xFFFFFFFFll, "row count out of range");
+    std::vector<ml_column> keys;
+    for (int k = 0; k < nkeys; k++) {
+        REQUIRE(key_cols[k] >= 0 && key_cols[k] < ncols, "key column out of range");
+        keys.push_back(cols[key_cols[k]]);
+    }
+    ctx->set_current();
+    std::lock_guard<std::mutex> g(ctx->op_mu);
+    cudaStream_t s = ctx->stream;
+    Staging st(ctx);
+    auto b = std::make_unique<ml_batch>();
+    b->ctx = ctx;
+    b->nrows = nrows;
+    b->res = std::make_unique<Reservation>(ctx, "Exchange");
+    std::vector<std::unique_ptr<DevColumn>> src;
+    for (int c = 0; c < ncols; c++) src.push_back(stage_column(ctx, cols[c], nrows, s, st, b->res.get()));
+    DevBuf h;
+    hash_rows(ctx, keys.data(), nkeys, nrows, nullptr, 0, s, st, h);
+    const int nb = xpart_blocks(nrows);
+    DevBuf bc(ctx, std::max<size_t>((size_t)nb * nparts * 4, 4), nullptr), offs;
+    launch_xpart_count(h.get<uint64_t>(), nrows, nparts, bc.get<uint32_t>(), s);
+    scan_counts(ctx, bc.get<uint32_t>(), (int64_t)nb * nparts, offs, s);
+    DevBuf perm(ctx, std::max<size_t>((size_t)nrows * 4, 4), nullptr);
+    launch_xpart_scatter(h.get<uint64_t>(), nrows, nparts, offs.get<uint64_t>(), perm.get<uint32_t>(), s);
+    ctx->count_launch(2);
+    for (auto& c : src) b->cols.push_back(gather_column(ctx, *c, perm.get<uint32_t>(), nrows, s, b->res.get()));
+    // partition p's rows start at offs[p * nb]; offs[nparts * nb] is the total
+    std::vector<uint64_t> starts(nparts + 1, 0);
+    if (nb) CK(cudaMemcpy2DAsync(starts.data(), 8, offs.get(), (size_t)nb * 8, 8, nparts + 1, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int p = 0; p < nparts; p++) counts[p] = (int64_t)(starts[p + 1] - starts[p]);
+    *out = b.release();
     API_END
 }
 

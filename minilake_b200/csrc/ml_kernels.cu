@@ -229,6 +229,45 @@ __global__ void __launch_bounds__(kThreads) k_agg_resume(const __grid_constant__
     smem_flush(A, smem);
 }
 
+// ---- exchange partitioning: rows grouped by key hash % nparts, input order kept ----------------
+// Per 1024-row block: counts[p * blocks + b] = rows of block b in partition p.
+__global__ void __launch_bounds__(kXPartRows) k_xpart_count(const uint64_t* h, int64_t n, int nparts, uint32_t* counts) {
+    __shared__ uint32_t hist[kMaxExchangeParts];
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const int64_t r = (int64_t)blockIdx.x * kXPartRows + threadIdx.x;
+    if (r < n) atomicAdd(&hist[h[r] % (uint64_t)nparts], 1u);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) counts[(int64_t)i * gridDim.x + blockIdx.x] = hist[i];
+}
+// perm[pos] = row: pos = the (partition, block) offset + the row's rank among the block's rows of
+// its partition (warps in order, lanes in order within a warp: a stable counting sort).
+__global__ void __launch_bounds__(kXPartRows) k_xpart_scatter(const uint64_t* h, int64_t n, int nparts,
+                                                             const uint64_t* offs, uint32_t* perm) {
+    __shared__ uint32_t wcnt[kXPartRows / 32][kMaxExchangeParts];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < (kXPartRows / 32) * kMaxExchangeParts; i += blockDim.x)
+        wcnt[i / kMaxExchangeParts][i % kMaxExchangeParts] = 0;
+    __syncthreads();
+    const int64_t r = (int64_t)blockIdx.x * kXPartRows + threadIdx.x;
+    const bool in = r < n;
+    const uint32_t p = in ? (uint32_t)(h[r] % (uint64_t)nparts) : 0xFFFFFFFFu;
+    const unsigned same = __match_any_sync(0xFFFFFFFFu, p);
+    const uint32_t rank = __popc(same & ((1u << lane) - 1u));
+    if (in && rank == 0) wcnt[w][p] = __popc(same);  // the group's lowest lane
+    __syncthreads();
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x) {  // exclusive prefix over the warps
+        uint32_t run = 0;
+        for (int ww = 0; ww < kXPartRows / 32; ww++) {
+            const uint32_t c = wcnt[ww][q];
+            wcnt[ww][q] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    if (in) perm[offs[(int64_t)p * gridDim.x + blockIdx.x] + wcnt[w][p] + rank] = (uint32_t)r;
+}
+
 __global__ void k_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                              int nwords, uint32_t* err) {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1165,6 +1204,13 @@ void launch_agg(const PipeArgs& P, const AggArgs& A, int smem_bytes, cudaStream_
 void launch_agg_resume(const PipeArgs& P, const AggArgs& A, const uint32_t* ctx, uint64_t count, int w, int smem_bytes,
                        cudaStream_t s) {
     k_agg_resume<<<grid_for((int64_t)count, 8), kThreads, smem_bytes, s>>>(P, A, ctx, count, w);
+}
+int xpart_blocks(int64_t n) { return (int)((n + kXPartRows - 1) / kXPartRows); }
+void launch_xpart_count(const uint64_t* h, int64_t n, int nparts, uint32_t* counts, cudaStream_t s) {
+    if (n > 0) k_xpart_count<<<xpart_blocks(n), kXPartRows, 0, s>>>(h, n, nparts, counts);
+}
+void launch_xpart_scatter(const uint64_t* h, int64_t n, int nparts, const uint64_t* offs, uint32_t* perm, cudaStream_t s) {
+    if (n > 0) k_xpart_scatter<<<xpart_blocks(n), kXPartRows, 0, s>>>(h, n, nparts, offs, perm);
 }
 void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                        int nwords, uint32_t* err, cudaStream_t s) {

@@ -18,6 +18,14 @@ int num_sms();  // of the current device
 constexpr int kPipelineThreads = 256;
 void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                        int nwords, uint32_t* err, cudaStream_t s);
+// Exchange partitioning of n rows by key hash h[r] % nparts (nparts <= kMaxExchangeParts), in
+// blocks of kXPartRows rows: per-(partition, block) counts (partition-major), then, from their
+// exclusive scan `offs`, the stable permutation perm[pos] = row.
+constexpr int kXPartRows = 1024;
+constexpr int kMaxExchangeParts = 64;
+int xpart_blocks(int64_t n);
+void launch_xpart_count(const uint64_t* h, int64_t n, int nparts, uint32_t* counts, cudaStream_t s);
+void launch_xpart_scatter(const uint64_t* h, int64_t n, int nparts, const uint64_t* offs, uint32_t* perm, cudaStream_t s);
 // Initialize group blocks [from, to) to the identities of the aggregates.
 void launch_acc_init(const AggArgs& A, uint32_t from, uint32_t to, cudaStream_t s);
 // Final values: keys decoded into `key_out` (fixed-width or u32 string ids), aggregates into

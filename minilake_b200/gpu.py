@@ -81,6 +81,7 @@ def _load():
         "ml_gpu_filter_static": ([VP, P(abi.MlExpr), P(abi.MlColumn), I32, I64, VP, I64, VP, P(I64)], C.c_int),
         "ml_gpu_project": ([VP, P(abi.MlExpr), P(abi.MlColumn), I32, I64, P(VP)], C.c_int),
         "ml_gpu_hash_columns": ([VP, P(abi.MlColumn), I32, I64, VP, I64, I32, VP], C.c_int),
+        "ml_gpu_partition": ([VP, P(abi.MlColumn), I32, I64, VP, I32, I32, P(VP), VP], C.c_int),
         "ml_gpu_hashagg_create": ([VP, P(abi.MlPipeOp), I32, VP, I32, P(abi.MlExpr), I32, P(abi.MlAggSpec), I32,
                                    I64, P(VP)], C.c_int),
         "ml_gpu_hashagg_local_create": ([VP, P(VP)], C.c_int),
@@ -262,6 +263,41 @@ class DeviceBatch:
                 col.validity = valid[:words]
             cols.append(col)
         return cols
+
+
+def partition(ctx: Context, cols, key_cols: Sequence[int], nparts: int):
+    """Rows grouped by hash_columns(key columns) % nparts (stable): (DeviceBatch, counts)."""
+    arr, nc, n, keep = _cols_arg(cols)
+    keys = (C.c_int32 * max(len(key_cols), 1))(*key_cols)
+    counts = np.zeros(max(nparts, 1), dtype=np.int64)
+    h = C.c_void_p()
+    _check(LIB.ml_gpu_partition(ctx.h, arr, nc, n, keys, len(key_cols), nparts, C.byref(h), _ptr(counts)))
+    return DeviceBatch(ctx, h), counts[:nparts]
+
+
+class _CudaArray:
+    """__cuda_array_interface__ of a device buffer, so torch can view it without a copy."""
+
+    _TYPESTR = {abi.BOOL: "|u1", abi.INT32: "<i4", abi.DATE: "<i4", abi.INT64: "<i8", abi.FLOAT64: "<f8"}
+
+    def __init__(self, ptr: int, n: int, dtype: int, owner):
+        self.owner = owner
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": self._TYPESTR[dtype], "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def column_tensor(batch: "DeviceBatch", i: int):
+    """Torch view (no copy) of fixed-width column i of a device batch; the batch must outlive it."""
+    import torch
+    arr, _ = batch.ml_columns()
+    c = arr[i]
+    if c.dtype not in _CudaArray._TYPESTR:
+        raise TypeError("column_tensor: fixed-width columns only")
+    n = batch.num_rows
+    if n == 0:
+        return torch.empty(0, dtype={abi.BOOL: torch.uint8, abi.INT32: torch.int32, abi.DATE: torch.int32,
+                                     abi.INT64: torch.int64, abi.FLOAT64: torch.float64}[c.dtype], device="cuda")
+    return torch.as_tensor(_CudaArray(c.data, n, c.dtype, batch), device="cuda")
 
 
 def _cols_arg(cols, location=None):

@@ -73,7 +73,8 @@ def test_operator_line_arithmetic():
 
 
 def test_bench_data_shards_and_traffic_record():
-    """bench.py: each rank's fact rows reference only its own keys (key % world == rank), the
+    """bench.py: every rank's share of the fact table references keys over all of 1..1.5M (a
+    split by row group, so the ranks' partial aggregates overlap and need the exchange), the
     dimension keys are a permutation of 1..1.5M, and the DRAM bytes per launch carried for the
     bench line's `roofline.traffic` cover at least the algorithmic bytes."""
     import bench
@@ -82,7 +83,7 @@ def test_bench_data_shards_and_traffic_record():
             key, fk, d, v = bench.make_data(rank, world, fact_rows=20_000)
             assert np.array_equal(np.sort(key), np.arange(1, bench.DIM_ROWS + 1))
             assert fk.min() >= 1 and fk.max() <= bench.DIM_ROWS
-            assert np.all(fk % world == rank)
+            assert len(np.unique(fk % 4)) == 4
             assert d.min() >= 0 and d.max() < 2557 and v.min() >= 900.0 and v.max() < 105000.0
     assert bench.NCU_DRAM_BYTES_PER_LAUNCH >= bench.FACT_ROWS * bench.BYTES_PER_ROW
     peak, kind = bench.measured_peak()
