@@ -72,16 +72,18 @@ def partial_plan(aggs: Sequence[AggSpec]) -> PartialPlan:
     return PartialPlan(partial, types, finals)
 
 
-def merge_aggs(plan: PartialPlan, nkeys: int, nullable: Sequence[bool], valid_col: Sequence[Optional[int]]):
+def _read(i: int, t: int, valid_col: Sequence[Optional[int]]):
+    """Exchanged column i as an expression: through its validity byte when it carries one."""
+    return Case([(Col(valid_col[i]), Col(i))], None, t) if valid_col[i] is not None else Col(i)
+
+
+def merge_aggs(plan: PartialPlan, nkeys: int, valid_col: Sequence[Optional[int]]):
     """Final-mode aggregates over the exchanged columns [keys, states, validity bytes]: counts
     and sums add, MIN/MAX fold; a state that can be NULL is read through its validity byte."""
     out = []
     for j, (a, t) in enumerate(zip(plan.partial, plan.state_types)):
-        arg = Col(nkeys + j)
-        if nullable[j]:
-            arg = Case([(Col(valid_col[j]), Col(nkeys + j))], None, t)
         func = MIN if a.func == MIN else MAX if a.func == MAX else SUM
-        out.append(AggSpec(func, arg, t))
+        out.append(AggSpec(func, _read(nkeys + j, t, valid_col), t))
     return out
 
 
@@ -101,17 +103,33 @@ def final_projection(plan: PartialPlan, key_types: Sequence[int]):
     return exprs
 
 
-def _all_to_all(t, counts, world: int, device):
-    """Exchange the row segments of tensor t (segment p goes to rank p; counts[p] rows each)."""
+def _agree(flags: Sequence[bool], device) -> List[bool]:
+    """The OR over the ranks of per-column flags (which columns carry validity bytes), so every
+    rank makes the same exchange calls."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([int(f) for f in flags], dtype=torch.int32, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [bool(x) for x in t.cpu().tolist()]
+
+
+def _recv_sizes(counts, world: int, device) -> List[int]:
+    """Rows this rank receives from each rank (every rank's `counts` gathered)."""
     import torch
     import torch.distributed as dist
     send = torch.tensor([int(c) for c in counts], dtype=torch.int64, device=device)
     got = [torch.empty_like(send) for _ in range(world)]
     dist.all_gather(got, send)
     rank = dist.get_rank()
-    recv_sizes = [int(g[rank].item()) for g in got]
+    return [int(g[rank].item()) for g in got]
+
+
+def _all_to_all(t, counts, recv_sizes, device):
+    """Exchange the row segments of tensor t (segment p, counts[p] rows, goes to rank p)."""
+    import torch
+    import torch.distributed as dist
     out = torch.empty(sum(recv_sizes), dtype=t.dtype, device=device)
-    dist.all_to_all_single(out, t.contiguous(), output_split_sizes=recv_sizes,
+    dist.all_to_all_single(out, t.contiguous(), output_split_sizes=list(recv_sizes),
                            input_split_sizes=[int(c) for c in counts])
     return out
 
@@ -136,22 +154,24 @@ class HostSide:
         dest = (np.asarray(h, dtype=np.uint64) % np.uint64(world)).astype(np.int64)
         order = np.argsort(dest, kind="stable")
         counts = np.bincount(dest, minlength=world)
+        if any(c.dtype not in FIXED_KEYS + (FLOAT64,) for c in cols):
+            raise TypeError("the exchange carries fixed-width columns only")
+        carry = _agree([c.validity is not None for c in cols], "cpu")
         out = []
-        for c in cols:
-            if c.dtype not in FIXED_KEYS + (FLOAT64,):
-                raise TypeError("the exchange carries fixed-width columns only")
-            valid = c.valid_mask()[order] if c.validity is not None else None
+        for c, cv in zip(cols, carry):
+            valid = c.valid_mask()[order] if cv else None
             out.append((c.dtype, np.ascontiguousarray(c.values[order]), valid))
         return out, counts, fixed
 
     def exchange(self, cols, counts, world):
         import torch
+        sizes = _recv_sizes(counts, world, "cpu")
         got = []
         for dt, vals, valid in cols:
-            r = _all_to_all(torch.from_numpy(vals), counts, world, "cpu").numpy()
+            r = _all_to_all(torch.from_numpy(vals), counts, sizes, "cpu").numpy()
             rv = None
             if valid is not None:
-                rv = _all_to_all(torch.from_numpy(valid.astype(np.uint8)), counts, world, "cpu").numpy()
+                rv = _all_to_all(torch.from_numpy(valid.astype(np.uint8)), counts, sizes, "cpu").numpy()
             got.append((dt, r, rv))
         return got
 
@@ -184,6 +204,7 @@ class DeviceSide:
                 raise TypeError("the exchange carries fixed-width columns only")
             types.append(t.value)
             nullable.append(bool(hv.value))
+        nullable = _agree(nullable, "cuda")
         # validity bytes of the nullable columns, computed on the device (IS NOT NULL)
         valid_batches = [gpu.ProjectionOperator(ctx, abi.IsNull(Col(i), negated=True), abi.BOOL).execute(batch)
                          for i, nb in enumerate(nullable) if nb]
@@ -206,10 +227,11 @@ class DeviceSide:
         return cols, counts, None
 
     def exchange(self, cols, counts, world):
+        sizes = _recv_sizes(counts, world, "cuda")
         got = []
         for dt, vals, valid in cols:
-            r = _all_to_all(vals, counts, world, "cuda")
-            rv = _all_to_all(valid, counts, world, "cuda") if valid is not None else None
+            r = _all_to_all(vals, counts, sizes, "cuda")
+            rv = _all_to_all(valid, counts, sizes, "cuda") if valid is not None else None
             got.append((dt, r, rv))
         self._keep.append(got)
         return got
@@ -239,14 +261,16 @@ def distributed_hashagg(engine, side, source, input_types, group, aggs, prologue
     partial = engine.hashagg(source, input_types, group, plan.partial, prologue)
     cols, counts, fixed_fn = side.partition(partial, nk, world)
     got = side.exchange(cols, counts, world)
-    nullable = [got[nk + j][2] is not None for j in range(len(plan.partial))]
+    # the validity bytes follow the exchanged columns, in column order (keys included: a NULL
+    # group key is its own group)
     valid_col, v = [], len(got)
-    for nb in nullable:
-        valid_col.append(v if nb else None)
-        v += 1 if nb else 0
-    merged_types = [dt for dt, _, _ in got] + [abi.BOOL] * sum(nullable)
-    final = engine.hashagg(side.source(got, fixed_fn), merged_types, [(Col(i), t) for i, t in enumerate(key_types)],
-                           merge_aggs(plan, nk, nullable, valid_col))
+    for _, _, rv in got:
+        valid_col.append(v if rv is not None else None)
+        v += 1 if rv is not None else 0
+    merged_types = [dt for dt, _, _ in got] + [abi.BOOL] * (v - len(got))
+    final = engine.hashagg(side.source(got, fixed_fn), merged_types,
+                           [(_read(i, t, valid_col), t) for i, t in enumerate(key_types)],
+                           merge_aggs(plan, nk, valid_col))
     return final, final_projection(plan, key_types)
 
 
