@@ -345,9 +345,11 @@ int ml_gpu_join_probe(ml_ctx* ctx, ml_join_table* table, const ml_expr* key_expr
                       int64_t nsel, int32_t location, uint32_t* probe_idx, uint32_t* build_idx,
                       int64_t cap, int64_t* npairs);
 
-/* ---- Sink: SortSink with a limit (top-N; operators/sort.rs:85-132, 186-267) ---- */
-/* Output = the input columns (after the prologue) of the best `limit` rows, sorted.
- * limit <= 4096. */
+/* ---- Sink: SortSink (ORDER BY [LIMIT]; operators/sort.rs:85-132, 186-267) ------- */
+/* Output = the input columns (after the prologue) of the best `limit` rows, sorted; limit < 0
+ * is ORDER BY without a limit (every row).  Limits up to 2048 keep each morsel's best rows with
+ * the per-warp top-N kernels; no limit, a larger one, or a dictionary-coded sort key sorts every
+ * row with a stable radix sort (equal keys keep their input order). */
 int ml_gpu_topn_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologue,
                        const int32_t* input_types, int32_t ninput, const ml_sort_key* keys,
                        int32_t nkeys, int64_t limit, ml_topn** out);

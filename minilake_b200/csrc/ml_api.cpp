@@ -445,8 +445,15 @@ struct SortKeySpec {
     bool asc, nulls_first;
 };
 
+std::unique_ptr<ml_batch> sort_batch(Ctx* ctx, ml_batch& b, const std::vector<SortKeySpec>& keys, int64_t limit,
+                                     cudaStream_t st, Reservation* res);
+
 std::unique_ptr<ml_batch> topn_batch(Ctx* ctx, ml_batch& b, const std::vector<SortKeySpec>& keys, int64_t limit,
                                      cudaStream_t st, Reservation* res) {
+    for (auto& key : keys)  // dictionary sort keys take the radix sort (ranks of the entries)
+        if (key.expr.kind == ML_EXPR_COLUMN && key.expr.index >= 0 && (size_t)key.expr.index < b.cols.size() &&
+            b.cols[key.expr.index]->kind == CK_DICT)
+            return sort_batch(ctx, b, keys, limit, st, res);
     int64_t n = b.nrows;
     int64_t k = std::min<int64_t>(limit, n);
     auto out = std::make_unique<ml_batch>();
@@ -552,6 +559,158 @@ std::unique_ptr<ml_batch> topn_batch(Ctx* ctx, ml_batch& b, const std::vector<So
         }
     }
     for (auto& c : b.cols) out->cols.push_back(gather_column(ctx, *c, in, k, st, res));
+    CK(cudaStreamSynchronize(st));
+    return out;
+}
+
+// ---- full ORDER BY (sort.rs:85-132 without a limit): stable LSD radix sort of row ids --------
+// The key words of each sort key, least significant first: value words (a fixed-width value; a
+// plain string's length, then its 8-byte chunks from the last; a dictionary entry's rank), then
+// the NULL flag.  Keys are taken last first, so the first key decides first.
+std::vector<SortWord> sort_words(Ctx* ctx, const std::vector<const DevColumn*>& cols, const std::vector<SortKeySpec>& keys,
+                                 std::vector<DevBuf>& hold, cudaStream_t st) {
+    std::vector<SortWord> words;
+    for (int k = (int)keys.size() - 1; k >= 0; k--) {
+        const DevColumn& c = *cols[k];
+        SortWord w{};
+        w.col.dt = c.dtype;
+        w.col.kind = c.kind;
+        w.col.data = c.dptr();
+        w.col.off = c.optr();
+        w.col.valid = c.vptr();
+        w.col.n = c.n;
+        w.desc = keys[k].asc ? 0 : 1;
+        w.nulls_first = keys[k].nulls_first ? 1 : 0;
+        if (c.kind == CK_DICT) {  // rank of each entry among the dictionary's strings (byte order)
+            const HostDict& hd = *c.dict;
+            std::vector<uint32_t> order(hd.len());
+            for (size_t e = 0; e < order.size(); e++) order[e] = (uint32_t)e;
+            std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return hd.get(a) < hd.get(b); });
+            std::vector<uint32_t> rank(hd.len() + 1, 0);
+            uint32_t rk = 0;
+            for (size_t i = 0; i < order.size(); i++) {
+                if (i && hd.get(order[i]) != hd.get(order[i - 1])) rk++;
+                rank[order[i]] = rk;
+            }
+            rank[hd.len()] = rk + 1;  // the clamp entry of an out-of-range code
+            hold.emplace_back(ctx, rank.size() * 4, nullptr);
+            h2d_now(hold.back().get(), rank.data(), rank.size() * 4);
+            w.col.dict_len = (uint32_t)hd.len();
+            w.what = SW_RANK;
+            w.rank = hold.back().get<uint32_t>();
+            words.push_back(w);
+        } else if (c.kind == CK_UTF8) {
+            DevBuf mx(ctx, 8, nullptr);
+            CK(cudaMemsetAsync(mx.get(), 0, 8, st));
+            launch_max_strlen(c.optr(), c.n, mx.get<unsigned int>(), st);
+            ctx->count_launch();
+            unsigned int maxlen = 0;
+            CK(cudaMemcpyAsync(&maxlen, mx.get(), 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            w.what = SW_LENGTH;
+            words.push_back(w);
+            for (int ch = (int)((maxlen + 7) / 8) - 1; ch >= 0; ch--) {
+                w.what = SW_CHUNK;
+                w.chunk = ch;
+                words.push_back(w);
+            }
+        } else {
+            w.what = SW_VALUE;
+            words.push_back(w);
+        }
+        if (c.vptr()) {  // NULLs present: the flag ranks them first or last, before the value
+            w.what = SW_NULL_FLAG;
+            w.desc = 0;
+            words.push_back(w);
+        }
+    }
+    return words;
+}
+
+// The sorted order of n rows (perm[i] = row at position i) by `words`; nullptr-free result.
+DevBuf radix_sort_rows(Ctx* ctx, const std::vector<SortWord>& words, int64_t n, cudaStream_t st, Reservation* res) {
+    DevBuf ka(ctx, std::max<size_t>((size_t)n * 8, 8), res), kb(ctx, std::max<size_t>((size_t)n * 8, 8), res);
+    DevBuf pa(ctx, std::max<size_t>((size_t)n * 4, 4), res), pb(ctx, std::max<size_t>((size_t)n * 4, 4), res);
+    DevBuf hist(ctx, 8 * 256 * 8, nullptr);
+    const int nb = radix_blocks(n);
+    DevBuf counts(ctx, std::max<size_t>((size_t)nb * 256 * 4, 4), nullptr);
+    bool have_perm = false;  // pa holds the current order (else: rows in input order)
+    std::vector<unsigned long long> h(8 * 256);
+    for (const SortWord& w : words) {
+        launch_sort_words(w, have_perm ? pa.get<uint32_t>() : nullptr, n, ka.get<uint64_t>(), st);
+        CK(cudaMemsetAsync(hist.get(), 0, 8 * 256 * 8, st));
+        launch_radix_hist8(ka.get<uint64_t>(), n, hist.get<unsigned long long>(), st);
+        ctx->count_launch(2);
+        CK(cudaMemcpyAsync(h.data(), hist.get(), 8 * 256 * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int b = 0; b < 8; b++) {
+            bool trivial = false;  // one digit for every row: the pass would not move anything
+            for (int d = 0; d < 256 && !trivial; d++) trivial = h[b * 256 + d] == (unsigned long long)n;
+            if (trivial) continue;
+            launch_radix_count(ka.get<uint64_t>(), n, 8 * b, counts.get<uint32_t>(), st);
+            DevBuf offs;
+            scan_counts(ctx, counts.get<uint32_t>(), (int64_t)nb * 256, offs, st);
+            launch_radix_scatter(ka.get<uint64_t>(), have_perm ? pa.get<uint32_t>() : nullptr, n, 8 * b,
+                                 offs.get<uint64_t>(), kb.get<uint64_t>(), pb.get<uint32_t>(), st);
+            ctx->count_launch(2);
+            std::swap(ka, kb);
+            std::swap(pa, pb);
+            have_perm = true;
+        }
+    }
+    if (!have_perm) launch_iota_u32(pa.get<uint32_t>(), n, st);
+    return pa;
+}
+
+// ORDER BY keys [LIMIT limit] over a device batch: the first min(limit, n) rows in sorted order
+// (a stable sort: equal keys keep their input order).  limit < 0: every row.
+std::unique_ptr<ml_batch> sort_batch(Ctx* ctx, ml_batch& b, const std::vector<SortKeySpec>& keys, int64_t limit,
+                                     cudaStream_t st, Reservation* res) {
+    const int64_t n = b.nrows;
+    const int64_t k = limit < 0 ? n : std::min<int64_t>(limit, n);
+    std::vector<int> types;
+    for (auto& c : b.cols) types.push_back(c->dtype);
+    Pipeline kp(ctx);
+    kp.build(nullptr, 0, types.data(), (int)types.size());
+    // key columns: plain column references read the batch; other expressions are evaluated
+    std::vector<Prog> progs(keys.size());
+    std::vector<int> direct(keys.size(), -1);
+    bool computed = false;
+    for (size_t i = 0; i < keys.size(); i++) {
+        const auto& key = keys[i];
+        if (key.expr.kind == ML_EXPR_COLUMN && key.expr.index >= 0 && (size_t)key.expr.index < types.size() &&
+            types[key.expr.index] == key.type) {
+            direct[i] = (int)key.expr.index;
+            continue;
+        }
+        if (key.type == ML_TYPE_UTF8) raise(ML_ERR_UNSUPPORTED, "sorting by a computed string expression on the GPU");
+        progs[i] = kp.C.compile_value(key.expr, kp.out, key.type);
+        computed = true;
+    }
+    std::vector<std::unique_ptr<DevColumn>> temps;
+    std::vector<const DevColumn*> kcols;
+    Staging stg(ctx);
+    Pipeline::Launch L;
+    if (computed) {
+        kp.upload();
+        auto views = device_views(b);
+        kp.prepare(L, views.data(), (int)views.size(), n, nullptr, 0, st, stg, nullptr);
+    }
+    for (size_t i = 0; i < keys.size(); i++) {
+        if (direct[i] >= 0) {
+            kcols.push_back(b.cols[direct[i]].get());
+        } else {
+            temps.push_back(project_column(ctx, L.P, progs[i], keys[i].type, st, nullptr));
+            kcols.push_back(temps.back().get());
+        }
+    }
+    std::vector<DevBuf> hold;
+    auto words = sort_words(ctx, kcols, keys, hold, st);
+    DevBuf perm = radix_sort_rows(ctx, words, n, st, nullptr);
+    auto out = std::make_unique<ml_batch>();
+    out->ctx = ctx;
+    out->nrows = k;
+    for (auto& c : b.cols) out->cols.push_back(gather_column(ctx, *c, perm.get<uint32_t>(), k, st, res));
     CK(cudaStreamSynchronize(st));
     return out;
 }
@@ -2192,11 +2351,14 @@ struct ml_topn {
     std::vector<Prog> out_progs;
     std::vector<SortKeySpec> keys;
     std::vector<int> out_types;
-    int64_t limit;
+    int64_t limit;  // < 0: ORDER BY without a limit
     std::mutex mu;
     std::vector<std::unique_ptr<ml_batch>> cands;
     SinkStreams streams;
     ml_topn(Ctx* c) : ctx(c), pipe(c), streams(c) {}
+    // No limit, or more rows than the per-warp top-N keeps: the morsels are kept as they come
+    // and sorted once at finalize (the radix sort), as SortLocal keeps its batches (sort.rs:239-249).
+    bool full_sort() const { return limit < 0 || limit > kMaxTopN; }
 };
 struct ml_topn_local {
     ml_topn* sink;
@@ -2220,7 +2382,7 @@ int ml_gpu_topn_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t nprologu
     HostTimer host_timer_(ctx, "host:topn_create");
     REQUIRE(ctx && out && keys && nkeys > 0, "bad arguments");
     REQUIRE(nkeys <= kMaxKeys, "too many sort keys");
-    REQUIRE(limit >= 0 && limit <= kMaxTopN, "limit out of range (0..2048)");
+
     ctx->set_current();
     auto t = std::make_unique<ml_topn>(ctx);
     t->pipe.build(prologue, nprologue, input_types, ninput);
@@ -2256,6 +2418,15 @@ int ml_gpu_topn_sink(ml_topn_local* local, const ml_column* cols, int32_t ncols,
     const uint32_t* dsel = device_sel(ctx, sel, nsel, sel_hold, local->s);
     Pipeline::Launch L;
     t->pipe.prepare(L, cols, ncols, nrows, dsel, nsel, local->s, local->st, nullptr);
+    if (t->full_sort()) {  // keep the morsel (an owned copy, charged to the sort)
+        auto r = std::make_unique<Reservation>(ctx, "Sort");
+        auto part = materialize(ctx, t->pipe, t->out_progs, L, local->s, r.get(), *local->ew, false);
+        part->res = std::move(r);
+        CK(cudaStreamSynchronize(local->s));
+        std::lock_guard<std::mutex> g(t->mu);
+        t->cands.push_back(std::move(part));
+        return ML_OK;
+    }
     auto part = materialize(ctx, t->pipe, t->out_progs, L, local->s, nullptr, *local->ew, true);
     auto r = std::make_unique<Reservation>(ctx, "Sort(candidates)");
     auto best = topn_batch(ctx, *part, t->keys, t->limit, local->s, r.get());
@@ -2288,7 +2459,7 @@ int ml_gpu_topn_finalize(ml_topn* t, ml_batch** out) {
         cands = std::move(t->cands);
     }
     cudaStream_t s = t->streams.own();
-    if (cands.size() == 1) {  // one local sink: its candidates are the sorted top N already
+    if (cands.size() == 1 && !t->full_sort()) {  // one local sink: its candidates are the sorted top N already
         *out = cands[0].release();
         return ML_OK;
     }
@@ -2312,7 +2483,8 @@ int ml_gpu_topn_finalize(ml_topn* t, ml_batch** out) {
         all = concat_batches(ctx, cands, t->out_types, s, nullptr);
     }
     auto res = std::make_unique<Reservation>(ctx, "Sort(output)");
-    auto best = topn_batch(ctx, *all, t->keys, t->limit, s, res.get());
+    auto best = t->full_sort() ? sort_batch(ctx, *all, t->keys, t->limit, s, res.get())
+                               : topn_batch(ctx, *all, t->keys, t->limit, s, res.get());
     best->res = std::move(res);
     *out = best.release();
     API_END

@@ -1175,6 +1175,107 @@ __global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortD
     }
 }
 
+// ---- full ORDER BY: stable LSD radix sort of row ids over 64-bit key words -------------------
+// sort_batches without a limit (sort.rs:85-132) is a stable sort by compare_rows; a stable LSD
+// radix sort over the key words below, least significant first, gives the same order: per key
+// (last key first) its value words, then its NULL flag; byte passes whose digit is the same for
+// every row are skipped.
+__device__ uint64_t sort_word(const SortWord& w, uint32_t r) {
+    const DCol& c = w.col;
+    const bool valid = valid_bit(c.valid, r);
+    if (w.what == SW_NULL_FLAG) return (valid == (w.nulls_first != 0)) ? 1ull : 0ull;
+    if (!valid) return 0ull;
+    uint64_t x;
+    if (w.what == SW_VALUE) {
+        const uint64_t v = load_value(c, r);
+        if (c.dt == ML_TYPE_FLOAT64) x = (uint64_t)total_key(as_f64(v)) ^ 0x8000000000000000ull;
+        else if (c.dt == ML_TYPE_BOOL) x = v;
+        else x = v ^ 0x8000000000000000ull;  // sign-extended integers
+    } else if (w.what == SW_CHUNK) {
+        const Str s = col_str(c, r);
+        x = 0;
+        const uint32_t b0 = 8u * (uint32_t)w.chunk;
+        for (uint32_t j = 0; j < 8; j++)
+            if (b0 + j < s.n) x |= (uint64_t)__ldg(s.p + b0 + j) << (56 - 8 * j);
+    } else if (w.what == SW_LENGTH) {
+        x = col_str(c, r).n;
+    } else {  // SW_RANK: the dictionary entry's rank among the dictionary's strings
+        x = __ldg(w.rank + dict_code(c, r));
+    }
+    return w.desc ? ~x : x;
+}
+__global__ void k_sort_words(const __grid_constant__ SortWord w, const uint32_t* perm, int64_t n, uint64_t* out) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = sort_word(w, perm ? perm[i] : (uint32_t)i);
+}
+// The eight byte histograms of a word array in one pass (hist: 8 x 256 counters, zeroed).
+__global__ void __launch_bounds__(256) k_radix_hist8(const uint64_t* keys, int64_t n, unsigned long long* hist) {
+    __shared__ uint32_t h[8][256];
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) h[i >> 8][i & 255] = 0;
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t k = keys[i];
+#pragma unroll
+        for (int b = 0; b < 8; b++) atomicAdd(&h[b][(k >> (8 * b)) & 255], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x)
+        if (h[i >> 8][i & 255]) atomicAdd(hist + i, (unsigned long long)h[i >> 8][i & 255]);
+}
+// Per 1024-row block: counts[digit * blocks + b] of the byte at `shift`.
+__global__ void __launch_bounds__(kRadixRows) k_radix_count(const uint64_t* keys, int64_t n, int shift, uint32_t* counts) {
+    __shared__ uint32_t h[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const int64_t r = (int64_t)blockIdx.x * kRadixRows + threadIdx.x;
+    if (r < n) atomicAdd(&h[(keys[r] >> shift) & 255], 1u);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) counts[(int64_t)i * gridDim.x + blockIdx.x] = h[i];
+}
+// Stable scatter of (key, row) pairs by the byte at `shift`: a row's position is its digit's
+// offset for the block plus its rank among the block's rows with that digit (warps in order,
+// lanes in order within a warp).  perm_in nullptr = rows in input order.
+__global__ void __launch_bounds__(kRadixRows) k_radix_scatter(const uint64_t* keys_in, const uint32_t* perm_in, int64_t n,
+                                                              int shift, const uint64_t* offs, uint64_t* keys_out,
+                                                              uint32_t* perm_out) {
+    __shared__ uint32_t wcnt[kRadixRows / 32][256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < (kRadixRows / 32) * 256; i += blockDim.x) wcnt[i >> 8][i & 255] = 0;
+    __syncthreads();
+    const int64_t r = (int64_t)blockIdx.x * kRadixRows + threadIdx.x;
+    const bool in = r < n;
+    const uint64_t k = in ? keys_in[r] : 0ull;
+    const uint32_t d = in ? (uint32_t)((k >> shift) & 255) : 256u;
+    const unsigned same = __match_any_sync(0xFFFFFFFFu, d);
+    const uint32_t rank = __popc(same & ((1u << lane) - 1u));
+    if (in && rank == 0) wcnt[w][d] = __popc(same);
+    __syncthreads();
+    for (int q = threadIdx.x; q < 256; q += blockDim.x) {
+        uint32_t run = 0;
+        for (int ww = 0; ww < kRadixRows / 32; ww++) {
+            const uint32_t c = wcnt[ww][q];
+            wcnt[ww][q] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    if (in) {
+        const uint64_t pos = offs[(int64_t)d * gridDim.x + blockIdx.x] + wcnt[w][d] + rank;
+        keys_out[pos] = k;
+        perm_out[pos] = perm_in ? perm_in[r] : (uint32_t)r;
+    }
+}
+// Longest string of a plain UTF8 column (for the number of 8-byte chunk words).
+__global__ void k_max_strlen(const uint32_t* off, int64_t n, unsigned int* out) {
+    uint32_t m = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) m = max(m, off[i + 1] - off[i]);
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
 }  // namespace
 
 // Temporaries of ml_gpu_filter_static: a fixed-size device array, so that call allocates no
@@ -1356,6 +1457,30 @@ void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* 
         case ML_TYPE_BOOL: k_topn_warp<ML_TYPE_BOOL><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
         default: k_topn_warp<-1><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
     }
+}
+__global__ void k_iota_u32(uint32_t* out, int64_t n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (uint32_t)i;
+}
+void launch_iota_u32(uint32_t* out, int64_t n, cudaStream_t s) {
+    if (n > 0) k_iota_u32<<<grid_for(n, 8), kThreads, 0, s>>>(out, n);
+}
+int radix_blocks(int64_t n) { return (int)((n + kRadixRows - 1) / kRadixRows); }
+void launch_sort_words(const SortWord& w, const uint32_t* perm, int64_t n, uint64_t* out, cudaStream_t s) {
+    if (n > 0) k_sort_words<<<grid_for(n, 8), kThreads, 0, s>>>(w, perm, n, out);
+}
+void launch_radix_hist8(const uint64_t* keys, int64_t n, unsigned long long* hist, cudaStream_t s) {
+    if (n > 0) k_radix_hist8<<<grid_for(n, 4), 256, 0, s>>>(keys, n, hist);
+}
+void launch_radix_count(const uint64_t* keys, int64_t n, int shift, uint32_t* counts, cudaStream_t s) {
+    if (n > 0) k_radix_count<<<radix_blocks(n), kRadixRows, 0, s>>>(keys, n, shift, counts);
+}
+void launch_radix_scatter(const uint64_t* keys_in, const uint32_t* perm_in, int64_t n, int shift, const uint64_t* offs,
+                          uint64_t* keys_out, uint32_t* perm_out, cudaStream_t s) {
+    if (n > 0) k_radix_scatter<<<radix_blocks(n), kRadixRows, 0, s>>>(keys_in, perm_in, n, shift, offs, keys_out, perm_out);
+}
+void launch_max_strlen(const uint32_t* off, int64_t n, unsigned int* out, cudaStream_t s) {
+    if (n > 0) k_max_strlen<<<grid_for(n, 4), kThreads, 0, s>>>(off, n, out);
 }
 void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, uint32_t* out, cudaStream_t s) {
     int64_t nb = (n + kTopNChunk - 1) / kTopNChunk;

@@ -100,6 +100,28 @@ void launch_count_dense(const uint32_t* dense, uint64_t n, unsigned long long* o
 // bits[i / 32] bit i % 32 = (dense[i] != kNone), for i < n.
 void launch_dense_bits(const uint32_t* dense, uint64_t n, uint32_t* bits, cudaStream_t s);
 void launch_topn_chunk(const SortDev& S, const uint32_t* in, int64_t n, int k, uint32_t* out, cudaStream_t s);
+
+// Full ORDER BY: one 64-bit word of the composite sort key per row (k_sort_words), the word's
+// eight byte histograms (hist8: 8 x 256 u64, zeroed), and per non-trivial byte a stable radix
+// pass: per-block digit counts (digit-major), their exclusive scan `offs`, the scatter.
+enum SortWordKind : int32_t { SW_VALUE = 0, SW_NULL_FLAG = 1, SW_CHUNK = 2, SW_LENGTH = 3, SW_RANK = 4 };
+struct SortWord {
+    DCol col;
+    int32_t what;          // SortWordKind
+    int32_t chunk;         // SW_CHUNK: bytes [8 * chunk, 8 * chunk + 8) of the string, big-endian
+    int32_t desc;          // descending key: the word is complemented (not the NULL flag)
+    int32_t nulls_first;
+    const uint32_t* rank;  // SW_RANK: rank of each dictionary code (dict_len + 1 entries)
+};
+constexpr int kRadixRows = 1024;
+int radix_blocks(int64_t n);
+void launch_sort_words(const SortWord& w, const uint32_t* perm, int64_t n, uint64_t* out, cudaStream_t s);
+void launch_radix_hist8(const uint64_t* keys, int64_t n, unsigned long long* hist, cudaStream_t s);
+void launch_radix_count(const uint64_t* keys, int64_t n, int shift, uint32_t* counts, cudaStream_t s);
+void launch_radix_scatter(const uint64_t* keys_in, const uint32_t* perm_in, int64_t n, int shift, const uint64_t* offs,
+                          uint64_t* keys_out, uint32_t* perm_out, cudaStream_t s);
+void launch_max_strlen(const uint32_t* off, int64_t n, unsigned int* out, cudaStream_t s);
+void launch_iota_u32(uint32_t* out, int64_t n, cudaStream_t s);  // out[i] = i
 // Top-k for k <= kTopNWarpMax: each CTA writes its best k rows (sorted) to out[block * k ..].
 constexpr int kTopNWarpMax = 32;
 int topn_warp_blocks(int64_t n);

@@ -1,5 +1,5 @@
 """Multi-GPU form of the aggregate queries: one process per GPU, torch.distributed for the
-collectives (NCCL between GPUs, gloo between CPU processes in the tests).
+collectives (NCCL between GPUs; the tests run the same plan between CPU processes over gloo).
 
 The plan is MiniLake's distributed mode (minilake-dist/src/split.rs:54-127) with the merge
 spread over the ranks:
@@ -132,54 +132,6 @@ def _all_to_all(t, counts, recv_sizes, device):
     dist.all_to_all_single(out, t.contiguous(), output_split_sizes=list(recv_sizes),
                            input_split_sizes=[int(c) for c in counts])
     return out
-
-
-class HostSide:
-    """The exchange over host columns (CPU engine, gloo): partitions with the oracle's hash."""
-
-    device = "cpu"
-
-    def __init__(self, engine):
-        self.engine = engine
-
-    def partition(self, batch, nkeys: int, world: int):
-        """([(dtype, values, valid-or-None)], counts): the batch's columns with their rows grouped
-        by destination rank."""
-        from oracle import orc
-
-        from .columns import fixed
-        cols = self.engine.fetch(batch)
-        n = len(cols[0]) if cols else 0
-        h = orc.hash_columns(cols[:nkeys]) if n else np.zeros(0, np.uint64)
-        dest = (np.asarray(h, dtype=np.uint64) % np.uint64(world)).astype(np.int64)
-        order = np.argsort(dest, kind="stable")
-        counts = np.bincount(dest, minlength=world)
-        if any(c.dtype not in FIXED_KEYS + (FLOAT64,) for c in cols):
-            raise TypeError("the exchange carries fixed-width columns only")
-        carry = _agree([c.validity is not None for c in cols], "cpu")
-        out = []
-        for c, cv in zip(cols, carry):
-            valid = c.valid_mask()[order] if cv else None
-            out.append((c.dtype, np.ascontiguousarray(c.values[order]), valid))
-        return out, counts, fixed
-
-    def exchange(self, cols, counts, world):
-        import torch
-        sizes = _recv_sizes(counts, world, "cpu")
-        got = []
-        for dt, vals, valid in cols:
-            r = _all_to_all(torch.from_numpy(vals), counts, sizes, "cpu").numpy()
-            rv = None
-            if valid is not None:
-                rv = _all_to_all(torch.from_numpy(valid.astype(np.uint8)), counts, sizes, "cpu").numpy()
-            got.append((dt, r, rv))
-        return got
-
-    def source(self, got, fixed_fn):
-        """Host columns [values..., validity bytes of the nullable ones] for the Final merge."""
-        cols = [fixed_fn(dt, v) for dt, v, _ in got]
-        cols += [fixed_fn(abi.BOOL, rv) for _, _, rv in got if rv is not None]
-        return cols
 
 
 class DeviceSide:

@@ -530,10 +530,11 @@ class HashJoinProbe:
 
 
 class SortSink:
-    """ORDER BY ... LIMIT n (top-N; operators/sort.rs:85-267); limit <= 2048."""
+    """ORDER BY ... [LIMIT n] (operators/sort.rs:85-267); limit None = every row."""
 
-    def __init__(self, ctx: Context, input_types: Sequence[int], keys: Sequence[abi.SortKey], limit: int,
+    def __init__(self, ctx: Context, input_types: Sequence[int], keys: Sequence[abi.SortKey], limit: Optional[int],
                  prologue: Sequence[abi.PipeOp] = ()):
+        limit = -1 if limit is None else limit
         self.ctx = ctx
         keep = abi.Keep()
         ops, nops = abi.encode_ops(prologue, keep)

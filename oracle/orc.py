@@ -220,7 +220,8 @@ class OracleEngine:
         ops, nops = abi.encode_ops(prologue, keep)
         k, nk = abi.encode_sort_keys(keys, keep)
         h = C.c_void_p()
-        check(LIB.orc_topn_run(arr, nm, nc, rows.ctypes.data, ops, nops, k, nk, limit, self.threads,
+        check(LIB.orc_topn_run(arr, nm, nc, rows.ctypes.data, ops, nops, k, nk, -1 if limit is None else limit,
+                               self.threads,
                                self.batch_size, C.byref(h)))
         return OBatch(h.value)
 

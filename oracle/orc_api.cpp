@@ -452,7 +452,8 @@ int orc_topn_run(const ml_column* cols, int nmorsels, int ncols, const int64_t* 
     auto ops = parse_prologue(pro, npro);
     std::vector<SortKey> sk;
     for (int k = 0; k < nkeys; k++) sk.push_back({parse_expr(keys[k].expr), keys[k].asc != 0, keys[k].nulls_first != 0});
-    size_t l = (size_t)limit;
+    // limit < 0: ORDER BY without a limit (sort.rs:85-132, `limit: None`)
+    const std::optional<size_t> l = limit < 0 ? std::nullopt : std::optional<size_t>((size_t)limit);
     size_t out_cols = (size_t)ncols;
     for (auto& op : ops) {
         if (op.kind == ML_PIPE_PROJECT) out_cols = op.exprs.size();
@@ -460,7 +461,8 @@ int orc_topn_run(const ml_column* cols, int nmorsels, int ncols, const int64_t* 
     }
     struct TLocal {  // SortLocal (sort.rs:178-267)
         const std::vector<SortKey>* keys;
-        size_t limit, ncols, rows = 0;
+        std::optional<size_t> limit;
+        size_t ncols, rows = 0;
         std::vector<Batch> batches;
         void truncate() {
             auto b = sort_batches(batches, *keys, limit, ncols);
@@ -472,7 +474,7 @@ int orc_topn_run(const ml_column* cols, int nmorsels, int ncols, const int64_t* 
         void sink(Batch b) {
             rows += b.active_rows();
             batches.push_back(b.compact());
-            if (rows > std::max<size_t>(4 * limit, 16384)) truncate();
+            if (limit && rows > std::max<size_t>(4 * *limit, 16384)) truncate();
         }
     };
     std::mutex mu;

@@ -11,7 +11,58 @@ import socket
 import numpy as np
 import torch.multiprocessing as mp
 
+from minilake_b200 import abi, exchange
+
 ROWS, DIM, GROUPS = 120_000, 40_000, 12
+
+
+class HostSide:
+    """The exchange step over host columns for the CPU engine (gloo): the counterpart of
+    minilake_b200.exchange.DeviceSide, partitioning with the oracle's hash_columns."""
+
+    device = "cpu"
+
+    def __init__(self, engine):
+        self.engine = engine
+
+    def partition(self, batch, nkeys: int, world: int):
+        """([(dtype, values, valid-or-None)], counts): the batch's columns with their rows grouped
+        by destination rank."""
+        from oracle import orc
+
+        from minilake_b200.columns import fixed
+        cols = self.engine.fetch(batch)
+        n = len(cols[0]) if cols else 0
+        h = orc.hash_columns(cols[:nkeys]) if n else np.zeros(0, np.uint64)
+        dest = (np.asarray(h, dtype=np.uint64) % np.uint64(world)).astype(np.int64)
+        order = np.argsort(dest, kind="stable")
+        counts = np.bincount(dest, minlength=world)
+        if any(c.dtype not in exchange.FIXED_KEYS + (abi.FLOAT64,) for c in cols):
+            raise TypeError("the exchange carries fixed-width columns only")
+        carry = exchange._agree([c.validity is not None for c in cols], "cpu")
+        out = []
+        for c, cv in zip(cols, carry):
+            valid = c.valid_mask()[order] if cv else None
+            out.append((c.dtype, np.ascontiguousarray(c.values[order]), valid))
+        return out, counts, fixed
+
+    def exchange(self, cols, counts, world):
+        import torch
+        sizes = exchange._recv_sizes(counts, world, "cpu")
+        got = []
+        for dt, vals, valid in cols:
+            r = exchange._all_to_all(torch.from_numpy(vals), counts, sizes, "cpu").numpy()
+            rv = None
+            if valid is not None:
+                rv = exchange._all_to_all(torch.from_numpy(valid.astype(np.uint8)), counts, sizes, "cpu").numpy()
+            got.append((dt, r, rv))
+        return got
+
+    def source(self, got, fixed_fn):
+        """Host columns [values..., validity bytes of the nullable ones] for the Final merge."""
+        cols = [fixed_fn(dt, v) for dt, v, _ in got]
+        cols += [fixed_fn(abi.BOOL, rv) for _, _, rv in got if rv is not None]
+        return cols
 
 
 def _free_port():
@@ -76,7 +127,6 @@ def _rank(rank, world, port, out):
 
     import torch.distributed as dist
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
-    from minilake_b200 import exchange
     from minilake_b200.abi import FLOAT64, INT32, INT64, Col
     from oracle import orc
     eng = orc.OracleEngine(threads=2)
@@ -84,7 +134,7 @@ def _rank(rank, world, port, out):
     j = eng.join_build(dim, [INT64], [(Col(0), INT64)])
     results = []
     for prologue, group, aggs in _queries(j):
-        final, proj = exchange.distributed_hashagg(eng, exchange.HostSide(eng), fact,
+        final, proj = exchange.distributed_hashagg(eng, HostSide(eng), fact,
                                                    [INT64, INT32, FLOAT64, FLOAT64], group, aggs, prologue, world)
         results.append(_final_rows(eng, final, proj))
     # the benchmark query's top 10: each rank's top 10 of the groups it owns, gathered and merged
@@ -97,7 +147,6 @@ def _rank(rank, world, port, out):
 
 
 def test_two_ranks_partial_exchange_final_match_single_process():
-    from minilake_b200 import exchange
     from minilake_b200.abi import FLOAT64, INT32, INT64, Col
     from oracle import orc
     ctx = mp.get_context("spawn")
