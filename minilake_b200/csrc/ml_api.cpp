@@ -1170,10 +1170,7 @@ int ml_gpu_join_build_create(ml_ctx* ctx, const ml_pipe_op* prologue, int32_t np
     for (auto& r : j->pipe.out) j->out_types.push_back(r.dtype);
     j->out_progs = compile_outputs(j->pipe);
     j->pipe.upload();
-    for (int k = 0; k < nkeys; k++) {
-        if (key_exprs[k].dtype == ML_TYPE_UTF8) raise(ML_ERR_UNSUPPORTED, "string join keys on the GPU");
-        j->keys.add(key_exprs[k]);
-    }
+    for (int k = 0; k < nkeys; k++) j->keys.add(key_exprs[k]);
     j->keys.finish();
     j->res = std::make_unique<Reservation>(ctx, "HashJoinBuild");
     *out = j.release();
@@ -1901,9 +1898,6 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
     const uint32_t* dsel = device_sel(ctx, sel, nsel, sel_hold, s);
     Pipeline::Launch L;
     h->pipe.prepare(L, cols, ncols, nrows, dsel, nsel, s, local->st, nullptr);
-    for (const KeyDecode& d : h->dec)
-        if (d.str_kind == 1 && L.P.cols[d.slot].kind != CK_DICT)
-            raise(ML_ERR_UNSUPPORTED, "GROUP BY on a plain (not dictionary-encoded) string column of the source");
     // seen-tracking: once an argument can be NULL, count valid inputs per group
     for (auto& a : h->aggs) {
         if (!a.has_arg || a.vcnt_on || a.kind == A_COUNT) continue;
@@ -2047,9 +2041,6 @@ int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t nc
     Staging st(ctx);
     Pipeline::Launch L;
     h->pipe.prepare(L, cols, ncols, nrows, nullptr, 0, s, st, nullptr, R.tables.get<uint8_t>(), R.tables.bytes());
-    for (const KeyDecode& d : h->dec)
-        if (d.str_kind == 1 && L.P.cols[d.slot].kind != CK_DICT)
-            raise(ML_ERR_UNSUPPORTED, "GROUP BY on a plain (not dictionary-encoded) string column of the source");
     for (auto& a : h->aggs)
         if (a.has_arg && !a.vcnt_on && a.kind != A_COUNT && (a.arg.maybe_null || h->pipe.reads_nullable(a.arg, L)))
             raise(ML_ERR_UNSUPPORTED, "ml_gpu_hashagg_run_resident: an aggregate input can be NULL; use a local sink");

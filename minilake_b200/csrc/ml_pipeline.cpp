@@ -59,11 +59,14 @@ KeyLayout Pipeline::key_layout(const ml_expr* exprs, int n, const Schema& schema
         KeyDecode d;
         d.type = types[k];
         if (types[k] == ML_TYPE_UTF8) {
-            if (!group) raise(ML_ERR_UNSUPPORTED, "string join keys on the GPU");
             int slot;
             L.prog[k] = C.compile_string_key(e, schema, &slot);
             d.slot = slot;
             const SlotInfo& si = C.slots[slot];
+            // join keys compare the context's global string ids, which the source's columns carry
+            // (a build side's strings carry canonical build rows instead)
+            if (!group && si.src != 0)
+                raise(ML_ERR_UNSUPPORTED, "a string join key read from an earlier join's build side on the GPU");
             if (si.src == 0) {
                 d.str_kind = 1;
             } else {
@@ -77,6 +80,41 @@ KeyLayout Pipeline::key_layout(const ml_expr* exprs, int n, const Schema& schema
         if (dec) dec->push_back(d);
     }
     return L;
+}
+
+DevBuf Pipeline::intern_plain_strings(const DevColumn& col, cudaStream_t s) {
+    const int64_t n = col.n;
+    DevBuf ids(ctx, std::max<size_t>((size_t)n * 4, 4), nullptr);
+    if (n == 0) return ids;
+    // canonical rows: equal strings of the batch share one row (a device hash table of strings)
+    const uint64_t cap = std::max<uint64_t>(16, 1ull << (64 - __builtin_clzll((uint64_t)n * 2)));
+    DevBuf tslots(ctx, cap * 16, nullptr), canon(ctx, (size_t)n * 4, nullptr), err(ctx, 8, nullptr);
+    CK(cudaMemsetAsync(tslots.get(), 0, cap * 16, s));
+    CK(cudaMemsetAsync(err.get(), 0, 4, s));
+    TableView tv{tslots.get<uint64_t>(), cap - 1, 1, 2};
+    launch_strid(col.optr(), (const uint8_t*)col.dptr(), col.vptr(), n, tv, canon.get<uint32_t>(), err.get<uint32_t>(), s);
+    ctx->count_launch();
+    std::vector<uint32_t> canon_h(n), off(n + 1), ids_h(n, 0);
+    uint32_t err_h = 0;
+    CK(cudaMemcpyAsync(canon_h.data(), canon.get(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(off.data(), col.optr(), (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&err_h, err.get(), 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (err_h) raise(ML_ERR_TIMEOUT, "a bounded wait ran out while hashing a string key column");
+    std::vector<uint8_t> bytes(off[n] - off[0]);
+    if (!bytes.empty())
+        CK(cudaMemcpyAsync(bytes.data(), (const uint8_t*)col.dptr() + off[0], bytes.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    {
+        std::lock_guard<std::mutex> g(intern.mu);
+        for (int64_t r = 0; r < n; r++)
+            if (canon_h[r] == (uint32_t)r)
+                ids_h[r] = intern.id(std::string((const char*)bytes.data() + (off[r] - off[0]), off[r + 1] - off[r]));
+    }
+    for (int64_t r = 0; r < n; r++) ids_h[r] = ids_h[canon_h[r] < (uint64_t)n ? canon_h[r] : r];
+    CK(cudaMemcpyAsync(ids.get(), ids_h.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));  // the host vector goes out of scope
+    return ids;
 }
 
 void Pipeline::build(const ml_pipe_op* ops, int nops, const int32_t* types, int ntypes) {
@@ -301,6 +339,16 @@ void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrow
             dict_at.push_back({(int)i, put(doff.data(), doff.size() * 4)});
             dbytes_at.push_back({(int)i, put(hd.bytes.data(), hd.bytes.size())});
         }
+    }
+    // plain strings read as keys: per-row global string ids (equal strings, equal ids)
+    L.strids.clear();
+    for (int slot : C.string_key_slots) {
+        const SlotInfo& si = C.slots[slot];
+        if (si.src != 0 || si.index < 0 || si.index >= (int)L.src.size()) continue;
+        const DevColumn& col = *L.src[si.index];
+        if (col.kind != CK_UTF8) continue;
+        L.strids.push_back(intern_plain_strings(col, s));
+        P.cols[slot].gid = L.strids.back().get<uint32_t>();
     }
     for (size_t l = 0; l < C.luts.size(); l++) {
         const LutSpec& spec = C.luts[l];

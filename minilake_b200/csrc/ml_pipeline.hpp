@@ -17,15 +17,6 @@ struct KeyDecode {
     int slot = -1;     // column slot the key reads
 };
 
-// Global string ids for dictionary-encoded source columns (the dictionaries differ per
-// row group; the ids are the pipeline's interning of their entries).
-struct StringIntern {
-    std::mutex mu;
-    std::unordered_map<std::string, uint32_t> ids;
-    std::vector<std::string> strs;
-    uint32_t id(const std::string& s);
-};
-
 struct ProbeInfo {
     ml_join_table* jt = nullptr;
     KeyLayout keys{};
@@ -33,7 +24,7 @@ struct ProbeInfo {
 
 class Pipeline {
    public:
-    Pipeline(Ctx* ctx) : ctx(ctx) {}
+    Pipeline(Ctx* ctx) : ctx(ctx), intern(ctx ? ctx->strings : own_strings_) {}
     Ctx* ctx;
     Compiler C;
     std::vector<int> input_types;
@@ -42,7 +33,12 @@ class Pipeline {
     Stage stages[kMaxFilters + kMaxProbes]{};
     std::vector<Prog> filters;
     std::vector<ProbeInfo> probes;
-    StringIntern intern;
+   private:
+    StringIntern own_strings_;  // only for a pipeline without a context (source generation)
+
+   public:
+    // The context's string ids: dictionary entries and plain strings that a key reads
+    StringIntern& intern;
     // The program and its arena in one device buffer (one copy per upload).
     DevBuf d_code;
     Instr* d_prog = nullptr;
@@ -66,11 +62,14 @@ class Pipeline {
         // dictionary-coded source slots: the least and greatest string id of this batch's
         // dictionary (clamp entry included); first > second for every other slot
         std::vector<std::pair<uint32_t, uint32_t>> gid_range;
+        std::vector<DevBuf> strids;  // global string ids of plain string key columns, per row
     };
     // With `tables_dst`, the per-batch tables are copied there (at most `tables_cap` bytes,
     // from pageable memory) instead of into a new device buffer.
     void prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrows, const uint32_t* sel, int64_t nsel,
                  cudaStream_t s, Staging& st, Reservation* res, uint8_t* tables_dst = nullptr, size_t tables_cap = 0);
+    // Global string ids (the context's intern table) of every row of a plain UTF8 column.
+    DevBuf intern_plain_strings(const DevColumn& col, cudaStream_t s);
     // Slot mask check: does program `p` read a column with a validity bitmap?
     bool reads_nullable(const Prog& p, const Launch& L) const;
 };

@@ -1110,6 +1110,8 @@ Prog Compiler::compile_string_key(const ExprNode& e, const Schema& schema, int* 
     CV c = compile(e, schema);
     if (c.kind != 2) raise(ML_ERR_UNSUPPORTED, "string key must be a column reference on the GPU");
     *slot_out = c.slot;
+    if (std::find(string_key_slots.begin(), string_key_slots.end(), c.slot) == string_key_slots.end())
+        string_key_slots.push_back(c.slot);
     Prog p{};
     p.start = (int)code.size();
     p.len = 1;

@@ -93,6 +93,16 @@ class DevBuf {
     Reservation* res_ = nullptr;
 };
 
+// Global string ids: every string a key reads (a dictionary entry, a plain string of a key
+// column) gets one id per context, so group keys, join build sides and probe sides that hold
+// equal strings hold equal ids whatever their encoding (the dictionaries differ per row group).
+struct StringIntern {
+    std::mutex mu;
+    std::unordered_map<std::string, uint32_t> ids;
+    std::vector<std::string> strs;
+    uint32_t id(const std::string& s);  // mu held
+};
+
 // ---- context ------------------------------------------------------------------------------
 class Ctx {
    public:
@@ -103,6 +113,7 @@ class Ctx {
     MemoryPool pool;
     cudaStream_t stream = nullptr;  // default stream of the context
     std::atomic<uint64_t> launches{0};
+    StringIntern strings;
 
     void* dalloc(size_t bytes, size_t* cap);
     void dfree(void* p, size_t cap);
@@ -279,6 +290,7 @@ class Compiler {
     std::vector<uint8_t> arena;
     std::vector<SlotInfo> slots;
     std::vector<LutSpec> luts;
+    std::vector<int> string_key_slots;  // slots read as string keys (global string ids)
 
     // Compile `e` (reading `schema`) as a value of type `out_type`.
     Prog compile_value(const ExprNode& e, const Schema& schema, int out_type);
