@@ -380,8 +380,9 @@ def test_group_by_join_key_with_duplicate_and_null_build_keys(gpu_engine, by_bui
 
 @pytest.mark.parametrize("kind", ["dense", "small_wide", "sparse", "negative_i32", "compound", "utf8"])
 def test_join_index_kinds_match_oracle(gpu_engine, kind):
-    """Dense integer keys use the direct index, all other keys the hash table; both must
-    give the oracle's matches (through the fused aggregate) and distinct-key counts."""
+    """Dense integer keys use the direct index, all other keys (string keys by their global
+    string ids) the hash table; both must give the oracle's matches (through the fused
+    aggregate) and distinct-key counts."""
     rng = np.random.default_rng(12)
     nd, nf = 4000, 30_000
     valid = rng.random(nd) > 0.03
@@ -417,11 +418,6 @@ def test_join_index_kinds_match_oracle(gpu_engine, kind):
     # fact columns [f.., v] then build columns [k.., x]: x is column 2 * nkey + 1
     group = [(Col(2 * nkey + 1), INT32)]
     aggs = [AggSpec(SUM, Col(nkey), FLOAT64), AggSpec(COUNT_STAR)]
-    if kind == "utf8":  # string join keys are refused with Unsupported on the GPU
-        from minilake_b200.gpu import MiniLakeError
-        with pytest.raises(MiniLakeError, match="string join keys"):
-            gpu_engine.join_build(dim, types + [INT32], keys)
-        return
     res, stats = {}, {}
     for name, eng in (("gpu", gpu_engine), ("oracle", orc.OracleEngine(threads=2))):
         j = eng.join_build(dim, types + [INT32], keys)
