@@ -6,8 +6,12 @@ sequential or Zipf(s in [0.5, 1.5]) key frequencies, NULL fraction uniform in [0
 generated directly in HBM.  For each the library computes the scan features
 (`ml_gpu_card_features`: HyperLogLog register histogram and scan statistics) and the plain
 engine computes the true number of groups.  The MLP is trained on the first instances and
-tested on the rest, where each query runs twice: with the plain resize-on-overflow table
-(no size hint) and presized from the MLP's prediction.  Both must give identical results.
+tested on the rest, where each query runs four ways: with the plain resize-on-overflow table
+(no size hint), presized from MiniLake's planner estimate (a tenth of the input rows), presized
+from the HyperLogLog estimate, and presized from the MLP's prediction; the last two are timed
+with the features scan (and the MLP's inference) they need.  All four must give identical
+results.  The size hint also decides shared-memory pre-aggregation (a table of at most 65,536
+groups is pre-aggregated per CTA in shared memory, a larger one is updated in L2).
 
 Zipf keys are drawn by inverse-CDF sampling of the bounded continuous power law on [1, D+1)
 (rank = floor(x) - 1), the usual stand-in for a finite Zipf law.
@@ -201,31 +205,54 @@ def run(instances: int = 2000, train: int = 1500, seed: int = 45, min_rows: int 
             aggregate(ctx, di, 0, fetch=False)
             aggregate(ctx, di, 2 * d, fetch=False)
             del di
-    # presized (learned) vs resize-on-overflow (plain) on the test instances
-    plain_ms, learned_ms, resizes_plain, resizes_learned, identical = [], [], [], [], True
+    # Four arms per test instance, each timed with everything it needs before the GROUP BY:
+    #   plain    no size hint: the table starts small and grows on overflow (swiss.rs:219-232);
+    #   planner  MiniLake's own estimate, a tenth of the input rows (physical_planner.rs:251-295);
+    #   hll      the features scan, then the HyperLogLog estimate x 1.25;
+    #   learned  the features scan and the MLP's inference, then its prediction x 1.25.
+    arms = ("plain", "planner", "hll", "learned")
+    ms = {a: [] for a in arms}
+    resizes = {a: [] for a in arms}
+    feat_ms, infer_ms, identical = [], [], True
     for j, inst in enumerate(insts[train:]):
         di = DeviceInstance(inst)
-        hint = int(pred[j] * 1.25) + 16
-        a = aggregate(ctx, di, 0)
-        b = aggregate(ctx, di, hint)
-        identical &= a[1] == b[1] == truth[train + j] and a[3] == b[3]
-        plain_ms.append(a[0])
-        learned_ms.append(b[0])
-        resizes_plain.append(a[2])
-        resizes_learned.append(b[2])
+        res = {"plain": aggregate(ctx, di, 0), "planner": aggregate(ctx, di, max(inst.rows // 10, 1))}
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        _, est = card_features(ctx, di.ml, di.keys)
+        t_feat = (time.perf_counter() - t0) * 1e3
+        res["hll"] = aggregate(ctx, di, int(est * 1.25) + 16)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        f, _ = card_features(ctx, di.ml, di.keys)
+        t1 = time.perf_counter()
+        p1 = float(np.exp2(model.predict(f[None, :])[0]))
+        t2 = time.perf_counter()
+        res["learned"] = aggregate(ctx, di, int(p1 * 1.25) + 16)
+        feat_ms.append((t1 - t0) * 1e3)
+        infer_ms.append((t2 - t1) * 1e3)
+        extra = {"plain": 0.0, "planner": 0.0, "hll": t_feat, "learned": (t2 - t0) * 1e3}
+        for a in arms:
+            ms[a].append(res[a][0] + extra[a])
+            resizes[a].append(res[a][2])
+            identical &= res[a][1] == truth[train + j] and res[a][3] == res["plain"][3]
         del di
     model.close()
     ctx.close()
     pct = lambda a, p: float(np.percentile(a, p))
+    tot = {a: float(np.sum(ms[a])) for a in arms}
     return {
         "instances": instances, "train": train, "test": instances - train, "seed": seed,
         "rows": [min_rows, max_rows], "train_seconds": train_s, "final_train_loss": loss,
         "q_error_mlp": {"median": pct(q_mlp, 50), "p90": pct(q_mlp, 90), "p99": pct(q_mlp, 99), "max": float(q_mlp.max())},
         "q_error_hll": {"median": pct(q_hll, 50), "p90": pct(q_hll, 90), "p99": pct(q_hll, 99), "max": float(q_hll.max())},
-        "plain_resize_ms_total": float(np.sum(plain_ms)), "learned_presize_ms_total": float(np.sum(learned_ms)),
-        "speedup_total": float(np.sum(plain_ms) / max(np.sum(learned_ms), 1e-9)),
-        "speedup_median": float(np.median(np.asarray(plain_ms) / np.maximum(learned_ms, 1e-9))),
-        "resizes_plain_mean": float(np.mean(resizes_plain)), "resizes_learned_mean": float(np.mean(resizes_learned)),
+        "total_ms": tot,
+        "median_ms": {a: float(np.median(ms[a])) for a in arms},
+        "resizes_mean": {a: float(np.mean(resizes[a])) for a in arms},
+        "features_ms_total": float(np.sum(feat_ms)), "inference_ms_total": float(np.sum(infer_ms)),
+        "learned_vs_plain": tot["plain"] / max(tot["learned"], 1e-9),
+        "learned_vs_hll": tot["hll"] / max(tot["learned"], 1e-9),
+        "learned_vs_planner": tot["planner"] / max(tot["learned"], 1e-9),
         "identical_results": bool(identical),
     }
 

@@ -113,14 +113,17 @@ def test_mlp_training_matches_torch_fp32(ctx):
 
 
 def test_learned_sizing_keeps_results_identical():
-    """A small sweep: the engine's group counts match torch.unique, and presized and
-    resize-on-overflow runs give identical results."""
+    """A small sweep: the engine's group counts match torch.unique, and the four arms
+    (resize-on-overflow, the planner's rows / 10, HyperLogLog- and MLP-presized) give identical
+    results, the presized arms with no more resizes than the plain one."""
     from minilake_b200 import cardinality
     from minilake_b200.gpu import Context
     res = cardinality.run(instances=24, train=16, seed=46, min_rows=10_000, max_rows=400_000, epochs=60,
                           log=lambda *a: None)
     assert res["identical_results"]
-    assert res["resizes_learned_mean"] <= res["resizes_plain_mean"]
+    assert res["resizes_mean"]["learned"] <= res["resizes_mean"]["plain"]
+    assert res["resizes_mean"]["hll"] <= res["resizes_mean"]["plain"]
+    assert set(res["total_ms"]) == {"plain", "planner", "hll", "learned"}
     ctx = Context(0)
     for inst in cardinality.make_instances(6, seed=47, min_rows=10_000, max_rows=200_000):
         di = cardinality.DeviceInstance(inst)
