@@ -184,8 +184,12 @@ typedef struct ml_topn_local ml_topn_local;
  * by default the filter, aggregate, join-build and cardinality pipelines are specialized at run
  * time (NVRTC, compiled once per pipeline shape and cached for the process).  Both give the same
  * results.  Floating-point SUM/AVG accumulate with atomics, so they agree with a sequential sum
- * within rounding, not bit for bit from run to run.  Any other flag bit is rejected. */
-enum { ML_CTX_PROFILE = 2, ML_CTX_INTERPRET = 4 };
+ * within rounding, not bit for bit from run to run.  ML_CTX_SPILL lets a hash aggregate outgrow the
+ * HBM budget (ExecConfig::spill_dir, context.rs:14-34): when the budget refuses a table resize,
+ * every group's partial state moves to host memory, split into 16 partitions by key hash, and
+ * finalize merges one partition at a time (aggregate/hash.rs:189-281, 330-425).  Any other flag
+ * bit is rejected. */
+enum { ML_CTX_PROFILE = 2, ML_CTX_INTERPRET = 4, ML_CTX_SPILL = 8 };
 
 /* ExecConfig (context.rs:14-34) for one device: hbm_budget_bytes is the query-wide
  * MemoryPool limit (memory.rs:22-26) applied to device bytes; 0 = unlimited. */
@@ -292,6 +296,9 @@ int ml_gpu_hashagg_combine(ml_hashagg_local* local);
 int ml_gpu_hashagg_finalize(ml_hashagg* sink, ml_batch** out);
 /* Number of groups, table capacity and number of resize-on-overflow events so far. */
 int ml_gpu_hashagg_stats(ml_hashagg* sink, int64_t* groups, int64_t* capacity, int64_t* resizes);
+/* With ML_CTX_SPILL: how often the groups moved to host memory and how many group states moved
+ * in all (the spill files and bytes of OperatorMetrics, aggregate/hash.rs:270-279). */
+int ml_gpu_hashagg_spill_stats(ml_hashagg* sink, int64_t* spills, int64_t* spilled_groups);
 int ml_gpu_hashagg_destroy(ml_hashagg* sink);
 
 /* ---- resident hash aggregates for a serving loop (no counterpart in the reference) ---- */

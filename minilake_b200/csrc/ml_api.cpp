@@ -739,7 +739,7 @@ int ml_gpu_last_budget_error(char* op, size_t op_cap, uint64_t* requested, uint6
 int ml_gpu_ctx_create(int device, uint64_t hbm_budget_bytes, uint32_t flags, ml_ctx** out) {
     API_BEGIN
     REQUIRE(out, "null output");
-    REQUIRE((flags & ~(uint32_t)(ML_CTX_PROFILE | ML_CTX_INTERPRET)) == 0, "unknown context flags");
+    REQUIRE((flags & ~(uint32_t)(ML_CTX_PROFILE | ML_CTX_INTERPRET | ML_CTX_SPILL)) == 0, "unknown context flags");
     *out = new ml_ctx(device, hbm_budget_bytes, flags);
     API_END
 }
@@ -1533,6 +1533,29 @@ struct ml_hashagg {
     ml_hashagg(Ctx* c) : ctx(c), pipe(c), streams(c) {}
     void resume_overflow(Pipeline::Launch& L, uint64_t count, DevBuf& ovf, int w, cudaStream_t s,
                          unsigned long long* d_count, uint64_t* h_count, ErrWord& ew);
+    // Out-of-HBM aggregation (ML_CTX_SPILL): when the HBM budget refuses a table resize, every
+    // group's partial state moves to host memory, split by spill partition (key hash bits
+    // 32..35), and the table starts empty again (aggregate/hash.rs:189-281, 330-351).
+    struct SpillChunk {
+        uint32_t n = 0;
+        std::vector<uint64_t> keys;    // key words: nwords planes of n
+        std::vector<uint32_t> nulls;   // null masks
+        std::vector<uint64_t> acc;     // group blocks: n x stride words
+        std::vector<uint64_t> vcnt;    // valid-input counts: one plane of n per aggregate in vaggs
+        std::vector<int> vaggs;        // aggregates that kept valid-input counts when it spilled
+    };
+    std::vector<SpillChunk> spills[kSpillParts];
+    uint64_t spill_events = 0, spilled_groups = 0;
+    void spill_state(cudaStream_t s, ErrWord& ew);
+    void merge_spilled(const SpillChunk& c, cudaStream_t s, ErrWord& ew);
+    void reset_groups(cudaStream_t s);
+    // Free the table and its group arrays (it holds no groups); grow() allocates a new one.
+    void release_table() {
+        slots.release(), gkeys.release(), gnull.release(), acc.release();
+        for (auto& a : aggs) a.vcnt.release();
+        cap = 0;
+        gid_cap = 0;
+    }
     ~ml_hashagg() {
         for (auto& g : run.graphs) cudaGraphExecDestroy(g.second);
         if (run.host_count) ctx->release_slot(run.host_count);
@@ -1721,8 +1744,16 @@ void ml_hashagg::resume_overflow(Pipeline::Launch& L, uint64_t count, DevBuf& ov
         CK(cudaStreamSynchronize(s));
         uint32_t ng = std::min(*ew.h, gid_cap);
         uint64_t want = std::max<uint64_t>((uint64_t)gid_cap * 2, (uint64_t)ng + std::min<uint64_t>(count, 1ull << 30));
-        grow(std::min<uint64_t>(want, 0x7FFFFFFFull), s, ew);
-        resizes++;
+        try {
+            grow(std::min<uint64_t>(want, 0x7FFFFFFFull), s, ew);
+            resizes++;
+        } catch (const MlError& e) {
+            // HashAggLocal::account (aggregate/hash.rs:330-351): with spilling on, a refused
+            // resize moves the groups to host memory and the rows that did not fit go into the
+            // emptied table; without it the refusal is the query's error
+            if (e.code != ML_ERR_BUDGET || !(ctx->flags & ML_CTX_SPILL) || ungrouped || group_probe >= 0) throw;
+            spill_state(s, ew);
+        }
         DevBuf ovf2(ctx, count * w * 4, nullptr);
         CK(cudaMemsetAsync(d_count, 0, 8, s));
         CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
@@ -1748,6 +1779,105 @@ void ml_hashagg::resume_overflow(Pipeline::Launch& L, uint64_t count, DevBuf& ov
         count = *h_count;
         ovf = std::move(ovf2);
     }
+}
+
+void ml_hashagg::reset_groups(cudaStream_t s) {
+    CK(cudaMemsetAsync(ngroups.get(), 0, 16, s));
+    if (cap) CK(cudaMemsetAsync(slots.get(), 0, cap * 8 * (keys.nwords == 1 ? 2 : 4), s));
+    AggArgs A = args(nullptr, nullptr, 0);
+    for (size_t k = 0; k < aggs.size(); k++) A.aggs[k].vcnt = aggs[k].vcnt.get<uint64_t>();
+    launch_acc_init(A, 0, gid_cap, s);
+    ctx->count_launch();
+}
+
+void ml_hashagg::spill_state(cudaStream_t s, ErrWord& ew) {
+    uint32_t ng = 0;
+    CK(cudaMemcpyAsync(ew.h, ngroups.get(), 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    ng = std::min(*ew.h, gid_cap);
+    spill_events++;
+    if (!ng) return;
+    const int nw = keys.nwords ? keys.nwords : 1;
+    std::vector<int> vc;  // aggregates keeping valid-input counts
+    for (size_t k = 0; k < aggs.size(); k++)
+        if (aggs[k].vcnt_on && aggs[k].kind != A_AVG) vc.push_back((int)k);
+    // group ids grouped by spill partition (a stable counting sort on the device)
+    DevBuf part(ctx, (size_t)ng * 8, nullptr), perm(ctx, (size_t)ng * 4, nullptr), offs;
+    launch_spill_part(gkeys.get<uint64_t>(), gnull.get<uint32_t>(), gid_cap, ng, nw, part.get<uint64_t>(), s);
+    const int nb = xpart_blocks(ng);
+    DevBuf bc(ctx, (size_t)nb * kSpillParts * 4, nullptr);
+    launch_xpart_count(part.get<uint64_t>(), ng, kSpillParts, bc.get<uint32_t>(), s);
+    scan_counts(ctx, bc.get<uint32_t>(), (int64_t)nb * kSpillParts, offs, s);
+    launch_xpart_scatter(part.get<uint64_t>(), ng, kSpillParts, offs.get<uint64_t>(), perm.get<uint32_t>(), s);
+    std::vector<uint64_t> starts(kSpillParts + 1);
+    CK(cudaMemcpy2DAsync(starts.data(), 8, offs.get(), (size_t)nb * 8, 8, kSpillParts + 1, cudaMemcpyDeviceToHost, s));
+    // the partial states in partition order, then to host memory
+    const uint32_t* pm = perm.get<uint32_t>();
+    DevBuf gk(ctx, (size_t)ng * 8 * nw, nullptr), gn(ctx, (size_t)ng * 4, nullptr);
+    DevBuf ga(ctx, (size_t)ng * 8 * stride, nullptr), gv(ctx, std::max<size_t>((size_t)ng * 8 * vc.size(), 8), nullptr);
+    for (int w = 0; w < nw; w++)
+        launch_gather_fixed(gkeys.get<uint64_t>() + (size_t)w * gid_cap, 8, pm, ng, gk.get<uint64_t>() + (size_t)w * ng, s);
+    launch_gather_fixed(gnull.get(), 4, pm, ng, gn.get(), s);
+    launch_gather_fixed(acc.get(), 8 * stride, pm, ng, ga.get(), s);
+    for (size_t v = 0; v < vc.size(); v++)
+        launch_gather_fixed(aggs[vc[v]].vcnt.get(), 8, pm, ng, gv.get<uint64_t>() + v * ng, s);
+    ctx->count_launch(4 + nw + vc.size());
+    std::vector<uint64_t> hk((size_t)ng * nw), ha((size_t)ng * stride), hv((size_t)ng * vc.size());
+    std::vector<uint32_t> hn(ng);
+    CK(cudaMemcpyAsync(hk.data(), gk.get(), hk.size() * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hn.data(), gn.get(), hn.size() * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(ha.data(), ga.get(), ha.size() * 8, cudaMemcpyDeviceToHost, s));
+    if (!hv.empty()) CK(cudaMemcpyAsync(hv.data(), gv.get(), hv.size() * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int p = 0; p < kSpillParts; p++) {
+        const uint64_t a = starts[p], b = starts[p + 1];
+        if (a == b) continue;
+        SpillChunk c;
+        c.n = (uint32_t)(b - a);
+        for (int w = 0; w < nw; w++) c.keys.insert(c.keys.end(), hk.begin() + (size_t)w * ng + a, hk.begin() + (size_t)w * ng + b);
+        c.nulls.assign(hn.begin() + a, hn.begin() + b);
+        c.acc.assign(ha.begin() + a * stride, ha.begin() + b * stride);
+        for (size_t v = 0; v < vc.size(); v++)
+            c.vcnt.insert(c.vcnt.end(), hv.begin() + v * ng + a, hv.begin() + v * ng + b);
+        c.vaggs = vc;
+        spills[p].push_back(std::move(c));
+    }
+    spilled_groups += ng;
+    reset_groups(s);
+    CK(cudaStreamSynchronize(s));
+}
+
+void ml_hashagg::merge_spilled(const SpillChunk& c, cudaStream_t s, ErrWord& ew) {
+    AggArgs A = args(nullptr, nullptr, 0);
+    for (size_t k = 0; k < aggs.size(); k++) A.aggs[k].vcnt = aggs[k].vcnt.get<uint64_t>();
+    CK(cudaMemsetAsync(ew.d.get(), 0, 4, s));
+    std::vector<int> vc;  // aggregates keeping valid-input counts now
+    for (size_t k = 0; k < aggs.size(); k++)
+        if (aggs[k].vcnt_on && aggs[k].kind != A_AVG) vc.push_back((int)k);
+    {
+        // valid-input counts in the order the merge reads them; an aggregate that started counting
+        // after this chunk spilled had only valid inputs before: its count is the group's rows
+        std::vector<uint64_t> planes((size_t)c.n * vc.size());
+        for (size_t v = 0; v < vc.size(); v++) {
+            const auto it = std::find(c.vaggs.begin(), c.vaggs.end(), vc[v]);
+            for (uint32_t r = 0; r < c.n; r++)
+                planes[v * c.n + r] = it != c.vaggs.end() ? c.vcnt[(size_t)(it - c.vaggs.begin()) * c.n + r]
+                                                          : c.acc[(size_t)r * stride];
+        }
+        DevBuf k(ctx, c.keys.size() * 8, nullptr), nl(ctx, c.nulls.size() * 4, nullptr), a(ctx, c.acc.size() * 8, nullptr);
+        DevBuf v(ctx, std::max<size_t>(planes.size() * 8, 8), nullptr);
+        CK(cudaMemcpyAsync(k.get(), c.keys.data(), c.keys.size() * 8, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(nl.get(), c.nulls.data(), c.nulls.size() * 4, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(a.get(), c.acc.data(), c.acc.size() * 8, cudaMemcpyHostToDevice, s));
+        if (!planes.empty()) CK(cudaMemcpyAsync(v.get(), planes.data(), planes.size() * 8, cudaMemcpyHostToDevice, s));
+        launch_agg_merge_spill(A, k.get<uint64_t>(), nl.get<uint32_t>(), a.get<uint64_t>(), v.get<uint64_t>(), c.n,
+                               ew.d.get<uint32_t>(), s);
+        ctx->count_launch();
+        CK(cudaStreamSynchronize(s));  // the chunk's device copies go out of scope
+    }
+    CK(cudaMemcpyAsync(ew.h, ew.d.get(), 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    check_device_error(ctx, *ew.h);
 }
 
 // The host side of HashAggregateSink::new: compile the prologue, the GROUP BY keys and the
@@ -2156,16 +2286,12 @@ int ml_gpu_hashagg_combine(ml_hashagg_local* local) {
 }
 
 // Sink::finalize -> final_batches (aggregate/hash.rs:307-314)
-int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
-    API_BEGIN
-    HostTimer host_timer_(h ? h->ctx : nullptr, "host:hashagg_finalize");
-    REQUIRE(h && out, "null argument");
+}  // extern "C"
+
+// The output batch of the sink's current groups (Sink::finalize's final values,
+// accumulator.rs:500-594): one row per group, key columns then one column per aggregate.
+std::unique_ptr<ml_batch> hashagg_emit(ml_hashagg* h, cudaStream_t s) {
     Ctx* ctx = h->ctx;
-    ctx->set_current();
-    std::unique_lock<std::shared_mutex> lk(h->rw);
-    h->streams.sync();
-    if (h->run.s) CK(cudaStreamSynchronize(h->run.s));
-    cudaStream_t s = h->streams.own();
     uint32_t ng = 1;
     DevBuf gids;  // output row -> group id (GROUP BY the join key: the non-empty build rows)
     if (h->group_probe >= 0) {
@@ -2295,7 +2421,62 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
     for (auto& c : keycols) b->cols.push_back(std::move(c));
     for (auto& c : aggcols) b->cols.push_back(std::move(c));
     CK(cudaStreamSynchronize(s));
-    *out = b.release();
+    return b;
+}
+
+extern "C" {
+
+int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
+    API_BEGIN
+    HostTimer host_timer_(h ? h->ctx : nullptr, "host:hashagg_finalize");
+    REQUIRE(h && out, "null argument");
+    Ctx* ctx = h->ctx;
+    ctx->set_current();
+    std::unique_lock<std::shared_mutex> lk(h->rw);
+    h->streams.sync();
+    if (h->run.s) CK(cudaStreamSynchronize(h->run.s));
+    cudaStream_t s = h->streams.own();
+    if (!h->spill_events) {
+        *out = hashagg_emit(h, s).release();
+        return ML_OK;
+    }
+    // Spilled: the groups in HBM go to host memory too, then one spill partition at a time is
+    // merged back into the (empty) table and emitted (aggregate/hash.rs:369-425), so the table
+    // holds about 1/16 of the groups at once.
+    ErrWord ew(ctx);
+    h->spill_state(s, ew);
+    std::vector<std::unique_ptr<ml_batch>> parts;
+    std::vector<int> types;
+    uint64_t total_groups = 0;
+    h->release_table();  // the table the spills emptied: the partitions start small
+    for (int p = 0; p < kSpillParts; p++) {
+        if (h->spills[p].empty()) continue;
+        h->grow(1024, s, ew);
+        for (const auto& c : h->spills[p]) {
+            CK(cudaMemcpyAsync(ew.h, h->ngroups.get(), 4, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            const uint64_t need = (uint64_t)std::min(*ew.h, h->gid_cap) + c.n;  // every row may be new
+            if (need > h->gid_cap) h->grow(need, s, ew);
+            h->merge_spilled(c, s, ew);
+        }
+        std::vector<ml_hashagg::SpillChunk>().swap(h->spills[p]);
+        auto part = hashagg_emit(h, s);
+        total_groups += part->nrows;
+        if (types.empty())
+            for (auto& c : part->cols) types.push_back(c->dtype);
+        parts.push_back(std::move(part));
+        h->release_table();
+    }
+    h->final_groups = (int64_t)total_groups;
+    if (parts.empty()) {
+        *out = hashagg_emit(h, s).release();
+        return ML_OK;
+    }
+    auto res = std::make_unique<Reservation>(ctx, "HashAggregate(output)");
+    auto all = concat_batches(ctx, parts, types, s, res.get());
+    all->res = std::move(res);
+    CK(cudaStreamSynchronize(s));
+    *out = all.release();
     API_END
 }
 
@@ -2305,7 +2486,7 @@ int ml_gpu_hashagg_stats(ml_hashagg* h, int64_t* groups, int64_t* capacity, int6
     h->ctx->set_current();
     if (groups) {
         uint32_t ng = 1;
-        if (h->group_probe >= 0) {
+        if (h->group_probe >= 0 || h->spill_events) {
             REQUIRE(h->final_groups >= 0, "the number of groups is known after finalize");
             ng = (uint32_t)h->final_groups;
         } else if (!h->ungrouped) {
@@ -2316,6 +2497,14 @@ int ml_gpu_hashagg_stats(ml_hashagg* h, int64_t* groups, int64_t* capacity, int6
     }
     if (capacity) *capacity = (int64_t)h->cap;
     if (resizes) *resizes = h->resizes;
+    API_END
+}
+
+int ml_gpu_hashagg_spill_stats(ml_hashagg* h, int64_t* spills, int64_t* spilled_groups) {
+    API_BEGIN
+    REQUIRE(h, "null sink");
+    if (spills) *spills = (int64_t)h->spill_events;
+    if (spilled_groups) *spilled_groups = (int64_t)h->spilled_groups;
     API_END
 }
 

@@ -268,6 +268,57 @@ __global__ void __launch_bounds__(kXPartRows) k_xpart_scatter(const uint64_t* h,
     if (in) perm[offs[(int64_t)p * gridDim.x + blockIdx.x] + wcnt[w][p] + rank] = (uint32_t)r;
 }
 
+// ---- out-of-HBM aggregation (aggregate/hash.rs:189-281, 369-425) ------------------------------
+// Spill partition of each group: bits 32..35 of its key hash, which the table's slot choice (the
+// low bits) does not use, so every partition's groups still hash well into a table of their own.
+__global__ void k_spill_part(const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ng, int nwords,
+                             uint64_t* part) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ng) return;
+    const uint64_t w[2] = {gkeys[g], nwords > 1 ? gkeys[(uint64_t)gid_cap + g] : 0ull};
+    part[g] = (key_hash(w, nwords, gnull[g]) >> 32) & (kSpillParts - 1);
+}
+// Merge spilled partial states (n groups: key words as nwords planes of n, null masks, group
+// blocks of A.stride words, valid-input counts as planes of n for the aggregates that keep them)
+// into the table: a group's block adds up (counts, sums, AVG's sum and count) or folds (MIN/MAX),
+// as HashAggState::merge_partial merges partial batches (aggregate/hash.rs:125-139).
+__global__ void k_agg_merge_spill(const __grid_constant__ AggArgs A, const uint64_t* keys, const uint32_t* nulls,
+                                  const uint64_t* acc, const uint64_t* vcnt, uint32_t n, uint32_t* err) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint64_t w[2] = {keys[r], A.keys.nwords > 1 ? keys[(uint64_t)n + r] : 0ull};
+    const uint32_t nm = nulls[r];
+    bool ins;
+    uint64_t slot;
+    const uint32_t g = table_upsert(A.t, w, nm, key_hash(w, A.keys.nwords, nm), err, [&]() -> uint32_t {
+        const uint32_t id = atomicAdd(A.ngroups, 1u);
+        return id < A.gid_cap ? id : kNone;
+    }, &ins, &slot, A.ngroups, A.gid_cap);
+    if (g == kNone) {  // the table is sized for every spilled row of the partition: not reached
+        atomicOr(err, (uint32_t)DE_OVERFLOW_LOST);
+        return;
+    }
+    if (ins) {
+        A.gkeys[g] = w[0];
+        if (A.keys.nwords > 1) A.gkeys[(uint64_t)A.gid_cap + g] = w[1];
+        A.gnull[g] = nm;
+    }
+    uint64_t* blk = A.acc + (uint64_t)g * A.stride;
+    const uint64_t* src = acc + (uint64_t)r * A.stride;
+    if (src[0]) atomicAdd((unsigned long long*)blk, (unsigned long long)src[0]);
+    int v = 0;
+    for (int k = 0; k < A.nagg; k++) {
+        const AggDev& a = A.aggs[k];
+        if (a.func == ML_AGG_COUNT_STAR) continue;
+        acc_merge(a.kind, blk + a.off, src + a.off);
+        if (a.vcnt) {
+            const uint64_t c = vcnt[(uint64_t)v * n + r];
+            if (c) atomicAdd((unsigned long long*)a.vcnt + g, (unsigned long long)c);
+            v++;
+        }
+    }
+}
+
 __global__ void k_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                              int nwords, uint32_t* err) {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -775,7 +826,14 @@ __global__ void k_gather_fixed(const uint8_t* src, int width, const uint32_t* id
         switch (width) {
             case 1: dst[i] = src[r]; break;
             case 4: ((uint32_t*)dst)[i] = ((const uint32_t*)src)[r]; break;
-            default: ((uint64_t*)dst)[i] = ((const uint64_t*)src)[r]; break;
+            case 8: ((uint64_t*)dst)[i] = ((const uint64_t*)src)[r]; break;
+            default: {  // rows of width / 8 words (a group's accumulator block)
+                const int w = width / 8;
+                const uint64_t* s8 = (const uint64_t*)src + r * w;
+                uint64_t* d8 = (uint64_t*)dst + i * w;
+                for (int j = 0; j < w; j++) d8[j] = s8[j];
+                break;
+            }
         }
     }
 }
@@ -1312,6 +1370,14 @@ void launch_xpart_count(const uint64_t* h, int64_t n, int nparts, uint32_t* coun
 }
 void launch_xpart_scatter(const uint64_t* h, int64_t n, int nparts, const uint64_t* offs, uint32_t* perm, cudaStream_t s) {
     if (n > 0) k_xpart_scatter<<<xpart_blocks(n), kXPartRows, 0, s>>>(h, n, nparts, offs, perm);
+}
+void launch_spill_part(const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ng, int nwords,
+                       uint64_t* part, cudaStream_t s) {
+    if (ng) k_spill_part<<<(ng + kThreads - 1) / kThreads, kThreads, 0, s>>>(gkeys, gnull, gid_cap, ng, nwords, part);
+}
+void launch_agg_merge_spill(const AggArgs& A, const uint64_t* keys, const uint32_t* nulls, const uint64_t* acc,
+                            const uint64_t* vcnt, uint32_t n, uint32_t* err, cudaStream_t s) {
+    if (n) k_agg_merge_spill<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(A, keys, nulls, acc, vcnt, n, err);
 }
 void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                        int nwords, uint32_t* err, cudaStream_t s) {

@@ -18,6 +18,13 @@ int num_sms();  // of the current device
 constexpr int kPipelineThreads = 256;
 void launch_agg_rehash(TableView t, const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ngroups,
                        int nwords, uint32_t* err, cudaStream_t s);
+// Out-of-HBM aggregation: the spill partition (key hash bits 32..35) of groups [0, ng), and the
+// merge of spilled partial states into a table (k_agg_merge_spill).
+constexpr int kSpillParts = 16;
+void launch_spill_part(const uint64_t* gkeys, const uint32_t* gnull, uint32_t gid_cap, uint32_t ng, int nwords,
+                       uint64_t* part, cudaStream_t s);
+void launch_agg_merge_spill(const AggArgs& A, const uint64_t* keys, const uint32_t* nulls, const uint64_t* acc,
+                            const uint64_t* vcnt, uint32_t n, uint32_t* err, cudaStream_t s);
 // Exchange partitioning of n rows by key hash h[r] % nparts (nparts <= kMaxExchangeParts), in
 // blocks of kXPartRows rows: per-(partition, block) counts (partition-major), then, from their
 // exclusive scan `offs`, the stable permutation perm[pos] = row.
@@ -83,6 +90,7 @@ void launch_strid(const uint32_t* off, const uint8_t* bytes, const uint64_t* val
                   uint32_t* canon, uint32_t* err, cudaStream_t s);
 
 // Gathers.
+// dst row i = src row idx[i]; width is 1, 4 or a multiple of 8 bytes
 void launch_gather_fixed(const void* src, int width, const uint32_t* idx, int64_t k, void* dst, cudaStream_t s);
 void launch_gather_valid(const uint64_t* src, const uint32_t* idx, int64_t k, uint32_t* dst, cudaStream_t s);
 void launch_utf8_lengths(const uint32_t* off, const uint32_t* idx, int64_t k, uint32_t* len, cudaStream_t s);

@@ -89,6 +89,7 @@ def _load():
         "ml_gpu_hashagg_combine": ([VP], C.c_int),
         "ml_gpu_hashagg_finalize": ([VP, P(VP)], C.c_int),
         "ml_gpu_hashagg_stats": ([VP, P(I64), P(I64), P(I64)], C.c_int),
+        "ml_gpu_hashagg_spill_stats": ([VP, P(I64), P(I64)], C.c_int),
         "ml_gpu_hashagg_destroy": ([VP], C.c_int),
         "ml_gpu_join_build_create": ([VP, P(abi.MlPipeOp), I32, VP, I32, P(abi.MlExpr), I32, P(VP)], C.c_int),
         "ml_gpu_join_build_local_create": ([VP, P(VP)], C.c_int),
@@ -132,6 +133,7 @@ def _ptr(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data
 
 
+SPILL = 8  # ML_CTX_SPILL
 PROFILE = 2  # ML_CTX_PROFILE
 INTERPRET = 4  # ML_CTX_INTERPRET: ahead-of-time interpreter kernels instead of specialized ones
 
@@ -442,7 +444,10 @@ class HashAggregateSink:
     def stats(self):
         g, c, r = C.c_int64(), C.c_int64(), C.c_int64()
         _check(LIB.ml_gpu_hashagg_stats(self.h, C.byref(g), C.byref(c), C.byref(r)))
-        return {"groups": g.value, "capacity": c.value, "resizes": r.value}
+        sp, sg = C.c_int64(), C.c_int64()
+        _check(LIB.ml_gpu_hashagg_spill_stats(self.h, C.byref(sp), C.byref(sg)))
+        return {"groups": g.value, "capacity": c.value, "resizes": r.value, "spills": sp.value,
+                "spilled_groups": sg.value}
 
     def close(self):
         if self.h:
