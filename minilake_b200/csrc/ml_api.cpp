@@ -438,6 +438,102 @@ std::unique_ptr<ml_batch> concat_batches(Ctx* ctx, std::vector<std::unique_ptr<m
     return out;
 }
 
+// A finished batch in host memory (fixed-width or plain UTF8 columns): the spilled aggregation
+// parks each partition's output here, so HBM holds the final output only once.
+struct HostCol {
+    int dtype = 0;
+    bool utf8 = false, has_valid = false;
+    std::vector<uint8_t> data;
+    std::vector<uint32_t> offs;   // UTF8: n + 1, rebased to 0
+    std::vector<uint64_t> valid;  // bit r of word r / 64
+};
+struct HostBatch {
+    int64_t n = 0;
+    std::vector<HostCol> cols;
+};
+
+HostBatch batch_to_host(const ml_batch& b, cudaStream_t st) {
+    HostBatch h;
+    h.n = b.nrows;
+    for (const auto& cp : b.cols) {
+        const DevColumn& c = *cp;
+        HostCol o;
+        o.dtype = c.dtype;
+        o.utf8 = c.kind == CK_UTF8;
+        if (c.kind == CK_DICT) raise(ML_ERR_UNSUPPORTED, "dictionary column in a spilled output");
+        if (o.utf8) {
+            o.offs.resize(c.n + 1);
+            CK(cudaMemcpyAsync(o.offs.data(), c.optr(), (size_t)(c.n + 1) * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            const uint32_t first = o.offs[0];
+            o.data.resize(o.offs[c.n] - first);
+            if (!o.data.empty())
+                CK(cudaMemcpyAsync(o.data.data(), (const uint8_t*)c.dptr() + first, o.data.size(), cudaMemcpyDeviceToHost, st));
+            for (auto& x : o.offs) x -= first;
+        } else {
+            o.data.resize((size_t)c.n * width_of(c.dtype));
+            if (!o.data.empty()) CK(cudaMemcpyAsync(o.data.data(), c.dptr(), o.data.size(), cudaMemcpyDeviceToHost, st));
+        }
+        if (c.vptr()) {
+            o.has_valid = true;
+            o.valid.resize((size_t)(c.n + 63) / 64);
+            if (!o.valid.empty()) CK(cudaMemcpyAsync(o.valid.data(), c.vptr(), o.valid.size() * 8, cudaMemcpyDeviceToHost, st));
+        }
+        h.cols.push_back(std::move(o));
+    }
+    CK(cudaStreamSynchronize(st));
+    return h;
+}
+
+// Concatenate host batches into one device batch, one column at a time.
+std::unique_ptr<ml_batch> host_batches_to_device(Ctx* ctx, const std::vector<HostBatch>& parts, const std::vector<int>& types,
+                                                 Reservation* res) {
+    auto out = std::make_unique<ml_batch>();
+    out->ctx = ctx;
+    int64_t n = 0;
+    for (const auto& p : parts) n += p.n;
+    out->nrows = n;
+    for (size_t c = 0; c < types.size(); c++) {
+        auto d = std::make_unique<DevColumn>();
+        d->dtype = types[c];
+        d->n = n;
+        const bool utf8 = types[c] == ML_TYPE_UTF8;
+        d->kind = utf8 ? CK_UTF8 : CK_FIXED;
+        std::vector<uint8_t> data;
+        std::vector<uint32_t> offs(utf8 ? 1 : 0, 0);
+        bool any_valid = false;
+        for (const auto& p : parts) {
+            const HostCol& s = p.cols[c];
+            any_valid |= s.has_valid;
+            if (utf8) {
+                const uint64_t base = data.size();
+                if (base + s.data.size() > 0xFFFFFFFFull) raise(ML_ERR_UNSUPPORTED, "string column larger than 4 GiB");
+                for (int64_t r = 1; r <= p.n; r++) offs.push_back((uint32_t)(base + s.offs[r]));
+            }
+            data.insert(data.end(), s.data.begin(), s.data.end());
+        }
+        d->data = DevBuf(ctx, std::max<size_t>(data.size(), 8), res);
+        h2d_now(d->data.get(), data.data(), data.size());
+        if (utf8) {
+            d->offsets = DevBuf(ctx, offs.size() * 4, res);
+            h2d_now(d->offsets.get(), offs.data(), offs.size() * 4);
+        }
+        if (any_valid) {
+            std::vector<uint64_t> bits((size_t)(n + 63) / 64 + 1, 0);
+            int64_t row = 0;
+            for (const auto& p : parts) {
+                const HostCol& s = p.cols[c];
+                for (int64_t r = 0; r < p.n; r++, row++)
+                    if (!s.has_valid || ((s.valid[r / 64] >> (r % 64)) & 1)) bits[row / 64] |= 1ull << (row % 64);
+            }
+            d->validity = DevBuf(ctx, bits.size() * 8, res);
+            h2d_now(d->validity.get(), bits.data(), bits.size() * 8);
+        }
+        out->cols.push_back(std::move(d));
+    }
+    return out;
+}
+
 // ---- top-N over a device batch (sort.rs:85-132) ------------------------------------------
 struct SortKeySpec {
     ExprNode expr;
@@ -1547,6 +1643,9 @@ struct ml_hashagg {
     std::vector<SpillChunk> spills[kSpillParts];
     uint64_t spill_events = 0, spilled_groups = 0;
     void spill_state(cudaStream_t s, ErrWord& ew);
+    bool can_spill() const { return (ctx->flags & ML_CTX_SPILL) && !ungrouped && group_probe < 0; }
+    void spill_and_regrow(uint64_t want, cudaStream_t s, ErrWord& ew);
+    void regrow(uint64_t want, cudaStream_t s, ErrWord& ew);
     void merge_spilled(const SpillChunk& c, cudaStream_t s, ErrWord& ew);
     void reset_groups(cudaStream_t s);
     // Free the table and its group arrays (it holds no groups); grow() allocates a new one.
@@ -1751,8 +1850,8 @@ void ml_hashagg::resume_overflow(Pipeline::Launch& L, uint64_t count, DevBuf& ov
             // HashAggLocal::account (aggregate/hash.rs:330-351): with spilling on, a refused
             // resize moves the groups to host memory and the rows that did not fit go into the
             // emptied table; without it the refusal is the query's error
-            if (e.code != ML_ERR_BUDGET || !(ctx->flags & ML_CTX_SPILL) || ungrouped || group_probe >= 0) throw;
-            spill_state(s, ew);
+            if (e.code != ML_ERR_BUDGET || !can_spill()) throw;
+            spill_and_regrow(std::min<uint64_t>(want, 0x7FFFFFFFull), s, ew);
         }
         DevBuf ovf2(ctx, count * w * 4, nullptr);
         CK(cudaMemsetAsync(d_count, 0, 8, s));
@@ -1788,6 +1887,25 @@ void ml_hashagg::reset_groups(cudaStream_t s) {
     for (size_t k = 0; k < aggs.size(); k++) A.aggs[k].vcnt = aggs[k].vcnt.get<uint64_t>();
     launch_acc_init(A, 0, gid_cap, s);
     ctx->count_launch();
+}
+
+void ml_hashagg::spill_and_regrow(uint64_t want, cudaStream_t s, ErrWord& ew) {
+    spill_state(s, ew);
+    regrow(want, s, ew);
+}
+
+void ml_hashagg::regrow(uint64_t want, cudaStream_t s, ErrWord& ew) {
+    // the emptied table is freed, then the largest table the budget admits replaces it (no old
+    // groups to copy now); below 1024 groups the refusal stands
+    release_table();
+    for (uint64_t w = want;; w /= 2) {
+        try {
+            grow(std::max<uint64_t>(w, 1024), s, ew);
+            return;
+        } catch (const MlError& e) {
+            if (e.code != ML_ERR_BUDGET || w <= 1024) throw;
+        }
+    }
 }
 
 void ml_hashagg::spill_state(cudaStream_t s, ErrWord& ew) {
@@ -2035,12 +2153,23 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
             std::unique_lock<std::shared_mutex> lk(h->rw);
             if (!a.vcnt_on) {
                 h->streams.sync();
-                a.vcnt = DevBuf(ctx, (size_t)h->gid_cap * 8, h->res.get());
-                // every contribution so far was valid: start from the groups' row counts
-                CK(cudaMemcpy2DAsync(a.vcnt.get(), 8, h->acc.get(), (size_t)h->stride * 8, 8, h->gid_cap,
-                                     cudaMemcpyDeviceToDevice, s));
-                CK(cudaStreamSynchronize(s));
-                a.vcnt_on = true;
+                try {
+                    a.vcnt = DevBuf(ctx, (size_t)h->gid_cap * 8, h->res.get());
+                    // every contribution so far was valid: start from the groups' row counts
+                    CK(cudaMemcpy2DAsync(a.vcnt.get(), 8, h->acc.get(), (size_t)h->stride * 8, 8, h->gid_cap,
+                                         cudaMemcpyDeviceToDevice, s));
+                    CK(cudaStreamSynchronize(s));
+                    a.vcnt_on = true;
+                } catch (const MlError& e) {
+                    // no room for the counts: the groups spill (their counts are their rows) and
+                    // a table with the counts, as large as the budget admits, replaces this one
+                    if (e.code != ML_ERR_BUDGET || !h->can_spill()) throw;
+                    ErrWord ew(ctx);
+                    const uint64_t want = h->gid_cap;
+                    h->spill_state(s, ew);
+                    a.vcnt_on = true;  // after the spill: the spilled chunk holds no counts for it
+                    h->regrow(want, s, ew);
+                }
             }
         }
     }
@@ -2445,7 +2574,8 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
     // holds about 1/16 of the groups at once.
     ErrWord ew(ctx);
     h->spill_state(s, ew);
-    std::vector<std::unique_ptr<ml_batch>> parts;
+    // finished partitions wait in host memory: HBM holds one partition's table, then the output
+    std::vector<HostBatch> parts;
     std::vector<int> types;
     uint64_t total_groups = 0;
     h->release_table();  // the table the spills emptied: the partitions start small
@@ -2464,7 +2594,8 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
         total_groups += part->nrows;
         if (types.empty())
             for (auto& c : part->cols) types.push_back(c->dtype);
-        parts.push_back(std::move(part));
+        parts.push_back(batch_to_host(*part, s));
+        part.reset();
         h->release_table();
     }
     h->final_groups = (int64_t)total_groups;
@@ -2473,9 +2604,8 @@ int ml_gpu_hashagg_finalize(ml_hashagg* h, ml_batch** out) {
         return ML_OK;
     }
     auto res = std::make_unique<Reservation>(ctx, "HashAggregate(output)");
-    auto all = concat_batches(ctx, parts, types, s, res.get());
+    auto all = host_batches_to_device(ctx, parts, types, res.get());
     all->res = std::move(res);
-    CK(cudaStreamSynchronize(s));
     *out = all.release();
     API_END
 }
