@@ -48,7 +48,8 @@ enum {
     ML_ERR_CUDA = 3,        /* a CUDA runtime call failed */
     ML_ERR_TIMEOUT = 4,     /* a bounded device-side wait ran out */
     ML_ERR_UNSUPPORTED = 5, /* MiniLakeError::Unsupported */
-    ML_ERR_INTERNAL = 6
+    ML_ERR_INTERNAL = 6,
+    ML_ERR_STALE_PLAN = 7   /* a prepared query's data no longer fits its plan: prepare it again */
 };
 
 /* ---- data types: crates/minilake-core/src/types.rs:15-28 -------------------- */
@@ -366,6 +367,47 @@ int ml_gpu_topn_sink(ml_topn_local* local, const ml_column* cols, int32_t ncols,
 int ml_gpu_topn_combine(ml_topn_local* local);
 int ml_gpu_topn_finalize(ml_topn* sink, ml_batch** out);
 int ml_gpu_topn_destroy(ml_topn* sink);
+
+/* ---- Prepared query: a plan's pipelines as one CUDA graph (executor.rs:270-288) ---- */
+/* The pipelines of one physical plan over device-resident batches, in dependency order: join
+ * builds, then one hash aggregate whose prologue probes their tables, then (optionally) a top-N
+ * of the aggregate's output.  The first ml_gpu_query_run runs them through the sink calls above
+ * and records what depends on the data: each dense join index's key range (or hash capacity),
+ * whether build keys repeat, the group table's capacity and the result's row count.  Every later
+ * run replays all of it as one CUDA graph launch over the same buffers -- the build columns are
+ * copied in and the join indexes rebuilt, the group table reset and the fused kernel run, the
+ * groups' final values written, the top-N taken -- so it recomputes the result from the current
+ * contents of the batches.  Kernels in the graph check each recorded choice against the data;
+ * a failed check returns ML_ERR_STALE_PLAN (no result; the sinks hold partial state) and every
+ * later run does too: create the sinks and the query again.  A plan the graph cannot replay
+ * (a build pipeline with filters or computed columns, string build columns or group keys,
+ * sort keys that are not output columns, a limit above 32, a spilled aggregate, an empty
+ * result) runs once; later runs return ML_ERR_UNSUPPORTED,
+ * and ml_gpu_query_stats gives the reason.  The sinks and batches must outlive the query, and
+ * nothing else may use the sinks meanwhile. */
+typedef struct ml_query ml_query;
+int ml_gpu_query_create(ml_ctx* ctx, ml_query** out);
+/* Runs the build pipeline over the device-resident batch now and returns its table, for the
+ * Probe operators of the aggregate's prologue. */
+int ml_gpu_query_add_build(ml_query* q, ml_join_build* sink, const ml_column* cols, int32_t ncols,
+                           int64_t nrows, ml_join_table** table);
+int ml_gpu_query_set_aggregate(ml_query* q, ml_hashagg* sink, const ml_column* cols,
+                               int32_t ncols, int64_t nrows);
+/* ORDER BY keys[] LIMIT limit (limit > 0) over the aggregate's output columns. */
+int ml_gpu_query_set_topn(ml_query* q, const ml_sort_key* keys, int32_t nkeys, int64_t limit);
+int ml_gpu_query_run(ml_query* q, ml_batch** out);
+/* A replay of a planned top-N query whose result goes to host memory inside the graph (no
+ * device batch): *nrows result rows, read with ml_gpu_query_result.  ML_ERR_UNSUPPORTED before
+ * the planning run (ml_gpu_query_run) or for a plan that is not replayed. */
+int ml_gpu_query_run_host(ml_query* q, int64_t* nrows);
+/* Column `col` of the last ml_gpu_query_run_host result: nrows values (fixed width) and, when
+ * the column has one, its validity words ((nrows + 63) / 64 u64). */
+int ml_gpu_query_result(const ml_query* q, int32_t col, void* values, uint64_t* validity,
+                        int32_t* has_validity);
+/* runs, graph replays, kernels per replay, and why the plan is not replayed ("" if it is). */
+int ml_gpu_query_stats(const ml_query* q, int64_t* runs, int64_t* replays, int32_t* kernels,
+                       char* why, int32_t why_cap);
+int ml_gpu_query_destroy(ml_query* q);
 
 /* ---- learned cardinality estimator (no counterpart in the reference) ------------- */
 /* Predicts log2 of the number of distinct keys (GROUP BY groups, join-build keys; a NULL key

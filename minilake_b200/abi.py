@@ -15,7 +15,7 @@ from typing import Any, List, Optional, Sequence
 import numpy as np
 
 # status codes (crates/minilake-core/src/error.rs:8-48)
-OK, ERR_INVALID, ERR_BUDGET, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_INTERNAL = range(7)
+OK, ERR_INVALID, ERR_BUDGET, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_INTERNAL, ERR_STALE_PLAN = range(8)
 
 # data types (crates/minilake-core/src/types.rs:15-28)
 BOOL, INT32, INT64, FLOAT64, DATE, UTF8, NULL = range(7)

@@ -1402,8 +1402,8 @@ int ml_gpu_join_build_finalize(ml_join_build* j, ml_join_table** table) {
         jt->dense = DevBuf(ctx, jt->drange * 4, jt->res.get());
         CK(cudaMemsetAsync(jt->dense.get(), 0xFF, jt->drange * 4, s));
         KernelTimer kt(ctx, s, "join_insert");
-        launch_dense_insert(kc->dptr(), kc->dtype, kc->vptr(), n, jt->dmin, jt->dense.get<uint32_t>(),
-                            jt->next.get<uint32_t>(), jt->dup.get<uint32_t>(), s);
+        launch_dense_insert(kc->dptr(), kc->dtype, kc->vptr(), n, jt->dmin, jt->drange, jt->dense.get<uint32_t>(),
+                            jt->next.get<uint32_t>(), jt->dup.get<uint32_t>(), nullptr, s);
         kt.stop();
         ctx->count_launch();
     }
@@ -2806,6 +2806,661 @@ int ml_gpu_topn_destroy(ml_topn* t) {
         t->ctx->set_current();
         t->streams.sync();
         delete t;
+    }
+    API_END
+}
+
+}  // extern "C"
+
+// =====================================================================================================
+// Prepared query (executor.rs:270-288 runs a physical plan's pipelines in dependency order)
+// =====================================================================================================
+// One plan over device-resident tables: join builds, then one hash aggregate whose prologue
+// probes them, then optionally a top-N of the aggregate's output.  The first run goes through
+// the sink calls and records what depends on the data (the dense-index range or hash capacity,
+// the group table, the result's row count); later runs replay every pipeline as one CUDA graph
+// over the same buffers: the build columns are copied in and the join index rebuilt, the group
+// table reset and the fused kernel run, the groups emitted, the top-N taken and read back.
+// Kernels check each recorded choice against the run's data (guard bits below); a failed check
+// makes the run return ML_ERR_STALE_PLAN.
+namespace {
+constexpr uint32_t kGuardRange = 1;      // a build key outside the dense index
+constexpr uint32_t kGuardDups = 2;       // duplicate build keys appeared or went away
+constexpr uint32_t kGuardOverflow = 4;   // the group table overflowed
+constexpr uint32_t kGuardRows = 8;       // the group count no longer gives the planned result rows
+constexpr uint32_t kGuardTopRows = 16;   // a top-k list came back short
+}  // namespace
+
+struct ml_query {
+    Ctx* ctx;
+    std::unique_ptr<Reservation> res;  // declared before everything charged to it
+    struct Build {
+        ml_join_build* sink = nullptr;
+        std::vector<ml_column> cols;
+        int64_t nrows = 0;
+        ml_join_table* jt = nullptr;
+        std::unique_ptr<Pipeline> kp;  // hash-table form: the key programs over the build batch
+        Pipeline::Launch LA;
+        KeyLayout L{};
+        void* jit = nullptr;
+    };
+    std::vector<std::unique_ptr<Build>> builds;
+    ml_hashagg* agg = nullptr;
+    std::vector<ml_column> agg_cols;
+    int64_t agg_rows = 0;
+    std::vector<SortKeySpec> keys;
+    int64_t limit = 0;
+    bool topn = false;
+    // ---- the replay ----
+    cudaStream_t s = nullptr;
+    std::unique_ptr<Staging> st;
+    std::unique_ptr<ErrWord> ew;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;  // around the fused aggregate kernel
+    std::string why_not;                     // why runs take the sink calls ("" while replaying)
+    int64_t runs = 0, replays = 0;
+    int nkernels = 0;   // kernels one replay launches
+    int64_t cap = 0;    // output rows the aggregate can emit (its group ids)
+    int64_t k = 0;      // result rows of the top-N
+    Pipeline::Launch AL;
+    AggArgs A{};
+    void* jit = nullptr;
+    int grid = 0, smem = 0;
+    DevBuf tables, ovf, count, guard, ng, gids, bits, counts, offs, scratch, tbuf;
+    std::vector<std::unique_ptr<DevColumn>> outcols, rescols;
+    FinalArgs F{};
+    uint32_t* hguard = nullptr;  // pinned readbacks
+    uint64_t* hng = nullptr;
+    std::vector<void*> hres;     // pinned copies of the top-N result: per column values, validity
+    explicit ml_query(Ctx* c) : ctx(c) {}
+    ~ml_query() {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (void* p : hres)
+            if (p) cudaFreeHost(p);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (hguard) ctx->release_slot(hguard);
+        if (hng) ctx->release_slot(hng);
+        if (s) {
+            cudaStreamSynchronize(s);
+            ctx->free_stream(s);
+        }
+    }
+};
+
+namespace {
+void check_status(int st) {
+    if (st != ML_OK) raise(st, last_error());
+}
+
+// Why a plan cannot be replayed as recorded ("" when it can).
+std::string query_replay_blocker(ml_query* q) {
+    for (auto& b : q->builds) {
+        const ml_join_build* j = b->sink;
+        if (j->pipe.nstages > 0) return "a join build pipeline filters its rows";
+        for (const ColRef& r : j->pipe.out)
+            if (r.kind != 0) return "a join build pipeline computes a column";
+        for (auto& c : b->jt->batch.cols)
+            if (c->kind != CK_FIXED) return "a join build side holds strings";
+        for (auto& c : b->cols)
+            if (c.location != ML_LOC_DEVICE) return "a join build source is not device-resident";
+    }
+    ml_hashagg* h = q->agg;
+    if (!h) return "no aggregate";
+    for (auto& c : q->agg_cols)
+        if (c.location != ML_LOC_DEVICE) return "the aggregate's source is not device-resident";
+    if (h->spill_events) return "the aggregate spilled";
+    for (auto& d : h->dec)
+        if (d.str_kind) return "a string group key";
+    for (auto& kk : q->keys)
+        if (kk.expr.kind != ML_EXPR_COLUMN) return "a computed sort key";
+    if (q->topn && (q->limit <= 0 || q->limit > kTopNWarpMax)) return "a limit above 32";
+    return "";
+}
+}  // namespace
+
+namespace {
+// Every launch of one run of the plan, on q->s; captured once into the query's graph.
+void query_enqueue(ml_query* q) {
+    cudaStream_t s = q->s;
+    int nk = 0;
+    uint32_t* guard = q->guard.get<uint32_t>();
+    CK(cudaMemsetAsync(guard, 0, 4, s));
+    CK(cudaMemsetAsync(q->ew->d.get(), 0, 4, s));
+    // 1. join builds (build_table, join.rs:160-203): the build columns, then the index
+    for (auto& bp : q->builds) {
+        ml_query::Build& b = *bp;
+        ml_join_table* jt = b.jt;
+        const int64_t n = jt->batch.nrows;
+        const ml_join_build* j = b.sink;
+        for (size_t c = 0; c < j->pipe.out.size(); c++) {
+            const ml_column& src = b.cols[j->pipe.out[c].index];
+            DevColumn& dst = *jt->batch.cols[c];
+            const size_t bytes = (size_t)n * width_of(dst.dtype);
+            if (bytes) CK(cudaMemcpyAsync(dst.data.get(), src.data, bytes, cudaMemcpyDeviceToDevice, s));
+            if (dst.validity && src.validity && n)
+                CK(cudaMemcpyAsync(dst.validity.get(), src.validity, (size_t)(n + 63) / 64 * 8, cudaMemcpyDeviceToDevice, s));
+        }
+        CK(cudaMemsetAsync(jt->next.get(), 0xFF, std::max<size_t>((size_t)n * 4, 4), s));
+        CK(cudaMemsetAsync(jt->dup.get(), 0, 8, s));
+        if (jt->dense) {
+            const DevColumn& kc = *jt->batch.cols[jt->key_cols[0]];
+            CK(cudaMemsetAsync(jt->dense.get(), 0xFF, jt->drange * 4, s));
+            launch_dense_insert(kc.dptr(), kc.dtype, kc.vptr(), n, jt->dmin, jt->drange, jt->dense.get<uint32_t>(),
+                                jt->next.get<uint32_t>(), jt->dup.get<uint32_t>(), guard, s);
+            nk++;
+            if (jt->member) {
+                launch_dense_bits(jt->dense.get<uint32_t>(), jt->drange, jt->member.get<uint32_t>(), s);
+                nk++;
+            }
+        } else {
+            CK(cudaMemsetAsync(jt->slots.get(), 0, jt->cap * 8 * (jt->nwords == 1 ? 2 : 4), s));
+            if (n) {
+                TableView tv = jt->view();
+                uint32_t* next = jt->next.get<uint32_t>();
+                uint32_t* dup = jt->dup.get<uint32_t>();
+                int64_t nn = n;
+                if (b.jit) {
+                    void* args[] = {&b.LA.P, &b.L, &tv, &next, &dup, &nn};
+                    jit_launch(b.jit, pipeline_grid(n), kPipelineThreads, 0, s, args);
+                } else {
+                    launch_join_insert(b.LA.P, b.L, tv, next, dup, n, s);
+                }
+                nk++;
+            }
+        }
+        // the probes were specialized on whether build keys repeat
+        launch_plan_check(jt->dup.get(), 4, 0, jt->has_dups ? 1 : 0, kGuardDups, guard, s);
+        nk++;
+    }
+    // 2. the aggregate (HashAggLocal::sink): reset the groups, the fused kernel
+    ml_hashagg* h = q->agg;
+    CK(cudaMemsetAsync(h->ngroups.get(), 0, 16, s));
+    if (h->cap) CK(cudaMemsetAsync(h->slots.get(), 0, h->cap * 8 * (h->keys.nwords == 1 ? 2 : 4), s));
+    launch_acc_init(q->A, 0, h->gid_cap, s);
+    nk++;
+    CK(cudaMemsetAsync(q->count.get(), 0, 8, s));
+    CK(cudaEventRecordWithFlags(q->e0, s, cudaEventRecordExternal));
+    if (q->AL.P.n) {
+        if (q->jit) {
+            void* args[] = {&q->AL.P, &q->A};
+            jit_launch(q->jit, q->grid, kPipelineThreads, q->smem, s, args);
+        } else {
+            launch_agg(q->AL.P, q->A, q->smem, s);
+        }
+        nk++;
+    }
+    CK(cudaEventRecordWithFlags(q->e1, s, cudaEventRecordExternal));
+    launch_plan_check(q->count.get(), 8, 0, 0, kGuardOverflow, guard, s);
+    nk++;
+    // 3. the groups' final values (accumulator.rs:500-594) at the table's capacity; the number
+    //    of groups stays on the device (q->F.ng64)
+    const uint64_t* ngd = q->F.ng64;
+    for (auto& c : q->outcols)
+        if (c->validity) CK(cudaMemsetAsync(c->validity.get(), 0, c->validity.bytes(), s));
+    if (h->group_probe >= 0) {  // GROUP BY the join key: the groups are matched build rows
+        const ml_join_table* jt = h->pipe.probes[h->group_probe].jt;
+        const int nb = select_blocks(q->cap);
+        launch_group_flags(h->acc.get<uint64_t>(), h->stride, q->cap, h->dense_groups ? jt->dense.get<uint32_t>() : nullptr,
+                           q->bits.get<uint32_t>(), q->counts.get<uint32_t>(), s);
+        launch_scan_u32(q->counts.get<uint32_t>(), q->offs.get<uint64_t>(), nb, q->scratch.get<uint64_t>(), s);
+        nk += 4;
+        if (!h->dense_groups)  // the key gathers read every position: past the groups, build row 0
+            CK(cudaMemsetAsync(q->gids.get(), 0, (size_t)q->cap * 4, s));
+        launch_index_write(q->cap, q->bits.get<uint32_t>(), q->offs.get<uint64_t>(), q->gids.get<uint32_t>(), s);
+        nk++;
+        if (h->dense_groups) {
+            DevColumn& kc = *q->outcols[0];
+            launch_dense_keys(q->gids.get<uint32_t>(), q->cap, jt->dmin, kc.dtype, kc.data.get(), s, ngd);
+            nk++;
+        } else {
+            for (size_t i = 0; i < h->group_build_cols.size(); i++) {
+                const DevColumn& src = *jt->batch.cols[h->group_build_cols[i]];
+                DevColumn& dst = *q->outcols[i];
+                launch_gather_fixed(src.dptr(), width_of(src.dtype), q->gids.get<uint32_t>(), q->cap, dst.data.get(), s);
+                nk++;
+                if (src.vptr()) {
+                    launch_gather_valid(src.vptr(), q->gids.get<uint32_t>(), q->cap, dst.validity.get<uint32_t>(), s);
+                    nk++;
+                }
+            }
+        }
+    } else if (!h->ungrouped) {
+        launch_plan_count(h->ngroups.get<uint32_t>(), h->gid_cap, q->ng.get<uint64_t>(), s);
+        nk++;
+    }
+    launch_agg_final(q->F, s);
+    nk++;
+    // 4. the top-N (sort.rs:117-122) and the result's read-back
+    if (q->topn) {
+        const int nb = topn_warp_blocks(q->cap);
+        const size_t rows_b = ((size_t)nb * q->k * 4 + 15) & ~(size_t)15, cand_b = (size_t)nb * q->k * topn_entry_bytes();
+        uint8_t* base = q->tbuf.get<uint8_t>();
+        uint32_t* rows = nullptr;
+        SortDev S{};
+        S.nkeys = (int)q->keys.size();
+        for (size_t i = 0; i < q->keys.size(); i++) {
+            const DevColumn& c = *q->outcols[q->keys[i].expr.index];
+            DCol& d = S.cols[i];
+            d.dt = c.dtype;
+            d.kind = CK_FIXED;
+            d.data = c.dptr();
+            d.valid = c.vptr();
+            d.n = q->cap;
+            S.asc[i] = q->keys[i].asc;
+            S.nulls_first[i] = q->keys[i].nulls_first;
+        }
+        if (nb > 1) {
+            unsigned int* done = (unsigned int*)(base + rows_b + cand_b);
+            rows = (uint32_t*)(done + 4);
+            CK(cudaMemsetAsync(done, 0, 16, s));
+            launch_topn_warp(S, q->cap, (int)q->k, nb, (uint32_t*)base, base + rows_b, done, rows, s, ngd);
+        } else {
+            rows = (uint32_t*)base;
+            launch_topn_warp(S, q->cap, (int)q->k, nb, rows, nullptr, nullptr, nullptr, s, ngd);
+        }
+        launch_plan_rows(rows, (int)q->k, ngd, q->cap, kGuardTopRows, guard, s);
+        // as many groups as the planned result needs: at least `limit`, or exactly the planned rows
+        launch_plan_check(ngd, 8, q->k < q->limit ? 0 : 1, (uint64_t)q->k, kGuardRows, guard, s);
+        nk += 3;
+        for (size_t c = 0; c < q->outcols.size(); c++) {
+            const DevColumn& src = *q->outcols[c];
+            DevColumn& dst = *q->rescols[c];
+            launch_gather_fixed(src.dptr(), width_of(src.dtype), rows, q->k, dst.data.get(), s);
+            nk++;
+            if (src.validity) {
+                CK(cudaMemsetAsync(dst.validity.get(), 0, dst.validity.bytes(), s));
+                launch_gather_valid(src.vptr(), rows, q->k, dst.validity.get<uint32_t>(), s);
+                nk++;
+            }
+            // the rows to host memory too (ml_gpu_query_run_host)
+            CK(cudaMemcpyAsync(q->hres[2 * c], dst.data.get(), (size_t)q->k * width_of(dst.dtype), cudaMemcpyDeviceToHost, s));
+            if (dst.validity)
+                CK(cudaMemcpyAsync(q->hres[2 * c + 1], dst.validity.get(), (size_t)(q->k + 63) / 64 * 8,
+                                   cudaMemcpyDeviceToHost, s));
+        }
+    } else {
+        CK(cudaMemcpyAsync(q->hng, ngd, 8, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaMemcpyAsync(q->hguard, guard, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(q->ew->h, q->ew->d.get(), 4, cudaMemcpyDeviceToHost, s));
+    q->nkernels = nk;
+}
+}  // namespace
+
+namespace {
+// Set up the replay of a planned query (buffers at the recorded sizes, the aggregate's launch
+// as ml_gpu_hashagg_run_resident sets it up) and capture it into one CUDA graph.
+void query_capture(ml_query* q) {
+    Ctx* ctx = q->ctx;
+    ml_hashagg* h = q->agg;
+    cudaStream_t s = q->s;
+    // hash-table builds: the key programs over the build batch (as ml_gpu_join_build_finalize)
+    for (auto& bp : q->builds) {
+        ml_query::Build& b = *bp;
+        ml_join_table* jt = b.jt;
+        if (jt->dense || jt->batch.nrows == 0) continue;
+        const ml_join_build* j = b.sink;
+        b.kp = std::make_unique<Pipeline>(ctx);
+        b.kp->build(nullptr, 0, j->out_types.data(), (int)j->out_types.size());
+        b.L = b.kp->key_layout(j->keys.exprs.data(), (int)j->keys.exprs.size(), b.kp->out, false, nullptr);
+        b.kp->upload();
+        auto views = device_views(jt->batch);
+        b.kp->prepare(b.LA, views.data(), (int)views.size(), jt->batch.nrows, nullptr, 0, s, *q->st, nullptr);
+        b.LA.P.err = q->ew->d.get<uint32_t>();
+        b.jit = jit_join_insert_kernel(ctx, *b.kp, b.LA.P, b.L);
+    }
+    // the aggregate's launch
+    q->tables = DevBuf(ctx, 64 << 10, nullptr);
+    h->pipe.prepare(q->AL, q->agg_cols.data(), (int)q->agg_cols.size(), q->agg_rows, nullptr, 0, s, *q->st, nullptr,
+                    q->tables.get<uint8_t>(), q->tables.bytes());
+    const int w = 1 + (int)h->pipe.probes.size();
+    const bool can_overflow = !h->ungrouped && h->group_probe < 0;
+    const uint64_t ovf_cap = can_overflow ? std::max<uint64_t>((uint64_t)q->AL.P.n, 1024) : 0;
+    q->ovf = DevBuf(ctx, std::max<uint64_t>(ovf_cap * w * 4, 16), nullptr);
+    q->count = DevBuf(ctx, 16, nullptr);
+    q->AL.P.err = q->ew->d.get<uint32_t>();
+    q->AL.P.head_probe = h->group_probe;
+    if (h->dense_groups) q->AL.P.probes[h->group_probe].late = 1;
+    semi_probes(ctx, q->AL.P, h->pipe, h->group_probe, s);
+    q->A = h->args(q->count.get<unsigned long long>(), q->ovf.get<uint32_t>(), ovf_cap);
+    h->direct_slots(q->A, q->AL);
+    q->jit = jit_agg_kernel(ctx, h->pipe, q->AL.P, q->A);
+    if (!q->jit) q->A.priv_groups = 0, q->A.dslots = 0;
+    q->smem = agg_smem_bytes(q->A);
+    q->grid = q->jit ? agg_grid(q->jit, q->AL.P, q->smem) : pipeline_grid(q->AL.P.n);
+    // the groups' output at the table's capacity
+    q->cap = h->ungrouped ? 1 : (int64_t)h->gid_cap;
+    const size_t vbytes = std::max<size_t>((size_t)(q->cap + 63) / 64 * 8, 8);
+    q->ng = DevBuf(ctx, 8, nullptr);
+    FinalArgs& F = q->F;
+    F = FinalArgs{};
+    F.ngroups = (uint32_t)q->cap;
+    F.gid_cap = h->gid_cap;
+    F.nkeys = h->ungrouped || h->group_probe >= 0 ? 0 : h->keys.nkeys;
+    F.nagg = (int)h->aggs.size();
+    F.ungrouped = h->ungrouped;
+    F.stride = h->stride;
+    F.gkeys = h->gkeys.get<uint64_t>();
+    F.gnull = h->gnull.get<uint32_t>();
+    F.acc = h->acc.get<uint64_t>();
+    F.ng64 = q->ng.get<uint64_t>();
+    if (h->ungrouped) {
+        const uint64_t one = 1;
+        h2d_now(q->ng.get(), &one, 8);
+    }
+    auto column = [&](int dtype, bool valid) {
+        auto d = std::make_unique<DevColumn>();
+        d->dtype = dtype;
+        d->kind = CK_FIXED;
+        d->n = q->cap;
+        d->data = DevBuf(ctx, std::max<size_t>((size_t)q->cap * width_of(dtype), 8), q->res.get());
+        if (valid) d->validity = DevBuf(ctx, vbytes, q->res.get());
+        return d;
+    };
+    q->outcols.clear();
+    for (int k = 0; k < F.nkeys; k++) {
+        F.f[k] = h->keys.f[k];
+        q->outcols.push_back(column(h->dec[k].type, true));
+        F.key_out[k] = q->outcols.back()->data.get();
+        F.key_valid[k] = q->outcols.back()->validity.get<uint32_t>();
+    }
+    if (h->group_probe >= 0) {
+        const ml_join_table* jt = h->pipe.probes[h->group_probe].jt;
+        const int nb = select_blocks(q->cap);
+        q->bits = DevBuf(ctx, std::max<size_t>((size_t)(q->cap + 31) / 32 * 4, 4), nullptr);
+        q->counts = DevBuf(ctx, std::max<size_t>((size_t)nb * 4, 4), nullptr);
+        q->offs = DevBuf(ctx, (size_t)(nb + 1) * 8, nullptr);
+        q->scratch = DevBuf(ctx, std::max<size_t>(scan_scratch_words(nb) * 8, 8), nullptr);
+        q->gids = DevBuf(ctx, std::max<size_t>((size_t)q->cap * 4, 4), q->res.get());
+        F.gids = q->gids.get<uint32_t>();
+        F.ng64 = q->offs.get<uint64_t>() + nb;  // the scan's total: the groups with rows
+        if (h->dense_groups) {  // the key is the index position plus the index's smallest key
+            q->outcols.push_back(column(jt->key_types[0], false));
+        } else {  // the build keys of the matched rows
+            for (int c : h->group_build_cols) {
+                const DevColumn& src = *jt->batch.cols[c];
+                q->outcols.push_back(column(src.dtype, src.vptr() != nullptr));
+            }
+        }
+    }
+    for (int k = 0; k < F.nagg; k++) {
+        const AggState& a = h->aggs[k];
+        AggDev& ad = F.aggs[k];
+        ad.kind = a.kind;
+        ad.func = a.func;
+        ad.off = a.off;
+        ad.vcnt = a.vcnt_on && a.kind != A_AVG ? a.vcnt.get<uint64_t>() : nullptr;
+        F.out_type[k] = a.out_type;
+        q->outcols.push_back(column(a.out_type, true));
+        F.agg_out[k] = q->outcols.back()->data.get();
+        F.agg_valid[k] = q->outcols.back()->validity.get<uint32_t>();
+    }
+    // the top-N's scratch and result
+    q->rescols.clear();
+    if (q->topn) {
+        for (auto& kk : q->keys) {
+            const int c = (int)kk.expr.index;
+            if (c < 0 || c >= (int)q->outcols.size() || q->outcols[c]->dtype != kk.type)
+                raise(ML_ERR_INVALID, "a sort key does not name an output column of its type");
+        }
+        const int nb = topn_warp_blocks(q->cap);
+        const size_t rows_b = ((size_t)nb * q->k * 4 + 15) & ~(size_t)15, cand_b = (size_t)nb * q->k * topn_entry_bytes();
+        q->tbuf = DevBuf(ctx, rows_b + cand_b + 16 + (size_t)q->k * 4, nullptr);
+        for (auto& c : q->outcols) {
+            auto d = std::make_unique<DevColumn>();
+            d->dtype = c->dtype;
+            d->kind = CK_FIXED;
+            d->n = q->k;
+            d->data = DevBuf(ctx, std::max<size_t>((size_t)q->k * width_of(c->dtype), 8), q->res.get());
+            if (c->validity) d->validity = DevBuf(ctx, std::max<size_t>((size_t)(q->k + 63) / 64 * 8, 8), q->res.get());
+            void* hv = nullptr;
+            void* hb = nullptr;
+            CK(cudaMallocHost(&hv, std::max<size_t>((size_t)q->k * width_of(c->dtype), 8)));
+            q->hres.push_back(hv);
+            if (c->validity) CK(cudaMallocHost(&hb, std::max<size_t>((size_t)(q->k + 63) / 64 * 8, 8)));
+            q->hres.push_back(hb);
+            q->rescols.push_back(std::move(d));
+        }
+    }
+    q->guard = DevBuf(ctx, 8, nullptr);
+    CK(cudaEventCreate(&q->e0));
+    CK(cudaEventCreate(&q->e1));
+    CK(cudaStreamSynchronize(s));  // the launch's tables and programs are on the device
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+        query_enqueue(q);
+    } catch (...) {
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    CK(cudaStreamEndCapture(s, &g));
+    cudaError_t e = cudaGraphInstantiate(&q->exec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+}
+
+// The first run: every pipeline through the sink calls; records the result's row count.
+std::unique_ptr<ml_batch> query_plan_run(ml_query* q) {
+    Ctx* ctx = q->ctx;
+    ml_hashagg* h = q->agg;
+    ml_hashagg_local* local = nullptr;
+    check_status(ml_gpu_hashagg_local_create(h, &local));
+    int st = ml_gpu_hashagg_sink(local, q->agg_cols.data(), (int32_t)q->agg_cols.size(), q->agg_rows, nullptr, 0);
+    const int st2 = ml_gpu_hashagg_combine(local);
+    check_status(st);
+    check_status(st2);
+    ml_batch* raw = nullptr;
+    check_status(ml_gpu_hashagg_finalize(h, &raw));
+    std::unique_ptr<ml_batch> groups(raw);
+    if (!q->topn) return groups;
+    auto res = std::make_unique<Reservation>(ctx, "Query(output)");
+    auto best = topn_batch(ctx, *groups, q->keys, q->limit, q->s, res.get());
+    best->res = std::move(res);
+    q->k = best->nrows;
+    return best;
+}
+
+void query_launch(ml_query* q) {
+    CK(cudaGraphLaunch(q->exec, q->s));
+    q->ctx->count_launch(q->nkernels);
+    if (q->jit) q->ctx->add_profile("jit_launch", 0);
+}
+
+// After a replay's stream work: the checks' verdict, device errors, the kernel's time.
+void query_finish(ml_query* q) {
+    Ctx* ctx = q->ctx;
+    if (const uint32_t g = *q->hguard) {
+        cudaGraphExecDestroy(q->exec);
+        q->exec = nullptr;
+        q->why_not = "stale";
+        raise(ML_ERR_STALE_PLAN, std::string("the data no longer fits the prepared plan:") +
+                                     (g & kGuardRange ? " a build key outside the dense index" : "") +
+                                     (g & kGuardDups ? " build-key duplicates changed" : "") +
+                                     (g & kGuardOverflow ? " the group table overflowed" : "") +
+                                     (g & (kGuardRows | kGuardTopRows) ? " the group count changed the result rows" : ""));
+    }
+    check_device_error(ctx, *q->ew->h);
+    if (ctx->profiling()) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, q->e0, q->e1) == cudaSuccess) ctx->add_profile("pipeline_aggregate", ms);
+        else (void)cudaGetLastError();
+    }
+    q->replays++;
+}
+
+// A replay: one graph launch, then the result out of the graph's buffers.
+std::unique_ptr<ml_batch> query_replay(ml_query* q) {
+    Ctx* ctx = q->ctx;
+    cudaStream_t s = q->s;
+    query_launch(q);
+    auto out = std::make_unique<ml_batch>();
+    out->ctx = ctx;
+    out->res = std::make_unique<Reservation>(ctx, "Query(output)");
+    if (q->topn) {
+        out->nrows = q->k;
+        for (auto& c : q->rescols) out->cols.push_back(copy_column(ctx, *c, s, out->res.get()));
+        CK(cudaStreamSynchronize(s));
+    } else {
+        CK(cudaStreamSynchronize(s));
+        const int64_t n = *q->hguard ? 0 : (int64_t)*q->hng;
+        out->nrows = n;
+        for (auto& c : q->outcols) {
+            DevColumn v;
+            v.dtype = c->dtype;
+            v.kind = CK_FIXED;
+            v.n = n;
+            v.data_p = c->dptr();
+            v.valid_p = c->vptr();
+            out->cols.push_back(copy_column(ctx, v, s, out->res.get()));
+        }
+        CK(cudaStreamSynchronize(s));
+    }
+    query_finish(q);
+    return out;
+}
+}  // namespace
+
+extern "C" {
+
+int ml_gpu_query_create(ml_ctx* ctx, ml_query** out) {
+    API_BEGIN
+    REQUIRE(ctx && out, "null argument");
+    ctx->set_current();
+    auto q = std::make_unique<ml_query>(ctx);
+    q->res = std::make_unique<Reservation>(ctx, "Query");
+    q->s = ctx->new_stream();
+    q->st = std::make_unique<Staging>(ctx);
+    q->ew = std::make_unique<ErrWord>(ctx);
+    q->hguard = (uint32_t*)ctx->pinned_slot();
+    q->hng = (uint64_t*)ctx->pinned_slot();
+    *out = q.release();
+    API_END
+}
+
+// The build pipeline runs now, through the sink calls (JoinBuildSink, join.rs:72-242).
+int ml_gpu_query_add_build(ml_query* q, ml_join_build* sink, const ml_column* cols, int32_t ncols, int64_t nrows,
+                           ml_join_table** table) {
+    API_BEGIN
+    REQUIRE(q && sink && table && (cols || ncols == 0) && nrows >= 0, "bad arguments");
+    REQUIRE(!q->agg, "join builds come before the aggregate");
+    REQUIRE(!sink->table, "the join build sink is already finalized");
+    q->ctx->set_current();
+    auto b = std::make_unique<ml_query::Build>();
+    b->sink = sink;
+    b->cols.assign(cols, cols + ncols);
+    b->nrows = nrows;
+    ml_join_build_local* local = nullptr;
+    check_status(ml_gpu_join_build_local_create(sink, &local));
+    const int st = ml_gpu_join_build_sink(local, cols, ncols, nrows, nullptr, 0);
+    const int st2 = ml_gpu_join_build_combine(local);
+    check_status(st);
+    check_status(st2);
+    check_status(ml_gpu_join_build_finalize(sink, &b->jt));
+    *table = b->jt;
+    q->builds.push_back(std::move(b));
+    API_END
+}
+
+int ml_gpu_query_set_aggregate(ml_query* q, ml_hashagg* sink, const ml_column* cols, int32_t ncols, int64_t nrows) {
+    API_BEGIN
+    REQUIRE(q && sink && (cols || ncols == 0) && nrows >= 0, "bad arguments");
+    REQUIRE(!q->agg, "the query has its aggregate");
+    q->agg = sink;
+    q->agg_cols.assign(cols, cols + ncols);
+    q->agg_rows = nrows;
+    API_END
+}
+
+int ml_gpu_query_set_topn(ml_query* q, const ml_sort_key* keys, int32_t nkeys, int64_t limit) {
+    API_BEGIN
+    REQUIRE(q && keys && nkeys > 0 && nkeys <= kMaxKeys, "bad arguments");
+    REQUIRE(limit > 0, "the top-N of a query needs a limit");
+    REQUIRE(!q->runs, "the query has run");
+    q->keys.clear();
+    for (int k = 0; k < nkeys; k++)
+        q->keys.push_back(SortKeySpec{parse_expr(keys[k].expr), keys[k].expr.dtype, keys[k].asc != 0, keys[k].nulls_first != 0});
+    q->limit = limit;
+    q->topn = true;
+    API_END
+}
+
+int ml_gpu_query_run(ml_query* q, ml_batch** out) {
+    API_BEGIN
+    HostTimer host_timer_(q ? q->ctx : nullptr, "host:query_run");
+    REQUIRE(q && out, "null argument");
+    REQUIRE(q->agg, "the query has no aggregate");
+    q->ctx->set_current();
+    if (q->runs == 0) {
+        q->runs++;
+        auto r = query_plan_run(q);
+        q->why_not = query_replay_blocker(q);
+        if (q->why_not.empty() && q->topn && q->k == 0) q->why_not = "an empty result";
+        if (q->why_not.empty()) query_capture(q);
+        *out = r.release();
+        return ML_OK;
+    }
+    if (!q->exec) {
+        if (q->why_not == "stale") raise(ML_ERR_STALE_PLAN, "the data no longer fits the prepared plan");
+        raise(ML_ERR_UNSUPPORTED, "this plan runs once (" + q->why_not + "); create it again to run it again");
+    }
+    q->runs++;
+    *out = query_replay(q).release();
+    API_END
+}
+
+int ml_gpu_query_run_host(ml_query* q, int64_t* nrows) {
+    API_BEGIN
+    HostTimer host_timer_(q ? q->ctx : nullptr, "host:query_run");
+    REQUIRE(q && nrows, "null argument");
+    if (!q->exec || !q->topn) {
+        if (q->why_not == "stale") raise(ML_ERR_STALE_PLAN, "the data no longer fits the prepared plan");
+        raise(ML_ERR_UNSUPPORTED, "ml_gpu_query_run_host replays a planned top-N query (plan it with ml_gpu_query_run)");
+    }
+    q->ctx->set_current();
+    q->runs++;
+    query_launch(q);
+    CK(cudaStreamSynchronize(q->s));
+    query_finish(q);
+    *nrows = q->k;
+    API_END
+}
+
+int ml_gpu_query_result(const ml_query* q, int32_t col, void* values, uint64_t* validity, int32_t* has_validity) {
+    API_BEGIN
+    REQUIRE(q && values, "null argument");
+    REQUIRE(q->topn && !q->hres.empty(), "no host result: the query has no replayed top-N");
+    REQUIRE(col >= 0 && (size_t)col < q->rescols.size(), "column out of range");
+    const DevColumn& c = *q->rescols[col];
+    memcpy(values, q->hres[2 * col], (size_t)q->k * width_of(c.dtype));
+    const void* hv = q->hres[2 * col + 1];
+    if (has_validity) *has_validity = hv != nullptr;
+    if (hv && validity) memcpy(validity, hv, (size_t)(q->k + 63) / 64 * 8);
+    API_END
+}
+
+int ml_gpu_query_stats(const ml_query* q, int64_t* runs, int64_t* replays, int32_t* kernels, char* why, int32_t why_cap) {
+    API_BEGIN
+    REQUIRE(q, "null query");
+    if (runs) *runs = q->runs;
+    if (replays) *replays = q->replays;
+    if (kernels) *kernels = q->nkernels;
+    if (why && why_cap > 0) {
+        const std::string& w = q->why_not;
+        const size_t n = std::min<size_t>(w.size(), (size_t)why_cap - 1);
+        memcpy(why, w.data(), n);
+        why[n] = 0;
+    }
+    API_END
+}
+
+int ml_gpu_query_destroy(ml_query* q) {
+    API_BEGIN
+    if (q) {
+        q->ctx->set_current();
+        delete q;
     }
     API_END
 }

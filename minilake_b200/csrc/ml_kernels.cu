@@ -345,7 +345,10 @@ __global__ void k_acc_init(AggArgs A, uint32_t from, uint32_t to) {
 // Final values (accumulator.rs:500-526): AVG = sum / count, empty -> NULL.
 __global__ void k_agg_final(const __grid_constant__ FinalArgs F) {
     uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
-    bool in = o < F.ngroups;
+    uint32_t ng = F.ngroups;
+    if (F.ng64) ng = (uint32_t)min((uint64_t)ng, __ldg(F.ng64));
+    if (F.ng32) ng = min(ng, __ldg(F.ng32));
+    bool in = o < ng;
     uint32_t g = in ? (F.gids ? F.gids[o] : o) : 0;
     uint32_t lane = threadIdx.x & 31;
     for (int k = 0; k < F.nkeys; k++) {
@@ -362,7 +365,7 @@ __global__ void k_agg_final(const __grid_constant__ FinalArgs F) {
             else ((uint64_t*)F.key_out[k])[o] = v;
         }
         uint32_t bits = __ballot_sync(0xFFFFFFFFu, in && valid);
-        if (lane == 0 && (o >> 5) < (F.ngroups + 31) / 32) F.key_valid[k][o >> 5] = bits;
+        if (lane == 0 && (o >> 5) < (ng + 31) / 32) F.key_valid[k][o >> 5] = bits;
     }
     const uint64_t* blk = F.acc + (uint64_t)g * F.stride;
     for (int k = 0; k < F.nagg; k++) {
@@ -402,7 +405,7 @@ __global__ void k_agg_final(const __grid_constant__ FinalArgs F) {
             }
         }
         uint32_t bits = __ballot_sync(0xFFFFFFFFu, in && valid);
-        if (lane == 0 && (o >> 5) < (F.ngroups + 31) / 32) F.agg_valid[k][o >> 5] = bits;
+        if (lane == 0 && (o >> 5) < (ng + 31) / 32) F.agg_valid[k][o >> 5] = bits;
     }
 }
 
@@ -732,13 +735,18 @@ __global__ void k_dense_bits(const uint32_t* dense, uint64_t n, uint32_t* bits) 
     }
 }
 
-__global__ void k_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint32_t* dense,
-                               uint32_t* next, uint32_t* dup_flag) {
+__global__ void k_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint64_t drange,
+                               uint32_t* dense, uint32_t* next, uint32_t* dup_flag, uint32_t* range_err) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         uint32_t r = (uint32_t)i;
         if (!valid_bit(valid, r)) continue;  // NULL keys never match
-        uint32_t old = atomicExch(dense + (norm_int_key(data, dt, r) - dmin), r);
+        const uint64_t pos = norm_int_key(data, dt, r) - dmin;
+        if (pos >= drange) {  // outside the index (a replayed plan's data changed): skipped, reported
+            if (range_err) atomicOr(range_err, 1u);
+            continue;
+        }
+        uint32_t old = atomicExch(dense + pos, r);
         if (old != kNone) {
             next[r] = old;
             if (*dup_flag == 0) atomicExch(dup_flag, 1u);
@@ -1186,7 +1194,9 @@ __device__ TopEntry warp_topk_fixed(const SortDev& S, int64_t n, int k, int64_t 
 // DT: the first sort key's type when it is a fixed-width column (warp_topk_fixed), -1 otherwise.
 template <int DT>
 __global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortDev S, int64_t n, int k, uint32_t* out,
-                                                   TopEntry* cand, unsigned int* done, uint32_t* final_out) {
+                                                   TopEntry* cand, unsigned int* done, uint32_t* final_out,
+                                                   const uint64_t* n_dev) {
+    if (n_dev) n = min(n, (int64_t)__ldcg(n_dev));  // a replayed plan's row count
     __shared__ TopEntry lists[8][32];
     __shared__ TopEntry queue[8][32];
     __shared__ bool last;
@@ -1407,7 +1417,8 @@ void launch_index_write(int64_t n, const uint32_t* bits, const uint64_t* block_o
     int nb = select_blocks(n);
     if (nb) k_index_write<<<nb, kThreads, 0, s>>>(n, nullptr, bits, block_offsets, out);
 }
-__global__ void k_dense_keys(const uint32_t* gids, int64_t n, uint64_t dmin, int dt, void* out) {
+__global__ void k_dense_keys(const uint32_t* gids, int64_t n, const uint64_t* n_dev, uint64_t dmin, int dt, void* out) {
+    if (n_dev) n = min(n, (int64_t)__ldg(n_dev));
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint64_t k = dmin + gids[i];  // the normalized key word
@@ -1415,8 +1426,9 @@ __global__ void k_dense_keys(const uint32_t* gids, int64_t n, uint64_t dmin, int
         else ((int32_t*)out)[i] = (int32_t)(uint32_t)k;
     }
 }
-void launch_dense_keys(const uint32_t* gids, int64_t n, uint64_t dmin, int dt, void* out, cudaStream_t s) {
-    if (n) k_dense_keys<<<grid_for(n, 8), kThreads, 0, s>>>(gids, n, dmin, dt, out);
+void launch_dense_keys(const uint32_t* gids, int64_t n, uint64_t dmin, int dt, void* out, cudaStream_t s,
+                       const uint64_t* n_dev) {
+    if (n) k_dense_keys<<<grid_for(n, 8), kThreads, 0, s>>>(gids, n, n_dev, dmin, dt, out);
 }
 void launch_group_flags(const uint64_t* acc, int stride, int64_t n, const uint32_t* member, uint32_t* bits,
                         uint32_t* block_counts, cudaStream_t s) {
@@ -1451,9 +1463,9 @@ void launch_join_insert(const PipeArgs& P, const KeyLayout& L, TableView t, uint
 void launch_key_range(const void* data, int dt, const uint64_t* valid, int64_t n, unsigned long long* mm, cudaStream_t s) {
     if (n) k_key_range<<<grid_for(n, 4), kThreads, 0, s>>>(data, dt, valid, n, mm);
 }
-void launch_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint32_t* dense,
-                         uint32_t* next, uint32_t* dup_flag, cudaStream_t s) {
-    if (n) k_dense_insert<<<grid_for(n, 8), kThreads, 0, s>>>(data, dt, valid, n, dmin, dense, next, dup_flag);
+void launch_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint64_t drange,
+                         uint32_t* dense, uint32_t* next, uint32_t* dup_flag, uint32_t* range_err, cudaStream_t s) {
+    if (n) k_dense_insert<<<grid_for(n, 8), kThreads, 0, s>>>(data, dt, valid, n, dmin, drange, dense, next, dup_flag, range_err);
 }
 void launch_dense_bits(const uint32_t* dense, uint64_t n, uint32_t* bits, cudaStream_t s) {
     const uint64_t words = (n + 31) / 32;
@@ -1505,25 +1517,60 @@ int topn_warp_blocks(int64_t n) {
     }();
     // at least 8 chunks of 128 rows per warp: a warp's first chunk mostly enters its list, later
     // ones mostly fall below the list's k-th entry or the launch-wide threshold
-    int64_t want = (n + 8191) / 8192;
+    int64_t rpc = 8192;
+    if (const char* e = getenv("MLG_TOPN_ROWS_PER_CTA")) rpc = atoll(e);
+    int64_t want = (n + rpc - 1) / rpc;
     int64_t cap = (int64_t)num_sms() * resident;
     return (int)std::max<int64_t>(1, std::min(want, cap));
 }
 size_t topn_entry_bytes() { return sizeof(TopEntry); }
 void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* out, void* cand, unsigned int* done,
-                      uint32_t* final_out, cudaStream_t s) {
+                      uint32_t* final_out, cudaStream_t s, const uint64_t* n_dev) {
     const DCol& c = S.cols[0];
     const int dt = S.nkeys > 0 && c.kind == CK_FIXED && c.src == 0 ? c.dt : -1;
     TopEntry* ce = (TopEntry*)cand;
     switch (dt) {
-        case ML_TYPE_FLOAT64: k_topn_warp<ML_TYPE_FLOAT64><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
-        case ML_TYPE_INT64: k_topn_warp<ML_TYPE_INT64><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
+        case ML_TYPE_FLOAT64: k_topn_warp<ML_TYPE_FLOAT64><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out, n_dev); break;
+        case ML_TYPE_INT64: k_topn_warp<ML_TYPE_INT64><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out, n_dev); break;
         case ML_TYPE_INT32:
-        case ML_TYPE_DATE: k_topn_warp<ML_TYPE_INT32><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
-        case ML_TYPE_BOOL: k_topn_warp<ML_TYPE_BOOL><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
-        default: k_topn_warp<-1><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out); break;
+        case ML_TYPE_DATE: k_topn_warp<ML_TYPE_INT32><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out, n_dev); break;
+        case ML_TYPE_BOOL: k_topn_warp<ML_TYPE_BOOL><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out, n_dev); break;
+        default: k_topn_warp<-1><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out, n_dev); break;
     }
 }
+// ---- prepared-query checks: a replayed plan's recorded choices against this run's data ------
+// *guard |= bit when the 4- or 8-byte value at p differs from v (op 0) or is below v (op 1).
+__global__ void k_plan_check(const void* p, int width, int op, uint64_t v, uint32_t bit, uint32_t* guard) {
+    const uint64_t x = width == 8 ? *(const uint64_t*)p : (uint64_t) * (const uint32_t*)p;
+    if (op == 0 ? x != v : x < v) atomicOr(guard, bit);
+}
+void launch_plan_check(const void* p, int width, int op, uint64_t v, uint32_t bit, uint32_t* guard, cudaStream_t s) {
+    k_plan_check<<<1, 1, 0, s>>>(p, width, op, v, bit, guard);
+}
+// out = min(*count, cap): a group counter as the 64-bit row count later kernels read.
+__global__ void k_plan_count(const uint32_t* count, uint64_t cap, uint64_t* out) {
+    const uint64_t c = *count;
+    *out = c < cap ? c : cap;
+}
+void launch_plan_count(const uint32_t* count, uint64_t cap, uint64_t* out, cudaStream_t s) {
+    k_plan_count<<<1, 1, 0, s>>>(count, cap, out);
+}
+// Row ids of a replayed top-k: an id at or past the rows that exist (the list had fewer than
+// k rows) becomes 0, so the gathers after it stay in bounds, and sets `bit`.
+__global__ void k_plan_rows(uint32_t* rows, int k, const uint64_t* n_dev, uint64_t cap, uint32_t bit, uint32_t* guard) {
+    const int i = threadIdx.x;
+    if (i >= k) return;
+    const uint64_t n = n_dev && *n_dev < cap ? *n_dev : cap;
+    if (rows[i] >= n) {
+        rows[i] = 0;
+        atomicOr(guard, bit);
+    }
+}
+void launch_plan_rows(uint32_t* rows, int k, const uint64_t* n_dev, uint64_t cap, uint32_t bit, uint32_t* guard,
+                      cudaStream_t s) {
+    if (k > 0) k_plan_rows<<<1, 32 * ((k + 31) / 32), 0, s>>>(rows, k, n_dev, cap, bit, guard);
+}
+
 __global__ void k_iota_u32(uint32_t* out, int64_t n) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (uint32_t)i;

@@ -51,6 +51,9 @@ struct FinalArgs {
     int32_t out_type[kMaxAggs];
     void* agg_out[kMaxAggs];
     uint32_t* agg_valid[kMaxAggs];
+    // optional device-side group count (a replayed plan's): the output has min(ngroups, *ng) rows
+    const uint64_t* ng64;
+    const uint32_t* ng32;
 };
 void launch_agg_final(const FinalArgs& F, cudaStream_t s);
 
@@ -65,7 +68,9 @@ void launch_select_write(const PipeArgs& P, const uint32_t* bits, const uint64_t
 void launch_group_flags(const uint64_t* acc, int stride, int64_t n, const uint32_t* member, uint32_t* bits,
                         uint32_t* block_counts, cudaStream_t s);
 // Key values of dense-index groups: out[i] = dmin + gids[i] as int64, or as int32 / date.
-void launch_dense_keys(const uint32_t* gids, int64_t n, uint64_t dmin, int dt, void* out, cudaStream_t s);
+// n_dev (optional): the device-side count of gids (at most n)
+void launch_dense_keys(const uint32_t* gids, int64_t n, uint64_t dmin, int dt, void* out, cudaStream_t s,
+                       const uint64_t* n_dev = nullptr);
 void launch_index_write(int64_t n, const uint32_t* bits, const uint64_t* block_offsets, uint32_t* out, cudaStream_t s);
 // Exclusive scan of u32 counts into u64 offsets (offsets[n] = total).
 void launch_scan_u32(const uint32_t* in, uint64_t* out, int64_t n, uint64_t* scratch, cudaStream_t s);
@@ -102,8 +107,9 @@ void launch_u64_to_u32(const uint64_t* in, uint32_t* out, int64_t n, cudaStream_
 // Dense join index: key range of a one-column integer build key (mm[0] = min, mm[1] = max,
 // initialized to ~0 / 0), the insert, and the count of distinct keys.
 void launch_key_range(const void* data, int dt, const uint64_t* valid, int64_t n, unsigned long long* mm, cudaStream_t s);
-void launch_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint32_t* dense,
-                         uint32_t* next, uint32_t* dup_flag, cudaStream_t s);
+// Keys outside [dmin, dmin + drange) are skipped and set bit 0 of *range_err (when given).
+void launch_dense_insert(const void* data, int dt, const uint64_t* valid, int64_t n, uint64_t dmin, uint64_t drange,
+                         uint32_t* dense, uint32_t* next, uint32_t* dup_flag, uint32_t* range_err, cudaStream_t s);
 void launch_count_dense(const uint32_t* dense, uint64_t n, unsigned long long* out, cudaStream_t s);
 // bits[i / 32] bit i % 32 = (dense[i] != kNone), for i < n.
 void launch_dense_bits(const uint32_t* dense, uint64_t n, uint32_t* bits, cudaStream_t s);
@@ -137,8 +143,17 @@ int topn_warp_blocks(int64_t n);
 // bytes: the finished-CTA counter and the launch's shared top-k threshold), the last CTA merges
 // every CTA's candidates into final_out[0 .. k): one launch.
 size_t topn_entry_bytes();
+// n_dev (optional): a device-side row count (at most n) read by the kernel.
 void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* out, void* cand, unsigned int* done,
-                      uint32_t* final_out, cudaStream_t s);
+                      uint32_t* final_out, cudaStream_t s, const uint64_t* n_dev = nullptr);
+
+// Prepared-query checks (one thread each): *guard |= bit when the 4- or 8-byte value at p
+// differs from v (op 0) or is below v (op 1); a u32 group counter as a u64 row count capped at
+// cap; top-k row ids at or past the device row count (or cap) replaced by 0, setting bit.
+void launch_plan_check(const void* p, int width, int op, uint64_t v, uint32_t bit, uint32_t* guard, cudaStream_t s);
+void launch_plan_count(const uint32_t* count, uint64_t cap, uint64_t* out, cudaStream_t s);
+void launch_plan_rows(uint32_t* rows, int k, const uint64_t* n_dev, uint64_t cap, uint32_t bit, uint32_t* guard,
+                      cudaStream_t s);
 
 // ---- static scratch of ml_gpu_filter_static ----------------------------------------------
 // One file-scope device array per device holds every temporary of the no-allocation filter:

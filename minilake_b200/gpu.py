@@ -42,6 +42,10 @@ class ResourcesExhausted(MiniLakeError):
         self.operator, self.requested, self.used, self.limit = operator, requested, used, limit
 
 
+class StalePlan(MiniLakeError):
+    """A prepared query's data no longer fits its plan (ML_ERR_STALE_PLAN): prepare it again."""
+
+
 def _load():
     if not os.path.exists(_LIB_PATH):
         raise ImportError(f"{_LIB_PATH} is missing: build the CUDA library first "
@@ -106,6 +110,15 @@ def _load():
         "ml_gpu_topn_combine": ([VP], C.c_int),
         "ml_gpu_topn_finalize": ([VP, P(VP)], C.c_int),
         "ml_gpu_topn_destroy": ([VP], C.c_int),
+        "ml_gpu_query_create": ([VP, P(VP)], C.c_int),
+        "ml_gpu_query_add_build": ([VP, VP, P(abi.MlColumn), I32, I64, P(VP)], C.c_int),
+        "ml_gpu_query_set_aggregate": ([VP, VP, P(abi.MlColumn), I32, I64], C.c_int),
+        "ml_gpu_query_set_topn": ([VP, P(abi.MlSortKey), I32, I64], C.c_int),
+        "ml_gpu_query_run": ([VP, P(VP)], C.c_int),
+        "ml_gpu_query_run_host": ([VP, P(I64)], C.c_int),
+        "ml_gpu_query_result": ([VP, I32, VP, VP, P(I32)], C.c_int),
+        "ml_gpu_query_stats": ([VP, P(I64), P(I64), P(I32), C.c_char_p, I32], C.c_int),
+        "ml_gpu_query_destroy": ([VP], C.c_int),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
@@ -126,6 +139,8 @@ def _check(status: int):
         r, u, l = C.c_uint64(), C.c_uint64(), C.c_uint64()
         LIB.ml_gpu_last_budget_error(op, 128, C.byref(r), C.byref(u), C.byref(l))
         raise ResourcesExhausted(status, msg, op.value.decode(), r.value, u.value, l.value)
+    if status == abi.ERR_STALE_PLAN:
+        raise StalePlan(status, msg)
     raise MiniLakeError(status, msg)
 
 
@@ -585,6 +600,90 @@ def card_features(ctx: Context, cols, keys: Sequence[tuple], sel=None):
     est = C.c_double()
     _check(LIB.ml_gpu_card_features(ctx.h, arr, nc, n, sp, ns, abi.LOC_HOST, k, nk, _ptr(f), C.byref(est)))
     return f, est.value
+
+
+class Query:
+    """A prepared plan over device-resident batches (ml_gpu_query_*, executor.rs:270-288): join
+    builds, one hash aggregate probing them, an optional top-N.  The first run() plans through
+    the sink calls; later runs replay the whole plan as one CUDA graph.  StalePlan when the data
+    no longer fits the plan; MiniLakeError(ERR_UNSUPPORTED) on a second run of a plan the graph
+    cannot replay (stats()["why_not"] says why)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self._keep = []  # sinks and batches the plan reads
+        h = C.c_void_p()
+        _check(LIB.ml_gpu_query_create(ctx.h, C.byref(h)))
+        self.h = h
+        ctx._own(self)
+
+    def add_build(self, sink: "JoinBuildSink", cols):
+        """Run the build pipeline now; returns the table handle for Probe operators."""
+        arr, nc, n, hold = _cols_arg(cols)
+        t = C.c_void_p()
+        _check(LIB.ml_gpu_query_add_build(self.h, sink.h, arr, nc, n, C.byref(t)))
+        sink.table = t.value
+        self._keep += [sink, cols, hold, arr]
+        return t.value
+
+    def set_aggregate(self, sink: "HashAggregateSink", cols):
+        arr, nc, n, hold = _cols_arg(cols)
+        _check(LIB.ml_gpu_query_set_aggregate(self.h, sink.h, arr, nc, n))
+        self._keep += [sink, cols, hold, arr]
+
+    def set_topn(self, keys: Sequence[abi.SortKey], limit: int):
+        keep = abi.Keep()
+        k, nk = abi.encode_sort_keys(keys, keep)
+        _check(LIB.ml_gpu_query_set_topn(self.h, k, nk, limit))
+        self._topn = True
+
+    def run(self) -> DeviceBatch:
+        out = C.c_void_p()
+        _check(LIB.ml_gpu_query_run(self.h, C.byref(out)))
+        return DeviceBatch(self.ctx, out)
+
+    def run_host(self) -> List[HostColumn]:
+        """One run with the result in host memory: replays of a top-N plan copy it inside the
+        graph (ml_gpu_query_run_host); the planning run and other plans fetch a device batch."""
+        if getattr(self, "_types", None) is None:
+            b = self.run()
+            cols = b.fetch()
+            b.close()
+            if getattr(self, "_topn", False) and self.stats()["why_not"] == "":
+                self._types = [c.dtype for c in cols]
+            return cols
+        n = C.c_int64()
+        _check(LIB.ml_gpu_query_run_host(self.h, C.byref(n)))
+        k = n.value
+        out = []
+        for i, t in enumerate(self._types):
+            vals = np.empty(max(k, 1), dtype=abi.NP_DTYPE[t])
+            valid = np.zeros(max((k + 63) // 64, 1), dtype=np.uint64)
+            hv = C.c_int32()
+            _check(LIB.ml_gpu_query_result(self.h, i, _ptr(vals), _ptr(valid), C.byref(hv)))
+            col = HostColumn(t, vals[:k])
+            if hv.value:
+                col.validity = valid[:(k + 63) // 64]
+            out.append(col)
+        return out
+
+    def stats(self):
+        r, p, k = C.c_int64(), C.c_int64(), C.c_int32()
+        why = C.create_string_buffer(256)
+        _check(LIB.ml_gpu_query_stats(self.h, C.byref(r), C.byref(p), C.byref(k), why, 256))
+        return {"runs": r.value, "replays": p.value, "kernels": k.value, "why_not": why.value.decode()}
+
+    def close(self):
+        if self.h:
+            LIB.ml_gpu_query_destroy(self.h)
+            self.h = None
+        self._keep = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class CardinalityModel:
