@@ -2914,6 +2914,8 @@ std::string query_replay_blocker(ml_query* q) {
         if (d.str_kind) return "a string group key";
     for (auto& kk : q->keys)
         if (kk.expr.kind != ML_EXPR_COLUMN) return "a computed sort key";
+    if (q->topn && h->keys.nkeys + (int)h->aggs.size() + (int)h->group_build_cols.size() + 1 > kMaxResultCols)
+        return "more than 16 output columns";
     if (q->topn && (q->limit <= 0 || q->limit > kTopNWarpMax)) return "a limit above 32";
     return "";
 }
@@ -3059,20 +3061,24 @@ void query_enqueue(ml_query* q) {
             rows = (uint32_t*)base;
             launch_topn_warp(S, q->cap, (int)q->k, nb, rows, nullptr, nullptr, nullptr, s, ngd);
         }
-        launch_plan_rows(rows, (int)q->k, ngd, q->cap, kGuardTopRows, guard, s);
-        // as many groups as the planned result needs: at least `limit`, or exactly the planned rows
-        launch_plan_check(ngd, 8, q->k < q->limit ? 0 : 1, (uint64_t)q->k, kGuardRows, guard, s);
-        nk += 3;
+        // as many groups as the planned result needs (at least `limit`, or exactly the planned
+        // rows), the row ids in range, then the result's columns
+        ResultCols G{};
+        G.ncols = (int)q->outcols.size();
         for (size_t c = 0; c < q->outcols.size(); c++) {
             const DevColumn& src = *q->outcols[c];
             DevColumn& dst = *q->rescols[c];
-            launch_gather_fixed(src.dptr(), width_of(src.dtype), rows, q->k, dst.data.get(), s);
-            nk++;
-            if (src.validity) {
-                CK(cudaMemsetAsync(dst.validity.get(), 0, dst.validity.bytes(), s));
-                launch_gather_valid(src.vptr(), rows, q->k, dst.validity.get<uint32_t>(), s);
-                nk++;
-            }
+            G.width[c] = width_of(src.dtype);
+            G.src[c] = src.dptr();
+            G.sval[c] = src.vptr();
+            G.dst[c] = dst.data.get();
+            G.dval[c] = src.vptr() ? dst.validity.get<uint32_t>() : nullptr;
+            if (dst.validity) CK(cudaMemsetAsync(dst.validity.get(), 0, dst.validity.bytes(), s));
+        }
+        launch_plan_result(rows, (int)q->k, ngd, q->cap, q->k < q->limit, kGuardTopRows, kGuardRows, guard, G, s);
+        nk += 2;
+        for (size_t c = 0; c < q->outcols.size(); c++) {
+            DevColumn& dst = *q->rescols[c];
             // the rows to host memory too (ml_gpu_query_run_host)
             CK(cudaMemcpyAsync(q->hres[2 * c], dst.data.get(), (size_t)q->k * width_of(dst.dtype), cudaMemcpyDeviceToHost, s));
             if (dst.validity)

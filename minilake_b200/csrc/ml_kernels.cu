@@ -1517,9 +1517,7 @@ int topn_warp_blocks(int64_t n) {
     }();
     // at least 8 chunks of 128 rows per warp: a warp's first chunk mostly enters its list, later
     // ones mostly fall below the list's k-th entry or the launch-wide threshold
-    int64_t rpc = 8192;
-    if (const char* e = getenv("MLG_TOPN_ROWS_PER_CTA")) rpc = atoll(e);
-    int64_t want = (n + rpc - 1) / rpc;
+    int64_t want = (n + 8191) / 8192;
     int64_t cap = (int64_t)num_sms() * resident;
     return (int)std::max<int64_t>(1, std::min(want, cap));
 }
@@ -1555,20 +1553,40 @@ __global__ void k_plan_count(const uint32_t* count, uint64_t cap, uint64_t* out)
 void launch_plan_count(const uint32_t* count, uint64_t cap, uint64_t* out, cudaStream_t s) {
     k_plan_count<<<1, 1, 0, s>>>(count, cap, out);
 }
-// Row ids of a replayed top-k: an id at or past the rows that exist (the list had fewer than
-// k rows) becomes 0, so the gathers after it stay in bounds, and sets `bit`.
-__global__ void k_plan_rows(uint32_t* rows, int k, const uint64_t* n_dev, uint64_t cap, uint32_t bit, uint32_t* guard) {
+// The rows of a replayed top-k (k <= 32, one warp): an id at or past the rows that exist (the
+// list came back short) reads row 0 instead, so the gathers stay in bounds, and sets `bit`; the
+// row count n must also give the planned result: n == k when `exact`, else n >= k (`rows_bit`).
+// Then every column's k values and validity bits are gathered.
+__global__ void k_plan_result(const uint32_t* rows, int k, const uint64_t* n_dev, uint64_t cap, int exact, uint32_t bit,
+                              uint32_t rows_bit, uint32_t* guard, const __grid_constant__ ResultCols G) {
     const int i = threadIdx.x;
-    if (i >= k) return;
     const uint64_t n = n_dev && *n_dev < cap ? *n_dev : cap;
-    if (rows[i] >= n) {
-        rows[i] = 0;
-        atomicOr(guard, bit);
+    if (i == 0 && (exact ? n != (uint64_t)k : n < (uint64_t)k)) atomicOr(guard, rows_bit);
+    uint32_t r = 0;
+    if (i < k) {
+        r = rows[i];
+        if (r >= n) {
+            r = 0;
+            atomicOr(guard, bit);
+        }
+    }
+    for (int c = 0; c < G.ncols; c++) {
+        if (i < k) {
+            const int w = G.width[c];
+            if (w == 8) ((uint64_t*)G.dst[c])[i] = ((const uint64_t*)G.src[c])[r];
+            else if (w == 4) ((uint32_t*)G.dst[c])[i] = ((const uint32_t*)G.src[c])[r];
+            else ((uint8_t*)G.dst[c])[i] = ((const uint8_t*)G.src[c])[r];
+        }
+        if (G.dval[c]) {
+            const bool v = i < k && ((G.sval[c][r >> 6] >> (r & 63)) & 1ull);
+            const unsigned b = __ballot_sync(0xFFFFFFFFu, v);
+            if (i == 0) G.dval[c][0] = b;
+        }
     }
 }
-void launch_plan_rows(uint32_t* rows, int k, const uint64_t* n_dev, uint64_t cap, uint32_t bit, uint32_t* guard,
-                      cudaStream_t s) {
-    if (k > 0) k_plan_rows<<<1, 32 * ((k + 31) / 32), 0, s>>>(rows, k, n_dev, cap, bit, guard);
+void launch_plan_result(const uint32_t* rows, int k, const uint64_t* n_dev, uint64_t cap, int exact, uint32_t bit,
+                        uint32_t rows_bit, uint32_t* guard, const ResultCols& G, cudaStream_t s) {
+    k_plan_result<<<1, 32, 0, s>>>(rows, k, n_dev, cap, exact, bit, rows_bit, guard, G);
 }
 
 __global__ void k_iota_u32(uint32_t* out, int64_t n) {

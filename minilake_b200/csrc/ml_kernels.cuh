@@ -149,11 +149,23 @@ void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* 
 
 // Prepared-query checks (one thread each): *guard |= bit when the 4- or 8-byte value at p
 // differs from v (op 0) or is below v (op 1); a u32 group counter as a u64 row count capped at
-// cap; top-k row ids at or past the device row count (or cap) replaced by 0, setting bit.
+// cap.
 void launch_plan_check(const void* p, int width, int op, uint64_t v, uint32_t bit, uint32_t* guard, cudaStream_t s);
 void launch_plan_count(const uint32_t* count, uint64_t cap, uint64_t* out, cudaStream_t s);
-void launch_plan_rows(uint32_t* rows, int k, const uint64_t* n_dev, uint64_t cap, uint32_t bit, uint32_t* guard,
-                      cudaStream_t s);
+// The result of a replayed top-k (k <= 32): its row ids checked against the device row count
+// (an id past it reads row 0 and sets `bit`; n != k when `exact`, else n < k, sets `rows_bit`),
+// then k values (1-, 4- or 8-byte) and the validity word of each column gathered.
+constexpr int kMaxResultCols = 16;
+struct ResultCols {
+    int ncols;
+    int width[kMaxResultCols];
+    const void* src[kMaxResultCols];
+    const uint64_t* sval[kMaxResultCols];  // nullptr: no validity
+    void* dst[kMaxResultCols];
+    uint32_t* dval[kMaxResultCols];        // nullptr: no validity; else the first u32 word
+};
+void launch_plan_result(const uint32_t* rows, int k, const uint64_t* n_dev, uint64_t cap, int exact, uint32_t bit,
+                        uint32_t rows_bit, uint32_t* guard, const ResultCols& G, cudaStream_t s);
 
 // ---- static scratch of ml_gpu_filter_static ----------------------------------------------
 // One file-scope device array per device holds every temporary of the no-allocation filter:
