@@ -164,6 +164,8 @@ std::unique_ptr<DevColumn> project_column(Ctx* ctx, const PipeArgs& P, Prog p, i
     return d;
 }
 
+void check_device_error(Ctx* ctx, uint32_t err);
+
 // hash_columns (kernels/hash.rs:16-23) of the active rows of `cols` into `o` (one u64 per row)
 // on stream s: dictionary columns hash each entry once on the host (kernels/hash.rs:66-77).
 void hash_rows(Ctx* ctx, const ml_column* cols, int ncols, int64_t nrows, const uint32_t* dsel, int64_t nsel,
@@ -172,6 +174,10 @@ void hash_rows(Ctx* ctx, const ml_column* cols, int ncols, int64_t nrows, const 
     PipeArgs P{};
     P.sel = dsel;
     P.n = dsel ? nsel : nrows;
+    P.nsrc = nrows;
+    DevBuf err(ctx, 8, nullptr);
+    CK(cudaMemsetAsync(err.get(), 0, 4, s));
+    P.err = err.get<uint32_t>();
     std::vector<DevBuf> dh;
     std::vector<const uint64_t*> dh_ptr(ncols, nullptr);
     for (int c = 0; c < ncols; c++) {
@@ -218,11 +224,15 @@ void hash_rows(Ctx* ctx, const ml_column* cols, int ncols, int64_t nrows, const 
     o = DevBuf(ctx, std::max<size_t>((size_t)P.n * 8, 8), nullptr);
     launch_hash_columns(P, ncols, ptrs.get<const uint64_t*>(), o.get<uint64_t>(), s);
     ctx->count_launch();
+    uint32_t e = 0;
+    CK(cudaMemcpyAsync(&e, err.get(), 4, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));  // the staged columns and tables go out of scope here
+    check_device_error(ctx, e);
 }
 
 void check_device_error(Ctx* ctx, uint32_t err) {
     (void)ctx;
+    if (err & DE_BAD_INDEX) raise(ML_ERR_INVALID, "a selection vector holds a row id past the batch's rows");
     if (err & DE_TIMEOUT) raise(ML_ERR_TIMEOUT, "a bounded device-side wait ran out");
     if (err & DE_OVERFLOW_LOST) raise(ML_ERR_INTERNAL, "hash-table overflow buffer exhausted");
     if (err) raise(ML_ERR_INTERNAL, "device error word " + std::to_string(err));
@@ -883,18 +893,19 @@ int ml_gpu_batch_upload(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64
     API_BEGIN
     REQUIRE(ctx && out && (cols || ncols == 0) && ncols >= 0 && nrows >= 0, "bad arguments");
     ctx->set_current();
-    std::lock_guard<std::mutex> g(ctx->op_mu);
+    OpStream op_stream(ctx);
+    const cudaStream_t s = op_stream.s;
     auto b = std::make_unique<ml_batch>();
     b->ctx = ctx;
     b->nrows = nrows;
     b->res = std::make_unique<Reservation>(ctx, "Batch");
     Staging st(ctx);
     for (int c = 0; c < ncols; c++) {
-        auto col = stage_column(ctx, cols[c], nrows, ctx->stream, st, b->res.get());
-        if (cols[c].location == ML_LOC_DEVICE) col = copy_column(ctx, *col, ctx->stream, b->res.get());
+        auto col = stage_column(ctx, cols[c], nrows, s, st, b->res.get());
+        if (cols[c].location == ML_LOC_DEVICE) col = copy_column(ctx, *col, s, b->res.get());
         b->cols.push_back(std::move(col));
     }
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaStreamSynchronize(s));
     *out = b.release();
     API_END
 }
@@ -1009,8 +1020,8 @@ int ml_gpu_filter(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols, int32
     API_BEGIN
     REQUIRE(ctx && pred && sel_out && nsel_out, "null argument");
     ctx->set_current();
-    std::lock_guard<std::mutex> g(ctx->op_mu);
-    cudaStream_t s = ctx->stream;
+    OpStream op_stream(ctx);
+    cudaStream_t s = op_stream.s;
     if (location == ML_LOC_HOST) check_sel_bounds(sel_in, nsel_in, nrows);
     std::vector<int32_t> types;
     for (int c = 0; c < ncols; c++) types.push_back(cols[c].dtype);
@@ -1087,8 +1098,8 @@ int ml_gpu_filter_static(ml_ctx* ctx, const ml_expr* pred, const ml_column* cols
         REQUIRE(g_static_base[ctx->device], "cudaGetSymbolAddress failed for the static filter scratch");
     }
     uint8_t* base = g_static_base[ctx->device];
-    std::lock_guard<std::mutex> g(ctx->op_mu);
-    cudaStream_t s = ctx->stream;
+    OpStream op_stream(ctx);
+    cudaStream_t s = op_stream.s;
     // Declared after the locks, so destroyed before them: whichever way the call ends (an error
     // raised after some copies or kernels were queued included), the stream has drained before
     // another call may touch the array.
@@ -1128,8 +1139,8 @@ int ml_gpu_project(ml_ctx* ctx, const ml_expr* expr, const ml_column* cols, int3
     API_BEGIN
     REQUIRE(ctx && expr && out, "null argument");
     ctx->set_current();
-    std::lock_guard<std::mutex> g(ctx->op_mu);
-    cudaStream_t s = ctx->stream;
+    OpStream op_stream(ctx);
+    cudaStream_t s = op_stream.s;
     std::vector<int32_t> types;
     for (int c = 0; c < ncols; c++) types.push_back(cols[c].dtype);
     Pipeline p(ctx);
@@ -1164,8 +1175,8 @@ int ml_gpu_hash_columns(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64
     REQUIRE(ctx && out && (cols || ncols == 0), "null argument");
     REQUIRE(ncols <= kMaxCols, "too many columns");
     ctx->set_current();
-    std::lock_guard<std::mutex> g(ctx->op_mu);
-    cudaStream_t s = ctx->stream;
+    OpStream op_stream(ctx);
+    cudaStream_t s = op_stream.s;
     if (location == ML_LOC_HOST) check_sel_bounds(sel, nsel, nrows);
     Staging st(ctx);
     DevBuf sel_hold;
@@ -1192,8 +1203,8 @@ int ml_gpu_partition(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int64_t 
         keys.push_back(cols[key_cols[k]]);
     }
     ctx->set_current();
-    std::lock_guard<std::mutex> g(ctx->op_mu);
-    cudaStream_t s = ctx->stream;
+    OpStream op_stream(ctx);
+    cudaStream_t s = op_stream.s;
     Staging st(ctx);
     auto b = std::make_unique<ml_batch>();
     b->ctx = ctx;
@@ -1497,8 +1508,8 @@ int ml_gpu_join_probe(ml_ctx* ctx, ml_join_table* table, const ml_expr* key_expr
     API_BEGIN
     REQUIRE(ctx && table && key_exprs && npairs, "null argument");
     ctx->set_current();
-    std::lock_guard<std::mutex> g(ctx->op_mu);
-    cudaStream_t s = ctx->stream;
+    OpStream op_stream(ctx);
+    cudaStream_t s = op_stream.s;
     if (location == ML_LOC_HOST) check_sel_bounds(sel, nsel, nrows);
     std::vector<int32_t> types;
     for (int c = 0; c < ncols; c++) types.push_back(cols[c].dtype);

@@ -7,7 +7,21 @@
 
 struct ml_ctx : mlg::Ctx {
     using mlg::Ctx::Ctx;
-    std::mutex op_mu;  // serializes the standalone operators on the context stream
+};
+
+// The stream of one standalone operator call (filter, projection, probe, hashing, upload),
+// taken from the context's pool: MiniLake calls Operator::execute on one shared operator from
+// every worker thread (pipeline.rs:52-57), so calls from different threads run concurrently on
+// the device.  The call's work is finished when it returns.
+struct OpStream {
+    mlg::Ctx* ctx;
+    cudaStream_t s;
+    explicit OpStream(mlg::Ctx* c) : ctx(c), s(c->new_stream()) {}
+    ~OpStream() {
+        cudaStreamSynchronize(s);
+        ctx->free_stream(s);
+    }
+    OpStream(const OpStream&) = delete;
 };
 
 // Every entry point returns a status: exceptions become ML_* codes with the message kept

@@ -37,6 +37,7 @@ struct ProbeDev {
 struct PipeArgs {
     int64_t n;               // rows to visit (selection length when `sel` is set)
     const uint32_t* sel;     // optional input selection vector
+    int64_t nsrc;            // rows of the source batch: every selected row id is below it
     const Instr* prog;
     const uint8_t* arena;
     uint32_t* err;
@@ -94,5 +95,21 @@ struct SortDev {
     DCol cols[kMaxKeys];
     int32_t asc[kMaxKeys], nulls_first[kMaxKeys];
 };
+
+#ifdef __CUDACC__
+// Row `i` of a launch: the selection's row id, checked against the batch (a device-resident
+// selection is not checked on the host).  An id past the batch's rows is skipped (ok = false)
+// and reported through the launch's error word.
+__device__ __forceinline__ uint32_t sel_row(const PipeArgs& P, int64_t i, bool& ok) {
+    if (!P.sel) return (uint32_t)i;
+    const uint32_t r = __ldg(P.sel + i);
+    if ((int64_t)r >= P.nsrc) {
+        if (P.err) atomicOr(P.err, (uint32_t)DE_BAD_INDEX);
+        ok = false;
+        return 0;
+    }
+    return r;
+}
+#endif
 
 }  // namespace mlg

@@ -32,7 +32,9 @@ __global__ void __launch_bounds__(256) k_hll(const __grid_constant__ PipeArgs P,
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {
         RowCtx x;
-        x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        bool ok = true;
+        x.r = sel_row(P, i, ok);
+        if (!ok) continue;
         x.b0 = x.b1 = x.b2 = x.b3 = 0;
         x.head = 0;
         uint64_t w[2];

@@ -102,8 +102,8 @@ int ml_gpu_card_features(ml_ctx* ctx, const ml_column* cols, int32_t ncols, int6
     API_BEGIN
     REQUIRE(ctx && keys && features && nkeys > 0 && (cols || ncols == 0), "bad arguments");
     ctx->set_current();
-    std::lock_guard<std::mutex> g(ctx->op_mu);
-    cudaStream_t s = ctx->stream;
+    OpStream op_stream(ctx);
+    cudaStream_t s = op_stream.s;
     std::vector<int32_t> types;
     for (int c = 0; c < ncols; c++) types.push_back(cols[c].dtype);
     Pipeline p(ctx);

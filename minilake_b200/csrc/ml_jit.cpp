@@ -782,7 +782,10 @@ std::string tile_rows(const PipeArgs& P, int K, bool contig, const std::string& 
         } else {
             s += ind + "const int64_t i" + J + " = base + " + J + " * (int64_t)blockDim.x + threadIdx.x;\n";
             s += ind + "bool " + a + " = i" + J + " < P.n;\n";
-            s += ind + x + ".r = " + a + " ? " + (P.sel ? "__ldg(P.sel + i" + J + ")" : "(uint32_t)i" + J) + " : 0u;\n";
+            if (P.sel)  // a selected row id past the batch is skipped and reported (sel_row)
+                s += ind + x + ".r = " + a + " ? sel_row(P, i" + J + ", " + a + ") : 0u;\n";
+            else
+                s += ind + x + ".r = " + a + " ? (uint32_t)i" + J + " : 0u;\n";
         }
         s += ind + x + ".b0 = " + x + ".b1 = " + x + ".b2 = " + x + ".b3 = 0;\n";
         s += ind + x + ".head = 0;\n";
@@ -806,7 +809,8 @@ std::string row_loop(const PipeArgs& P, bool batched, const std::string& body, i
         s += "    const int64_t stride = (int64_t)gridDim.x * blockDim.x;\n";
         s += "    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {\n";
         s += "        RowCtx x;\n";
-        s += P.sel ? "        x.r = __ldg(P.sel + i);\n" : "        x.r = (uint32_t)i;\n";
+        s += P.sel ? "        bool sel_ok = true;\n        x.r = sel_row(P, i, sel_ok);\n        if (!sel_ok) continue;\n"
+                   : "        x.r = (uint32_t)i;\n";
         s += "        x.b0 = x.b1 = x.b2 = x.b3 = 0;\n        x.head = 0;\n";
     } else {
         s += "    const int64_t tile = (int64_t)" + num(K) + " * blockDim.x;\n";

@@ -198,7 +198,9 @@ __global__ void __launch_bounds__(kThreads) k_agg(const __grid_constant__ PipeAr
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {
         RowCtx x;
-        x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        bool ok = true;
+        x.r = sel_row(P, i, ok);
+        if (!ok) continue;
         x.b0 = x.b1 = x.b2 = x.b3 = 0;
         x.head = 0;
         run_stages(P, env, x, [&](const RowCtx& c) { agg_update(P, A, env, c, smem); });
@@ -420,11 +422,12 @@ __global__ void __launch_bounds__(kThreads) k_select_flags(const __grid_constant
     for (int it = 0; it < 8; it++) {
         int64_t i = base + it * kThreads + threadIdx.x;
         bool pass = false;
-        if (i < P.n) {
-            RowCtx x;
-            x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        bool ok = i < P.n;
+        RowCtx x;
+        if (ok) x.r = sel_row(P, i, ok);
+        if (ok) {
             x.b0 = x.b1 = x.b2 = x.b3 = 0;
-        x.head = 0;
+            x.head = 0;
             run_stages(P, env, x, [&](const RowCtx&) { pass = true; });
         }
         uint32_t b = __ballot_sync(0xFFFFFFFFu, pass);
@@ -590,11 +593,11 @@ __global__ void __launch_bounds__(kThreads) k_project(const __grid_constant__ Pi
     for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < P.n; i0 += stride) {
         int64_t i = i0 + threadIdx.x;
         bool in = i < P.n, ok = false;
+        RowCtx x;
+        if (in) x.r = sel_row(P, i, in);
         if (in) {
-            RowCtx x;
-            x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
             x.b0 = x.b1 = x.b2 = x.b3 = 0;
-        x.head = 0;
+            x.head = 0;
             uint64_t v;
             eval_prog(env, prog, x, v, ok);
             switch (out_type) {
@@ -615,7 +618,12 @@ __global__ void k_hash_columns(const __grid_constant__ PipeArgs P, int ncols, co
                                uint64_t* out) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {
-        uint32_t r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        bool ok = true;
+        const uint32_t r = sel_row(P, i, ok);
+        if (!ok) {
+            out[i] = 0;
+            continue;
+        }
         uint64_t h = kSeed;
         for (int c = 0; c < ncols; c++) {
             const DCol& col = P.cols[c];
@@ -671,11 +679,12 @@ __global__ void k_probe_count(const __grid_constant__ PipeArgs P, uint32_t* coun
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {
         RowCtx x;
-        x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        bool ok = true;
+        x.r = sel_row(P, i, ok);
         x.b0 = x.b1 = x.b2 = x.b3 = 0;
         x.head = 0;
         uint32_t c = 0;
-        run_stages(P, env, x, [&](const RowCtx&) { c++; });
+        if (ok) run_stages(P, env, x, [&](const RowCtx&) { c++; });
         counts[i] = c;
     }
 }
@@ -684,7 +693,9 @@ __global__ void k_probe_write(const __grid_constant__ PipeArgs P, const uint64_t
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {
         RowCtx x;
-        x.r = P.sel ? __ldg(P.sel + i) : (uint32_t)i;
+        bool ok = true;
+        x.r = sel_row(P, i, ok);
+        if (!ok) continue;  // counted no pairs
         x.b0 = x.b1 = x.b2 = x.b3 = 0;
         x.head = 0;
         uint64_t o = offsets[i];

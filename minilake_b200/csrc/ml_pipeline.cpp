@@ -272,6 +272,7 @@ void Pipeline::prepare(Launch& L, const ml_column* cols, int ncols, int64_t nrow
     P = PipeArgs{};
     P.n = sel ? nsel : nrows;
     P.sel = sel;
+    P.nsrc = nrows;
     P.prog = d_prog;
     P.arena = d_arena;
     P.nstages = nstages;
