@@ -12,8 +12,10 @@ __device__ __forceinline__ uint64_t agg_identity(int kind) {
     switch (kind) {
         case A_MIN_I64: return 0x7FFFFFFFFFFFFFFFull;
         case A_MAX_I64: return 0x8000000000000000ull;
-        case A_MIN_F64: return ~0ull;
-        case A_MAX_F64: return 0ull;
+        case A_MIN_F64:
+        case A_MIN_STR: return ~0ull;
+        case A_MAX_F64:
+        case A_MAX_STR: return 0ull;
         default: return 0ull;
     }
 }
@@ -31,8 +33,14 @@ __device__ __forceinline__ void acc_apply(int kind, uint64_t* w, uint64_t v) {
         case A_MAX_I64: atomicMax((long long*)w, (long long)v); break;
         case A_MIN_F64: atomicMin((unsigned long long*)w, (unsigned long long)f64_order(as_f64(v))); break;
         case A_MAX_F64: atomicMax((unsigned long long*)w, (unsigned long long)f64_order(as_f64(v))); break;
+        case A_MIN_STR: atomicMin((unsigned long long*)w, (unsigned long long)v); break;  // v packed (str_pack)
+        case A_MAX_STR: atomicMax((unsigned long long*)w, (unsigned long long)v); break;
         default: atomicAdd((unsigned long long*)w, 1ull); break;  // COUNT(x)
     }
+}
+// A string id as the packed word of A_MIN_STR / A_MAX_STR.
+__device__ __forceinline__ uint64_t str_pack(const uint32_t* rank, uint32_t id) {
+    return ((uint64_t)(__ldg(rank + id) + 1u) << 32) | id;
 }
 // acc_apply for accumulators known to be in global memory: fire-and-forget reductions
 // (red.global), so no thread waits for the L2 to answer.
@@ -72,8 +80,10 @@ __device__ __forceinline__ void acc_merge(int kind, uint64_t* dst, const uint64_
             break;
         case A_MIN_I64: atomicMin((long long*)dst, (long long)v); break;
         case A_MAX_I64: atomicMax((long long*)dst, (long long)v); break;
-        case A_MIN_F64: atomicMin((unsigned long long*)dst, (unsigned long long)v); break;
-        case A_MAX_F64: atomicMax((unsigned long long*)dst, (unsigned long long)v); break;
+        case A_MIN_F64:
+        case A_MIN_STR: atomicMin((unsigned long long*)dst, (unsigned long long)v); break;
+        case A_MAX_F64:
+        case A_MAX_STR: atomicMax((unsigned long long*)dst, (unsigned long long)v); break;
     }
 }
 

@@ -1653,8 +1653,14 @@ struct ml_hashagg {
     };
     std::vector<SpillChunk> spills[kSpillParts];
     uint64_t spill_events = 0, spilled_groups = 0;
+    // MIN/MAX over strings (accumulator.rs:156-160): the context's interned strings ranked in
+    // byte order, rebuilt when strings were interned since (rank_strings = how many it ranks)
+    bool str_minmax = false;
+    DevBuf str_rank;
+    size_t rank_strings = 0;
+    void refresh_ranks(cudaStream_t s);
     void spill_state(cudaStream_t s, ErrWord& ew);
-    bool can_spill() const { return (ctx->flags & ML_CTX_SPILL) && !ungrouped && group_probe < 0; }
+    bool can_spill() const { return (ctx->flags & ML_CTX_SPILL) && !ungrouped && group_probe < 0 && !str_minmax; }
     void spill_and_regrow(uint64_t want, cudaStream_t s, ErrWord& ew);
     void regrow(uint64_t want, cudaStream_t s, ErrWord& ew);
     void merge_spilled(const SpillChunk& c, cudaStream_t s, ErrWord& ew);
@@ -1734,6 +1740,7 @@ struct ml_hashagg {
         A.ovf = ovf;
         A.ovf_count = ovf_count;
         A.ovf_cap = ovf_cap;
+        A.str_rank = str_rank.get<uint32_t>();
         for (size_t k = 0; k < aggs.size(); k++) {
             AggDev& d = A.aggs[k];
             const AggState& a = aggs[k];
@@ -1891,6 +1898,31 @@ void ml_hashagg::resume_overflow(Pipeline::Launch& L, uint64_t count, DevBuf& ov
     }
 }
 
+// Called with the sink's lock held exclusively and its launches drained.
+void ml_hashagg::refresh_ranks(cudaStream_t s) {
+    std::vector<uint32_t> rank;
+    {
+        std::lock_guard<std::mutex> g(pipe.intern.mu);
+        const auto& strs = pipe.intern.strs;
+        if (str_rank && strs.size() == rank_strings) return;
+        std::vector<uint32_t> order(strs.size());
+        for (size_t i = 0; i < order.size(); i++) order[i] = (uint32_t)i;
+        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return strs[a] < strs[b]; });
+        rank.assign(std::max<size_t>(strs.size(), 1), 0);
+        for (size_t i = 0; i < order.size(); i++) rank[order[i]] = (uint32_t)i;
+        rank_strings = strs.size();
+    }
+    DevBuf nr(ctx, rank.size() * 4, res.get());
+    CK(cudaMemcpyAsync(nr.get(), rank.data(), rank.size() * 4, cudaMemcpyHostToDevice, s));
+    RerankOffs R{};
+    for (const AggState& a : aggs)
+        if (a.kind == A_MIN_STR || a.kind == A_MAX_STR) R.off[R.n++] = a.off;
+    if (gid_cap) launch_str_rerank(acc.get<uint64_t>(), stride, gid_cap, R, nr.get<uint32_t>(), s);
+    ctx->count_launch();
+    CK(cudaStreamSynchronize(s));  // `rank` is read by the copy; the states use the new ranks
+    str_rank = std::move(nr);
+}
+
 void ml_hashagg::reset_groups(cudaStream_t s) {
     CK(cudaMemsetAsync(ngroups.get(), 0, 16, s));
     if (cap) CK(cudaMemsetAsync(slots.get(), 0, cap * 8 * (keys.nwords == 1 ? 2 : 4), s));
@@ -2043,6 +2075,12 @@ void compile_hashagg(ml_hashagg* h, const ml_pipe_op* prologue, int32_t nprologu
                 bool mn = a.func == ML_AGG_MIN;
                 if (t == ML_TYPE_INT32 || t == ML_TYPE_INT64 || t == ML_TYPE_DATE) { a.kind = mn ? A_MIN_I64 : A_MAX_I64; a.in_type = ML_TYPE_INT64; a.out_type = t; }
                 else if (t == ML_TYPE_FLOAT64) { a.kind = mn ? A_MIN_F64 : A_MAX_F64; a.in_type = t; a.out_type = t; }
+                else if (t == ML_TYPE_UTF8) {  // the argument is the string's id (compile_string_key)
+                    a.kind = mn ? A_MIN_STR : A_MAX_STR;
+                    a.in_type = ML_TYPE_UTF8;
+                    a.out_type = ML_TYPE_UTF8;
+                    h->str_minmax = true;
+                }
                 else bad();
                 break;
             }
@@ -2157,6 +2195,12 @@ int ml_gpu_hashagg_sink(ml_hashagg_local* local, const ml_column* cols, int32_t 
     const uint32_t* dsel = device_sel(ctx, sel, nsel, sel_hold, s);
     Pipeline::Launch L;
     h->pipe.prepare(L, cols, ncols, nrows, dsel, nsel, s, local->st, nullptr);
+    if (h->str_minmax) {  // this batch's strings are interned now: rank them with the rest
+        std::unique_lock<std::shared_mutex> lk(h->rw);
+        h->streams.sync();
+        if (h->run.s) CK(cudaStreamSynchronize(h->run.s));
+        h->refresh_ranks(s);
+    }
     // seen-tracking: once an argument can be NULL, count valid inputs per group
     for (auto& a : h->aggs) {
         if (!a.has_arg || a.vcnt_on || a.kind == A_COUNT) continue;
@@ -2311,6 +2355,10 @@ int ml_gpu_hashagg_run_resident(ml_hashagg* h, const ml_column* cols, int32_t nc
     Staging st(ctx);
     Pipeline::Launch L;
     h->pipe.prepare(L, cols, ncols, nrows, nullptr, 0, s, st, nullptr, R.tables.get<uint8_t>(), R.tables.bytes());
+    if (h->str_minmax) {
+        h->streams.sync();
+        h->refresh_ranks(s);
+    }
     for (auto& a : h->aggs)
         if (a.has_arg && !a.vcnt_on && a.kind != A_COUNT && (a.arg.maybe_null || h->pipe.reads_nullable(a.arg, L)))
             raise(ML_ERR_UNSUPPORTED, "ml_gpu_hashagg_run_resident: an aggregate input can be NULL; use a local sink");
@@ -2524,6 +2572,33 @@ std::unique_ptr<ml_batch> hashagg_emit(ml_hashagg* h, cudaStream_t s) {
     launch_agg_final(F, s);
     ctx->count_launch();
     CK(cudaStreamSynchronize(s));
+    // global string ids (dictionary keys, string MIN/MAX) become the strings on the host
+    auto strings_of_ids = [&](DevColumn& c, const void* id_dev) {
+        std::vector<uint32_t> ids(ng);
+        if (ng) CK(cudaMemcpy(ids.data(), id_dev, (size_t)ng * 4, cudaMemcpyDeviceToHost));
+        std::vector<uint64_t> valid((ng + 63) / 64 + 1, 0);
+        if (ng) CK(cudaMemcpy(valid.data(), c.validity.get(), (size_t)(ng + 63) / 64 * 8, cudaMemcpyDeviceToHost));
+        std::vector<uint32_t> off(ng + 1, 0);
+        std::string bytes;
+        {
+            std::lock_guard<std::mutex> g(h->pipe.intern.mu);
+            for (uint32_t g2 = 0; g2 < ng; g2++) {
+                bool v = (valid[g2 / 64] >> (g2 % 64)) & 1;
+                if (v) bytes += h->pipe.intern.strs.at(ids[g2]);
+                off[g2 + 1] = (uint32_t)bytes.size();
+            }
+        }
+        c.kind = CK_UTF8;
+        c.offsets = DevBuf(ctx, (size_t)(ng + 1) * 4, b->res.get());
+        c.data = DevBuf(ctx, std::max<size_t>(bytes.size(), 1), b->res.get());
+        h2d_now(c.offsets.get(), off.data(), (size_t)(ng + 1) * 4);
+        h2d_now(c.data.get(), bytes.data(), bytes.size());
+    };
+    for (int k = 0; k < F.nagg; k++)
+        if (h->aggs[k].out_type == ML_TYPE_UTF8) {
+            DevBuf ids = std::move(aggcols[k]->data);
+            strings_of_ids(*aggcols[k], ids.get());
+        }
     // string keys: dictionary ids decode on the host, build-side ids gather on the device
     for (int k = 0; k < F.nkeys; k++) {
         const KeyDecode& d = h->dec[k];
@@ -2531,24 +2606,7 @@ std::unique_ptr<ml_batch> hashagg_emit(ml_hashagg* h, cudaStream_t s) {
         auto& kc = keycols[k];
         kc->kind = CK_UTF8;
         if (d.str_kind == 1) {
-            std::vector<uint32_t> ids(ng);
-            if (ng) CK(cudaMemcpy(ids.data(), id_bufs[k].get(), (size_t)ng * 4, cudaMemcpyDeviceToHost));
-            std::vector<uint64_t> valid((ng + 63) / 64 + 1, 0);
-            if (ng) CK(cudaMemcpy(valid.data(), kc->validity.get(), (size_t)(ng + 63) / 64 * 8, cudaMemcpyDeviceToHost));
-            std::vector<uint32_t> off(ng + 1, 0);
-            std::string bytes;
-            {
-                std::lock_guard<std::mutex> g(h->pipe.intern.mu);
-                for (uint32_t g2 = 0; g2 < ng; g2++) {
-                    bool v = (valid[g2 / 64] >> (g2 % 64)) & 1;
-                    if (v) bytes += h->pipe.intern.strs.at(ids[g2]);
-                    off[g2 + 1] = (uint32_t)bytes.size();
-                }
-            }
-            kc->offsets = DevBuf(ctx, (size_t)(ng + 1) * 4, b->res.get());
-            kc->data = DevBuf(ctx, std::max<size_t>(bytes.size(), 1), b->res.get());
-            h2d_now(kc->offsets.get(), off.data(), (size_t)(ng + 1) * 4);
-            h2d_now(kc->data.get(), bytes.data(), bytes.size());
+            strings_of_ids(*kc, id_bufs[k].get());
         } else {
             const DevColumn& src = *h->pipe.probes[d.build].jt->batch.cols[d.build_col];
             DevColumn tmp;
@@ -2923,6 +2981,7 @@ std::string query_replay_blocker(ml_query* q) {
     if (h->spill_events) return "the aggregate spilled";
     for (auto& d : h->dec)
         if (d.str_kind) return "a string group key";
+    if (h->str_minmax) return "a string MIN or MAX";
     for (auto& kk : q->keys)
         if (kk.expr.kind != ML_EXPR_COLUMN) return "a computed sort key";
     if (q->topn && h->keys.nkeys + (int)h->aggs.size() + (int)h->group_build_cols.size() + 1 > kMaxResultCols)

@@ -76,6 +76,7 @@ struct AggArgs {
     uint32_t dslots;
     uint32_t dmul[kMaxKeys];
     uint32_t dbase[kMaxKeys];
+    const uint32_t* str_rank;  // string id -> rank in byte order (A_MIN_STR / A_MAX_STR)
     AggDev aggs[kMaxAggs];
 };
 

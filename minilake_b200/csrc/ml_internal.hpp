@@ -142,6 +142,10 @@ enum AccKind : int32_t {
     A_AVG,         // f64 sum + u64 count of valid inputs
     A_MIN_I64, A_MAX_I64,
     A_MIN_F64, A_MAX_F64,
+    // MIN/MAX of a string: (rank + 1) << 32 | string id, the rank being the string's place in
+    // byte order among the context's interned strings (AggArgs::str_rank); ranks are renumbered
+    // in the group blocks when new strings are interned, so u64 min/max compare strings.
+    A_MIN_STR, A_MAX_STR,
 };
 
 struct AggDev {

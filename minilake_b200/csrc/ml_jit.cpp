@@ -1156,8 +1156,15 @@ void* memoized(const Pipeline& pipe, std::string key, Make make) {
 
 }  // namespace
 
+// String MIN/MAX look their strings' ranks up (AggArgs::str_rank): the interpreter kernels do.
+bool has_string_minmax(const AggArgs& A) {
+    for (int k = 0; k < A.nagg; k++)
+        if (A.aggs[k].kind == A_MIN_STR || A.aggs[k].kind == A_MAX_STR) return true;
+    return false;
+}
+
 void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {
-    if (!jit_enabled(ctx)) return nullptr;
+    if (!jit_enabled(ctx) || has_string_minmax(A)) return nullptr;
     const bool contig = batchable(P) && contig_ok(P);
     return memoized(pipe, signature('a', P, &A, nullptr) + std::string((const char*)&ctx->device, sizeof(int)) +
                               (contig ? "c" : "s"),
@@ -1165,7 +1172,7 @@ void* jit_agg_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const Ag
 }
 
 void* jit_agg_resume_kernel(Ctx* ctx, const Pipeline& pipe, const PipeArgs& P, const AggArgs& A) {
-    if (!jit_enabled(ctx)) return nullptr;
+    if (!jit_enabled(ctx) || has_string_minmax(A)) return nullptr;
     // the rows a full table sent to the overflow list, aggregated again after the table grew
     Gen g(pipe.C.code, P);
     g.fail = "break;";

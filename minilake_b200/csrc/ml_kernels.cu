@@ -150,6 +150,7 @@ __device__ __forceinline__ void agg_fold(const PipeArgs& P, const AggArgs& A, co
         bool ok = true;
         if (a.has_arg) eval_prog(env, a.arg, x, v, ok);
         if (!ok) continue;
+        if (a.kind == A_MIN_STR || a.kind == A_MAX_STR) v = str_pack(A.str_rank, (uint32_t)v);
         acc_apply(a.kind, blk + a.off, v);
         if (a.count_valid) atomicAdd((unsigned long long*)a.vcnt + g, 1ull);
     }
@@ -395,6 +396,8 @@ __global__ void k_agg_final(const __grid_constant__ FinalArgs F) {
                     }
                     case A_MIN_F64:
                     case A_MAX_F64: ((double*)F.agg_out[k])[o] = valid ? f64_unorder(v) : 0.0; break;
+                    case A_MIN_STR:
+                    case A_MAX_STR: ((uint32_t*)F.agg_out[k])[o] = valid ? (uint32_t)v : 0u; break;  // the id
                     case A_MIN_I64:
                     case A_MAX_I64:
                         if (F.out_type[k] == ML_TYPE_INT32 || F.out_type[k] == ML_TYPE_DATE)
@@ -1547,6 +1550,24 @@ void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* 
         default: k_topn_warp<-1><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out, n_dev); break;
     }
 }
+// The packed words of string MIN/MAX states (A_MIN_STR / A_MAX_STR) after the rank table
+// changed: each holds a string id in its low half; the identities (no value yet) stay.
+__global__ void k_str_rerank(uint64_t* acc, int stride, uint32_t ngroups, const __grid_constant__ RerankOffs R,
+                             const uint32_t* rank) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroups) return;
+    uint64_t* blk = acc + (uint64_t)g * stride;
+    for (int j = 0; j < R.n; j++) {
+        const uint64_t w = blk[R.off[j]];
+        if (w == 0ull || w == ~0ull) continue;
+        blk[R.off[j]] = str_pack(rank, (uint32_t)w);
+    }
+}
+void launch_str_rerank(uint64_t* acc, int stride, uint32_t ngroups, const RerankOffs& R, const uint32_t* rank,
+                       cudaStream_t s) {
+    if (ngroups && R.n) k_str_rerank<<<(ngroups + kThreads - 1) / kThreads, kThreads, 0, s>>>(acc, stride, ngroups, R, rank);
+}
+
 // ---- prepared-query checks: a replayed plan's recorded choices against this run's data ------
 // *guard |= bit when the 4- or 8-byte value at p differs from v (op 0) or is below v (op 1).
 __global__ void k_plan_check(const void* p, int width, int op, uint64_t v, uint32_t bit, uint32_t* guard) {

@@ -147,6 +147,15 @@ size_t topn_entry_bytes();
 void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* out, void* cand, unsigned int* done,
                       uint32_t* final_out, cudaStream_t s, const uint64_t* n_dev = nullptr);
 
+// String MIN/MAX states of groups [0, ngroups): new ranks from `rank` for the packed words at
+// the listed block offsets (the rank table changed when new strings were interned).
+struct RerankOffs {
+    int n;
+    int32_t off[kMaxAggs];
+};
+void launch_str_rerank(uint64_t* acc, int stride, uint32_t ngroups, const RerankOffs& R, const uint32_t* rank,
+                       cudaStream_t s);
+
 // Prepared-query checks (one thread each): *guard |= bit when the 4- or 8-byte value at p
 // differs from v (op 0) or is below v (op 1); a u32 group counter as a u64 row count capped at
 // cap.

@@ -89,3 +89,57 @@ def test_string_join_probe_pairs(ctx, gpu_engine):
         # one build batch in row-group order on both sides: build rows index the same rows
         assert sorted(zip(gp.tolist(), gb.tolist())) == sorted(zip(op.tolist(), ob.tolist()))
         assert np.array_equal(gp, np.sort(gp, kind="stable")), "pairs ordered by probe row"
+
+
+# MIN/MAX over strings (accumulator.rs:156-160): byte order (bytes >= 0x80 after ASCII), a
+# prefix before its extensions, the empty string first; later batches bring strings the earlier
+# ones did not have (the group states' ranks are renumbered); NULL inputs skipped, a group with
+# only NULLs gives NULL.
+MM_POOL = [b"", b"a", b"ab", b"abc", b"abd", b"b", b"\xc3\xa9t\xc3\xa9", b"zz", b"Zz", b"a\x00b", b"a\x00"] + \
+          [b"s%04d" % i for i in range(400)]
+
+
+def _mm_table(rng, groups, plain_first):
+    rgs = []
+    for g in range(groups):
+        n = 6000
+        hi = 60 + g * 60  # each row group reaches further into the pool: new strings arrive late
+        idx = rng.integers(0, min(hi, len(MM_POOL)), n)
+        valid = rng.random(n) > 0.1
+        k = rng.integers(0, 50, n).astype(np.int64)
+        k[k == 49] = 1000 + g  # groups seen in one row group only
+        s = utf8_plain([MM_POOL[i] for i in idx], valid) if (g % 2 == 0) == plain_first \
+            else encode_strings(MM_POOL, idx, valid)
+        rgs.append([fixed(INT64, k), s, fixed(FLOAT64, rng.random(n))])
+    only_nulls = [fixed(INT64, np.full(5, 7777, dtype=np.int64)), utf8_plain([b"x"] * 5, np.zeros(5, bool)),
+                  fixed(FLOAT64, np.ones(5))]
+    rgs.append(only_nulls)
+    return Table("t", ["k", "s", "v"], rgs)
+
+
+@pytest.mark.parametrize("plain_first", [True, False])
+def test_min_max_of_strings(gpu_engine, plain_first):
+    from minilake_b200.abi import MAX, MIN
+    from minilake_b200.engine import GpuEngine
+    rng = np.random.default_rng(31 + plain_first)
+    t = _mm_table(rng, 6, plain_first)
+    types = [INT64, UTF8, FLOAT64]
+    aggs = [AggSpec(MIN, Col(1), UTF8), AggSpec(MAX, Col(1), UTF8), AggSpec(COUNT_STAR), AggSpec(SUM, Col(2), FLOAT64)]
+    for group in ([(Col(0), INT64)], []):
+        want = orc.OracleEngine(threads=1).fetch(orc.OracleEngine(threads=1).hashagg(t, types, group, aggs))
+        for eng in (gpu_engine, GpuEngine(gpu_engine.ctx, threads=3)):
+            got = eng.fetch(eng.hashagg(t, types, group, aggs))
+            assert_same_rows(got, want, len(group), {len(group) + 3})
+
+
+def test_min_max_of_strings_grouped_by_a_string(gpu_engine):
+    from minilake_b200.abi import MAX, MIN
+    rng = np.random.default_rng(37)
+    fact = _fact(rng, 20_000, 4, 300)  # [s, v, d]
+    # GROUP BY d % 7 as an int, MIN/MAX of the string; and GROUP BY the string, MIN of itself
+    types = [UTF8, FLOAT64, INT32]
+    for group, aggs in (([(Col(2), INT32)], [AggSpec(MIN, Col(0), UTF8), AggSpec(MAX, Col(0), UTF8)]),
+                        ([(Col(0), UTF8)], [AggSpec(MIN, Col(0), UTF8), AggSpec(COUNT_STAR)])):
+        want = orc.OracleEngine(threads=2).fetch(orc.OracleEngine(threads=2).hashagg(fact, types, group, aggs))
+        got = gpu_engine.fetch(gpu_engine.hashagg(fact, types, group, aggs))
+        assert_same_rows(got, want, 1)
