@@ -368,6 +368,32 @@ int ml_gpu_topn_combine(ml_topn_local* local);
 int ml_gpu_topn_finalize(ml_topn* sink, ml_batch** out);
 int ml_gpu_topn_destroy(ml_topn* sink);
 
+/* ---- Parquet column-chunk decode (parquet_reader.rs:215-294 read_column_chunk,
+ *      :176-212 encode_strings) ------------------------------------------------------ */
+/* Parquet physical types (parquet.thrift Type) and compression codecs (CompressionCodec). */
+enum { ML_PQ_BOOLEAN = 0, ML_PQ_INT32 = 1, ML_PQ_INT64 = 2, ML_PQ_FLOAT = 4, ML_PQ_DOUBLE = 5,
+       ML_PQ_BYTE_ARRAY = 6, ML_PQ_FIXED_LEN_BYTE_ARRAY = 7 };
+enum { ML_PQ_CODEC_UNCOMPRESSED = 0, ML_PQ_CODEC_SNAPPY = 1 };
+/* Conversion (parquet_reader.rs:31-56): how the leaf column becomes a MiniLake column. */
+enum { ML_PQ_CONV_BOOL = 0, ML_PQ_CONV_INT32, ML_PQ_CONV_DATE, ML_PQ_CONV_INT64, ML_PQ_CONV_FLOAT,
+       ML_PQ_CONV_DOUBLE, ML_PQ_CONV_UTF8, ML_PQ_CONV_DECIMAL_I32, ML_PQ_CONV_DECIMAL_I64,
+       ML_PQ_CONV_DECIMAL_BYTES };
+/* Decode one column chunk of a row group: `chunk` holds its pages as stored in the file (the
+ * dictionary page, when there is one, then the data pages, each after its Thrift page header),
+ * in host memory; `num_rows` is the row group's row count and `max_def` the column's maximum
+ * definition level (0: required).  Pages may be PLAIN, RLE_DICTIONARY / PLAIN_DICTIONARY or
+ * (booleans) RLE encoded, DATA_PAGE or DATA_PAGE_V2, uncompressed or Snappy.  The one-column
+ * batch holds what read_column_chunk returns: one slot per row (NULL rows hold 0), a validity
+ * bitmap only when some value is NULL, FLOAT and DECIMAL(scale) as f64 (x / 10^scale), and
+ * strings dictionary-encoded in order of first occurrence when there are at most
+ * clamp(num_rows / 8, 1, 65536) distinct values (NULL rows count as ""), else plain.
+ * Decompression, level and index decoding, value conversion and the string dictionary run on
+ * the device; the host reads the page headers.  ML_ERR_INVALID for a malformed chunk,
+ * ML_ERR_UNSUPPORTED for other codecs, encodings or repeated columns. */
+int ml_gpu_parquet_decode(ml_ctx* ctx, const uint8_t* chunk, int64_t chunk_bytes, int32_t physical_type,
+                          int32_t type_length, int32_t conversion, int32_t scale, int32_t codec,
+                          int64_t num_rows, int32_t max_def, ml_batch** out);
+
 /* ---- Prepared query: a plan's pipelines as one CUDA graph (executor.rs:270-288) ---- */
 /* The pipelines of one physical plan over device-resident batches, in dependency order: join
  * builds, then one hash aggregate whose prologue probes their tables, then (optionally) a top-N

@@ -1418,6 +1418,7 @@ void launch_agg_final(const FinalArgs& F, cudaStream_t s) {
 }
 
 int select_blocks(int64_t n) { return (int)((n + kSelRowsPerBlock - 1) / kSelRowsPerBlock); }
+int select_rows_per_block() { return kSelRowsPerBlock; }
 void launch_select_flags(const PipeArgs& P, uint32_t* bits, uint32_t* block_counts, cudaStream_t s) {
     int nb = select_blocks(P.n);
     if (nb) k_select_flags<<<nb, kThreads, 0, s>>>(P, bits, block_counts);

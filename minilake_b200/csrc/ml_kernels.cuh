@@ -59,6 +59,7 @@ void launch_agg_final(const FinalArgs& F, cudaStream_t s);
 
 // Filter: pass bits (u32 words) + per-block counts, then ordered compaction.
 int select_blocks(int64_t n);
+int select_rows_per_block();  // rows of one select_blocks block
 void launch_select_flags(const PipeArgs& P, uint32_t* bits, uint32_t* block_counts, cudaStream_t s);
 void launch_select_write(const PipeArgs& P, const uint32_t* bits, const uint64_t* block_offsets, uint32_t* out,
                          cudaStream_t s);

@@ -110,6 +110,7 @@ def _load():
         "ml_gpu_topn_combine": ([VP], C.c_int),
         "ml_gpu_topn_finalize": ([VP, P(VP)], C.c_int),
         "ml_gpu_topn_destroy": ([VP], C.c_int),
+        "ml_gpu_parquet_decode": ([VP, VP, I64, I32, I32, I32, I32, I32, I64, I32, P(VP)], C.c_int),
         "ml_gpu_query_create": ([VP, P(VP)], C.c_int),
         "ml_gpu_query_add_build": ([VP, VP, P(abi.MlColumn), I32, I64, P(VP)], C.c_int),
         "ml_gpu_query_set_aggregate": ([VP, VP, P(abi.MlColumn), I32, I64], C.c_int),
@@ -280,6 +281,17 @@ class DeviceBatch:
                 col.validity = valid[:words]
             cols.append(col)
         return cols
+
+
+def parquet_decode(ctx: Context, chunk, physical_type: int, type_length: int, conversion: int, scale: int,
+                   codec: int, num_rows: int, max_def: int) -> DeviceBatch:
+    """One Parquet column chunk (its pages as stored in the file) decoded on the device into a
+    one-column batch (read_column_chunk, parquet_reader.rs:215-294)."""
+    buf = np.frombuffer(chunk, dtype=np.uint8) if not isinstance(chunk, np.ndarray) else chunk
+    h = C.c_void_p()
+    _check(LIB.ml_gpu_parquet_decode(ctx.h, buf.ctypes.data if len(buf) else None, len(buf), physical_type, type_length,
+                                     conversion, scale, codec, num_rows, max_def, C.byref(h)))
+    return DeviceBatch(ctx, h)
 
 
 def partition(ctx: Context, cols, key_cols: Sequence[int], nparts: int):
