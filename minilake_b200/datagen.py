@@ -132,3 +132,25 @@ def star_join(fact_rows: int = 60_000_000, row_groups: int = 128, a_rows: int = 
                      [(abi.INT32, k1), (abi.INT32, k2), (abi.INT64, a), (abi.FLOAT64, v),
                       (abi.FLOAT64, w)], row_groups)
     return fact, A, B, C
+
+
+def filter_groupby_parquet(path: str, rows: int = 1_000_000, row_groups: int = 8, seed: int = 42,
+                           compression: str = "snappy") -> None:
+    """The filter + GROUP BY table (the same seeded values as filter_groupby) written as a Parquet
+    file with `row_groups` row groups: d int32, f1 and f2 strings, qty / price / disc / tax double."""
+    import pyarrow as pa
+    import pyarrow.parquet as pq
+    rng = np.random.Generator(np.random.PCG64(seed))
+    d = rng.integers(0, 2557, rows, dtype=np.int32)
+    f1 = rng.integers(0, 3, rows)
+    f2 = rng.integers(0, 2, rows)
+    qty = rng.integers(1, 51, rows).astype(np.float64)
+    price = rng.integers(90_000, 10_500_000, rows) / 100.0
+    disc = rng.integers(0, 11, rows) / 100.0
+    tax = rng.integers(0, 9, rows) / 100.0
+    strings = lambda pool, idx: pa.DictionaryArray.from_arrays(pa.array(idx, pa.int32()),  # noqa: E731
+                                                               pa.array([s.decode() for s in pool])).cast(pa.string())
+    t = pa.table({"d": d, "f1": strings(F1_VALUES, f1), "f2": strings(F2_VALUES, f2), "qty": qty, "price": price,
+                  "disc": disc, "tax": tax})
+    per = -(-rows // row_groups)
+    pq.write_table(t, path, row_group_size=per, compression=compression)

@@ -72,3 +72,30 @@ def read_row_group(ctx: gpu.Context, path: str, row_group: int,
         out.append(gpu.parquet_decode(ctx, chunk_bytes(path, meta), PHYSICAL[col.physical_type], col.length or 0, conv,
                                       scale, CODECS[meta.compression], md.num_rows, col.max_definition_level))
     return out
+
+
+class Morsel:
+    """One row group's decoded columns as a morsel for the sinks and operators (the MlColumn
+    array they take); it keeps the single-column batches alive."""
+
+    def __init__(self, batches: List[gpu.DeviceBatch]):
+        from . import abi
+        self.batches = batches
+        arr = (abi.MlColumn * max(len(batches), 1))()
+        for i, b in enumerate(batches):
+            cols, _ = b.ml_columns()
+            arr[i] = cols[0]
+        self.ml = (arr, len(batches), batches[0].num_rows if batches else 0)
+
+    def close(self):
+        for b in self.batches:
+            b.close()
+        self.batches = []
+
+
+def read_table(ctx: gpu.Context, path: str, columns: Optional[Sequence[str]] = None) -> List[Morsel]:
+    """Every row group of a file decoded on the device, one morsel per row group (the scan's
+    morsels, scheduler.rs:44-144)."""
+    import pyarrow.parquet as pq
+    n = pq.ParquetFile(path).metadata.num_row_groups
+    return [Morsel(read_row_group(ctx, path, rg, columns)) for rg in range(n)]

@@ -167,3 +167,24 @@ def test_a_truncated_chunk_is_refused(ctx, tmp_path):
     # the context is still usable
     got = parquet.read_row_group(ctx, path, 0, ["i32"])[0]
     assert got.num_rows == pf.metadata.row_group(0).num_rows
+
+
+def test_filter_groupby_from_a_parquet_file(ctx, tmp_path):
+    """Configuration 0 as MiniLake runs it: the seeded Parquet file's row groups decoded on the
+    device are the scan's morsels; the result equals the oracle's over the same values."""
+    from minilake_b200 import datagen, parquet, workloads
+    from minilake_b200.engine import GpuEngine
+    from oracle import orc
+    from test_gpu_parity import assert_same_rows
+    path = str(tmp_path / "cfg0.parquet")
+    datagen.filter_groupby_parquet(path, rows=1_000_000, row_groups=8)
+    morsels = parquet.read_table(ctx, path, workloads.FG_SCAN)
+    assert len(morsels) == 8
+    got = workloads.run_filter_groupby(GpuEngine(ctx, threads=3), [m.ml for m in morsels])
+    want = workloads.run_filter_groupby(orc.OracleEngine(threads=2), datagen.filter_groupby(1_000_000, 8))
+    assert_same_rows(got, want, 2, {2, 3, 4})
+    # f1 / f2 came back dictionary-encoded per row group (3 and 2 values)
+    arr, _ = morsels[0].batches[1].ml_columns()
+    assert arr[0].encoding == abi.ENC_DICT and arr[0].dict_len == 3
+    for m in morsels:
+        m.close()
