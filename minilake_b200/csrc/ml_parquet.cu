@@ -213,6 +213,37 @@ __device__ bool snap_varint(const uint8_t* s, uint32_t n, uint32_t& pos, uint32_
     return false;
 }
 
+// The warp copies len bytes from s to d (the ranges do not overlap): bytes until d is 8-byte
+// aligned, then aligned 8-byte words built from the two source words each one straddles (up to
+// 8 bytes past the source range are read: the buffers are padded), four words per lane in
+// flight, then the tail bytes.
+__device__ void warp_copy(uint8_t* d, const uint8_t* s, uint32_t len, int lane) {
+    uint32_t head = (uint32_t)((8 - ((uintptr_t)d & 7)) & 7);
+    if (head > len) head = len;
+    if ((uint32_t)lane < head) d[lane] = s[lane];
+    d += head;
+    s += head;
+    len -= head;
+    const uint32_t words = len >> 3, sh = (uint32_t)((uintptr_t)s & 7);
+    const uint64_t* sa = (const uint64_t*)(s - sh);
+    uint64_t* da = (uint64_t*)d;
+    for (uint32_t w0 = 0; w0 < words; w0 += 128) {
+        uint64_t v[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint32_t w = w0 + k * 32 + lane;
+            v[k] = 0;
+            if (w < words) v[k] = sh ? (sa[w] >> (8 * sh)) | (sa[w + 1] << (64 - 8 * sh)) : sa[w];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint32_t w = w0 + k * 32 + lane;
+            if (w < words) da[w] = v[k];
+        }
+    }
+    for (uint32_t i = words * 8 + lane; i < len; i += 32) d[i] = s[i];
+}
+
 __global__ void k_pq_snappy(const SnapJob* jobs, int njobs, uint32_t* err) {
     const int w = (int)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
@@ -274,10 +305,11 @@ __global__ void k_pq_snappy(const SnapJob* jobs, int njobs, uint32_t* err) {
         from = __shfl_sync(0xFFFFFFFFu, from, 0);
         out = __shfl_sync(0xFFFFFFFFu, out, 0);
         if (kind == 0) {
-            for (uint32_t i = lane; i < len; i += 32) J.dst[out + i] = J.src[from + i];
+            warp_copy(J.dst + out, J.src + from, len, lane);
         } else {
             const uint32_t period = out - from;  // a copy may overlap itself: it repeats with this period
-            for (uint32_t i = lane; i < len; i += 32) J.dst[out + i] = J.dst[from + (i % period)];
+            if (period >= len && len >= 64) warp_copy(J.dst + out, J.dst + from, len, lane);
+            else for (uint32_t i = lane; i < len; i += 32) J.dst[out + i] = J.dst[from + (i % period)];
         }
         __syncwarp();
         out += len;
@@ -898,14 +930,10 @@ extern "C" int ml_gpu_parquet_decode(ml_ctx* ctx, const uint8_t* chunk, int64_t 
     }
 
     // 1. the chunk to the device, then every page uncompressed
-    DevBuf dchunk(ctx, std::max<int64_t>(chunk_bytes, 16), nullptr), upages(ctx, std::max<int64_t>(ubytes, 16), nullptr);
-    {
-        Staging st(ctx);
-        void* h = st.get((size_t)chunk_bytes);
-        memcpy(h, chunk, (size_t)chunk_bytes);
-        CK(cudaMemcpyAsync(dchunk.get(), h, (size_t)chunk_bytes, cudaMemcpyHostToDevice, s));
-        CK(cudaStreamSynchronize(s));
-    }
+    // 64 bytes of padding: warp_copy reads up to 8 bytes past a copy's source
+    DevBuf dchunk(ctx, (size_t)chunk_bytes + 64, nullptr), upages(ctx, (size_t)ubytes + 64, nullptr);
+    // from the caller's (pageable) buffer: a pinned staging buffer per call costs more than it saves
+    CK(cudaMemcpyAsync(dchunk.get(), chunk, (size_t)chunk_bytes, cudaMemcpyHostToDevice, s));
     const uint8_t* dc = dchunk.get<uint8_t>();
     uint8_t* up = upages.get<uint8_t>();
     std::vector<SnapJob> jobs;

@@ -216,10 +216,74 @@ def main():
     ap.add_argument("--iters", type=int, default=5)
     ap.add_argument("--rows-filter", type=int, default=100_000_000)
     ap.add_argument("--rows-join", type=int, default=60_000_000)
+    ap.add_argument("--parquet", action="store_true", help="only the Parquet decode comparison")
     a = ap.parse_args()
+    if a.parquet:
+        import sys
+        print(json.dumps(parquet_decode(log=lambda *m: print(*m, file=sys.stderr, flush=True))), flush=True)
+        return
     import sys
     out = run(a.iters, a.rows_filter, a.rows_join, log=lambda *m: print(*m, file=sys.stderr, flush=True))
     print(json.dumps(out), flush=True)
+
+
+
+def parquet_decode(rows: int = 20_000_000, row_groups: int = 160, threads: int = 16, iters: int = 3, log=print):
+    """Configuration 0's table as a seeded Snappy Parquet file (rows / row_groups rows per row
+    group), its six scanned columns decoded on the GPU (ml_gpu_parquet_decode per column chunk,
+    `threads` host threads calling it at once, each call on its own stream) against pyarrow's
+    multi-threaded CPU decode of the same columns.  Wall-clock time from file bytes in host
+    memory to decoded columns (GPU: in HBM), best of `iters`; the file is read once beforehand."""
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+
+    import pyarrow.parquet as pq
+
+    from . import datagen, gpu, parquet, workloads
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "cfg0.parquet")
+        datagen.filter_groupby_parquet(path, rows=rows, row_groups=row_groups)
+        pf = pq.ParquetFile(path)
+        names = [pf.schema.column(i).name for i in range(len(pf.schema))]
+        cols = [names.index(c) for c in workloads.FG_SCAN]
+        jobs, compressed = [], 0
+        for rg in range(pf.metadata.num_row_groups):
+            md = pf.metadata.row_group(rg)
+            for ci in cols:
+                meta, sch = md.column(ci), pf.schema.column(ci)
+                conv, scale = parquet.conversion(sch)
+                data = parquet.chunk_bytes(path, meta)
+                compressed += len(data)
+                jobs.append((data, parquet.PHYSICAL[sch.physical_type], sch.length or 0, conv, scale,
+                             parquet.CODECS[meta.compression], md.num_rows, sch.max_definition_level))
+        ctx = gpu.Context(0)
+
+        def one(j):
+            gpu.parquet_decode(ctx, *j).close()
+
+        def gpu_run():
+            with ThreadPoolExecutor(threads) as ex:
+                list(ex.map(one, jobs))
+        gpu_run()
+        best_gpu = min(_wall(gpu_run) for _ in range(iters))
+        cpu_threads = os.cpu_count() or 1
+        pq.read_table(path, columns=workloads.FG_SCAN, use_threads=True)
+        best_cpu = min(_wall(lambda: pq.read_table(path, columns=workloads.FG_SCAN, use_threads=True))
+                       for _ in range(iters))
+        ctx.close()
+    out = {"rows": rows, "row_groups": row_groups, "column_chunks": len(jobs), "compressed_bytes": compressed,
+           "gpu_ms": round(best_gpu * 1e3, 2), "gpu_rows_per_s": rows / best_gpu,
+           "gpu_compressed_gbs": round(compressed / best_gpu / 1e9, 3), "gpu_host_threads": threads,
+           "cpu_pyarrow_ms": round(best_cpu * 1e3, 2), "cpu_rows_per_s": rows / best_cpu, "cpu_threads": cpu_threads}
+    log(f"parquet_decode: {out}")
+    return out
+
+
+def _wall(fn):
+    import time
+    t0 = time.perf_counter()
+    fn()
+    return time.perf_counter() - t0
 
 
 if __name__ == "__main__":

@@ -265,7 +265,10 @@ class Server:
         """Run the stream in real time; returns the queries with their timings and results."""
         from .gpu import ResourcesExhausted
         pending: "queue.Queue[Optional[Query]]" = queue.Queue()
-        sinks_per_slot = [dict() for _ in range(self.slots)]
+        # the slots' resident sinks (and their captured graphs) carry over from stream to stream
+        if not hasattr(self, "sinks_per_slot"):
+            self.sinks_per_slot = [dict() for _ in range(self.slots)]
+        sinks_per_slot = self.sinks_per_slot
         if warmup:
             # the star join's filtered dimension is indexed directly or hashed depending on the
             # prefix: compile both kernel variants (the kernel cache is shared by all slots)
@@ -354,15 +357,20 @@ class Server:
         if gc_was_enabled:
             gc.enable()
         gc.unfreeze()
+        seen = self.__dict__.setdefault("graph_seen", {})
         for d in sinks_per_slot:
             for s in d.values():
                 g = s.graph_stats()
-                self.graphs["built"] += g["built"]
-                self.graphs["replayed"] += g["replayed"]
-                s.close()
+                b0, r0 = seen.get(id(s), (0, 0))
+                self.graphs["built"] += g["built"] - b0
+                self.graphs["replayed"] += g["replayed"] - r0
+                seen[id(s)] = (g["built"], g["replayed"])
         return stream
 
     def close(self):
+        for d in getattr(self, "sinks_per_slot", []):
+            for s in d.values():
+                s.close()
         for j in (self.dim_join, self.b_join, self.c_join):
             j.close()
         for b in (self.dim, self.A, self.B, self.C):
@@ -402,10 +410,28 @@ def main():
     ap.add_argument("--max-rows", type=int, default=200_000_000)
     ap.add_argument("--learned", choices=["on", "off", "both"], default="both")
     ap.add_argument("--seed", type=int, default=46)
+    ap.add_argument("--sweep", default="", help="comma-separated arrival rates (q/s): a load sweep, "
+                                                  "--queries queries at each rate over the same tables")
     a = ap.parse_args()
     import sys
     log = lambda *m: print(*m, file=sys.stderr, flush=True)
     out = {}
+    if a.sweep:
+        rates = [float(r) for r in a.sweep.split(",")]
+        for mode in (["on", "off"] if a.learned == "both" else [a.learned]):
+            server = Server(a.tables_per_shape, a.min_rows, a.max_rows, a.slots, mode == "on", a.seed, log)
+            rows = []
+            for i, rate in enumerate(rates):
+                stream = make_stream(a.queries, rate, a.tables_per_shape, a.seed + i)
+                server.serve(stream, warmup=i == 0)
+                r = summarize(stream, server)
+                rows.append({"rate": rate, **{k: r[k] for k in ("completed", "failed", "p50_ms", "p99_ms", "p999_ms",
+                                                                 "max_ms", "queries_per_s", "algorithmic_GB_per_s")}})
+                log(f"learned {mode} rate {rate}: {json.dumps(rows[-1])}")
+            out["sweep_learned_" + mode] = rows
+            server.close()
+        print(json.dumps(out), flush=True)
+        return
     for mode in (["on", "off"] if a.learned == "both" else [a.learned]):
         server = Server(a.tables_per_shape, a.min_rows, a.max_rows, a.slots, mode == "on", a.seed, log)
         stream = make_stream(a.queries, a.rate, a.tables_per_shape, a.seed)
