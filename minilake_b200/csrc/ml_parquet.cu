@@ -195,127 +195,116 @@ constexpr uint32_t PQ_ERR_SNAPPY = 1, PQ_ERR_LAYOUT = 2, PQ_ERR_RUNS = 4, PQ_ERR
 constexpr int kPqTile = 8192;  // rows per decode tile: 256 threads x one 32-row validity word
 
 // ---- 1. Snappy (the format's public description: a varint length, then literal and copy
-// elements), one warp per page --------------------------------------------------------------
+// elements), one thread per page: the element stream is sequential and most elements are a few
+// bytes, so one thread walks it from a shared-memory window of the source and resolves copies
+// from a 64 KB shared-memory ring of the output it wrote (older offsets read global memory).
 struct SnapJob {
     const uint8_t* src;
     uint8_t* dst;
     uint32_t src_len, dst_len;
 };
+constexpr uint32_t kSnapRing = 1u << 16;  // output history in shared memory
+constexpr uint32_t kSnapWin = 4096;       // source window in shared memory
+constexpr int kSnapSmem = (int)(kSnapRing + kSnapWin + 16);
 
-__device__ bool snap_varint(const uint8_t* s, uint32_t n, uint32_t& pos, uint32_t& v) {
-    v = 0;
-    for (int shift = 0; shift < 35; shift += 7) {
-        if (pos >= n) return false;
-        const uint8_t b = s[pos++];
-        v |= (uint32_t)(b & 0x7F) << shift;
-        if (!(b & 0x80)) return true;
-    }
-    return false;
-}
-
-// The warp copies len bytes from s to d (the ranges do not overlap): bytes until d is 8-byte
-// aligned, then aligned 8-byte words built from the two source words each one straddles (up to
-// 8 bytes past the source range are read: the buffers are padded), four words per lane in
-// flight, then the tail bytes.
-__device__ void warp_copy(uint8_t* d, const uint8_t* s, uint32_t len, int lane) {
-    uint32_t head = (uint32_t)((8 - ((uintptr_t)d & 7)) & 7);
-    if (head > len) head = len;
-    if ((uint32_t)lane < head) d[lane] = s[lane];
-    d += head;
-    s += head;
-    len -= head;
-    const uint32_t words = len >> 3, sh = (uint32_t)((uintptr_t)s & 7);
-    const uint64_t* sa = (const uint64_t*)(s - sh);
-    uint64_t* da = (uint64_t*)d;
-    for (uint32_t w0 = 0; w0 < words; w0 += 128) {
-        uint64_t v[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const uint32_t w = w0 + k * 32 + lane;
-            v[k] = 0;
-            if (w < words) v[k] = sh ? (sa[w] >> (8 * sh)) | (sa[w + 1] << (64 - 8 * sh)) : sa[w];
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const uint32_t w = w0 + k * 32 + lane;
-            if (w < words) da[w] = v[k];
-        }
-    }
-    for (uint32_t i = words * 8 + lane; i < len; i += 32) d[i] = s[i];
-}
-
-__global__ void k_pq_snappy(const SnapJob* jobs, int njobs, uint32_t* err) {
-    const int w = (int)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (w >= njobs) return;
-    const SnapJob J = jobs[w];
-    uint32_t pos = 0, out = 0, total = 0;
+__global__ void __launch_bounds__(32) k_pq_snappy(const SnapJob* jobs, int njobs, uint32_t* err) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    if (blockIdx.x >= (unsigned)njobs || threadIdx.x != 0) return;
+    uint8_t* ring = sm;
+    uint8_t* win = sm + kSnapRing;
+    const SnapJob J = jobs[blockIdx.x];
+    int64_t wbase = 0, wend = 0;  // the window holds src[wbase, wend) (wbase may be below 0)
+    // the window from `pos`: 16-byte loads from the 16-byte boundary at or below it up to the
+    // end of the source (the buffer is padded: the last load may pass that end by 15 bytes)
+    auto fill = [&](uint32_t pos) {
+        const uintptr_t a = (uintptr_t)(J.src + pos);
+        const uint4* v = (const uint4*)(a & ~(uintptr_t)15);
+        const int64_t lead = (int64_t)(a & 15);
+        const uint64_t need = ((uint64_t)(J.src_len - pos) + (uint64_t)lead + 15) / 16;
+        const uint32_t nvec = (uint32_t)(need < kSnapWin / 16 ? need : kSnapWin / 16);
+        for (uint32_t i = 0; i < nvec; i++) ((uint4*)win)[i] = __ldg(v + i);
+        wbase = (int64_t)pos - lead;
+        wend = wbase + 16 * (int64_t)nvec;
+    };
+    auto at = [&](uint32_t p) -> uint32_t {  // source byte p (p < src_len)
+        if ((int64_t)p < wbase || (int64_t)p >= wend) fill(p);
+        return win[(int64_t)p - wbase];
+    };
     bool ok = true;
-    if (lane == 0) ok = snap_varint(J.src, J.src_len, pos, total) && total == J.dst_len;
-    ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
-    while (ok) {
-        // lane 0 reads the element: kind 0 = literal (from src at `from`), 1 = copy (from dst)
-        uint32_t kind = 0, len = 0, from = 0, done = 0;
-        if (lane == 0) {
-            if (out >= total) {
-                done = 1;
-                if (pos != J.src_len) ok = false;
-            } else if (pos >= J.src_len) {
-                ok = false;
-            } else {
-                const uint8_t tag = J.src[pos++];
-                const uint32_t t = tag & 3;
-                if (t == 0) {
-                    uint32_t l = tag >> 2;
-                    if (l >= 60) {
-                        const uint32_t nb = l - 59;
-                        if (pos + nb > J.src_len) ok = false;
-                        l = 0;
-                        for (uint32_t i = 0; ok && i < nb; i++) l |= (uint32_t)J.src[pos + i] << (8 * i);
-                        pos += nb;
-                    }
-                    len = l + 1;
-                    from = pos;
-                    if (ok && (pos + len > J.src_len || out + len > total)) ok = false;
-                    pos += len;
-                } else {
-                    uint32_t off = 0;
-                    if (t == 1) {
-                        len = 4 + ((tag >> 2) & 7);
-                        if (pos + 1 > J.src_len) ok = false;
-                        else off = ((uint32_t)(tag >> 5) << 8) | J.src[pos++];
-                    } else {
-                        len = (tag >> 2) + 1;
-                        const uint32_t nb = t == 2 ? 2 : 4;
-                        if (pos + nb > J.src_len) ok = false;
-                        for (uint32_t i = 0; ok && i < nb; i++) off |= (uint32_t)J.src[pos + i] << (8 * i);
-                        pos += nb;
-                    }
-                    if (ok && (off == 0 || off > out || out + len > total)) ok = false;
-                    kind = 1;
-                    from = out - off;
+    uint32_t pos = 0, out = 0, total = 0;
+    for (int shift = 0; shift < 35; shift += 7) {  // the uncompressed length
+        if (pos >= J.src_len) {
+            ok = false;
+            break;
+        }
+        const uint32_t b = at(pos++);
+        total |= (b & 0x7F) << shift;
+        if (!(b & 0x80)) break;
+    }
+    if (total != J.dst_len) ok = false;
+    while (ok && out < total) {
+        if (pos >= J.src_len) {
+            ok = false;
+            break;
+        }
+        const uint32_t tag = at(pos++), t = tag & 3;
+        uint32_t len, off = 0;
+        if (t == 0) {
+            len = tag >> 2;
+            if (len >= 60) {
+                const uint32_t nb = len - 59;
+                if (pos + nb > J.src_len) {
+                    ok = false;
+                    break;
                 }
+                len = 0;
+                for (uint32_t i = 0; i < nb; i++) len |= at(pos + i) << (8 * i);
+                pos += nb;
+            }
+            len += 1;
+            if (len > J.src_len - pos || len > total - out) {
+                ok = false;
+                break;
+            }
+            for (uint32_t i = 0; i < len; i++) {
+                const uint8_t b = (uint8_t)at(pos + i);
+                ring[(out + i) & (kSnapRing - 1)] = b;
+                J.dst[out + i] = b;
+            }
+            pos += len;
+        } else {
+            if (t == 1) {
+                if (pos + 1 > J.src_len) {
+                    ok = false;
+                    break;
+                }
+                len = 4 + ((tag >> 2) & 7);
+                off = ((tag >> 5) << 8) | at(pos++);
+            } else {
+                const uint32_t nb = t == 2 ? 2 : 4;
+                if (pos + nb > J.src_len) {
+                    ok = false;
+                    break;
+                }
+                len = (tag >> 2) + 1;
+                for (uint32_t i = 0; i < nb; i++) off |= at(pos + i) << (8 * i);
+                pos += nb;
+            }
+            if (off == 0 || off > out || len > total - out) {
+                ok = false;
+                break;
+            }
+            for (uint32_t i = 0; i < len; i++) {  // byte by byte: a copy may overlap itself
+                const uint32_t from = out + i - off;
+                const uint8_t b = off <= kSnapRing ? ring[from & (kSnapRing - 1)] : J.dst[from];
+                ring[(out + i) & (kSnapRing - 1)] = b;
+                J.dst[out + i] = b;
             }
         }
-        ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
-        done = __shfl_sync(0xFFFFFFFFu, done, 0);
-        if (!ok || done) break;
-        kind = __shfl_sync(0xFFFFFFFFu, kind, 0);
-        len = __shfl_sync(0xFFFFFFFFu, len, 0);
-        from = __shfl_sync(0xFFFFFFFFu, from, 0);
-        out = __shfl_sync(0xFFFFFFFFu, out, 0);
-        if (kind == 0) {
-            warp_copy(J.dst + out, J.src + from, len, lane);
-        } else {
-            const uint32_t period = out - from;  // a copy may overlap itself: it repeats with this period
-            if (period >= len && len >= 64) warp_copy(J.dst + out, J.dst + from, len, lane);
-            else for (uint32_t i = lane; i < len; i += 32) J.dst[out + i] = J.dst[from + (i % period)];
-        }
-        __syncwarp();
         out += len;
-        pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
     }
-    if (!ok && lane == 0) atomicOr(err, PQ_ERR_SNAPPY);
+    if (ok && pos != J.src_len) ok = false;
+    if (!ok) atomicOr(err, PQ_ERR_SNAPPY);
 }
 
 // ---- 2. page layout and RLE / bit-packed hybrid run tables -----------------------------------
@@ -958,7 +947,10 @@ extern "C" int ml_gpu_parquet_decode(ml_ctx* ctx, const uint8_t* chunk, int64_t 
     if (!jobs.empty()) {
         DevBuf dj(ctx, jobs.size() * sizeof(SnapJob), nullptr);
         CK(cudaMemcpyAsync(dj.get(), jobs.data(), jobs.size() * sizeof(SnapJob), cudaMemcpyHostToDevice, s));
-        k_pq_snappy<<<(int)((jobs.size() * 32 + 255) / 256), 256, 0, s>>>(dj.get<SnapJob>(), (int)jobs.size(), derr);
+        static const bool smem_ok = cudaFuncSetAttribute(k_pq_snappy, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         kSnapSmem) == cudaSuccess;
+        if (!smem_ok) raise(ML_ERR_CUDA, "parquet: the Snappy kernel's shared memory is not available");
+        k_pq_snappy<<<(int)jobs.size(), 32, kSnapSmem, s>>>(dj.get<SnapJob>(), (int)jobs.size(), derr);
         ctx->count_launch();
         CK(cudaStreamSynchronize(s));  // `jobs` and its device copy go out of scope
     }

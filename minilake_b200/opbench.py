@@ -220,7 +220,8 @@ def main():
     a = ap.parse_args()
     if a.parquet:
         import sys
-        print(json.dumps(parquet_decode(log=lambda *m: print(*m, file=sys.stderr, flush=True))), flush=True)
+        lg = lambda *m: print(*m, file=sys.stderr, flush=True)  # noqa: E731
+        print(json.dumps([parquet_decode(log=lg, compression=c) for c in ("snappy", "none")]), flush=True)
         return
     import sys
     out = run(a.iters, a.rows_filter, a.rows_join, log=lambda *m: print(*m, file=sys.stderr, flush=True))
@@ -228,7 +229,8 @@ def main():
 
 
 
-def parquet_decode(rows: int = 20_000_000, row_groups: int = 160, threads: int = 16, iters: int = 3, log=print):
+def parquet_decode(rows: int = 20_000_000, row_groups: int = 160, threads: int = 16, iters: int = 3, log=print,
+                   compression: str = "snappy"):
     """Configuration 0's table as a seeded Snappy Parquet file (rows / row_groups rows per row
     group), its six scanned columns decoded on the GPU (ml_gpu_parquet_decode per column chunk,
     `threads` host threads calling it at once, each call on its own stream) against pyarrow's
@@ -242,7 +244,7 @@ def parquet_decode(rows: int = 20_000_000, row_groups: int = 160, threads: int =
     from . import datagen, gpu, parquet, workloads
     with tempfile.TemporaryDirectory() as tmp:
         path = os.path.join(tmp, "cfg0.parquet")
-        datagen.filter_groupby_parquet(path, rows=rows, row_groups=row_groups)
+        datagen.filter_groupby_parquet(path, rows=rows, row_groups=row_groups, compression=compression)
         pf = pq.ParquetFile(path)
         names = [pf.schema.column(i).name for i in range(len(pf.schema))]
         cols = [names.index(c) for c in workloads.FG_SCAN]
@@ -271,7 +273,8 @@ def parquet_decode(rows: int = 20_000_000, row_groups: int = 160, threads: int =
         best_cpu = min(_wall(lambda: pq.read_table(path, columns=workloads.FG_SCAN, use_threads=True))
                        for _ in range(iters))
         ctx.close()
-    out = {"rows": rows, "row_groups": row_groups, "column_chunks": len(jobs), "compressed_bytes": compressed,
+    out = {"compression": compression, "rows": rows, "row_groups": row_groups, "column_chunks": len(jobs),
+           "compressed_bytes": compressed,
            "gpu_ms": round(best_gpu * 1e3, 2), "gpu_rows_per_s": rows / best_gpu,
            "gpu_compressed_gbs": round(compressed / best_gpu / 1e9, 3), "gpu_host_threads": threads,
            "cpu_pyarrow_ms": round(best_cpu * 1e3, 2), "cpu_rows_per_s": rows / best_cpu, "cpu_threads": cpu_threads}
