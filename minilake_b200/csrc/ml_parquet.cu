@@ -4,8 +4,9 @@
 //
 // The host parses the chunk's page headers (Thrift compact protocol, parquet.thrift PageHeader)
 // and copies the chunk to the device once.  Then, on the device:
-//   1. Snappy pages are decompressed, one warp per page (the element stream is sequential; the
-//      lanes copy each literal or match together);
+//   1. Snappy pages are decompressed: a header walk per page finds where each of the
+//      compressor's independent 64 KB fragments starts, then one thread per fragment decodes it
+//      (a page that does not split that way is decoded by one thread);
 //   2. every RLE / bit-packed hybrid stream (definition levels, dictionary indices) gets a run
 //      table (one thread per stream walks the run headers, counting first, then filling);
 //   3. rows are decoded in 8,192-row tiles: definition levels give the validity bits, a block
@@ -195,115 +196,170 @@ constexpr uint32_t PQ_ERR_SNAPPY = 1, PQ_ERR_LAYOUT = 2, PQ_ERR_RUNS = 4, PQ_ERR
 constexpr int kPqTile = 8192;  // rows per decode tile: 256 threads x one 32-row validity word
 
 // ---- 1. Snappy (the format's public description: a varint length, then literal and copy
-// elements), one thread per page: the element stream is sequential and most elements are a few
-// bytes, so one thread walks it from a shared-memory window of the source and resolves copies
-// from a 64 KB shared-memory ring of the output it wrote (older offsets read global memory).
+// elements).  The element stream is sequential, but the compressor works on 64 KB fragments of
+// its input and no match reaches back past its fragment's start, so a page of N fragments is N
+// independent decodes once their starts in the stream are known: one thread walks the element
+// headers (no bytes copied) to find them, then one thread per fragment decodes it, reading the
+// source through a shared-memory window.  A page whose elements cross a fragment boundary, or
+// whose matches reach into an earlier fragment, is decoded by one thread from start to end.
 struct SnapJob {
     const uint8_t* src;
     uint8_t* dst;
     uint32_t src_len, dst_len;
 };
-constexpr uint32_t kSnapRing = 1u << 16;  // output history in shared memory
-constexpr uint32_t kSnapWin = 4096;       // source window in shared memory
-constexpr int kSnapSmem = (int)(kSnapRing + kSnapWin + 16);
+constexpr uint32_t kSnapFrag = 1u << 16;  // the compressor's fragment
+constexpr int kSnapFrags = 32;            // fragments decoded at once (one thread each)
+constexpr uint32_t kSnapWin = 2048;       // each thread's source window
 
-__global__ void __launch_bounds__(32) k_pq_snappy(const SnapJob* jobs, int njobs, uint32_t* err) {
-    extern __shared__ __align__(16) uint8_t sm[];
-    if (blockIdx.x >= (unsigned)njobs || threadIdx.x != 0) return;
-    uint8_t* ring = sm;
-    uint8_t* win = sm + kSnapRing;
-    const SnapJob J = jobs[blockIdx.x];
+struct SnapSrc {  // the compressed stream through a shared-memory window
+    const uint8_t* src;
+    uint32_t len;
+    uint8_t* win;
     int64_t wbase = 0, wend = 0;  // the window holds src[wbase, wend) (wbase may be below 0)
-    // the window from `pos`: 16-byte loads from the 16-byte boundary at or below it up to the
-    // end of the source (the buffer is padded: the last load may pass that end by 15 bytes)
-    auto fill = [&](uint32_t pos) {
-        const uintptr_t a = (uintptr_t)(J.src + pos);
+    // 16-byte loads from the boundary at or below p, up to the stream's end (the buffer is padded:
+    // the last load may pass that end by 15 bytes)
+    __device__ void fill(uint32_t p) {
+        const uintptr_t a = (uintptr_t)(src + p);
         const uint4* v = (const uint4*)(a & ~(uintptr_t)15);
         const int64_t lead = (int64_t)(a & 15);
-        const uint64_t need = ((uint64_t)(J.src_len - pos) + (uint64_t)lead + 15) / 16;
+        const uint64_t need = ((uint64_t)(len - p) + (uint64_t)lead + 15) / 16;
         const uint32_t nvec = (uint32_t)(need < kSnapWin / 16 ? need : kSnapWin / 16);
-        for (uint32_t i = 0; i < nvec; i++) ((uint4*)win)[i] = __ldg(v + i);
-        wbase = (int64_t)pos - lead;
+        for (uint32_t i = 0; i < nvec; i += 4) {  // 4 loads in flight, then their stores
+            uint4 r[4];
+#pragma unroll
+            for (uint32_t k = 0; k < 4; k++)
+                if (i + k < nvec) r[k] = __ldg(v + i + k);
+#pragma unroll
+            for (uint32_t k = 0; k < 4; k++)
+                if (i + k < nvec) ((uint4*)win)[i + k] = r[k];
+        }
+        wbase = (int64_t)p - lead;
         wend = wbase + 16 * (int64_t)nvec;
-    };
-    auto at = [&](uint32_t p) -> uint32_t {  // source byte p (p < src_len)
+    }
+    __device__ uint32_t at(uint32_t p) {  // p < len
         if ((int64_t)p < wbase || (int64_t)p >= wend) fill(p);
         return win[(int64_t)p - wbase];
-    };
-    bool ok = true;
-    uint32_t pos = 0, out = 0, total = 0;
-    for (int shift = 0; shift < 35; shift += 7) {  // the uncompressed length
-        if (pos >= J.src_len) {
-            ok = false;
-            break;
-        }
-        const uint32_t b = at(pos++);
-        total |= (b & 0x7F) << shift;
-        if (!(b & 0x80)) break;
     }
-    if (total != J.dst_len) ok = false;
-    while (ok && out < total) {
-        if (pos >= J.src_len) {
-            ok = false;
-            break;
+};
+
+// One element's header at `pos` (pos < end): kind (0 literal, 1 copy), length, copy offset, and
+// the position of the element's data (a literal's bytes) or of the next element.
+__device__ bool snap_element(SnapSrc& S, uint32_t& pos, uint32_t end, uint32_t& kind, uint32_t& len, uint32_t& off) {
+    const uint32_t tag = S.at(pos++), t = tag & 3;
+    off = 0;
+    if (t == 0) {
+        kind = 0;
+        len = tag >> 2;
+        if (len >= 60) {
+            const uint32_t nb = len - 59;
+            if (nb > end - pos) return false;
+            len = 0;
+            for (uint32_t i = 0; i < nb; i++) len |= S.at(pos + i) << (8 * i);
+            pos += nb;
         }
-        const uint32_t tag = at(pos++), t = tag & 3;
-        uint32_t len, off = 0;
-        if (t == 0) {
-            len = tag >> 2;
-            if (len >= 60) {
-                const uint32_t nb = len - 59;
-                if (pos + nb > J.src_len) {
-                    ok = false;
-                    break;
-                }
-                len = 0;
-                for (uint32_t i = 0; i < nb; i++) len |= at(pos + i) << (8 * i);
-                pos += nb;
-            }
-            len += 1;
-            if (len > J.src_len - pos || len > total - out) {
-                ok = false;
-                break;
-            }
-            for (uint32_t i = 0; i < len; i++) {
-                const uint8_t b = (uint8_t)at(pos + i);
-                ring[(out + i) & (kSnapRing - 1)] = b;
-                J.dst[out + i] = b;
-            }
+        len += 1;
+        return len <= end - pos;
+    }
+    kind = 1;
+    if (t == 1) {
+        if (pos >= end) return false;
+        len = 4 + ((tag >> 2) & 7);
+        off = ((tag >> 5) << 8) | S.at(pos++);
+    } else {
+        const uint32_t nb = t == 2 ? 2 : 4;
+        if (nb > end - pos) return false;
+        len = (tag >> 2) + 1;
+        for (uint32_t i = 0; i < nb; i++) off |= S.at(pos + i) << (8 * i);
+        pos += nb;
+    }
+    return true;
+}
+
+// Decode the elements in [pos, end) into dst[out, out_end); copies may not reach below `floor`.
+__device__ bool snap_decode(SnapSrc& S, uint32_t pos, uint32_t end, uint8_t* dst, uint32_t out, uint32_t out_end,
+                            uint32_t floor) {
+    while (out < out_end) {
+        if (pos >= end) return false;
+        uint32_t kind, len, off;
+        if (!snap_element(S, pos, end, kind, len, off) || len > out_end - out) return false;
+        if (kind == 0) {
+            for (uint32_t i = 0; i < len; i++) dst[out + i] = (uint8_t)S.at(pos + i);
             pos += len;
         } else {
-            if (t == 1) {
-                if (pos + 1 > J.src_len) {
-                    ok = false;
-                    break;
-                }
-                len = 4 + ((tag >> 2) & 7);
-                off = ((tag >> 5) << 8) | at(pos++);
-            } else {
-                const uint32_t nb = t == 2 ? 2 : 4;
-                if (pos + nb > J.src_len) {
-                    ok = false;
-                    break;
-                }
-                len = (tag >> 2) + 1;
-                for (uint32_t i = 0; i < nb; i++) off |= at(pos + i) << (8 * i);
-                pos += nb;
-            }
-            if (off == 0 || off > out || len > total - out) {
-                ok = false;
-                break;
-            }
-            for (uint32_t i = 0; i < len; i++) {  // byte by byte: a copy may overlap itself
-                const uint32_t from = out + i - off;
-                const uint8_t b = off <= kSnapRing ? ring[from & (kSnapRing - 1)] : J.dst[from];
-                ring[(out + i) & (kSnapRing - 1)] = b;
-                J.dst[out + i] = b;
-            }
+            if (off == 0 || off > out - floor) return false;
+            for (uint32_t i = 0; i < len; i++) dst[out + i] = dst[out + i - off];  // may overlap itself
         }
         out += len;
     }
-    if (ok && pos != J.src_len) ok = false;
+    return pos == end;
+}
+
+// The header walk, one block (one working thread) per page: the page's mode (0 malformed, 1 one
+// thread decodes it, 2 its fragments decode in parallel) and, for mode 2, where each fragment's
+// elements start (plan: [mode, first element, fragment starts..., stream end], kSnapFrags + 3).
+__global__ void __launch_bounds__(32) k_pq_snappy_walk(const SnapJob* jobs, int njobs, uint32_t* plan) {
+    __shared__ __align__(16) uint8_t win[kSnapWin + 16];
+    if (blockIdx.x >= (unsigned)njobs || threadIdx.x) return;
+    const SnapJob J = jobs[blockIdx.x];
+    uint32_t* pl = plan + (size_t)blockIdx.x * (kSnapFrags + 3);
+    SnapSrc S{J.src, J.src_len, win};
+    uint32_t start = 0, total = 0;
+    bool ok = false;
+    for (int shift = 0; shift < 35 && start < J.src_len; shift += 7) {  // the uncompressed length
+        const uint32_t b = S.at(start++);
+        total |= (b & 0x7F) << shift;
+        if (!(b & 0x80)) {
+            ok = true;
+            break;
+        }
+    }
+    uint32_t mode = ok && total == J.dst_len ? 1 : 0;
+    pl[1] = start;
+    const uint32_t nfrag = (total + kSnapFrag - 1) / kSnapFrag;
+    if (mode && nfrag > 1 && nfrag <= (uint32_t)kSnapFrags) {
+        uint32_t pos = start, out = 0;
+        bool split = true;
+        while (split && out < total) {
+            if (out % kSnapFrag == 0) pl[2 + out / kSnapFrag] = pos;
+            if (pos >= J.src_len) {
+                split = false;
+                break;
+            }
+            uint32_t kind, len, off;
+            if (!snap_element(S, pos, J.src_len, kind, len, off) || len > total - out) {
+                split = false;
+                break;
+            }
+            const uint32_t frag0 = out - out % kSnapFrag;
+            if ((out + len - 1) / kSnapFrag != out / kSnapFrag) split = false;  // crosses a fragment end
+            if (kind == 0) pos += len;
+            else if (off == 0 || off > out - frag0) split = false;  // reaches an earlier fragment
+            out += len;
+        }
+        pl[2 + nfrag] = J.src_len;
+        if (split && out == total) mode = 2;
+    }
+    pl[0] = mode;
+}
+
+// The decode, one block (one working thread) per page and fragment.
+__global__ void __launch_bounds__(32) k_pq_snappy(const SnapJob* jobs, int njobs, const uint32_t* plan, uint32_t* err) {
+    __shared__ __align__(16) uint8_t win[kSnapWin + 16];
+    const int page = blockIdx.x / kSnapFrags, frag = blockIdx.x % kSnapFrags;
+    if (page >= njobs || threadIdx.x) return;
+    const SnapJob J = jobs[page];
+    const uint32_t* pl = plan + (size_t)page * (kSnapFrags + 3);
+    SnapSrc S{J.src, J.src_len, win};
+    bool ok = true;
+    if (pl[0] == 2) {
+        const uint32_t nfrag = (J.dst_len + kSnapFrag - 1) / kSnapFrag;
+        if ((uint32_t)frag < nfrag) {
+            const uint32_t o0 = frag * kSnapFrag, o1 = min(J.dst_len, o0 + kSnapFrag);
+            ok = snap_decode(S, pl[2 + frag], pl[3 + frag], J.dst, o0, o1, o0);
+        }
+    } else if (frag == 0) {
+        ok = pl[0] == 1 && snap_decode(S, pl[1], J.src_len, J.dst, 0, J.dst_len, 0);
+    }
     if (!ok) atomicOr(err, PQ_ERR_SNAPPY);
 }
 
@@ -944,15 +1000,15 @@ extern "C" int ml_gpu_parquet_decode(ml_ctx* ctx, const uint8_t* chunk, int64_t 
     DevBuf err(ctx, 16, nullptr);
     CK(cudaMemsetAsync(err.get(), 0, 4, s));
     uint32_t* derr = err.get<uint32_t>();
-    DevBuf dj;  // read by the Snappy kernel: lives to the end of the call
+    DevBuf dj, splan;  // read by the Snappy kernels: live to the end of the call
     if (!jobs.empty()) {
         dj = DevBuf(ctx, jobs.size() * sizeof(SnapJob), nullptr);
         CK(cudaMemcpyAsync(dj.get(), jobs.data(), jobs.size() * sizeof(SnapJob), cudaMemcpyHostToDevice, s));
-        static const bool smem_ok = cudaFuncSetAttribute(k_pq_snappy, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         kSnapSmem) == cudaSuccess;
-        if (!smem_ok) raise(ML_ERR_CUDA, "parquet: the Snappy kernel's shared memory is not available");
-        k_pq_snappy<<<(int)jobs.size(), 32, kSnapSmem, s>>>(dj.get<SnapJob>(), (int)jobs.size(), derr);
-        ctx->count_launch();
+        const int nj = (int)jobs.size();
+        splan = DevBuf(ctx, (size_t)nj * (kSnapFrags + 3) * 4, nullptr);
+        k_pq_snappy_walk<<<nj, 32, 0, s>>>(dj.get<SnapJob>(), nj, splan.get<uint32_t>());
+        k_pq_snappy<<<nj * kSnapFrags, 32, 0, s>>>(dj.get<SnapJob>(), nj, splan.get<uint32_t>(), derr);
+        ctx->count_launch(2);
         // wait here: a long Snappy kernel with the decode queued behind it holds up other calls'
         // work that shares its hardware queue (measured: 3.6 s instead of 0.9 s for 960 chunks
         // decoded from 16 threads)

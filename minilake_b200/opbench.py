@@ -217,11 +217,16 @@ def main():
     ap.add_argument("--rows-filter", type=int, default=100_000_000)
     ap.add_argument("--rows-join", type=int, default=60_000_000)
     ap.add_argument("--parquet", action="store_true", help="only the Parquet decode comparison")
+    ap.add_argument("--parquet-threads", type=int, default=16, help="host threads calling the decoder at once")
     a = ap.parse_args()
     if a.parquet:
         import sys
+        # one hardware work queue per calling thread (up to 32): calls on different streams do not
+        # wait behind each other's long Snappy kernels (read when the CUDA context is created)
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", str(min(max(a.parquet_threads, 8), 32)))
         lg = lambda *m: print(*m, file=sys.stderr, flush=True)  # noqa: E731
-        print(json.dumps([parquet_decode(log=lg, compression=c) for c in ("snappy", "none")]), flush=True)
+        print(json.dumps([parquet_decode(log=lg, compression=c, threads=a.parquet_threads) for c in ("snappy", "none")]),
+              flush=True)
         return
     import sys
     out = run(a.iters, a.rows_filter, a.rows_join, log=lambda *m: print(*m, file=sys.stderr, flush=True))
