@@ -139,7 +139,13 @@ static size_t round_cap(size_t b) {
         while (p < b) p <<= 1;
         return p;
     }
-    return (b + (1ull << 20) - 1) & ~((1ull << 20) - 1);  // 1 MiB granules above 1 MiB
+    // above 1 MiB, eight size classes per power of two (at most 12.5 % unused): buffers whose
+    // sizes vary from query to query (tables presized from an estimate) still reuse cached
+    // blocks, where exact sizes each needed a cudaMalloc, and cudaMalloc may stall the device
+    size_t p = 1ull << 20;
+    while (p * 2 <= b) p <<= 1;
+    const size_t step = p / 8;
+    return (b + step - 1) / step * step;
 }
 void* Ctx::dalloc(size_t bytes, size_t* cap) {
     size_t c = round_cap(bytes);

@@ -389,7 +389,19 @@ def summarize(stream: List[Query], server: Server) -> dict:
         if len(l):
             per_shape[name] = {"queries": int(len(l)), "p50_ms": float(np.percentile(l, 50)),
                                "p99_ms": float(np.percentile(l, 99))}
+    # the slowest queries: when they arrived, how long they queued before a slot took them
+    slow = sorted(ok, key=lambda q: q.arrival - q.done)[:12]
+    slowest = [{"arrival_s": round(q.arrival, 4), "queued_ms": round((q.start - q.arrival) * 1e3, 3),
+                "run_ms": round((q.done - q.start) * 1e3, 3), "shape": SHAPES[q.shape], "table": q.table}
+               for q in slow]
+    # host-side events that can stall every slot at once: device and pinned allocations, kernel
+    # compilations, graph captures (count, total ms since the server started)
+    ctx = getattr(server, "ctx", None)
+    events = {k: [int(v) if i == 0 else round(v, 2) for i, v in enumerate(ctx.profile(k))]
+              for k in ("device_alloc", "pinned_alloc", "jit_compile", "graph_capture")} if ctx else {}
     return {
+        "slowest": slowest,
+        "host_events": events,
         "queries": len(stream), "completed": len(ok), "failed": len(stream) - len(ok),
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
         "p999_ms": float(np.percentile(lat, 99.9)), "max_ms": float(lat.max()),
