@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -198,95 +199,157 @@ constexpr int kPqTile = 8192;  // rows per decode tile: 256 threads x one 32-row
 // ---- 1. Snappy (the format's public description: a varint length, then literal and copy
 // elements).  The element stream is sequential, but the compressor works on 64 KB fragments of
 // its input and no match reaches back past its fragment's start, so a page of N fragments is N
-// independent decodes once their starts in the stream are known: one thread walks the element
-// headers (no bytes copied) to find them, then one thread per fragment decodes it, reading the
-// source through a shared-memory window.  A page whose elements cross a fragment boundary, or
-// whose matches reach into an earlier fragment, is decoded by one thread from start to end.
+// independent decodes once their starts in the stream are known.
+//
+// Both passes read the stream through a shared-memory window of kSnapWin bytes and first parse,
+// with all 32 lanes, the element header that WOULD start at every byte of the window (its size
+// with a literal's bytes, and its output length); following the real chain of elements through
+// the window is then one shared-memory load per element for one lane.
+//  * the walk (one warp per page) follows the chain over the whole page and records where each
+//    64 KB fragment's elements start;
+//  * the decode (one warp per fragment) takes the chain 32 elements at a time, one per lane: a
+//    prefix sum gives each element's output position, literals are copied in parallel (long ones
+//    by the whole warp), and copies run in rounds of those whose source bytes are already written.
+//    The fragment is built in shared memory and written out with 16-byte stores;
+//  * a page whose elements cross a fragment boundary, or whose copies reach into an earlier
+//    fragment, is decoded again by one thread from start to end (the serial pass), which is also
+//    the pass that reports a malformed stream.
 struct SnapJob {
     const uint8_t* src;
     uint8_t* dst;
     uint32_t src_len, dst_len;
+    uint32_t plan;   // the page's plan in the plan buffer: [mode, first element, nfrag + 1 starts]
+    uint32_t nfrag;  // 64 KB fragments of its output
 };
 constexpr uint32_t kSnapFrag = 1u << 16;  // the compressor's fragment
-constexpr int kSnapFrags = 32;            // fragments decoded at once (one thread each)
-constexpr uint32_t kSnapWin = 2048;       // each thread's source window
+constexpr uint32_t kSnapWin = 2048;       // stream bytes parsed per window
+constexpr uint32_t kSnapWinLoad = kSnapWin + 32;  // with room for the last headers' bytes
+// plan modes: 0 the length varint is malformed, 1 the serial pass decodes the page, 2 its
+// fragments decode in parallel
+constexpr uint32_t kSnapSerial = 1, kSnapSplit = 2;
+constexpr size_t kSnapFragSmem = kSnapFrag + kSnapWinLoad + kSnapWin * 2 + 32 * 4;
 
-struct SnapSrc {  // the compressed stream through a shared-memory window
-    const uint8_t* src;
-    uint32_t len;
-    uint8_t* win;
-    int64_t wbase = 0, wend = 0;  // the window holds src[wbase, wend) (wbase may be below 0)
-    // 16-byte loads from the boundary at or below p, up to the stream's end (the buffer is padded:
-    // the last load may pass that end by 15 bytes)
-    __device__ void fill(uint32_t p) {
-        const uintptr_t a = (uintptr_t)(src + p);
-        const uint4* v = (const uint4*)(a & ~(uintptr_t)15);
-        const int64_t lead = (int64_t)(a & 15);
-        const uint64_t need = ((uint64_t)(len - p) + (uint64_t)lead + 15) / 16;
-        const uint32_t nvec = (uint32_t)(need < kSnapWin / 16 ? need : kSnapWin / 16);
-        for (uint32_t i = 0; i < nvec; i += 4) {  // 4 loads in flight, then their stores
-            uint4 r[4];
-#pragma unroll
-            for (uint32_t k = 0; k < 4; k++)
-                if (i + k < nvec) r[k] = __ldg(v + i + k);
-#pragma unroll
-            for (uint32_t k = 0; k < 4; k++)
-                if (i + k < nvec) ((uint4*)win)[i + k] = r[k];
-        }
-        wbase = (int64_t)p - lead;
-        wend = wbase + 16 * (int64_t)nvec;
-    }
-    __device__ uint32_t at(uint32_t p) {  // p < len
-        if ((int64_t)p < wbase || (int64_t)p >= wend) fill(p);
-        return win[(int64_t)p - wbase];
-    }
-};
-
-// One element's header at `pos` (pos < end): kind (0 literal, 1 copy), length, copy offset, and
-// the position of the element's data (a literal's bytes) or of the next element.
-__device__ bool snap_element(SnapSrc& S, uint32_t& pos, uint32_t end, uint32_t& kind, uint32_t& len, uint32_t& off) {
-    const uint32_t tag = S.at(pos++), t = tag & 3;
+// One element header at s[0..avail): its size h (tag plus length or offset bytes), kind (0
+// literal, 1 copy), output length and copy offset; false if it does not fit in `avail`.
+__device__ __forceinline__ bool snap_hdr(const uint8_t* s, uint32_t avail, uint32_t& h, uint32_t& kind,
+                                         uint32_t& len, uint32_t& off) {
+    if (avail == 0) return false;
+    const uint32_t tag = s[0], t = tag & 3;
     off = 0;
     if (t == 0) {
         kind = 0;
         len = tag >> 2;
+        h = 1;
         if (len >= 60) {
             const uint32_t nb = len - 59;
-            if (nb > end - pos) return false;
+            if (nb >= avail) return false;
             len = 0;
-            for (uint32_t i = 0; i < nb; i++) len |= S.at(pos + i) << (8 * i);
-            pos += nb;
+            for (uint32_t i = 0; i < nb; i++) len |= (uint32_t)s[1 + i] << (8 * i);
+            h = 1 + nb;
         }
         len += 1;
-        return len <= end - pos;
+        return len != 0 && len <= avail - h;  // 0: a four-byte length of 2^32
     }
     kind = 1;
     if (t == 1) {
-        if (pos >= end) return false;
+        if (avail < 2) return false;
+        h = 2;
         len = 4 + ((tag >> 2) & 7);
-        off = ((tag >> 5) << 8) | S.at(pos++);
+        off = ((tag >> 5) << 8) | s[1];
     } else {
         const uint32_t nb = t == 2 ? 2 : 4;
-        if (nb > end - pos) return false;
+        if (avail < 1 + nb) return false;
+        h = 1 + nb;
         len = (tag >> 2) + 1;
-        for (uint32_t i = 0; i < nb; i++) off |= S.at(pos + i) << (8 * i);
-        pos += nb;
+        for (uint32_t i = 0; i < nb; i++) off |= (uint32_t)s[1 + i] << (8 * i);
     }
     return true;
 }
 
-// Decode the elements in [pos, end) into dst[out, out_end); copies may not reach below `floor`.
-__device__ bool snap_decode(SnapSrc& S, uint32_t pos, uint32_t end, uint8_t* dst, uint32_t out, uint32_t out_end,
-                            uint32_t floor) {
+// The warp loads src[base, base + kSnapWinLoad) into `win`, base being the 16-byte boundary at or
+// below pos (it may lie before the stream: those bytes are not used), 16 bytes per lane-load,
+// stopping at the first boundary at or past `len` (the chunk buffer is padded past its end).
+// Returns base (as a stream offset) and the bytes loaded.
+__device__ __forceinline__ int64_t snap_load(const uint8_t* src, uint32_t len, uint32_t pos, uint8_t* win,
+                                             uint32_t& loaded) {
+    const uintptr_t a = (uintptr_t)(src + pos);
+    const uint4* v = (const uint4*)(a & ~(uintptr_t)15);
+    const int64_t base = (int64_t)pos - (int64_t)(a & 15);
+    const uint64_t need = ((uint64_t)((int64_t)len - base) + 15) / 16;
+    const uint32_t nvec = (uint32_t)(need < kSnapWinLoad / 16 ? need : kSnapWinLoad / 16);
+    const uint32_t lane = threadIdx.x & 31;
+    constexpr uint32_t kPer = (kSnapWinLoad / 16 + 31) / 32;
+    uint4 r[kPer];
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; k++)
+        if (lane + 32 * k < nvec) r[k] = __ldg(v + lane + 32 * k);
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; k++)
+        if (lane + 32 * k < nvec) ((uint4*)win)[lane + 32 * k] = r[k];
+    __syncwarp();
+    loaded = 16 * nvec;
+    return base;
+}
+
+// The record of the element that would start at window offset q (stream offset base + q):
+// walk records pack the step to the next element (header plus a literal's bytes) in bits 0-15
+// and the output length in bits 16-31; 0 = the header does not parse (or q lies before `from`);
+// a step of 0xFFFF = too long for the record: read the header again.
+__device__ __forceinline__ uint32_t snap_record(const uint8_t* win, int64_t base, uint32_t q, uint32_t from,
+                                                uint32_t end) {
+    const int64_t p = base + q;
+    if (p < (int64_t)from || p >= (int64_t)end) return 0;
+    uint32_t h, kind, len, off;
+    if (!snap_hdr(win + q, end - (uint32_t)p, h, kind, len, off)) return 0;
+    const uint64_t step = (uint64_t)h + (kind == 0 ? len : 0);
+    return step > 0xFFFE ? 0xFFFFu : (uint32_t)step | (len << 16);
+}
+
+// One thread's decode of the elements in [pos, end) into dst[out, out_end); copies may not reach
+// below `floor`.  The serial pass: source bytes come through the thread's shared-memory window.
+struct SnapSrc {
+    const uint8_t* src;
+    uint32_t len;
+    uint8_t* win;
+    int64_t wbase = 0, wend = 0;  // the window holds src[wbase, wend) (wbase may be below 0)
+    __device__ uint32_t at(uint32_t p) {  // p < len
+        if ((int64_t)p < wbase || (int64_t)p >= wend) {
+            const uintptr_t a = (uintptr_t)(src + p);
+            const uint4* v = (const uint4*)(a & ~(uintptr_t)15);
+            const int64_t lead = (int64_t)(a & 15);
+            const uint64_t need = ((uint64_t)(len - p) + (uint64_t)lead + 15) / 16;
+            const uint32_t nvec = (uint32_t)(need < kSnapWin / 16 ? need : kSnapWin / 16);
+            for (uint32_t i = 0; i < nvec; i += 4) {  // 4 loads in flight, then their stores
+                uint4 r[4];
+#pragma unroll
+                for (uint32_t k = 0; k < 4; k++)
+                    if (i + k < nvec) r[k] = __ldg(v + i + k);
+#pragma unroll
+                for (uint32_t k = 0; k < 4; k++)
+                    if (i + k < nvec) ((uint4*)win)[i + k] = r[k];
+            }
+            wbase = (int64_t)p - lead;
+            wend = wbase + 16 * (int64_t)nvec;
+        }
+        return win[(int64_t)p - wbase];
+    }
+};
+
+__device__ bool snap_decode_serial(SnapSrc& S, uint32_t pos, uint32_t end, uint8_t* dst, uint32_t out_end) {
+    uint32_t out = 0;
     while (out < out_end) {
         if (pos >= end) return false;
-        uint32_t kind, len, off;
-        if (!snap_element(S, pos, end, kind, len, off) || len > out_end - out) return false;
+        uint8_t hb[5];
+        const uint32_t avail = end - pos, nh = avail < 5 ? avail : 5;
+        for (uint32_t i = 0; i < nh; i++) hb[i] = (uint8_t)S.at(pos + i);
+        uint32_t h, kind, len, off;
+        if (!snap_hdr(hb, avail, h, kind, len, off) || len > out_end - out) return false;
+        pos += h;
         if (kind == 0) {
             for (uint32_t i = 0; i < len; i++) dst[out + i] = (uint8_t)S.at(pos + i);
             pos += len;
         } else {
-            if (off == 0 || off > out - floor) return false;
+            if (off == 0 || off > out) return false;
             for (uint32_t i = 0; i < len; i++) dst[out + i] = dst[out + i - off];  // may overlap itself
         }
         out += len;
@@ -294,73 +357,254 @@ __device__ bool snap_decode(SnapSrc& S, uint32_t pos, uint32_t end, uint8_t* dst
     return pos == end;
 }
 
-// The header walk, one block (one working thread) per page: the page's mode (0 malformed, 1 one
-// thread decodes it, 2 its fragments decode in parallel) and, for mode 2, where each fragment's
-// elements start (plan: [mode, first element, fragment starts..., stream end], kSnapFrags + 3).
-__global__ void __launch_bounds__(32) k_pq_snappy_walk(const SnapJob* jobs, int njobs, uint32_t* plan) {
-    __shared__ __align__(16) uint8_t win[kSnapWin + 16];
-    if (blockIdx.x >= (unsigned)njobs || threadIdx.x) return;
+// The walk, one warp per page: the page's mode and, for a split page, where each fragment's
+// elements start (plan: [mode, first element, nfrag fragment starts, stream end]).
+__global__ void __launch_bounds__(32) k_pq_snappy_walk(const SnapJob* jobs, uint32_t* plan) {
+    __shared__ __align__(16) uint8_t win[kSnapWinLoad];
+    __shared__ uint32_t rec[kSnapWin];
     const SnapJob J = jobs[blockIdx.x];
-    uint32_t* pl = plan + (size_t)blockIdx.x * (kSnapFrags + 3);
-    SnapSrc S{J.src, J.src_len, win};
+    uint32_t* pl = plan + J.plan;
+    const uint32_t lane = threadIdx.x & 31;
     uint32_t start = 0, total = 0;
     bool ok = false;
     for (int shift = 0; shift < 35 && start < J.src_len; shift += 7) {  // the uncompressed length
-        const uint32_t b = S.at(start++);
+        const uint32_t b = J.src[start++];
+        if (shift == 28 && (b & 0x70)) break;  // past 32 bits
         total |= (b & 0x7F) << shift;
         if (!(b & 0x80)) {
             ok = true;
             break;
         }
     }
-    uint32_t mode = ok && total == J.dst_len ? 1 : 0;
-    pl[1] = start;
-    const uint32_t nfrag = (total + kSnapFrag - 1) / kSnapFrag;
-    if (mode && nfrag > 1 && nfrag <= (uint32_t)kSnapFrags) {
-        uint32_t pos = start, out = 0;
+    uint32_t mode = ok && total == J.dst_len ? kSnapSerial : 0;
+    if (lane == 0) pl[1] = start;
+    if (mode && J.nfrag >= 1) {
         bool split = true;
-        while (split && out < total) {
-            if (out % kSnapFrag == 0) pl[2 + out / kSnapFrag] = pos;
-            if (pos >= J.src_len) {
-                split = false;
-                break;
+        if (J.nfrag > 1) {
+            uint32_t pos = start, out = 0;
+            while (split && out < total) {
+                if (pos >= J.src_len) {
+                    split = false;
+                    break;
+                }
+                uint32_t loaded;
+                const int64_t base = snap_load(J.src, J.src_len, pos, win, loaded);
+                for (uint32_t q = lane; q < kSnapWin; q += 32) rec[q] = snap_record(win, base, q, pos, J.src_len);
+                __syncwarp();
+                if (lane == 0) {  // the chain through the window
+                    uint32_t q = (uint32_t)(pos - base);
+                    while (q < kSnapWin && out < total) {
+                        if ((out & (kSnapFrag - 1)) == 0) pl[2 + (out >> 16)] = (uint32_t)(base + q);
+                        const uint32_t r = rec[q];
+                        uint32_t step = r & 0xFFFF, olen = r >> 16;
+                        if (step == 0xFFFF) {  // a long literal: its header again
+                            const uint32_t p = (uint32_t)(base + q);
+                            uint32_t h, kind, len, off;
+                            step = 0;
+                            if (snap_hdr(J.src + p, J.src_len - p, h, kind, len, off)) {
+                                step = h + (kind == 0 ? len : 0);
+                                olen = len;
+                            }
+                        }
+                        // malformed, or crossing a fragment's end: the serial pass decodes the page
+                        if (step == 0 || olen > total - out || (out & (kSnapFrag - 1)) + olen > kSnapFrag) {
+                            split = false;
+                            break;
+                        }
+                        q += step;
+                        out += olen;
+                    }
+                    pos = (uint32_t)(base + q);
+                }
+                pos = __shfl_sync(~0u, pos, 0);
+                out = __shfl_sync(~0u, out, 0);
+                split = __shfl_sync(~0u, split, 0);
+                __syncwarp();  // the window and the records are reused
             }
-            uint32_t kind, len, off;
-            if (!snap_element(S, pos, J.src_len, kind, len, off) || len > total - out) {
-                split = false;
-                break;
-            }
-            const uint32_t frag0 = out - out % kSnapFrag;
-            if ((out + len - 1) / kSnapFrag != out / kSnapFrag) split = false;  // crosses a fragment end
-            if (kind == 0) pos += len;
-            else if (off == 0 || off > out - frag0) split = false;  // reaches an earlier fragment
-            out += len;
         }
-        pl[2 + nfrag] = J.src_len;
-        if (split && out == total) mode = 2;
+        if (lane == 0) {
+            if (J.nfrag == 1) pl[2] = start;
+            pl[2 + J.nfrag] = J.src_len;
+        }
+        if (split) mode = kSnapSplit;
     }
-    pl[0] = mode;
+    if (lane == 0) pl[0] = mode;
 }
 
-// The decode, one block (one working thread) per page and fragment.
-__global__ void __launch_bounds__(32) k_pq_snappy(const SnapJob* jobs, int njobs, const uint32_t* plan, uint32_t* err) {
-    __shared__ __align__(16) uint8_t win[kSnapWin + 16];
-    const int page = blockIdx.x / kSnapFrags, frag = blockIdx.x % kSnapFrags;
-    if (page >= njobs || threadIdx.x) return;
-    const SnapJob J = jobs[page];
-    const uint32_t* pl = plan + (size_t)page * (kSnapFrags + 3);
-    SnapSrc S{J.src, J.src_len, win};
-    bool ok = true;
-    if (pl[0] == 2) {
-        const uint32_t nfrag = (J.dst_len + kSnapFrag - 1) / kSnapFrag;
-        if ((uint32_t)frag < nfrag) {
-            const uint32_t o0 = frag * kSnapFrag, o1 = min(J.dst_len, o0 + kSnapFrag);
-            ok = snap_decode(S, pl[2 + frag], pl[3 + frag], J.dst, o0, o1, o0);
+// A literal longer than a lane's share, by the whole warp: aligned 16-byte loads from the stream,
+// bytes stored into the fragment (the loads may pass the literal's ends by 15 bytes, inside the
+// padded chunk buffer).
+__device__ __forceinline__ void snap_warp_copy(const uint8_t* src, uint32_t len, uint8_t* dst) {
+    const uintptr_t a = (uintptr_t)src;
+    const uint4* v = (const uint4*)(a & ~(uintptr_t)15);
+    const int32_t lead = (int32_t)(a & 15);
+    const uint32_t nvec = ((uint32_t)lead + len + 15) / 16;
+    const uint32_t lane = threadIdx.x & 31;
+    auto put = [&](const uint4& r, uint32_t i) {
+        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int b = 0; b < 16; b++) {
+            const int32_t idx = (int32_t)(16 * i) + b - lead;
+            if (idx >= 0 && (uint32_t)idx < len) dst[idx] = (uint8_t)(w[b >> 2] >> (8 * (b & 3)));
         }
-    } else if (frag == 0) {
-        ok = pl[0] == 1 && snap_decode(S, pl[1], J.src_len, J.dst, 0, J.dst_len, 0);
+    };
+    for (uint32_t i = lane; i < nvec; i += 64) {
+        const uint4 r0 = __ldg(v + i);
+        const bool two = i + 32 < nvec;
+        uint4 r1 = r0;
+        if (two) r1 = __ldg(v + i + 32);
+        put(r0, i);
+        if (two) put(r1, i + 32);
     }
-    if (!ok) atomicOr(err, PQ_ERR_SNAPPY);
+}
+
+// One copy element by one lane: o[at, at + len) from o[at - off, ...), the source bytes read as the
+// repeating pattern o[at - off, at) (what a byte-by-byte copy of an overlapping match produces), so
+// the loads never depend on this copy's stores.
+__device__ __forceinline__ void snap_copy(uint8_t* o, uint32_t at, uint32_t off, uint32_t len) {
+    const uint8_t* s = o + at - off;
+    uint32_t j = 0;
+    for (uint32_t i = 0; i < len; i += 8) {
+        uint8_t t[8];
+#pragma unroll
+        for (uint32_t k = 0; k < 8; k++) {
+            t[k] = i + k < len ? s[j] : 0;
+            j = j + 1 == off ? 0 : j + 1;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < 8; k++)
+            if (i + k < len) o[at + i + k] = t[k];
+    }
+}
+
+// The decode, one warp per fragment of a split page (frags[i] = {page, fragment}); a fragment that
+// does not decode as a unit hands its page to the serial pass.
+__global__ void __launch_bounds__(32) k_pq_snappy_frag(const SnapJob* jobs, const uint2* frags, uint32_t* plan) {
+    extern __shared__ __align__(16) uint8_t snap_smem[];
+    uint8_t* o = snap_smem;                                    // the fragment, kSnapFrag bytes
+    uint8_t* win = o + kSnapFrag;                              // the stream window
+    uint16_t* rec = (uint16_t*)(win + kSnapWinLoad);           // steps to the next element
+    uint32_t* list = (uint32_t*)(rec + kSnapWin);              // a batch's element starts
+    const uint2 f = frags[blockIdx.x];
+    const SnapJob J = jobs[f.x];
+    uint32_t* pl = plan + J.plan;
+    if (pl[0] != kSnapSplit) return;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t o0 = f.y * kSnapFrag, n = min(J.dst_len - o0, kSnapFrag);
+    uint32_t pos = pl[2 + f.y], out = 0;
+    const uint32_t end = pl[3 + f.y];
+    bool ok = true;
+    while (ok && out < n) {
+        if (pos >= end) {
+            ok = false;
+            break;
+        }
+        uint32_t loaded;
+        const int64_t base = snap_load(J.src, end, pos, win, loaded);
+        for (uint32_t q = lane; q < kSnapWin; q += 32) rec[q] = (uint16_t)(snap_record(win, base, q, pos, end) & 0xFFFF);
+        __syncwarp();
+        uint32_t q0 = (uint32_t)(pos - base);
+        while (ok && out < n && q0 < kSnapWin && base + q0 < end) {
+            uint32_t m = 0;
+            if (lane == 0) {  // up to 32 elements of the chain
+                uint32_t q = q0;
+                while (m < 32 && q < kSnapWin && base + q < end) {
+                    const uint32_t r = rec[q];
+                    list[m++] = q;
+                    if (r == 0 || r == 0xFFFF) break;  // its lane reads the header (or finds it malformed)
+                    q += r;
+                }
+            }
+            m = __shfl_sync(~0u, m, 0);
+            __syncwarp();
+            uint32_t h = 0, kind = 0, len = 0, off = 0, q = 0;
+            bool good = true;
+            if (lane < m) {
+                q = list[lane];
+                good = snap_hdr(win + q, end - (uint32_t)(base + q), h, kind, len, off);
+            }
+            // output positions: the exclusive prefix sum of the lengths
+            const uint32_t x = lane < m && good ? len : 0;
+            uint32_t incl = x;
+#pragma unroll
+            for (uint32_t d = 1; d < 32; d <<= 1) {
+                const uint32_t t = __shfl_up_sync(~0u, incl, d);
+                if (lane >= d) incl += t;
+            }
+            const uint32_t my = out + incl - x;
+            if (lane < m && good) {
+                if (my > n || len > n - my) good = false;
+                else if (kind == 1 && (off == 0 || off > my)) good = false;  // before the fragment
+            }
+            if (__any_sync(~0u, lane < m && !good)) {
+                ok = false;
+                break;
+            }
+            // literals: short ones by their lane, long ones by the whole warp
+            const uint32_t lit = (uint32_t)(base + q) + h;  // stream offset of a literal's bytes
+            const bool is_lit = lane < m && kind == 0;
+            if (is_lit && len <= 32) {
+                if ((int64_t)lit - base + len <= (int64_t)loaded) {
+                    const uint8_t* s = win + (lit - base);
+                    for (uint32_t i = 0; i < len; i++) o[my + i] = s[i];
+                } else {
+                    for (uint32_t i = 0; i < len; i++) o[my + i] = __ldg(J.src + lit + i);
+                }
+            }
+            uint32_t longs = __ballot_sync(~0u, is_lit && len > 32);
+            while (longs) {
+                const uint32_t l = __ffs(longs) - 1;
+                longs &= longs - 1;
+                const uint32_t ls = __shfl_sync(~0u, lit, l), ll = __shfl_sync(~0u, len, l), lo = __shfl_sync(~0u, my, l);
+                snap_warp_copy(J.src + ls, ll, o + lo);
+            }
+            __syncwarp();
+            // copies in rounds: a copy runs once every byte it reads is written, i.e. its source
+            // ends at or before the output position of the earliest copy still waiting
+            uint32_t pend = __ballot_sync(~0u, lane < m && kind == 1);
+            const uint32_t need = kind == 1 ? (off >= len ? my - off + len : my) : 0;
+            while (pend) {
+                const uint32_t lim = __shfl_sync(~0u, my, __ffs(pend) - 1);
+                const uint32_t ready = pend & __ballot_sync(~0u, need <= lim);
+                if ((ready >> lane) & 1) snap_copy(o, my, off, len);
+                __syncwarp();
+                pend &= ~ready;
+            }
+            // the next batch starts after the last element
+            const uint32_t nxt = (uint32_t)(base + q) + h + (kind == 0 ? len : 0);
+            pos = __shfl_sync(~0u, nxt, m - 1);
+            out += __shfl_sync(~0u, incl, 31);
+            q0 = (uint32_t)(pos - base);
+        }
+        __syncwarp();  // the window and the records are reused
+    }
+    if (ok && pos != end) ok = false;
+    if (!ok) {
+        if (lane == 0) atomicExch(pl, kSnapSerial);
+        return;
+    }
+    __syncwarp();
+    uint8_t* d = J.dst + o0;
+    if (((uintptr_t)d & 15) == 0) {
+        const uint32_t nv = n / 16;
+        for (uint32_t i = lane; i < nv; i += 32) ((uint4*)d)[i] = ((const uint4*)o)[i];
+        for (uint32_t i = 16 * nv + lane; i < n; i += 32) d[i] = o[i];
+    } else {
+        for (uint32_t i = lane; i < n; i += 32) d[i] = o[i];
+    }
+}
+
+// The serial pass, one thread per page not decoded by fragments: it decodes the page from start
+// to end or reports it malformed.
+__global__ void __launch_bounds__(32) k_pq_snappy_serial(const SnapJob* jobs, const uint32_t* plan, uint32_t* err) {
+    __shared__ __align__(16) uint8_t win[kSnapWin + 16];
+    if (threadIdx.x) return;
+    const SnapJob J = jobs[blockIdx.x];
+    const uint32_t* pl = plan + J.plan;
+    const uint32_t mode = pl[0];
+    if (mode == kSnapSplit) return;
+    SnapSrc S{J.src, J.src_len, win};
+    if (mode != kSnapSerial || !snap_decode_serial(S, pl[1], J.src_len, J.dst, J.dst_len)) atomicOr(err, PQ_ERR_SNAPPY);
 }
 
 // ---- 2. page layout and RLE / bit-packed hybrid run tables -----------------------------------
@@ -982,6 +1226,8 @@ extern "C" int ml_gpu_parquet_decode(ml_ctx* ctx, const uint8_t* chunk, int64_t 
     const uint8_t* dc = dchunk.get<uint8_t>();
     uint8_t* up = upages.get<uint8_t>();
     std::vector<SnapJob> jobs;
+    std::vector<uint2> frags;  // {page, fragment} per 64 KB of Snappy output
+    uint32_t plan_words = 0;
     for (size_t i = 0; i < pages.size(); i++) {
         const Page& pg = pages[i];
         const bool v2 = pg.type == PAGE_DATA_V2;
@@ -989,8 +1235,12 @@ extern "C" int ml_gpu_parquet_decode(ml_ctx* ctx, const uint8_t* chunk, int64_t 
         if (lv) CK(cudaMemcpyAsync(up + uoff[i], dc + pg.payload, (size_t)lv, cudaMemcpyDeviceToDevice, s));
         const bool compressed = codec == ML_PQ_CODEC_SNAPPY && (!v2 || pg.v2_compressed);
         if (compressed) {
-            jobs.push_back(SnapJob{dc + pg.payload + lv, up + uoff[i] + lv, (uint32_t)(pg.compressed - lv),
-                                   (uint32_t)(pg.uncompressed - lv)});
+            const uint32_t dlen = (uint32_t)(pg.uncompressed - lv);
+            const uint32_t nfrag = (uint32_t)(((uint64_t)dlen + kSnapFrag - 1) / kSnapFrag);
+            for (uint32_t k = 0; k < nfrag; k++) frags.push_back(uint2{(uint32_t)jobs.size(), k});
+            jobs.push_back(SnapJob{dc + pg.payload + lv, up + uoff[i] + lv, (uint32_t)(pg.compressed - lv), dlen,
+                                   plan_words, nfrag});
+            plan_words += nfrag + 3;
         } else {
             if (pg.compressed != pg.uncompressed) raise(ML_ERR_INVALID, "parquet: an uncompressed page changes size");
             if (pg.compressed > lv)
@@ -1002,13 +1252,25 @@ extern "C" int ml_gpu_parquet_decode(ml_ctx* ctx, const uint8_t* chunk, int64_t 
     uint32_t* derr = err.get<uint32_t>();
     DevBuf dj, splan;  // read by the Snappy kernels: live to the end of the call
     if (!jobs.empty()) {
-        dj = DevBuf(ctx, jobs.size() * sizeof(SnapJob), nullptr);
-        CK(cudaMemcpyAsync(dj.get(), jobs.data(), jobs.size() * sizeof(SnapJob), cudaMemcpyHostToDevice, s));
-        const int nj = (int)jobs.size();
-        splan = DevBuf(ctx, (size_t)nj * (kSnapFrags + 3) * 4, nullptr);
-        k_pq_snappy_walk<<<nj, 32, 0, s>>>(dj.get<SnapJob>(), nj, splan.get<uint32_t>());
-        k_pq_snappy<<<nj * kSnapFrags, 32, 0, s>>>(dj.get<SnapJob>(), nj, splan.get<uint32_t>(), derr);
-        ctx->count_launch(2);
+        // the jobs and the fragment table in one upload
+        const size_t jb = jobs.size() * sizeof(SnapJob), fb = frags.size() * sizeof(uint2);
+        std::vector<uint8_t> hj(jb + fb);
+        std::memcpy(hj.data(), jobs.data(), jb);
+        if (fb) std::memcpy(hj.data() + jb, frags.data(), fb);
+        dj = DevBuf(ctx, hj.size(), nullptr);
+        CK(cudaMemcpyAsync(dj.get(), hj.data(), hj.size(), cudaMemcpyHostToDevice, s));
+        const SnapJob* J = dj.get<SnapJob>();
+        const uint2* F = (const uint2*)(dj.get<uint8_t>() + jb);
+        const int nj = (int)jobs.size(), nf = (int)frags.size();
+        splan = DevBuf(ctx, (size_t)plan_words * 4, nullptr);
+        static std::once_flag smem_once;
+        std::call_once(smem_once, [] {
+            CK(cudaFuncSetAttribute(k_pq_snappy_frag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSnapFragSmem));
+        });
+        k_pq_snappy_walk<<<nj, 32, 0, s>>>(J, splan.get<uint32_t>());
+        if (nf) k_pq_snappy_frag<<<nf, 32, kSnapFragSmem, s>>>(J, F, splan.get<uint32_t>());
+        k_pq_snappy_serial<<<nj, 32, 0, s>>>(J, splan.get<uint32_t>(), derr);
+        ctx->count_launch(nf ? 3 : 2);
         // wait here: a long Snappy kernel with the decode queued behind it holds up other calls'
         // work that shares its hardware queue (measured: 3.6 s instead of 0.9 s for 960 chunks
         // decoded from 16 threads)

@@ -188,3 +188,85 @@ def test_filter_groupby_from_a_parquet_file(ctx, tmp_path):
     assert arr[0].encoding == abi.ENC_DICT and arr[0].dict_len == 3
     for m in morsels:
         m.close()
+
+
+def test_pages_of_many_fragments(ctx, tmp_path):
+    """1 MB pages (16 fragments of Snappy output each): incompressible values (64 KB literals),
+    long runs (copies overlapping themselves, each depending on the one before), dictionary pages
+    of 100k+ distinct doubles, and strings of random letters (short literals and copies)."""
+    import pyarrow as pa
+    rng = np.random.default_rng(21)
+    n = 400_000
+    valid = rng.random(n) > 0.05
+    letters = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz", dtype=np.uint8)
+    txt = [bytes(letters[rng.integers(0, 26, k)]).decode() if ok else None
+           for k, ok in zip(rng.integers(0, 40, n), valid)]
+    t = pa.table({
+        "rnd": pa.array(rng.integers(-2**63, 2**63 - 1, n, dtype=np.int64)),
+        "runs": pa.array(np.repeat(rng.integers(0, 1 << 40, n // 2000), 2000).astype(np.int64)),
+        "price": pa.array(rng.integers(90_000, 10_500_000, n) / 100.0),
+        "txt": pa.array(txt, pa.string()),
+    })
+    p1 = str(tmp_path / "plain.parquet")
+    _write(p1, t, use_dictionary=False, compression="SNAPPY", data_page_size=1 << 20, row_group_size=n)
+    _check_file(ctx, p1)
+    p2 = str(tmp_path / "dict.parquet")
+    _write(p2, t, compression="SNAPPY", data_page_size=1 << 20, row_group_size=n // 2)
+    _check_file(ctx, p2)
+
+
+@pytest.mark.parametrize("shape", ["compressor", "literal_only", "crossing", "reaching_back", "short_literals"])
+def test_snappy_streams_of_every_shape(ctx, tmp_path, shape):
+    """The same column chunk re-compressed as Snappy streams the fragment decode cannot split
+    (elements crossing 64 KB boundaries, copies reaching into an earlier fragment), which the serial
+    pass decodes, and ones it can: every one decodes to pyarrow's values."""
+    import pyarrow as pa
+    import pyarrow.parquet as pq
+    import snappy_streams as ss
+    from minilake_b200 import gpu, parquet
+    rng = np.random.default_rng(33)
+    n = 60_000
+    v = np.where(rng.random(n) < 0.5, rng.integers(0, 50, n), rng.integers(0, 1 << 40, n)).astype(np.int64)
+    v[10_000:20_000] = 7
+    path = str(tmp_path / "u.parquet")
+    pq.write_table(pa.table({"v": pa.array(v, mask=rng.random(n) < 0.1)}), path, compression="NONE",
+                   use_dictionary=False, data_page_size=1 << 22)
+    pf = pq.ParquetFile(path)
+    meta = pf.metadata.row_group(0).column(0)
+    kw = {"compressor": {}, "literal_only": {"block": None, "matches": False}, "crossing": {"block": None},
+          "reaching_back": {"reach": 65535}, "short_literals": {"max_literal": 7}}[shape]
+    chunk = ss.recompress_chunk(parquet.chunk_bytes(path, meta), lambda b: ss.encode(b, **kw))
+    conv, scale = parquet.conversion(pf.schema.column(0))
+    got = gpu.parquet_decode(ctx, chunk, parquet.PHYSICAL["INT64"], 0, conv, scale, parquet.CODECS["SNAPPY"], n, 1)
+    want = expected_column(pf.read_row_group(0).column("v"), conv, scale)
+    h = got.fetch()[0]
+    assert np.array_equal(h.valid_mask(), want["validity"])
+    assert np.array_equal(h.values.view(np.uint64), want["values"].view(np.uint64))
+    got.close()
+
+
+def test_a_snappy_stream_of_the_wrong_length_is_refused(ctx, tmp_path):
+    import pyarrow as pa
+    import pyarrow.parquet as pq
+    import snappy_streams as ss
+    from minilake_b200 import gpu, parquet
+    n = 40_000
+    path = str(tmp_path / "u.parquet")
+    pq.write_table(pa.table({"v": np.arange(n, dtype=np.int64)}), path, compression="NONE", use_dictionary=False,
+                   data_page_size=1 << 22)
+    pf = pq.ParquetFile(path)
+    chunk = parquet.chunk_bytes(path, pf.metadata.row_group(0).column(0))
+    conv, scale = parquet.conversion(pf.schema.column(0))
+    max_def = pf.schema.column(0).max_definition_level
+    bad = [lambda b: ss.varint(len(b) + 1) + ss.encode(b)[len(ss.varint(len(b))):],   # declares a byte more
+           lambda b: ss.varint(len(b)) + ss.encode(b[:-8])[len(ss.varint(len(b) - 8)):]
+           + ss.copy(len(b), 8)]                                                     # a copy before the output
+    for f in bad:
+        with pytest.raises(gpu.MiniLakeError) as ei:
+            gpu.parquet_decode(ctx, ss.recompress_chunk(chunk, f), parquet.PHYSICAL["INT64"], 0, conv, scale,
+                               parquet.CODECS["SNAPPY"], n, max_def)
+        assert ei.value.code == abi.ERR_INVALID
+    ok = gpu.parquet_decode(ctx, ss.recompress_chunk(chunk, ss.encode), parquet.PHYSICAL["INT64"], 0, conv, scale,
+                            parquet.CODECS["SNAPPY"], n, max_def)
+    assert np.array_equal(ok.fetch()[0].values, np.arange(n, dtype=np.int64))
+    ok.close()
