@@ -643,9 +643,9 @@ std::unique_ptr<ml_batch> topn_batch(Ctx* ctx, ml_batch& b, const std::vector<So
             CK(cudaMemsetAsync(done, 0, 16, st));  // finished-CTA counter and the shared top-k threshold
         }
         KernelTimer kt(ctx, st, "topn");
-        launch_topn_warp(S, n, (int)k, nb, a.get<uint32_t>(), cand, done, final_out, st);
+        const int launched = launch_topn_warp(S, n, (int)k, nb, a.get<uint32_t>(), cand, done, final_out, st);
         kt.stop();
-        ctx->count_launch();
+        ctx->count_launch(launched);
         in = nb > 1 ? final_out : a.get<uint32_t>();
     } else {  // rounds of chunk sorts until one chunk remains
         int64_t m = n;
@@ -3126,10 +3126,10 @@ void query_enqueue(ml_query* q) {
             unsigned int* done = (unsigned int*)(base + rows_b + cand_b);
             rows = (uint32_t*)(done + 4);
             CK(cudaMemsetAsync(done, 0, 16, s));
-            launch_topn_warp(S, q->cap, (int)q->k, nb, (uint32_t*)base, base + rows_b, done, rows, s, ngd);
+            nk += launch_topn_warp(S, q->cap, (int)q->k, nb, (uint32_t*)base, base + rows_b, done, rows, s, ngd);
         } else {
             rows = (uint32_t*)base;
-            launch_topn_warp(S, q->cap, (int)q->k, nb, rows, nullptr, nullptr, nullptr, s, ngd);
+            nk += launch_topn_warp(S, q->cap, (int)q->k, nb, rows, nullptr, nullptr, nullptr, s, ngd);
         }
         // as many groups as the planned result needs (at least `limit`, or exactly the planned
         // rows), the row ids in range, then the result's columns
@@ -3146,7 +3146,7 @@ void query_enqueue(ml_query* q) {
             if (dst.validity) CK(cudaMemsetAsync(dst.validity.get(), 0, dst.validity.bytes(), s));
         }
         launch_plan_result(rows, (int)q->k, ngd, q->cap, q->k < q->limit, kGuardTopRows, kGuardRows, guard, G, s);
-        nk += 2;
+        nk += 1;
         for (size_t c = 0; c < q->outcols.size(); c++) {
             DevColumn& dst = *q->rescols[c];
             // the rows to host memory too (ml_gpu_query_run_host)

@@ -913,7 +913,9 @@ __device__ __forceinline__ int64_t total_key(double d) {
     int64_t x = __double_as_longlong(d);
     return x ^ (int64_t)(((uint64_t)(x >> 63)) >> 1);
 }
-__device__ int cmp_rows(const SortDev& S, uint32_t a, uint32_t b) {
+// Not inlined: the sorting networks call it only when two prefixes tie, and inlining it into
+// every compare-exchange multiplies their code size.
+__device__ __noinline__ int cmp_rows(const SortDev& S, uint32_t a, uint32_t b) {
     if (a == kNone || b == kNone) return (a == kNone) - (b == kNone);  // padding sorts last
     for (int k = 0; k < S.nkeys; k++) {
         const DCol& c = S.cols[k];
@@ -1031,8 +1033,12 @@ __device__ __forceinline__ TopEntry cmp_exchange(const SortDev& S, TopEntry e, i
     if (keep_min) return swap ? hi : lo;
     return swap ? lo : hi;
 }
+// The networks' loops stay rolled: these kernels run them a few times per warp from a cold
+// instruction cache, where fetching unrolled copies costs more than the loop overhead.
 __device__ __forceinline__ TopEntry warp_sort32(const SortDev& S, TopEntry e, int lane) {
+#pragma unroll 1
     for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll 1
         for (int j = k >> 1; j > 0; j >>= 1) e = cmp_exchange(S, e, lane, j, (lane & k) == 0);
     return e;
 }
@@ -1040,8 +1046,32 @@ __device__ __forceinline__ TopEntry warp_sort32(const SortDev& S, TopEntry e, in
 __device__ __forceinline__ TopEntry warp_merge32(const SortDev& S, TopEntry l, TopEntry n, int lane) {
     TopEntry rev = shfl_entry(n, 31 - lane);
     TopEntry e = entry_less(S, rev, l) ? rev : l;  // bitonic: the 32 smallest of the union
+#pragma unroll 1
     for (int j = 16; j > 0; j >>= 1) e = cmp_exchange(S, e, lane, j, true);
     return e;
+}
+
+// The qn queued entries into the warp's sorted list: a few are inserted one at a time (a ballot
+// for the position, a shuffle to move the larger entries up one lane), more are sorted in groups
+// of 32 and merged.  Queued rows are never in the list already.  One out-of-line copy serves
+// every call site (the whole warp calls it).
+__device__ __noinline__ TopEntry warp_absorb(const SortDev& S, TopEntry best, const TopEntry* queue, int qn, int lane) {
+    if (qn <= 8) {
+#pragma unroll 1
+        for (int i = 0; i < qn; i++) {
+            const TopEntry c = queue[i];
+            const int pos = __popc(__ballot_sync(0xFFFFFFFFu, entry_less(S, best, c)));
+            const TopEntry up{__shfl_up_sync(0xFFFFFFFFu, best.p, 1), __shfl_up_sync(0xFFFFFFFFu, best.r, 1)};
+            if (lane >= pos) best = lane == pos ? c : up;
+        }
+    } else {
+#pragma unroll 1
+        for (int i = 0; i < qn; i += 32) {
+            const TopEntry e = i + lane < qn ? queue[i + lane] : TopEntry{~0ull, kNone};
+            best = warp_merge32(S, best, warp_sort32(S, e, lane), lane);
+        }
+    }
+    return best;
 }
 
 // Rows that beat the warp's current k-th entry are queued in shared memory; a full queue
@@ -1056,9 +1086,9 @@ __device__ TopEntry warp_topk(const SortDev& S, int64_t n, int k, int64_t batch,
     TopEntry kth = best;
     int qn = 0;  // entries in the warp's queue (warp-uniform)
     auto flush = [&]() {
-        TopEntry e = lane < qn ? queue[lane] : TopEntry{~0ull, kNone};
         __syncwarp();
-        best = warp_merge32(S, best, warp_sort32(S, e, lane), lane);
+        best = warp_absorb(S, best, queue, qn, lane);
+        __syncwarp();
         kth = shfl_entry(best, k - 1);
         qn = 0;
     };
@@ -1097,12 +1127,76 @@ struct Quad {
     uint64_t v0, v1, v2, v3;
 };
 
+// Four consecutive rows of the key column from r0 (one or two 16-byte loads when the column is
+// aligned and the four rows exist; rows past n read as 0 and are never queued).
+template <int DT>
+__device__ __forceinline__ Quad load_quad(const DCol& c, bool vec, uint32_t n32, uint32_t r0) {
+    Quad q{0ull, 0ull, 0ull, 0ull};
+    if (vec && (uint64_t)r0 + 4u <= (uint64_t)n32) {
+        if (DT == ML_TYPE_FLOAT64 || DT == ML_TYPE_INT64) {
+            uint64_t t[2], u[2];
+            ld_stream_v2_u64((const unsigned long long*)c.data + r0, t);
+            ld_stream_v2_u64((const unsigned long long*)c.data + r0 + 2, u);
+            q = Quad{t[0], t[1], u[0], u[1]};
+        } else if (DT == ML_TYPE_BOOL) {
+            const uint32_t w = ld_stream_u32((const uint8_t*)c.data + r0);
+            q = Quad{w & 0xFFu, (w >> 8) & 0xFFu, (w >> 16) & 0xFFu, w >> 24};
+        } else {
+            uint32_t w[4];
+            ld_stream_v4_u32((const uint32_t*)c.data + r0, w);
+            q = Quad{(uint64_t)(int64_t)(int32_t)w[0], (uint64_t)(int64_t)(int32_t)w[1],
+                     (uint64_t)(int64_t)(int32_t)w[2], (uint64_t)(int64_t)(int32_t)w[3]};
+        }
+    } else {
+        const uint64_t r = r0;
+        if (r < n32) q.v0 = load_value(c, r0);
+        if (r + 1u < n32) q.v1 = load_value(c, r0 + 1u);
+        if (r + 2u < n32) q.v2 = load_value(c, r0 + 2u);
+        if (r + 3u < n32) q.v3 = load_value(c, r0 + 3u);
+    }
+    return q;
+}
+
+// Queues the lane's four rows from r0 that can still be in the top k: prefix at or below
+// `bound` (the warp's k-th entry and the launch-wide threshold) and ahead of the k-th entry.
+// The queue holds (at most) 31 entries carried over plus the 128 of a half-step.
+template <int DT>
+__device__ __forceinline__ void queue_quad(const SortDev& S, const DCol& c, const Quad& q, uint32_t r0, uint32_t n32,
+                                           uint64_t flip, uint64_t nullp, uint64_t bound, TopEntry kth,
+                                           TopEntry* queue, int lane, int& qn) {
+    const uint32_t rem = r0 < n32 ? n32 - r0 : 0u;  // rows of the four that exist
+    uint32_t vb = 0xFu;
+    if (c.valid && rem) vb = (uint32_t)(__ldg(c.valid + (r0 >> 6)) >> (r0 & 63u));
+    const uint64_t p0 = fixed_prefix<DT>(q.v0, vb & 1u, flip, nullp);
+    const uint64_t p1 = fixed_prefix<DT>(q.v1, vb & 2u, flip, nullp);
+    const uint64_t p2 = fixed_prefix<DT>(q.v2, vb & 4u, flip, nullp);
+    const uint64_t p3 = fixed_prefix<DT>(q.v3, vb & 8u, flip, nullp);
+    const bool any = (rem > 0 && p0 <= bound) || (rem > 1 && p1 <= bound) || (rem > 2 && p2 <= bound) ||
+                     (rem > 3 && p3 <= bound);
+    if (!__any_sync(0xFFFFFFFFu, any)) return;
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (uint32_t j = 0; j < 4; j++) {
+        const uint64_t p = j == 0 ? p0 : j == 1 ? p1 : j == 2 ? p2 : p3;
+        const TopEntry e{p, r0 + j};
+        const bool take = rem > j && p <= bound && entry_less(S, e, kth);
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, take);
+        if (take) queue[qn + __popc(m & lt)] = e;
+        qn += __popc(m);
+    }
+}
+
 // warp_topk over the source rows when the first sort key is a fixed-width column of type DT:
-// each lane reads 4 consecutive rows (one or two 16-byte loads when the column is aligned), the
-// next 128-row chunk is loaded before the current one is compared, and a chunk is skipped unless
-// some row beats the k-th entry.  `shared_thr` (optional, starts at 0) holds ~T for the smallest
-// full-list k-th prefix T any warp of the launch has published: k rows have prefixes <= T, so a
+// 256-row steps, each lane reading 4 consecutive rows of each 128-row half (one or two 16-byte
+// loads when the column is aligned); the next step's values and the shared threshold are loaded
+// before the current step is compared, so a warp keeps 4 KB in flight.  Each half queues the
+// rows that beat the k-th entry (usually none: it costs its loads and compares), and a queue of
+// 32 or more goes into the list (warp_absorb, one out-of-line copy; the warp's state stays in
+// registers).
+// `shared_thr` (optional, starts at 0) holds ~T for the smallest full-list k-th prefix T any warp
+// of the launch has published: k rows have prefixes <= T, so a
 // row with a larger prefix cannot be in the top k and no warp queues it.
+constexpr int kTopNQueue = 160;  // 31 carried over + the 128 rows of a half-step, rounded up
 template <int DT>
 __device__ TopEntry warp_topk_fixed(const SortDev& S, int64_t n, int k, int64_t chunk, int64_t chunks, TopEntry* queue,
                                     int lane, unsigned long long* shared_thr) {
@@ -1114,10 +1208,14 @@ __device__ TopEntry warp_topk_fixed(const SortDev& S, int64_t n, int k, int64_t 
     TopEntry kth = best;
     int qn = 0;  // entries in the warp's queue (warp-uniform)
     uint64_t thr = ~0ull;
-    auto flush = [&]() {
-        TopEntry e = lane < qn ? queue[lane] : TopEntry{~0ull, kNone};
+    const Quad zero{0ull, 0ull, 0ull, 0ull};
+    int64_t base = chunk * 256;
+    Quad qa = zero, qb = zero;
+    uint64_t pc = 0;
+    auto absorb = [&]() {  // the queue into the list; publish a tighter k-th
         __syncwarp();
-        best = warp_merge32(S, best, warp_sort32(S, e, lane), lane);
+        best = warp_absorb(S, best, queue, qn, lane);
+        __syncwarp();
         kth = shfl_entry(best, k - 1);
         qn = 0;
         if (shared_thr && kth.r != kNone && kth.p < thr) {
@@ -1125,80 +1223,35 @@ __device__ TopEntry warp_topk_fixed(const SortDev& S, int64_t n, int k, int64_t 
             if (lane == 0) atomicMax(shared_thr, ~kth.p);
         }
     };
-    auto load = [&](uint32_t r0) -> Quad {
-        Quad q{0ull, 0ull, 0ull, 0ull};
-        if (vec && (uint64_t)r0 + 4u <= (uint64_t)n32) {
-            if (DT == ML_TYPE_FLOAT64 || DT == ML_TYPE_INT64) {
-                uint64_t t[2], u[2];
-                ld_stream_v2_u64((const unsigned long long*)c.data + r0, t);
-                ld_stream_v2_u64((const unsigned long long*)c.data + r0 + 2, u);
-                q = Quad{t[0], t[1], u[0], u[1]};
-            } else if (DT == ML_TYPE_BOOL) {
-                const uint32_t w = ld_stream_u32((const uint8_t*)c.data + r0);
-                q = Quad{w & 0xFFu, (w >> 8) & 0xFFu, (w >> 16) & 0xFFu, w >> 24};
-            } else {
-                uint32_t w[4];
-                ld_stream_v4_u32((const uint32_t*)c.data + r0, w);
-                q = Quad{(uint64_t)(int64_t)(int32_t)w[0], (uint64_t)(int64_t)(int32_t)w[1],
-                         (uint64_t)(int64_t)(int32_t)w[2], (uint64_t)(int64_t)(int32_t)w[3]};
-            }
-        } else {
-            const uint64_t r = r0;
-            if (r < n32) q.v0 = load_value(c, r0);
-            if (r + 1u < n32) q.v1 = load_value(c, r0 + 1u);
-            if (r + 2u < n32) q.v2 = load_value(c, r0 + 2u);
-            if (r + 3u < n32) q.v3 = load_value(c, r0 + 3u);
-        }
-        return q;
-    };
-    auto offer = [&](TopEntry e) {  // every lane of the warp calls it with one entry
-        bool take = e.r != kNone && e.p <= thr && entry_less(S, e, kth);
-        unsigned m = __ballot_sync(0xFFFFFFFFu, take);
-        if (!m) return;
-        if (qn + __popc(m) > 32) {
-            flush();
-            take = take && e.p <= thr && entry_less(S, e, kth);
-            m = __ballot_sync(0xFFFFFFFFu, take);
-        }
-        if (take) queue[qn + __popc(m & ((1u << lane) - 1))] = e;
-        qn += __popc(m);
-        __syncwarp();
-    };
-    auto process = [&](uint32_t r0, const Quad& q, uint64_t published) {
-        const uint32_t rem = r0 < n32 ? n32 - r0 : 0u;  // rows of this lane's four that exist
-        uint32_t vb = 0xFu;
-        if (c.valid && rem) vb = (uint32_t)(__ldg(c.valid + (r0 >> 6)) >> (r0 & 63u));
-        thr = ~published < thr ? ~published : thr;
-        const uint64_t bound = kth.p < thr ? kth.p : thr;
-        const uint64_t p0 = fixed_prefix<DT>(q.v0, vb & 1u, flip, nullp);
-        const uint64_t p1 = fixed_prefix<DT>(q.v1, vb & 2u, flip, nullp);
-        const uint64_t p2 = fixed_prefix<DT>(q.v2, vb & 4u, flip, nullp);
-        const uint64_t p3 = fixed_prefix<DT>(q.v3, vb & 8u, flip, nullp);
-        const bool any = (rem > 0 && p0 <= bound) || (rem > 1 && p1 <= bound) || (rem > 2 && p2 <= bound) ||
-                         (rem > 3 && p3 <= bound);
-        if (!__any_sync(0xFFFFFFFFu, any)) return;
-        offer(rem > 0 ? TopEntry{p0, r0} : TopEntry{~0ull, kNone});
-        offer(rem > 1 ? TopEntry{p1, r0 + 1u} : TopEntry{~0ull, kNone});
-        offer(rem > 2 ? TopEntry{p2, r0 + 2u} : TopEntry{~0ull, kNone});
-        offer(rem > 3 ? TopEntry{p3, r0 + 3u} : TopEntry{~0ull, kNone});
-    };
-    // the shared threshold is read together with the next chunk's values (off the critical path)
-    int64_t base = chunk * 128;
-    Quad qc{0ull, 0ull, 0ull, 0ull};
-    uint64_t pc = 0, pn = 0;
-    if (base < n) qc = load((uint32_t)base + (uint32_t)lane * 4u);
-    for (; base < n; base += chunks * 128) {
-        const int64_t next = base + chunks * 128;
-        Quad qn4{0ull, 0ull, 0ull, 0ull};
-        if (next < n) {
-            qn4 = load((uint32_t)next + (uint32_t)lane * 4u);
-            if (shared_thr) pn = __ldcg(shared_thr);
-        }
-        process((uint32_t)base + (uint32_t)lane * 4u, qc, pc);
-        qc = qn4;
-        pc = pn;
+    if (base < n) {
+        qa = load_quad<DT>(c, vec, n32, (uint32_t)base + (uint32_t)lane * 4u);
+        qb = load_quad<DT>(c, vec, n32, (uint32_t)base + 128u + (uint32_t)lane * 4u);
     }
-    if (qn) flush();
+    for (;;) {
+        const bool more = base < n;
+        if (more) {
+            const int64_t next = base + chunks * 256;
+            Quad na = zero, nb = zero;
+            uint64_t pn = pc;
+            if (next < n) {
+                na = load_quad<DT>(c, vec, n32, (uint32_t)next + (uint32_t)lane * 4u);
+                nb = load_quad<DT>(c, vec, n32, (uint32_t)next + 128u + (uint32_t)lane * 4u);
+                if (shared_thr) pn = __ldcg(shared_thr);
+            }
+            thr = ~pc < thr ? ~pc : thr;
+            queue_quad<DT>(S, c, qa, (uint32_t)base + (uint32_t)lane * 4u, n32, flip, nullp,
+                           kth.p < thr ? kth.p : thr, kth, queue, lane, qn);
+            if (qn >= 32) absorb();
+            queue_quad<DT>(S, c, qb, (uint32_t)base + 128u + (uint32_t)lane * 4u, n32, flip, nullp,
+                           kth.p < thr ? kth.p : thr, kth, queue, lane, qn);
+            qa = na;
+            qb = nb;
+            pc = pn;
+            base = next;
+        }
+        if (qn >= 32 || (!more && qn)) absorb();
+        if (!more) break;
+    }
     return best;
 }
 
@@ -1207,12 +1260,12 @@ __device__ TopEntry warp_topk_fixed(const SortDev& S, int64_t n, int k, int64_t 
 // at zero) merges all CTAs' entries into final_out[0 .. k): the whole top-k in one launch.
 // DT: the first sort key's type when it is a fixed-width column (warp_topk_fixed), -1 otherwise.
 template <int DT>
-__global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortDev S, int64_t n, int k, uint32_t* out,
+__global__ void __launch_bounds__(256, 2) k_topn_warp(const __grid_constant__ SortDev S, int64_t n, int k, uint32_t* out,
                                                    TopEntry* cand, unsigned int* done, uint32_t* final_out,
                                                    const uint64_t* n_dev) {
     if (n_dev) n = min(n, (int64_t)__ldcg(n_dev));  // a replayed plan's row count
     __shared__ TopEntry lists[8][32];
-    __shared__ TopEntry queue[8][32];
+    __shared__ TopEntry queue[8][kTopNQueue];
     __shared__ bool last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     TopEntry best;
@@ -1227,6 +1280,7 @@ __global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortD
     lists[warp][lane] = best;
     __syncthreads();
     if (warp == 0) {
+#pragma unroll 1
         for (int w = 1; w < 8; w++) best = warp_merge32(S, best, lists[w][lane], lane);
         if (lane < k) {
             out[(int64_t)blockIdx.x * k + lane] = best.r;
@@ -1242,16 +1296,48 @@ __global__ void __launch_bounds__(256) k_topn_warp(const __grid_constant__ SortD
     __threadfence();
     const int64_t m = (int64_t)gridDim.x * k;
     // k rows of some warp's full list have prefixes <= the published threshold, so a candidate
-    // above it cannot be in the top k: most CTAs' lists drop out here without a sort
+    // above it cannot be in the top k: most CTAs' lists drop out here without a sort.  Each warp
+    // loads four batches of 32 candidates at once, queues those that can be in the top k, and
+    // takes its queue into its list from one place once it holds 32 or the candidates are done.
     const uint64_t bound = thr ? ~__ldcg(thr) : ~0ull;
-    best = warp_topk(S, m, k, warp, 8, queue[warp], lane, [&](int64_t i) {
-        const TopEntry* e = cand + i;
-        const TopEntry t{__ldcg((const unsigned long long*)&e->p), __ldcg(&e->r)};
-        return t.p <= bound ? t : TopEntry{~0ull, kNone};
-    });
+    {
+        TopEntry* qw = queue[warp];
+        best = TopEntry{~0ull, kNone};
+        TopEntry kth = best;
+        int qn = 0;
+        for (int64_t b0 = (int64_t)warp * 32;; b0 += 8 * 32 * 4) {
+            const bool more = b0 < m;
+            if (more) {
+                TopEntry e[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int64_t i = b0 + j * 256 + lane;
+                    e[j] = TopEntry{~0ull, kNone};
+                    if (i < m) e[j] = TopEntry{__ldcg((const unsigned long long*)&cand[i].p), __ldcg(&cand[i].r)};
+                }
+                const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const bool take = e[j].r != kNone && e[j].p <= bound && entry_less(S, e[j], kth);
+                    const unsigned mk = __ballot_sync(0xFFFFFFFFu, take);
+                    if (take) qw[qn + __popc(mk & lt)] = e[j];
+                    qn += __popc(mk);
+                }
+            }
+            if (qn >= 32 || (!more && qn)) {
+                __syncwarp();
+                best = warp_absorb(S, best, qw, qn, lane);
+                __syncwarp();
+                kth = shfl_entry(best, k - 1);
+                qn = 0;
+            }
+            if (!more) break;
+        }
+    }
     lists[warp][lane] = best;
     __syncthreads();
     if (warp == 0) {
+#pragma unroll 1
         for (int w = 1; w < 8; w++) best = warp_merge32(S, best, lists[w][lane], lane);
         if (lane < k) final_out[lane] = best.r;
     }
@@ -1537,8 +1623,8 @@ int topn_warp_blocks(int64_t n) {
     return (int)std::max<int64_t>(1, std::min(want, cap));
 }
 size_t topn_entry_bytes() { return sizeof(TopEntry); }
-void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* out, void* cand, unsigned int* done,
-                      uint32_t* final_out, cudaStream_t s, const uint64_t* n_dev) {
+int launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* out, void* cand, unsigned int* done,
+                     uint32_t* final_out, cudaStream_t s, const uint64_t* n_dev) {
     const DCol& c = S.cols[0];
     const int dt = S.nkeys > 0 && c.kind == CK_FIXED && c.src == 0 ? c.dt : -1;
     TopEntry* ce = (TopEntry*)cand;
@@ -1550,6 +1636,7 @@ void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* 
         case ML_TYPE_BOOL: k_topn_warp<ML_TYPE_BOOL><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out, n_dev); break;
         default: k_topn_warp<-1><<<blocks, 256, 0, s>>>(S, n, k, out, ce, done, final_out, n_dev); break;
     }
+    return 1;
 }
 // The packed words of string MIN/MAX states (A_MIN_STR / A_MAX_STR) after the rank table
 // changed: each holds a string id in its low half; the identities (no value yet) stay.

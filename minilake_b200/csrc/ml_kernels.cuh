@@ -144,9 +144,10 @@ int topn_warp_blocks(int64_t n);
 // bytes: the finished-CTA counter and the launch's shared top-k threshold), the last CTA merges
 // every CTA's candidates into final_out[0 .. k): one launch.
 size_t topn_entry_bytes();
-// n_dev (optional): a device-side row count (at most n) read by the kernel.
-void launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* out, void* cand, unsigned int* done,
-                      uint32_t* final_out, cudaStream_t s, const uint64_t* n_dev = nullptr);
+// n_dev (optional): a device-side row count (at most n) read by the kernel.  Returns the
+// kernels launched.
+int launch_topn_warp(const SortDev& S, int64_t n, int k, int blocks, uint32_t* out, void* cand, unsigned int* done,
+                     uint32_t* final_out, cudaStream_t s, const uint64_t* n_dev = nullptr);
 
 // String MIN/MAX states of groups [0, ngroups): new ranks from `rank` for the packed words at
 // the listed block offsets (the rank table changed when new strings were interned).
