@@ -205,8 +205,9 @@ constexpr int kPqTile = 8192;  // rows per decode tile: 256 threads x one 32-row
 // with all 32 lanes, the element header that WOULD start at every byte of the window (its size
 // with a literal's bytes, and its output length); following the real chain of elements through
 // the window is then one shared-memory load per element for one lane.
-//  * the walk (one warp per page) follows the chain over the whole page and records where each
-//    64 KB fragment's elements start;
+//  * the walk (one warp per page) follows the chain over the whole page, one lane listing each
+//    window's element starts through next-element records, then all lanes sum the listed
+//    elements' output lengths and record where each 64 KB fragment's elements start;
 //  * the decode (one warp per fragment) takes the chain 32 elements at a time, one per lane: a
 //    prefix sum gives each element's output position, literals are copied in parallel (long ones
 //    by the whole warp), and copies run in rounds of those whose source bytes are already written.
@@ -292,9 +293,9 @@ __device__ __forceinline__ int64_t snap_load(const uint8_t* src, uint32_t len, u
 }
 
 // The record of the element that would start at window offset q (stream offset base + q):
-// walk records pack the step to the next element (header plus a literal's bytes) in bits 0-15
-// and the output length in bits 16-31; 0 = the header does not parse (or q lies before `from`);
-// a step of 0xFFFF = too long for the record: read the header again.
+// the step to the next element (header plus a literal's bytes) in bits 0-15 and the output
+// length in bits 16-31 (the fragment decode keeps the step); 0 = the header does not parse (or q
+// lies before `from`); a step of 0xFFFF = too long for the record: read the header again.
 __device__ __forceinline__ uint32_t snap_record(const uint8_t* win, int64_t base, uint32_t q, uint32_t from,
                                                 uint32_t end) {
     const int64_t p = base + q;
@@ -357,11 +358,37 @@ __device__ bool snap_decode_serial(SnapSrc& S, uint32_t pos, uint32_t end, uint8
     return pos == end;
 }
 
+// The walk's record for window offset q (stream offset base + q): the window offset of the next
+// element if an element started at q (q + its header + a literal's bytes), or kSnapNone when no
+// element can start there (the header or the literal runs past `end`, or q lies before `from`).
+// Branch-free: the five bytes a header can span are read at once and every form is computed.
+constexpr uint32_t kSnapNone = 0xFFFFFFFFu;
+__device__ __forceinline__ uint32_t snap_next(const uint8_t* win, int64_t base, uint32_t q, uint32_t from,
+                                              uint32_t end) {
+    const int64_t p = base + q;
+    const int64_t avail = (int64_t)end - p;
+    const uint32_t b0 = win[q], b1 = win[q + 1], b2 = win[q + 2], b3 = win[q + 3], b4 = win[q + 4];
+    const uint32_t t = b0 & 3, l6 = b0 >> 2;
+    const uint32_t nb = l6 >= 60 ? l6 - 59 : 0;  // a literal's length bytes
+    const uint32_t ext = b1 | (nb >= 2 ? b2 << 8 : 0u) | (nb >= 3 ? b3 << 16 : 0u) | (nb >= 4 ? b4 << 24 : 0u);
+    const uint64_t len = (uint64_t)(nb ? ext : l6) + 1;  // a literal's bytes (up to 2^32)
+    const uint64_t step = t == 0 ? 1 + nb + len : t == 1 ? 2 : t == 2 ? 3 : 5;
+    const bool ok = p >= (int64_t)from && avail > 0 && (int64_t)step <= avail && step < (1ull << 31);
+    return ok ? q + (uint32_t)step : kSnapNone;
+}
+
 // The walk, one warp per page: the page's mode and, for a split page, where each fragment's
-// elements start (plan: [mode, first element, nfrag fragment starts, stream end]).
+// elements start (plan: [mode, first element, nfrag fragment starts, stream end]).  Per window:
+// all lanes build the next-element records; one lane follows the chain, listing the element
+// starts (one shared-memory load per element); then all lanes read the listed headers' output
+// lengths, prefix-sum them, record each fragment's first element and check that no element
+// crosses a fragment boundary.
+constexpr uint32_t kSnapList = kSnapWin / 2 + 1;  // elements in a window (each spans >= 2 bytes)
 __global__ void __launch_bounds__(32) k_pq_snappy_walk(const SnapJob* jobs, uint32_t* plan) {
     __shared__ __align__(16) uint8_t win[kSnapWinLoad];
-    __shared__ uint32_t rec[kSnapWin];
+    __shared__ uint32_t nxt[kSnapWin];
+    __shared__ uint16_t list[kSnapList];
+    __shared__ uint32_t olen[kSnapList];
     const SnapJob J = jobs[blockIdx.x];
     uint32_t* pl = plan + J.plan;
     const uint32_t lane = threadIdx.x & 31;
@@ -389,36 +416,65 @@ __global__ void __launch_bounds__(32) k_pq_snappy_walk(const SnapJob* jobs, uint
                 }
                 uint32_t loaded;
                 const int64_t base = snap_load(J.src, J.src_len, pos, win, loaded);
-                for (uint32_t q = lane; q < kSnapWin; q += 32) rec[q] = snap_record(win, base, q, pos, J.src_len);
+#pragma unroll 4
+                for (uint32_t q = lane; q < kSnapWin; q += 32) nxt[q] = snap_next(win, base, q, pos, J.src_len);
                 __syncwarp();
-                if (lane == 0) {  // the chain through the window
+                uint32_t m = 0, qe = 0;
+                if (lane == 0) {  // the chain through the window, up to the stream's end
+                    const int64_t rest = (int64_t)J.src_len - base;
+                    const uint32_t qlim = rest < (int64_t)kSnapWin ? (uint32_t)rest : kSnapWin;
                     uint32_t q = (uint32_t)(pos - base);
-                    while (q < kSnapWin && out < total) {
-                        if ((out & (kSnapFrag - 1)) == 0) pl[2 + (out >> 16)] = (uint32_t)(base + q);
-                        const uint32_t r = rec[q];
-                        uint32_t step = r & 0xFFFF, olen = r >> 16;
-                        if (step == 0xFFFF) {  // a long literal: its header again
-                            const uint32_t p = (uint32_t)(base + q);
-                            uint32_t h, kind, len, off;
-                            step = 0;
-                            if (snap_hdr(J.src + p, J.src_len - p, h, kind, len, off)) {
-                                step = h + (kind == 0 ? len : 0);
-                                olen = len;
-                            }
-                        }
-                        // malformed, or crossing a fragment's end: the serial pass decodes the page
-                        if (step == 0 || olen > total - out || (out & (kSnapFrag - 1)) + olen > kSnapFrag) {
-                            split = false;
-                            break;
-                        }
-                        q += step;
-                        out += olen;
+                    while (q < qlim) {
+                        list[m++] = (uint16_t)q;
+                        q = nxt[q];
                     }
-                    pos = (uint32_t)(base + q);
+                    qe = q;
                 }
-                pos = __shfl_sync(~0u, pos, 0);
-                out = __shfl_sync(~0u, out, 0);
-                split = __shfl_sync(~0u, split, 0);
+                m = __shfl_sync(~0u, m, 0);
+                qe = __shfl_sync(~0u, qe, 0);
+                __syncwarp();
+                // output lengths of the listed elements; a long literal's next position, which
+                // its record could not hold, comes from its header
+                const uint32_t per = (m + 31) / 32, i0 = lane * per, i1 = min(m, i0 + per);
+                uint32_t sum = 0;
+                bool bad = false;
+                for (uint32_t i = i0; i < i1; i++) {
+                    const uint32_t q = list[i];
+                    const uint32_t p = (uint32_t)(base + q);
+                    uint32_t h, kind, len, off;
+                    if (!snap_hdr(win + q, J.src_len - p, h, kind, len, off)) {
+                        bad = true;
+                        len = 0;
+                    }
+                    olen[i] = len;
+                    sum += len;
+                    if (i == m - 1 && qe == kSnapNone && !bad) qe = q + h + (kind == 0 ? len : 0);
+                }
+                // exclusive prefix of the lanes' sums
+                uint32_t incl = sum;
+#pragma unroll
+                for (uint32_t d = 1; d < 32; d <<= 1) {
+                    const uint32_t v = __shfl_up_sync(~0u, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                uint32_t o = out + incl - sum;
+                for (uint32_t i = i0; i < i1 && !bad; i++) {
+                    const uint32_t l = olen[i];
+                    if (o > total || l > total - o || (o & (kSnapFrag - 1)) + l > kSnapFrag) {
+                        bad = true;  // past the end, or crossing a fragment's end
+                        break;
+                    }
+                    if ((o & (kSnapFrag - 1)) == 0 && o < total) pl[2 + (o >> 16)] = (uint32_t)(base + list[i]);
+                    o += l;
+                }
+                qe = __shfl_sync(~0u, qe, (m - 1) / per);  // the lane that holds the last element
+                const uint32_t wsum = __shfl_sync(~0u, incl, 31);
+                if (__any_sync(~0u, bad) || qe == kSnapNone || wsum > total - out) {
+                    split = false;
+                    break;
+                }
+                out += wsum;
+                pos = (uint32_t)(base + qe);
                 __syncwarp();  // the window and the records are reused
             }
         }
