@@ -205,9 +205,10 @@ constexpr int kPqTile = 8192;  // rows per decode tile: 256 threads x one 32-row
 // with all 32 lanes, the element header that WOULD start at every byte of the window (its size
 // with a literal's bytes, and its output length); following the real chain of elements through
 // the window is then one shared-memory load per element for one lane.
-//  * the walk (one warp per page) follows the chain over the whole page, one lane listing each
-//    window's element starts through next-element records, then all lanes sum the listed
-//    elements' output lengths and record where each 64 KB fragment's elements start;
+//  * the walk (one 4-warp block per page) follows the chain over the whole page, one thread
+//    listing each window's element starts through next-element records (two elements per
+//    shared-memory round trip), then the block sums the listed elements' output lengths and
+//    records where each 64 KB fragment's elements start;
 //  * the decode (one warp per fragment) takes the chain 32 elements at a time, one per lane: a
 //    prefix sum gives each element's output position, literals are copied in parallel (long ones
 //    by the whole warp), and copies run in rounds of those whose source bytes are already written.
@@ -377,21 +378,25 @@ __device__ __forceinline__ uint32_t snap_next(const uint8_t* win, int64_t base, 
     return ok ? q + (uint32_t)step : kSnapNone;
 }
 
-// The walk, one warp per page: the page's mode and, for a split page, where each fragment's
-// elements start (plan: [mode, first element, nfrag fragment starts, stream end]).  Per window:
-// all lanes build the next-element records; one lane follows the chain, listing the element
-// starts (one shared-memory load per element); then all lanes read the listed headers' output
-// lengths, prefix-sum them, record each fragment's first element and check that no element
-// crosses a fragment boundary.
+// The walk, one 4-warp block per page: the page's mode and, for a split page, where each
+// fragment's elements start (plan: [mode, first element, nfrag fragment starts, stream end]).
+// Per window: the block builds the next-element records and, from them, the element after next;
+// one thread follows the chain two elements per shared-memory round trip, listing the element
+// starts; then the block reads the listed headers' output lengths, prefix-sums them, records each
+// fragment's first element and checks that no element crosses a fragment boundary.  Every loop
+// and barrier is block-uniform: its conditions are read from shared memory after a barrier.
 constexpr uint32_t kSnapList = kSnapWin / 2 + 1;  // elements in a window (each spans >= 2 bytes)
-__global__ void __launch_bounds__(32) k_pq_snappy_walk(const SnapJob* jobs, uint32_t* plan) {
+constexpr int kWalkThreads = 128;
+__global__ void __launch_bounds__(kWalkThreads) k_pq_snappy_walk(const SnapJob* jobs, uint32_t* plan) {
     __shared__ __align__(16) uint8_t win[kSnapWinLoad];
-    __shared__ uint32_t nxt[kSnapWin];
+    __shared__ uint32_t nxt[kSnapWin], nxt2[kSnapWin];
     __shared__ uint16_t list[kSnapList];
     __shared__ uint32_t olen[kSnapList];
+    __shared__ uint32_t wsum[kWalkThreads / 32];
+    __shared__ uint32_t sh_m, sh_qe, sh_bad;
     const SnapJob J = jobs[blockIdx.x];
     uint32_t* pl = plan + J.plan;
-    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     uint32_t start = 0, total = 0;
     bool ok = false;
     for (int shift = 0; shift < 35 && start < J.src_len; shift += 7) {  // the uncompressed length
@@ -404,38 +409,57 @@ __global__ void __launch_bounds__(32) k_pq_snappy_walk(const SnapJob* jobs, uint
         }
     }
     uint32_t mode = ok && total == J.dst_len ? kSnapSerial : 0;
-    if (lane == 0) pl[1] = start;
+    if (tid == 0) pl[1] = start;
     if (mode && J.nfrag >= 1) {
         bool split = true;
         if (J.nfrag > 1) {
-            uint32_t pos = start, out = 0;
+            uint32_t pos = start, out = 0;  // the same in every thread
             while (split && out < total) {
                 if (pos >= J.src_len) {
                     split = false;
                     break;
                 }
-                uint32_t loaded;
-                const int64_t base = snap_load(J.src, J.src_len, pos, win, loaded);
+                // the window: src[base, base + kSnapWinLoad) from the 16-byte boundary at or below pos
+                const uintptr_t a = (uintptr_t)(J.src + pos);
+                const uint4* v = (const uint4*)(a & ~(uintptr_t)15);
+                const int64_t base = (int64_t)pos - (int64_t)(a & 15);
+                const uint64_t need = ((uint64_t)((int64_t)J.src_len - base) + 15) / 16;
+                const uint32_t nvec = (uint32_t)(need < kSnapWinLoad / 16 ? need : kSnapWinLoad / 16);
+                for (uint32_t i = tid; i < nvec; i += kWalkThreads) ((uint4*)win)[i] = __ldg(v + i);
+                __syncthreads();
 #pragma unroll 4
-                for (uint32_t q = lane; q < kSnapWin; q += 32) nxt[q] = snap_next(win, base, q, pos, J.src_len);
-                __syncwarp();
-                uint32_t m = 0, qe = 0;
-                if (lane == 0) {  // the chain through the window, up to the stream's end
+                for (uint32_t q = tid; q < kSnapWin; q += kWalkThreads) nxt[q] = snap_next(win, base, q, pos, J.src_len);
+                __syncthreads();
+#pragma unroll 4
+                for (uint32_t q = tid; q < kSnapWin; q += kWalkThreads) {
+                    const uint32_t n = nxt[q];
+                    nxt2[q] = n < kSnapWin ? nxt[n] : kSnapNone;
+                }
+                __syncthreads();
+                if (tid == 0) {  // the chain through the window, up to the stream's end
                     const int64_t rest = (int64_t)J.src_len - base;
                     const uint32_t qlim = rest < (int64_t)kSnapWin ? (uint32_t)rest : kSnapWin;
-                    uint32_t q = (uint32_t)(pos - base);
+                    uint32_t q = (uint32_t)(pos - base), m = 0;
                     while (q < qlim) {
+                        const uint32_t n1 = nxt[q], n2 = nxt2[q];
                         list[m++] = (uint16_t)q;
-                        q = nxt[q];
+                        if (n1 >= qlim) {
+                            q = n1;
+                            break;
+                        }
+                        list[m++] = (uint16_t)n1;
+                        q = n2;
                     }
-                    qe = q;
+                    sh_m = m;
+                    sh_qe = q;
+                    sh_bad = 0;
                 }
-                m = __shfl_sync(~0u, m, 0);
-                qe = __shfl_sync(~0u, qe, 0);
-                __syncwarp();
-                // output lengths of the listed elements; a long literal's next position, which
-                // its record could not hold, comes from its header
-                const uint32_t per = (m + 31) / 32, i0 = lane * per, i1 = min(m, i0 + per);
+                __syncthreads();
+                const uint32_t m = sh_m;
+                uint32_t qe = sh_qe;
+                // output lengths of the listed elements (a long literal's next position, which its
+                // record could not hold, from its header), each thread a consecutive run of them
+                const uint32_t per = (m + kWalkThreads - 1) / kWalkThreads, i0 = tid * per, i1 = min(m, i0 + per);
                 uint32_t sum = 0;
                 bool bad = false;
                 for (uint32_t i = i0; i < i1; i++) {
@@ -448,16 +472,23 @@ __global__ void __launch_bounds__(32) k_pq_snappy_walk(const SnapJob* jobs, uint
                     }
                     olen[i] = len;
                     sum += len;
-                    if (i == m - 1 && qe == kSnapNone && !bad) qe = q + h + (kind == 0 ? len : 0);
+                    if (i == m - 1) sh_qe = qe == kSnapNone && !bad ? q + h + (kind == 0 ? len : 0) : qe;
                 }
-                // exclusive prefix of the lanes' sums
+                // exclusive prefix of the threads' sums: within the warp, then over the warps
                 uint32_t incl = sum;
 #pragma unroll
                 for (uint32_t d = 1; d < 32; d <<= 1) {
-                    const uint32_t v = __shfl_up_sync(~0u, incl, d);
-                    if (lane >= d) incl += v;
+                    const uint32_t t = __shfl_up_sync(~0u, incl, d);
+                    if (lane >= d) incl += t;
                 }
-                uint32_t o = out + incl - sum;
+                if (lane == 31) wsum[warp] = incl;
+                __syncthreads();
+                uint32_t before = 0, all = 0;
+                for (uint32_t w = 0; w < kWalkThreads / 32; w++) {
+                    before += w < warp ? wsum[w] : 0;
+                    all += wsum[w];
+                }
+                uint32_t o = out + before + incl - sum;
                 for (uint32_t i = i0; i < i1 && !bad; i++) {
                     const uint32_t l = olen[i];
                     if (o > total || l > total - o || (o & (kSnapFrag - 1)) + l > kSnapFrag) {
@@ -467,24 +498,26 @@ __global__ void __launch_bounds__(32) k_pq_snappy_walk(const SnapJob* jobs, uint
                     if ((o & (kSnapFrag - 1)) == 0 && o < total) pl[2 + (o >> 16)] = (uint32_t)(base + list[i]);
                     o += l;
                 }
-                qe = __shfl_sync(~0u, qe, (m - 1) / per);  // the lane that holds the last element
-                const uint32_t wsum = __shfl_sync(~0u, incl, 31);
-                if (__any_sync(~0u, bad) || qe == kSnapNone || wsum > total - out) {
+                if (bad) atomicOr(&sh_bad, 1u);
+                __syncthreads();
+                qe = sh_qe;
+                const bool stop = sh_bad || qe == kSnapNone || all > total - out;
+                __syncthreads();  // sh_* and the window are rewritten by the next window
+                if (stop) {
                     split = false;
                     break;
                 }
-                out += wsum;
+                out += all;
                 pos = (uint32_t)(base + qe);
-                __syncwarp();  // the window and the records are reused
             }
         }
-        if (lane == 0) {
+        if (tid == 0) {
             if (J.nfrag == 1) pl[2] = start;
             pl[2 + J.nfrag] = J.src_len;
         }
         if (split) mode = kSnapSplit;
     }
-    if (lane == 0) pl[0] = mode;
+    if (tid == 0) pl[0] = mode;
 }
 
 // A literal longer than a lane's share, by the whole warp: aligned 16-byte loads from the stream,
@@ -1323,7 +1356,7 @@ extern "C" int ml_gpu_parquet_decode(ml_ctx* ctx, const uint8_t* chunk, int64_t 
         std::call_once(smem_once, [] {
             CK(cudaFuncSetAttribute(k_pq_snappy_frag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSnapFragSmem));
         });
-        k_pq_snappy_walk<<<nj, 32, 0, s>>>(J, splan.get<uint32_t>());
+        k_pq_snappy_walk<<<nj, kWalkThreads, 0, s>>>(J, splan.get<uint32_t>());
         if (nf) k_pq_snappy_frag<<<nf, 32, kSnapFragSmem, s>>>(J, F, splan.get<uint32_t>());
         k_pq_snappy_serial<<<nj, 32, 0, s>>>(J, splan.get<uint32_t>(), derr);
         ctx->count_launch(nf ? 3 : 2);
