@@ -31,6 +31,15 @@ def powi(a: float, b: int) -> float:
     return 1.0 / r if recip else r
 
 
+def be_i128(b: bytes) -> int:
+    """be_i128 (parquet_reader.rs:158-168): the sign from the first byte, then the first 16 bytes
+    shifted in, the shifts wrapping at 128 bits as i128 shifts do."""
+    v = -1 if b and b[0] & 0x80 else 0
+    for x in b[:16]:
+        v = (((v << 8) | x) + (1 << 127)) % (1 << 128) - (1 << 127)
+    return v
+
+
 def encode_strings(rows):
     """encode_strings (parquet_reader.rs:176-212): ("dict", entries, codes) or ("plain", rows)."""
     n = len(rows)
