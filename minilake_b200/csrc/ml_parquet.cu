@@ -20,7 +20,6 @@
 
 #include <algorithm>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1352,10 +1351,8 @@ extern "C" int ml_gpu_parquet_decode(ml_ctx* ctx, const uint8_t* chunk, int64_t 
         const uint2* F = (const uint2*)(dj.get<uint8_t>() + jb);
         const int nj = (int)jobs.size(), nf = (int)frags.size();
         splan = DevBuf(ctx, (size_t)plan_words * 4, nullptr);
-        static std::once_flag smem_once;
-        std::call_once(smem_once, [] {
-            CK(cudaFuncSetAttribute(k_pq_snappy_frag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSnapFragSmem));
-        });
+        // per call: the attribute belongs to the current device's copy of the kernel
+        CK(cudaFuncSetAttribute(k_pq_snappy_frag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSnapFragSmem));
         k_pq_snappy_walk<<<nj, kWalkThreads, 0, s>>>(J, splan.get<uint32_t>());
         if (nf) k_pq_snappy_frag<<<nf, 32, kSnapFragSmem, s>>>(J, F, splan.get<uint32_t>());
         k_pq_snappy_serial<<<nj, 32, 0, s>>>(J, splan.get<uint32_t>(), derr);
