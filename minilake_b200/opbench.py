@@ -211,6 +211,39 @@ def run(iters: int = 5, rows_filter: int = 100_000_000, rows_join: int = 60_000_
     return {"peak_gbs": peak, "peak_kind": peak_kind, "ops": res}
 
 
+def parquet_column_chunk(column: str = "price", rows: int = 250_000, row_groups: int = 2, iters: int = 4,
+                         log=print) -> dict:
+    """One column chunk decoded alone: row group 0's chunk of `column` from configuration 0's table
+    as a seeded Snappy Parquet file (rows / row_groups rows per row group), `iters` calls of
+    ml_gpu_parquet_decode one after another; wall-clock milliseconds per call (the first call
+    includes the context's first use of each kernel)."""
+    import tempfile
+
+    import pyarrow.parquet as pq
+
+    from . import datagen, gpu, parquet
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "cfg0.parquet")
+        datagen.filter_groupby_parquet(path, rows=rows, row_groups=row_groups)
+        pf = pq.ParquetFile(path)
+        names = [pf.schema.column(i).name for i in range(len(pf.schema))]
+        md = pf.metadata.row_group(0)
+        ci = names.index(column)
+        sch, meta = pf.schema.column(ci), md.column(ci)
+        conv, scale = parquet.conversion(sch)
+        data = parquet.chunk_bytes(path, meta)
+        args = (data, parquet.PHYSICAL[sch.physical_type], sch.length or 0, conv, scale,
+                parquet.CODECS[meta.compression], md.num_rows, sch.max_definition_level)
+    ctx = gpu.Context(0)
+    times = []
+    for _ in range(iters):
+        times.append(_wall(lambda: gpu.parquet_decode(ctx, *args).close()))
+    ctx.close()
+    out = {"column": column, "rows": md.num_rows, "chunk_bytes": len(data), "ms": [round(t * 1e3, 2) for t in times]}
+    log(f"parquet_column_chunk: {out}")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--iters", type=int, default=5)
@@ -218,7 +251,11 @@ def main():
     ap.add_argument("--rows-join", type=int, default=60_000_000)
     ap.add_argument("--parquet", action="store_true", help="only the Parquet decode comparison")
     ap.add_argument("--parquet-threads", type=int, default=16, help="host threads calling the decoder at once")
+    ap.add_argument("--parquet-column", help="only one column chunk of a small file, decoded alone (e.g. price)")
     a = ap.parse_args()
+    if a.parquet_column:
+        print(json.dumps(parquet_column_chunk(a.parquet_column)), flush=True)
+        return
     if a.parquet:
         import sys
         # one hardware work queue per calling thread (up to 32): calls on different streams do not
