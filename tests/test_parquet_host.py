@@ -118,3 +118,30 @@ def test_chunk_bytes_are_the_chunks_pages(tmp_path):
             assert sum(len(h) + len(p) for h, _, p in pages) == len(chunk)
             assert (pages[0][1] == 2) == bool(meta.has_dictionary_page)  # 2: DICTIONARY_PAGE
             assert all(t in (0, 2, 3) for _, t, _ in pages) and len(pages) > 1
+
+
+def test_the_per_chunk_command_finds_its_chunk(monkeypatch):
+    """`opbench --parquet-column price` (the command behind the per-chunk figures) builds its
+    file and hands the decoder row group 0's price chunk; the device calls are stubbed."""
+    from minilake_b200 import gpu, opbench, parquet
+    calls = []
+
+    class Ctx:
+        def __init__(self, device):
+            pass
+
+        def close(self):
+            pass
+
+    class Batch:
+        def close(self):
+            pass
+
+    monkeypatch.setattr(gpu, "Context", Ctx)
+    monkeypatch.setattr(gpu, "parquet_decode", lambda ctx, *a: calls.append(a) or Batch())
+    out = opbench.parquet_column_chunk("price", iters=2, log=lambda *m: None)
+    assert out["rows"] == 125_000 and len(out["ms"]) == 2 and len(calls) == 2
+    chunk, physical, _, conv, _, codec, rows, max_def = calls[0]
+    assert len(chunk) == out["chunk_bytes"] and physical == parquet.PHYSICAL["DOUBLE"]
+    assert conv == parquet.CONV_DOUBLE and codec == parquet.CODECS["SNAPPY"] and rows == 125_000
+    assert ss.pages(chunk)[0][1] == 2  # its dictionary page first
