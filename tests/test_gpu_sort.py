@@ -122,3 +122,49 @@ def test_sort_of_20m_rows_is_a_sorted_permutation(engine):
     got = out.fetch()[0].values
     ref = np.sort(v.cpu().numpy())[::-1]
     assert np.array_equal(got, ref)
+
+
+def _stable_top(cols, keys, k):
+    """Row ids of the first k rows of a stable sort by `keys` (numpy): for each key its NULL
+    placement, then its value (negated when descending), the row id last: the GPU's documented
+    tie rule, the earlier row first."""
+    n = len(cols[0][0])
+    lex = [np.arange(n)]
+    for key in reversed(keys):
+        vals, valid = cols[key.expr.i64]
+        v = np.where(valid, vals.astype(np.float64), 0.0)
+        lex.append(-v if not key.asc else v)
+        lex.append(np.where(valid, 1, 0) if key.nulls_first else np.where(valid, 0, 1))
+    return np.lexsort(lex)[:k]
+
+
+def test_limits_over_heavy_ties_keep_the_earlier_rows(engine):
+    """Top-N with k <= 32 over 2M rows (the multi-CTA scan with its shared threshold and final
+    merge) on keys where thousands of rows tie at the limit, with NULLs first and last: the rows
+    kept and their order are those of a stable sort (the row id breaks the last tie)."""
+    rng = np.random.default_rng(17)
+    n = 2_000_000
+    c0 = rng.integers(0, 100, n).astype(np.int32)
+    c1 = rng.integers(0, 50, n).astype(np.float64)
+    v1 = rng.random(n) > 0.1
+    c2 = rng.permutation(n).astype(np.int64)
+    c3 = (rng.random(n) > 0.5).astype(np.uint8)
+    c4 = rng.integers(0, 10, n).astype(np.int32)
+    ones = np.ones(n, bool)
+    cols = [(c0, ones), (c1, v1), (c2, ones), (c3, ones), (c4, ones)]
+    types = [INT32, FLOAT64, INT64, BOOL, DATE]
+    t = Table("t", ["c0", "c1", "c2", "c3", "c4"],
+              [[fixed(INT32, c0), fixed(FLOAT64, c1, v1), fixed(INT64, c2), fixed(BOOL, c3), fixed(DATE, c4)]])
+    cases = [([SortKey(Col(0), INT32, asc=False)], 32),
+             ([SortKey(Col(1), FLOAT64, nulls_first=True)], 10),
+             ([SortKey(Col(1), FLOAT64, asc=False), SortKey(Col(0), INT32)], 17),
+             ([SortKey(Col(3), BOOL, asc=False)], 7),
+             ([SortKey(Col(4), DATE), SortKey(Col(2), INT64, asc=False)], 1),
+             ([SortKey(Col(1), FLOAT64)], 32)]
+    for keys, k in cases:
+        got = engine.fetch(engine.topn(t, types, keys, k))
+        rows = _stable_top(cols, keys, k)
+        assert len(got[0]) == k, keys
+        for c, (vals, valid) in enumerate(cols):
+            assert np.array_equal(got[c].valid_mask(), valid[rows]), (keys, c)
+            assert np.array_equal(got[c].values[valid[rows]], vals[rows][valid[rows]]), (keys, c)
